@@ -1,0 +1,349 @@
+// FED payload walk, raw -> digi unpacking with gain calibration, and module
+// starts. Restates SiPixelRawToClusterCUDA.jl:75-131 (payload walk),
+// SiPixelRawToClusterGPUKernel.jl:537-658 (raw_to_digi_kernal),
+// gpu_calib_pixel.jl:28-71 (calib_digis) and gpu_clustering.jl:52-74
+// (count_modules) for a batch of events.
+#include <cstddef>
+
+#include "pxl_internal.cuh"
+
+namespace pxl {
+
+namespace {
+
+// Single-block scan of one EvInfo count field into a base field over E events;
+// ev[E] receives the batch total in both fields.
+__global__ void k_ev_scan(EvInfo* ev, int E, int count_off, int base_off) {
+  __shared__ uint32_t sh[33];
+  __shared__ uint32_t carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  char* base = reinterpret_cast<char*>(ev);
+  for (int b = 0; b < E; b += blockDim.x) {
+    int e = b + threadIdx.x;
+    uint32_t v = e < E ? *reinterpret_cast<uint32_t*>(base + size_t(e) * sizeof(EvInfo) + count_off) : 0u;
+    uint32_t tot;
+    uint32_t ex = block_excl_scan(v, sh, &tot);
+    if (e < E) *reinterpret_cast<uint32_t*>(base + size_t(e) * sizeof(EvInfo) + base_off) = carry + ex;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    *reinterpret_cast<uint32_t*>(base + size_t(E) * sizeof(EvInfo) + base_off) = carry;
+    *reinterpret_cast<uint32_t*>(base + size_t(E) * sizeof(EvInfo) + count_off) = carry;
+  }
+}
+
+__device__ __forceinline__ int32_t ld_i32(const uint8_t* p) {
+  // records sit on 4-byte boundaries when the blob does; read bytewise to stay safe otherwise
+  uint32_t v = uint32_t(p[0]) | (uint32_t(p[1]) << 8) | (uint32_t(p[2]) << 16) | (uint32_t(p[3]) << 24);
+  return int32_t(v);
+}
+
+// One block per event: FedRawDataCollection directory (bin/ReadRAW.jl:23-31), then the
+// payload word counts in fedIds order (SiPixelRawToClusterCUDA.jl:75-131: skip FED 40,
+// skip empty FEDs, payload = bytes [8, size-8)).
+__global__ void k_fed_table(Dev d, const int16_t* __restrict__ fed_slot_of) {
+  const int e = blockIdx.x;
+  const int NF = d.n_fed_slots;
+  __shared__ uint64_t s_src[kMaxFedSlots];
+  __shared__ uint32_t s_nw[kMaxFedSlots];
+  __shared__ uint32_t sh[33];
+  __shared__ uint32_t s_warn;
+  for (int f = threadIdx.x; f < NF; f += blockDim.x) { s_nw[f] = 0; s_src[f] = 0; }
+  if (threadIdx.x == 0) s_warn = 0;
+  __syncthreads();
+  const uint64_t off0 = d.ev_off[e], off1 = d.ev_off[e + 1];
+  const uint8_t* ev = d.raw + off0;
+  const uint64_t nbytes = off1 - off0;
+  if (threadIdx.x == 0) {
+    if (nbytes >= 4) {
+      int32_t nfeds = ld_i32(ev);
+      uint64_t p = 4;
+      for (int32_t k = 0; k < nfeds; ++k) {
+        if (p + 8 > nbytes) { s_warn |= kWarnBuffer; break; }
+        int32_t fid = ld_i32(ev + p), size = ld_i32(ev + p + 4);
+        if (size < 0 || p + 8 + uint64_t(size) > nbytes) { s_warn |= kWarnBuffer; break; }
+        if (fid >= 0 && fid < 4096) {
+          int slot = fed_slot_of[fid];
+          if (slot >= 0) {
+            uint32_t nw64 = uint32_t(size) / 8;
+            uint32_t nw32 = nw64 == 0 ? 0u : (size >= 16 ? uint32_t(size - 16) / 4 : 0u);
+            s_nw[slot] = nw32;
+            s_src[slot] = off0 + p + 8 + 8;
+          }
+        }
+        p += 8 + uint64_t(size);
+      }
+    }
+  }
+  __syncthreads();
+  uint32_t carry = 0;
+  for (int b = 0; b < NF; b += blockDim.x) {
+    int f = b + threadIdx.x;
+    uint32_t v = f < NF ? s_nw[f] : 0u;
+    uint32_t tot;
+    uint32_t ex = block_excl_scan(v, sh, &tot);
+    if (f < NF) {
+      d.fed_src[size_t(e) * NF + f] = s_src[f];
+      d.fed_nw[size_t(e) * NF + f] = v;
+      d.fed_wo[size_t(e) * NF + f] = carry + ex;
+    }
+    carry += tot;
+  }
+  if (threadIdx.x == 0) {
+    EvInfo& E = d.ev[e];
+    E.raw_off = off0;
+    E.n_words = carry;
+    E.warnings = s_warn;
+    E.n_errors = 0;
+  }
+}
+
+// raw_to_digi_kernal + calib_digis for the words of one FED (blockIdx.x = FED slot).
+__global__ void k_unpack(Dev d) {
+  const int f = blockIdx.x, e = blockIdx.y;
+  const int NF = d.n_fed_slots;
+  const size_t fs = size_t(e) * NF + f;
+  const uint32_t nw = d.fed_nw[fs];
+  if (nw == 0) return;
+  const EvInfo& E = d.ev[e];
+  const uint32_t wo = d.fed_wo[fs];
+  const uint64_t gbase = uint64_t(E.word_base) + wo;
+  if (gbase + nw > uint64_t(d.cap_words)) {
+    if (threadIdx.x == 0) { atomic_or_warn(&d.ev[e], kWarnBuffer); atomicOr(d.status, kWarnBuffer); }
+    return;
+  }
+  const uint8_t* src = d.raw + d.fed_src[fs];
+  const uint8_t fed = uint8_t(d.c.fed_ids[f] - 1200u);
+  const Conditions& c = d.c;
+  for (uint32_t k = threadIdx.x; k < nw; k += blockDim.x) {
+    const uint64_t g = gbase + k;
+    const uint32_t local = wo + k;
+    uint32_t ww;
+    memcpy(&ww, src + 4ull * k, 4);
+    int16_t xx = 0, yy = 0, mid = int16_t(kInvId);
+    int32_t adc = 0;
+    uint32_t pdigi = 0, rawid = 0;
+    d.clus[g] = int32_t(local + 1);  // count_modules: clus[i] = i
+    if (ww != 0) {
+      const uint32_t link = (ww >> 26) & 0x3Fu, roc = (ww >> 21) & 0x1Fu;
+      const uint32_t index = uint32_t(fed) * kMaxLink * kMaxRoc + (link - 1u) * kMaxRoc + roc + 1u;  // 1-based
+      // check_roc: only code 25 survives the reference's comparisons (SiPixelRawToClusterGPUKernel.jl:394-468)
+      const uint8_t etype = (roc == 25u) ? 25 : 0;
+      const bool skip_roc = roc < 8u ? false : (etype != 0);
+      bool keep = true;
+      if (d.include_errors && skip_roc) {
+        uint32_t pos = atomicAdd(&d.ev[e].n_errors, 1u);
+        uint32_t gp = atomicAdd(d.err_count, 1u);
+        if (gp < uint32_t(d.cap_words)) {
+          d.err[5 * size_t(gp) + 0] = uint32_t(e);
+          d.err[5 * size_t(gp) + 1] = local;
+          d.err[5 * size_t(gp) + 2] = 0xffffffffu;
+          d.err[5 * size_t(gp) + 3] = ww;
+          d.err[5 * size_t(gp) + 4] = 25u | (uint32_t(fed) << 8);
+        }
+        (void)pos;
+        keep = false;
+      }
+      uint64_t cab = 0;
+      if (keep) {
+        if (index < 1u || index > kCablingSize) { atomic_or_warn(&d.ev[e], kWarnModules); keep = false; }
+        else cab = c.cab[index - 1];
+      }
+      if (keep && d.use_quality && ((cab >> 56) & 1u)) keep = false;
+      if (keep) {
+        const uint32_t raw_id = uint32_t(cab);
+        const bool barrel = ((raw_id >> 25) & 0x7u) == 1u;
+        const uint32_t layer = barrel ? ((raw_id >> 20) & 0xFu) : 0u;
+        const uint32_t the_module = barrel ? ((raw_id >> 2) & 0x3FFu) : 0u;
+        const uint32_t panel = barrel ? 0u : ((raw_id >> 10) & 0x3u);
+        const int side = barrel ? ((the_module < 5u) ? -1 : 1) : ((panel == 1u) ? -1 : 1);
+        const uint32_t roc_in_det = uint32_t((cab >> 48) & 0xFFu);
+        int32_t row, col;
+        bool conv_err = false;
+        if (layer == 1u) {
+          col = int32_t((ww >> 15) & 0x3Fu);
+          row = int32_t((ww >> 8) & 0x7Fu);
+          if (d.include_errors && !(row < 80 && col < 52)) conv_err = true;
+        } else {
+          const int32_t dcol = int32_t((ww >> 16) & 0x1Fu), pxid = int32_t((ww >> 8) & 0xFFu);
+          row = 80 - pxid / 2;
+          col = dcol * 2 + pxid % 2;
+          if (row < 0) { atomic_or_warn(&d.ev[e], kWarnModules); keep = false; }
+          else if (d.include_errors && !((dcol < 26) & (2 <= pxid) & (pxid < 162))) conv_err = true;
+        }
+        if (keep && conv_err) {
+          atomicAdd(&d.ev[e].n_errors, 1u);
+          uint32_t gp = atomicAdd(d.err_count, 1u);
+          if (gp < uint32_t(d.cap_words)) {
+            d.err[5 * size_t(gp) + 0] = uint32_t(e);
+            d.err[5 * size_t(gp) + 1] = local;
+            d.err[5 * size_t(gp) + 2] = raw_id;
+            d.err[5 * size_t(gp) + 3] = ww;
+            d.err[5 * size_t(gp) + 4] = 37u | (uint32_t(fed) << 8);
+          }
+          keep = false;
+        }
+        if (keep) {
+          // frame_conversion, SiPixelRawToClusterGPUKernel.jl:271-350
+          int32_t sr, sc, ro, co;
+          const bool flip = barrel ? (side == -1 && layer != 1u) : true;
+          if (flip) {
+            if (roc_in_det < 8u) { sr = 1; sc = -1; ro = 0; co = (8 - int32_t(roc_in_det)) * 52 - 1; }
+            else { sr = -1; sc = 1; ro = 159; co = (int32_t(roc_in_det) - 8) * 52; }
+          } else {
+            if (roc_in_det < 8u) { sr = -1; sc = 1; ro = 159; co = int32_t(roc_in_det) * 52; }
+            else { sr = 1; sc = -1; ro = 0; co = (16 - int32_t(roc_in_det)) * 52 - 1; }
+          }
+          const int32_t grow = sr * row + ro, gcol = sc * col + co;
+          if (grow < 0 || gcol < 0) {
+            atomic_or_warn(&d.ev[e], kWarnModules);
+          } else {
+            xx = int16_t(grow);
+            yy = int16_t(gcol);
+            adc = int32_t(ww & 0xFFu);
+            const uint32_t a = uint32_t(adc) < 1023u ? uint32_t(adc) : 1023u;
+            pdigi = uint32_t(grow) | (uint32_t(gcol) << 11) | (a << 22);
+            mid = int16_t(uint32_t(cab >> 32) & 0xFFFFu);
+            rawid = raw_id;
+            // calib_digis, gpu_calib_pixel.jl:41-70, with get_ped_and_gain
+            if (mid != int16_t(kInvId) && (mid < 0 || mid >= kMaxNumModules)) {
+              atomic_or_warn(&d.ev[e], kWarnModules);  // the reference indexes its 2000-entry gain table out of range
+              mid = int16_t(kInvId);
+            }
+            if (mid != int16_t(kInvId)) {
+              const float cf = mid < 96 ? 50.f : 47.f;
+              const float off = mid < 96 ? -670.f : -60.f;
+              const int m = mid;
+              const uint32_t offset = c.gain_first[m] + uint32_t(int32_t(yy)) * c.gain_lcd[m] +
+                                      2u * (uint32_t(int32_t(xx)) / c.rows_avg);
+              const uint32_t kk = offset / 2;
+              if (kk >= c.n_gain_pairs) {
+                atomic_or_warn(&d.ev[e], kWarnModules);
+              } else {
+                const uint16_t pr = c.gain_pairs[kk];
+                const uint32_t sg = pr & 0xFFu, sp = pr >> 8;
+                const bool bad = sp == c.dead_flag || sp == c.noisy_flag;
+                const float ped = __fadd_rn(__fmul_rn(float(sp), c.ped_prec), c.min_ped);
+                const float gain = __fadd_rn(__fmul_rn(float(sg), c.gain_prec), c.min_gain);
+                if (bad) {
+                  mid = int16_t(kInvId);
+                  adc = 0;
+                } else {
+                  const float vcal = __fsub_rn(__fmul_rn(float(adc), gain), __fmul_rn(ped, gain));
+                  const float v = __fadd_rn(__fmul_rn(vcal, cf), off);
+                  const int32_t t = int32_t(truncf(v));
+                  adc = t > 100 ? t : 100;
+                }
+              }
+            }
+          }
+        }
+      }
+    }
+    d.xx[g] = xx; d.yy[g] = yy; d.adc[g] = adc; d.mid[g] = mid; d.pdigi[g] = pdigi; d.rawid[g] = rawid;
+  }
+}
+
+// count_modules flag: a valid digi whose previous valid digi (in the event) has another id.
+__device__ __forceinline__ bool module_start_flag(const Dev& d, uint64_t ebase, uint32_t i) {
+  const int16_t id = d.mid[ebase + i];
+  if (id == int16_t(kInvId)) return false;
+  int64_t j = int64_t(i) - 1;
+  while (j >= 0 && d.mid[ebase + j] == int16_t(kInvId)) --j;
+  return j < 0 || d.mid[ebase + j] != id;
+}
+
+__global__ void k_modstart_count(Dev d) {
+  const int f = blockIdx.x, e = blockIdx.y;
+  const int NF = d.n_fed_slots;
+  const size_t fs = size_t(e) * NF + f;
+  const uint32_t nw = d.fed_nw[fs], wo = d.fed_wo[fs];
+  __shared__ uint32_t sh[33];
+  uint32_t cnt = 0;
+  const uint64_t ebase = d.ev[e].word_base;
+  if (ebase + wo + nw <= uint64_t(d.cap_words))
+    for (uint32_t k = threadIdx.x; k < nw; k += blockDim.x) cnt += module_start_flag(d, ebase, wo + k) ? 1u : 0u;
+  uint32_t tot;
+  block_excl_scan(cnt, sh, &tot);
+  if (threadIdx.x == 0) d.fed_nmod[fs] = tot;
+}
+
+// per event: module-start offsets per FED slot, n_modules; zero the cluster counters
+__global__ void k_modstart_scan(Dev d) {
+  const int e = blockIdx.x;
+  const int NF = d.n_fed_slots;
+  __shared__ uint32_t sh[33];
+  uint32_t carry = 0;
+  for (int b = 0; b < NF; b += blockDim.x) {
+    int f = b + threadIdx.x;
+    uint32_t v = f < NF ? d.fed_nmod[size_t(e) * NF + f] : 0u;
+    uint32_t tot;
+    uint32_t ex = block_excl_scan(v, sh, &tot);
+    if (f < NF) d.fed_nmod[size_t(e) * NF + f] = carry + ex;
+    carry += tot;
+  }
+  uint32_t* cim = d.clus_in_module + size_t(e) * kMaxNumModules;
+  for (int i = threadIdx.x; i < kMaxNumModules; i += blockDim.x) cim[i] = 0;
+  if (threadIdx.x == 0) {
+    uint32_t nm = carry < uint32_t(kMaxNumModules) ? carry : uint32_t(kMaxNumModules);
+    d.ev[e].n_modules = nm;
+    d.module_start[size_t(e) * (kMaxNumModules + 1)] = nm;
+    d.module_start[size_t(e) * (kMaxNumModules + 1) + kMaxNumModules] = 0;
+    d.clus_module_start[size_t(e) * (kMaxNumModules + 1)] = 0;
+    if (carry > uint32_t(kMaxNumModules)) atomic_or_warn(&d.ev[e], kWarnModules);
+  }
+}
+
+__global__ void k_modstart_fill(Dev d) {
+  const int f = blockIdx.x, e = blockIdx.y;
+  const int NF = d.n_fed_slots;
+  const size_t fs = size_t(e) * NF + f;
+  const uint32_t nw = d.fed_nw[fs], wo = d.fed_wo[fs];
+  const uint64_t ebase = d.ev[e].word_base;
+  if (ebase + wo + nw > uint64_t(d.cap_words)) return;
+  __shared__ uint32_t sh[33];
+  uint32_t carry = d.fed_nmod[fs];
+  uint32_t* ms = d.module_start + size_t(e) * (kMaxNumModules + 1);
+  for (uint32_t b = 0; b < nw; b += blockDim.x) {
+    uint32_t k = b + threadIdx.x;
+    bool fl = k < nw && module_start_flag(d, ebase, wo + k);
+    uint32_t tot;
+    uint32_t ex = block_excl_scan(fl ? 1u : 0u, sh, &tot);
+    if (fl) {
+      uint32_t r = carry + ex;
+      uint32_t i1 = wo + k + 1;  // 1-based digi index
+      if (r < uint32_t(kMaxNumModules - 1)) ms[r + 1] = i1;
+      else atomicMax(&ms[kMaxNumModules], i1);
+    }
+    carry += tot;
+  }
+}
+
+}  // namespace
+
+void launch_raw(const Dev& d, const Launch& L, const int16_t* fed_slot_of) {
+  const int NF = d.n_fed_slots;
+  k_fed_table<<<d.E, 256, 0, L.s>>>(d, fed_slot_of);
+  k_ev_scan<<<1, 1024, 0, L.s>>>(d.ev, d.E, int(offsetof(EvInfo, n_words)), int(offsetof(EvInfo, word_base)));
+  dim3 g(NF, d.E);
+  k_unpack<<<g, 256, 0, L.s>>>(d);
+  k_modstart_count<<<g, 256, 0, L.s>>>(d);
+  k_modstart_scan<<<d.E, 256, 0, L.s>>>(d);
+  k_modstart_fill<<<g, 256, 0, L.s>>>(d);
+}
+
+void launch_modstart(const Dev& d, const Launch& L) {
+  dim3 g(d.n_fed_slots, d.E);
+  k_modstart_count<<<g, 256, 0, L.s>>>(d);
+  k_modstart_scan<<<d.E, 256, 0, L.s>>>(d);
+  k_modstart_fill<<<g, 256, 0, L.s>>>(d);
+}
+
+void launch_ev_scan(const Dev& d, cudaStream_t s, int count_off, int base_off) {
+  k_ev_scan<<<1, 1024, 0, s>>>(d.ev, d.E, count_off, base_off);
+}
+
+}  // namespace pxl

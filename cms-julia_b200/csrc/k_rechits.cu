@@ -1,0 +1,266 @@
+// CPE rechits and the phi binner. Restates gpuPixelRecHits.jl:31-338
+// (getHits), pixelCPEforGPU.jl:246-577 (position_corr, correction,
+// errorFromDB), phase1PixelTopology.jl:249-296, SOARotation.jl:126-136,
+// approx_atan2.jl:159-184 (unsafe_atan2s), PixelRecHits.jl:20-82 and
+// hist_to_container.jl:217-270 (fill_many_from_vector).
+// One CTA per module; per-cluster reductions use shared-memory integer
+// atomics (order independent), then one thread per cluster evaluates the CPE
+// in FP32 with round-to-nearest and no contraction, as the reference does.
+#include "pxl_internal.cuh"
+
+namespace pxl {
+
+namespace {
+
+__device__ __forceinline__ uint16_t local_x(uint16_t px) {
+  int shift = 0;
+  if (px > 79) shift += 1;
+  if (px > 80) shift += 1;
+  return uint16_t(px + shift);
+}
+__device__ __forceinline__ uint16_t local_y(uint16_t py) {
+  int roc = py / 52;
+  int shift = 2 * roc;
+  int yin = py - 52 * roc;
+  if (yin > 0) shift += 1;
+  return uint16_t(py + shift);
+}
+__device__ __forceinline__ bool big_x(uint32_t px) { return px == 79 || px == 80; }
+__device__ __forceinline__ bool big_y(uint32_t py) { uint32_t ly = py - 52 * (py / 52); return ly == 0 || ly == 51; }
+
+__device__ __forceinline__ int16_t atan2s(float y, float x) {
+  const int16_t pi4 = 8192, pi34 = 24576;
+  float r = __fdiv_rn(__fsub_rn(fabsf(x), fabsf(y)), __fadd_rn(fabsf(x), fabsf(y)));
+  if (x < 0) r = -r;
+  int16_t angle = (x >= 0) ? pi4 : pi34;
+  float z = __fmul_rn(r, r);
+  float p = __fmul_rn(r, __fadd_rn(-10422.177734375f,
+                     __fmul_rn(z, __fadd_rn(3349.97412109375f,
+                     __fmul_rn(z, __fadd_rn(-1525.589599609375f, __fmul_rn(z, 406.64190673828125f)))))));
+  angle = int16_t(angle + int16_t(truncf(p)));
+  return (y < 0) ? int16_t(-angle) : angle;
+}
+
+__device__ float correction(uint32_t sizeM1, int32_t q_f, int32_t q_l, uint16_t upper, uint16_t lower, float lorentz,
+                            float thick, float cot, float pitch, bool first_big, bool last_big) {
+  if (sizeM1 == 0) return 0.0f;
+  float w_eff = 0.0f;
+  bool simple = true;
+  if (sizeM1 == 1) {
+    float w_inner = __fmul_rn(pitch, float(uint16_t(lower - upper)));
+    float w_pred = __fsub_rn(__fmul_rn(thick, cot), lorentz);
+    w_eff = __fsub_rn(fabsf(w_pred), w_inner);
+    simple = (w_eff < 0.0f) || (w_eff > pitch);
+  }
+  if (simple) {
+    float s = 2.0f;
+    s = __fadd_rn(s, first_big ? 1.0f : 0.0f);
+    s = __fadd_rn(s, last_big ? 1.0f : 0.0f);
+    w_eff = __fmul_rn(__fmul_rn(pitch, 0.5f), s);
+  }
+  float qdiff = float(q_l - q_f);
+  float qsum = float(q_l + q_f);
+  qsum = qsum == 0.0f ? 1.0f : qsum;
+  return __fmul_rn(__fmul_rn(0.5f, __fdiv_rn(qdiff, qsum)), w_eff);
+}
+
+constexpr int kMaxClus = 1024;
+
+__global__ void __launch_bounds__(256) k_get_hits(Dev d) {
+  const int e = blockIdx.y;
+  __shared__ uint32_t s_minr[kMaxClus], s_maxr[kMaxClus], s_minc[kMaxClus], s_maxc[kMaxClus];
+  __shared__ int32_t s_q[kMaxClus], s_qfx[kMaxClus], s_qlx[kMaxClus], s_qfy[kMaxClus], s_qly[kMaxClus];
+  const EvInfo& E = d.ev[e];
+  const uint32_t nmod = E.n_modules, n_el = E.n_words;
+  const uint64_t eb = E.word_base;
+  if (eb + n_el > uint64_t(d.cap_words)) return;
+  const uint32_t hb = E.hit_base;
+  const uint32_t* ms = d.module_start + size_t(e) * (kMaxNumModules + 1);
+  const uint32_t* cim = d.clus_in_module + size_t(e) * kMaxNumModules;
+  const uint32_t* cms = d.clus_module_start + size_t(e) * (kMaxNumModules + 1);
+  const uint32_t hcap = d.hits_per_event;
+  const Conditions& c = d.c;
+  for (uint32_t m = blockIdx.x; m < nmod; m += gridDim.x) {
+    const uint32_t me = d.module_id[size_t(e) * kMaxNumModules + m];
+    if (me >= uint32_t(kMaxNumModules) || int32_t(me) >= c.n_det) continue;
+    uint32_t nclus = cim[me];
+    if (nclus == 0) continue;
+    if (nclus > uint32_t(kMaxClus)) nclus = kMaxClus;
+    const uint32_t first0 = ms[m + 1] - 1;
+    const uint32_t end0 = (m + 1 < nmod) ? ms[m + 2] - 1 : n_el;
+    if (ms[m + 1] < 1 || end0 < first0 || end0 > n_el) continue;
+    for (uint32_t k = threadIdx.x; k < nclus; k += blockDim.x) {
+      s_minr[k] = 0xFFFFFFFFu; s_maxr[k] = 0; s_minc[k] = 0xFFFFFFFFu; s_maxc[k] = 0;
+      s_q[k] = 0; s_qfx[k] = 0; s_qlx[k] = 0; s_qfy[k] = 0; s_qly[k] = 0;
+    }
+    __syncthreads();
+    for (uint32_t i = first0 + threadIdx.x; i < end0; i += blockDim.x) {
+      const uint64_t g = eb + i;
+      const int16_t id = d.mid[g];
+      if (id == int16_t(kInvId) || uint32_t(int32_t(id)) != me) continue;
+      const int32_t cl = d.clus[g];
+      if (cl < 1 || uint32_t(cl) > nclus) continue;
+      const uint32_t x = uint32_t(int32_t(d.xx[g])), y = uint32_t(int32_t(d.yy[g]));
+      atomicMin(&s_minr[cl - 1], x); atomicMax(&s_maxr[cl - 1], x);
+      atomicMin(&s_minc[cl - 1], y); atomicMax(&s_maxc[cl - 1], y);
+    }
+    __syncthreads();
+    for (uint32_t i = first0 + threadIdx.x; i < end0; i += blockDim.x) {
+      const uint64_t g = eb + i;
+      const int16_t id = d.mid[g];
+      if (id == int16_t(kInvId) || uint32_t(int32_t(id)) != me) continue;
+      const int32_t cl = d.clus[g];
+      if (cl < 1 || uint32_t(cl) > nclus) continue;
+      const uint32_t x = uint32_t(int32_t(d.xx[g])), y = uint32_t(int32_t(d.yy[g]));
+      const int32_t a = d.adc[g];
+      const int32_t ch = a < 65535 ? a : 65535;
+      const int k = cl - 1;
+      atomicAdd(&s_q[k], ch);
+      if (s_minr[k] == x) atomicAdd(&s_qfx[k], ch);
+      if (s_maxr[k] == x) atomicAdd(&s_qlx[k], ch);
+      if (s_minc[k] == y) atomicAdd(&s_qfy[k], ch);
+      if (s_maxc[k] == y) atomicAdd(&s_qly[k], ch);
+    }
+    __syncthreads();
+    const DetParamsD& dp = c.det[me];
+    for (uint32_t k = threadIdx.x; k < nclus; k += blockDim.x) {
+      const uint32_t h = cms[me] + k;  // 0-based event-local hit index
+      if (h >= hcap) continue;
+      if (uint64_t(hb) + h >= uint64_t(d.cap_hits)) { atomic_or_warn(&d.ev[e], kWarnBuffer); continue; }
+      const uint32_t min_row = s_minr[k], max_row = s_maxr[k], min_col = s_minc[k], max_col = s_maxc[k];
+      const int32_t qfx = s_qfx[k], qlx = s_qlx[k], qfy = s_qfy[k], qly = s_qly[k];
+      // position_corr
+      const uint16_t llx = uint16_t(min_row + 1), lly = uint16_t(min_col + 1), urx = uint16_t(max_row), ury = uint16_t(max_col);
+      const uint16_t llxl = local_x(llx), llyl = local_y(lly), urxl = local_x(urx), uryl = local_y(ury);
+      const uint16_t mx = uint16_t(llxl + urxl), my = uint16_t(llyl + uryl);
+      int32_t xsize = int32_t(urxl) + 2 - int32_t(llxl);
+      int32_t ysize = int32_t(uryl) + 2 - int32_t(llyl);
+      if (big_x(min_row)) xsize += 1;
+      if (big_x(max_row)) xsize += 1;
+      if (big_y(min_col)) ysize += 1;
+      if (big_y(max_col)) ysize += 1;
+      const int32_t unb_x = int32_t(trunc(__ddiv_rn(__dmul_rn(8.0, double(fabsf(float(qfx - qlx)))), double(float(qfx + qlx)))));
+      const int32_t unb_y = int32_t(trunc(__ddiv_rn(__dmul_rn(8.0, double(fabsf(float(qfy - qly)))), double(float(qfy + qly)))));
+      xsize = 8 * xsize - unb_x;
+      ysize = 8 * ysize - unb_y;
+      int16_t sxs = int16_t(xsize < 1023 ? xsize : 1023);
+      int16_t sys = int16_t(ysize < 1023 ? ysize : 1023);
+      if (min_row == 0 || max_row == 159) sxs = int16_t(-sxs);
+      if (min_col == 0 || max_col == 415) sys = int16_t(-sys);
+      float xpos = __fadd_rn(dp.shift_x, __fmul_rn(c.pitch_x, __fadd_rn(__fmul_rn(0.5f, float(mx)), -81.0f)));
+      float ypos = __fadd_rn(dp.shift_y, __fmul_rn(c.pitch_y, __fadd_rn(__fmul_rn(0.5f, float(my)), -216.0f)));
+      const float gvz = __fdiv_rn(-1.0f, dp.z0);
+      const float cota = __fmul_rn(__fsub_rn(xpos, dp.x0), gvz);
+      const float cotb = __fmul_rn(__fsub_rn(ypos, dp.y0), gvz);
+      const float thick = dp.is_barrel ? c.thick_b : c.thick_e;
+      const float xcorr = correction(max_row - min_row, qfx, qlx, llxl, urxl, dp.cw_x, thick, cota, c.pitch_x, big_x(min_row), big_x(max_row));
+      const float ycorr = correction(max_col - min_col, qfy, qly, llyl, uryl, dp.cw_y, thick, cotb, c.pitch_y, big_y(min_col), big_y(max_col));
+      xpos = __fadd_rn(xpos, xcorr);
+      ypos = __fadd_rn(ypos, ycorr);
+      // errorFromDB
+      float xerr = 0.0050f, yerr = 0.0085f;
+      {
+        const uint32_t sx = max_row - min_row, sy = max_col - min_col;
+        const bool edge_x = min_row == 0 || max_row == 159, edge_y = min_col == 0 || max_col == 415;
+        int ix = sx == 0 ? 1 : 0, iy = sy == 0 ? 1 : 0;
+        ix += (sx == 0 && big_x(min_row)) ? 1 : 0;
+        iy += (sy == 0 && big_y(min_col)) ? 1 : 0;
+        if (!edge_x) xerr = dp.sx[ix];
+        if (!edge_y) yerr = dp.sy[iy];
+      }
+      // toGlobal_Special and beam spot
+      float ux = __fadd_rn(__fmul_rn(dp.R[0], xpos), __fmul_rn(dp.R[3], ypos));
+      float uy = __fadd_rn(__fmul_rn(dp.R[1], xpos), __fmul_rn(dp.R[4], ypos));
+      float uz = __fadd_rn(__fmul_rn(dp.R[2], xpos), __fmul_rn(dp.R[5], ypos));
+      ux = __fadd_rn(ux, dp.px); uy = __fadd_rn(uy, dp.py); uz = __fadd_rn(uz, dp.pz);
+      const float xg = __fsub_rn(ux, c.bs_x), yg = __fsub_rn(uy, c.bs_y), zg = __fsub_rn(uz, c.bs_z);
+      const size_t o = size_t(hb) + h;
+      d.charge[o] = uint32_t(s_q[k]);
+      d.detind[o] = int16_t(me);
+      d.xl[o] = xpos; d.yl[o] = ypos;
+      d.xsize[o] = sxs; d.ysize[o] = sys;
+      d.xerr[o] = __fmul_rn(xerr, xerr); d.yerr[o] = __fmul_rn(yerr, yerr);
+      d.xg[o] = xg; d.yg[o] = yg; d.zg[o] = zg;
+      d.rg[o] = __fsqrt_rn(__fadd_rn(__fmul_rn(xg, xg), __fmul_rn(yg, yg)));
+      d.iphi[o] = atan2s(yg, xg);
+    }
+    __syncthreads();
+  }
+}
+
+// setHitsLayerStart + fill_many_from_vector for the 10x128 phi histogram, one block per event.
+// Bins end up holding hit ids in decreasing order (the reference fill decrements the bin cursor).
+__global__ void __launch_bounds__(1024) k_phi_binner(Dev d) {
+  const int e = blockIdx.x;
+  __shared__ uint32_t s_off[kPhiTotBins + 3];
+  __shared__ uint32_t s_hls[11];
+  __shared__ uint32_t sh[33];
+  const EvInfo& E = d.ev[e];
+  const uint32_t hb = E.hit_base;
+  const uint32_t nh = E.n_hits;
+  const uint32_t* cms = d.clus_module_start + size_t(e) * (kMaxNumModules + 1);
+  if (threadIdx.x < 11) {
+    const uint32_t ls = d.c.layer_start[threadIdx.x];
+    s_hls[threadIdx.x] = cms[ls <= uint32_t(kMaxNumModules) ? ls : uint32_t(kMaxNumModules)];
+  }
+  for (int b = threadIdx.x; b < kPhiTotBins + 3; b += blockDim.x) s_off[b] = 0;
+  __syncthreads();
+  if (threadIdx.x < 11) d.hits_layer_start[size_t(e) * 11 + threadIdx.x] = s_hls[threadIdx.x];
+  uint32_t* poff = d.phi_off + size_t(e) * kPhiTotBins;
+  if (nh == 0 || uint64_t(hb) + nh > uint64_t(d.cap_hits)) {
+    for (int b = threadIdx.x; b < kPhiTotBins; b += blockDim.x) poff[b] = 0;
+    return;
+  }
+  const uint32_t ntot = s_hls[10];
+  auto layer_of = [&](uint32_t i) -> int {
+    int k = 0;
+    while (k < 11 && s_hls[k] < i) ++k;  // searchsortedfirst
+    return (k < 11 && s_hls[k] == i) ? k : k - 1;
+  };
+  auto bin_of = [&](uint32_t i) -> uint32_t {
+    const int16_t t = d.iphi[hb + i];
+    return ((uint32_t(int32_t(t >> 9)) & 127u) + 1u) + 128u * uint32_t(layer_of(i));
+  };
+  for (uint32_t i = threadIdx.x; i < ntot; i += blockDim.x) atomicAdd(&s_off[bin_of(i) - 1], 1u);
+  __syncthreads();
+  // inclusive scan of 1281 counters
+  {
+    uint32_t carry = 0;
+    for (int b = 0; b < kPhiTotBins; b += blockDim.x) {
+      int k = b + threadIdx.x;
+      uint32_t v = k < kPhiTotBins ? s_off[k] : 0u;
+      uint32_t tot;
+      uint32_t ex = block_excl_scan(v, sh, &tot);
+      if (k < kPhiTotBins) s_off[k] = carry + ex + v;
+      carry += tot;
+    }
+  }
+  __syncthreads();
+  uint16_t* bins = d.phi_bins + hb;
+  for (uint32_t i = threadIdx.x; i < ntot; i += blockDim.x) {
+    uint32_t w = atomicSub(&s_off[bin_of(i) - 1], 1u);
+    bins[w - 1] = uint16_t(i + 1);
+  }
+  __syncthreads();
+  // order each bin by decreasing hit id
+  for (int b = threadIdx.x; b < kPhiTotBins - 1; b += blockDim.x) {
+    const uint32_t lo = s_off[b], hi = s_off[b + 1];
+    for (uint32_t p = lo + 1; p < hi; ++p) {
+      uint16_t v = bins[p];
+      uint32_t q = p;
+      while (q > lo && bins[q - 1] < v) { bins[q] = bins[q - 1]; --q; }
+      bins[q] = v;
+    }
+  }
+  for (int b = threadIdx.x; b < kPhiTotBins; b += blockDim.x) poff[b] = s_off[b];
+}
+
+}  // namespace
+
+void launch_rechits(const Dev& d, const Launch& L) {
+  dim3 g(L.bpe > 0 ? L.bpe : 64, d.E);
+  k_get_hits<<<g, 256, 0, L.s>>>(d);
+  k_phi_binner<<<d.E, 1024, 0, L.s>>>(d);
+}
+
+}  // namespace pxl

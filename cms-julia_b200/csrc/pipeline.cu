@@ -1,0 +1,636 @@
+// Context, conditions upload, batch buffers, launch sequence, CUDA graph and
+// the C ABI declared in include/pxl.h.
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstddef>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/pxl.h"
+#include "pxl_internal.cuh"
+
+using namespace pxl;
+
+struct PxlCtx {
+  PxlParams p{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  Dev d{};
+  std::vector<void*> allocs;
+  int16_t* fed_slot_of = nullptr;
+  // host copy of the conditions needed at copy-out
+  std::vector<float> avg_geom;
+  // graph
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  uint32_t graph_mask = 0;
+  int graph_E = -1;
+  // last run
+  int32_t last_E = 0;
+  uint32_t last_mask = 0;
+  uint32_t done_mask = 0;
+  std::vector<EvInfo> ev_host;
+  bool ev_host_valid = false;
+  // pinned staging for offsets
+  uint64_t* h_off = nullptr;
+  size_t raw_cap = 0;
+  uint64_t* d_ev_off = nullptr;
+  uint8_t* d_raw = nullptr;
+};
+
+namespace {
+
+#define CK(x)                                                                     \
+  do {                                                                            \
+    cudaError_t err__ = (x);                                                      \
+    if (err__ != cudaSuccess) {                                                   \
+      std::fprintf(stderr, "pxl: %s failed: %s\n", #x, cudaGetErrorString(err__)); \
+      return PXL_ERR_CUDA;                                                        \
+    }                                                                             \
+  } while (0)
+
+template <class T>
+int dalloc(PxlCtx* c, T** p, int64_t n) {
+  size_t bytes = size_t(std::max<int64_t>(n, 1)) * sizeof(T);
+  void* q = nullptr;
+  cudaError_t err = cudaMalloc(&q, bytes);
+  if (err != cudaSuccess) {
+    std::fprintf(stderr, "pxl: cudaMalloc(%zu) failed: %s\n", bytes, cudaGetErrorString(err));
+    return PXL_ERR_CUDA;
+  }
+  c->allocs.push_back(q);
+  *p = static_cast<T*>(q);
+  return 0;
+}
+
+template <class T>
+int upload(PxlCtx* c, const T** dst, const std::vector<T>& v) {
+  T* q = nullptr;
+  int rc = dalloc(c, &q, int64_t(v.size()));
+  if (rc) return rc;
+  if (!v.empty()) CK(cudaMemcpy(q, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  *dst = q;
+  return 0;
+}
+
+struct Rd {
+  const uint8_t* p;
+  size_t n, off = 0;
+  bool ok = true;
+  template <class T> T get() {
+    T v{};
+    if (off + sizeof(T) > n) { ok = false; return v; }
+    std::memcpy(&v, p + off, sizeof(T));
+    off += sizeof(T);
+    return v;
+  }
+  template <class T> void get_n(T* dst, size_t k) {
+    if (off + k * sizeof(T) > n) { ok = false; return; }
+    std::memcpy(dst, p + off, k * sizeof(T));
+    off += k * sizeof(T);
+  }
+  void skip(size_t k) { if (off + k > n) ok = false; else off += k; }
+};
+
+// ES products -> device conditions (layouts: SiPixelFedCablingMapGPUWrapperESProducer.jl:27-57,
+// SiPixelGainCalibrationForHLTGPUESProducer.jl:14-46, PixelCPEFastESProducer.jl:16-103,
+// BeamSpotESProducer.jl:11-28)
+int load_conditions(PxlCtx* ctx, const PxlConditions* cd) {
+  Conditions& c = ctx->d.c;
+  {
+    Rd r{cd->cabling_map, cd->cabling_map_bytes};
+    std::vector<uint32_t> a[6];
+    for (auto& v : a) { v.resize(kCablingSize); r.get_n(v.data(), kCablingSize); }
+    std::vector<uint8_t> bad(kCablingSize);
+    r.get_n(bad.data(), kCablingSize);
+    if (!r.ok) return PXL_ERR_CONDITIONS;
+    std::vector<uint64_t> cab(kCablingSize);
+    for (uint32_t i = 0; i < kCablingSize; ++i) {
+      uint64_t raw = a[3][i], mod = a[5][i] & 0xFFFFu, rd = std::min<uint32_t>(a[4][i], 255u);
+      cab[i] = raw | (mod << 32) | (rd << 48) | (uint64_t(bad[i] != 0) << 56);
+    }
+    int rc = upload(ctx, &c.cab, cab);
+    if (rc) return rc;
+  }
+  {
+    Rd r{cd->fed_ids, cd->fed_ids_bytes};
+    uint32_t n = r.get<uint32_t>();
+    std::vector<uint32_t> ids(n);
+    r.get_n(ids.data(), n);
+    if (!r.ok || n > uint32_t(kMaxFedSlots)) return PXL_ERR_CONDITIONS;
+    // slots follow the fedIds order, skipping FED 40 (SiPixelRawToClusterCUDA.jl:75-81)
+    std::vector<uint32_t> slots;
+    std::vector<int16_t> slot_of(4096, -1);
+    for (uint32_t id : ids) {
+      if (id == 40 || id < 1200 || id >= 4096) continue;
+      slot_of[id] = int16_t(slots.size());
+      slots.push_back(id);
+    }
+    c.n_fed_ids = int32_t(slots.size());
+    ctx->d.n_fed_slots = int32_t(slots.size());
+    int rc = upload(ctx, &c.fed_ids, slots);
+    if (rc) return rc;
+    const int16_t* q;
+    rc = upload(ctx, &q, slot_of);
+    if (rc) return rc;
+    ctx->fed_slot_of = const_cast<int16_t*>(q);
+  }
+  {
+    Rd r{cd->gain, cd->gain_bytes};
+    r.skip(8);
+    std::vector<uint32_t> first(2000), lcd(2000);
+    for (int i = 0; i < 2000; ++i) {
+      uint32_t f = r.get<uint32_t>(), l = r.get<uint32_t>();
+      int32_t cols = r.get<int32_t>();
+      first[i] = f;
+      lcd[i] = cols != 0 ? (l - f) / uint32_t(cols) : 0u;
+    }
+    float fv[6];
+    r.get_n(fv, 6);
+    uint32_t uv[4];
+    r.get_n(uv, 4);
+    uint32_t nbytes = r.get<uint32_t>();
+    uint32_t n = nbytes / 2;
+    std::vector<uint16_t> pairs(n);
+    for (uint32_t i = 0; i < n; ++i) { uint8_t g = r.get<uint8_t>(), p = r.get<uint8_t>(); pairs[i] = uint16_t(g | (p << 8)); }
+    if (!r.ok) return PXL_ERR_CONDITIONS;
+    c.min_ped = fv[0]; c.min_gain = fv[2]; c.ped_prec = fv[4]; c.gain_prec = fv[5];
+    c.rows_avg = uv[0]; c.dead_flag = uv[2]; c.noisy_flag = uv[3];
+    c.n_gain_pairs = n;
+    int rc = upload(ctx, &c.gain_first, first);
+    if (!rc) rc = upload(ctx, &c.gain_lcd, lcd);
+    if (!rc) rc = upload(ctx, &c.gain_pairs, pairs);
+    if (rc) return rc;
+  }
+  float bsv[11];
+  {
+    Rd r{cd->beamspot, cd->beamspot_bytes};
+    r.get_n(bsv, 11);
+    if (!r.ok) return PXL_ERR_CONDITIONS;
+    c.bs_x = bsv[0]; c.bs_y = bsv[1]; c.bs_z = bsv[2];
+  }
+  {
+    Rd r{cd->cpe, cd->cpe_bytes};
+    c.thick_b = r.get<float>(); c.thick_e = r.get<float>(); c.pitch_x = r.get<float>(); c.pitch_y = r.get<float>();
+    uint32_t n = r.get<uint32_t>();
+    std::vector<DetParamsD> det(n);
+    for (uint32_t i = 0; i < n; ++i) {
+      DetParamsD& dp = det[i];
+      dp.is_barrel = r.get<uint8_t>() != 0;
+      r.get<uint8_t>(); r.get<uint16_t>(); r.get<uint16_t>(); r.skip(2); r.get<uint32_t>();
+      dp.shift_x = r.get<float>(); dp.shift_y = r.get<float>(); dp.cw_x = r.get<float>(); dp.cw_y = r.get<float>();
+      dp.x0 = r.get<float>(); dp.y0 = r.get<float>(); dp.z0 = r.get<float>();
+      r.get_n(dp.sx, 3); r.get_n(dp.sy, 3);
+      dp.px = r.get<float>(); dp.py = r.get<float>(); dp.pz = r.get<float>();
+      r.get_n(dp.R, 9);
+    }
+    float lad[6][kLadders];
+    for (int k = 0; k < 6; ++k) r.get_n(lad[k], kLadders);  // Z, X, Y, R, MinZ, MaxZ
+    float ecz[2];
+    r.get_n(ecz, 2);
+    r.get_n(c.layer_start, 11);
+    if (!r.ok) return PXL_ERR_CONDITIONS;
+    c.n_det = int32_t(n);
+    int rc = upload(ctx, &c.det, det);
+    if (rc) return rc;
+    // average geometry shifted by the beam spot (gpuPixelRecHits.jl:45-67), Float32
+    std::vector<float> ag(6 * kLadders + 2);
+    for (int il = 0; il < kLadders; ++il) {
+      float z = lad[0][il] - c.bs_z, x = lad[1][il] - c.bs_x, y = lad[2][il] - c.bs_y;
+      ag[il] = z;
+      ag[kLadders + il] = x;
+      ag[2 * kLadders + il] = y;
+      ag[3 * kLadders + il] = std::sqrt(x * x + y * y);
+      ag[4 * kLadders + il] = lad[4][il] - c.bs_z;
+      ag[5 * kLadders + il] = lad[5][il] - c.bs_z;
+    }
+    ag[6 * kLadders] = ecz[0] - c.bs_z;
+    ag[6 * kLadders + 1] = ecz[1] - c.bs_z;
+    ctx->avg_geom = ag;
+    rc = upload(ctx, &c.avg_geom, ag);
+    if (rc) return rc;
+  }
+  c.b_field = float(0.0114256972711507);
+  return 0;
+}
+
+int alloc_batch(PxlCtx* ctx) {
+  Dev& d = ctx->d;
+  const PxlParams& p = ctx->p;
+  const int64_t E = p.max_events;
+  d.cap_words = p.max_words;
+  d.cap_hits = p.max_hits;
+  d.cap_cells = p.max_doublets;
+  d.cap_tuples = p.max_tuples;
+  d.cap_tuple_hits = 5 * p.max_tuples;
+  d.cap_items = 8 * p.max_hits;  // inner-hit items over 19 layer pairs: each hit is inner in at most 6 pairs
+  d.cap_pairs = 2 * p.max_doublets;
+  d.hits_per_event = uint32_t(p.hits_per_event);
+  d.doublets_per_event = uint32_t(p.doublets_per_event);
+  d.tuples_per_event = uint32_t(p.tuples_per_event);
+  d.fits_per_mult = uint32_t(p.fits_per_multiplicity);
+  d.include_errors = p.include_errors;
+  d.use_quality = p.use_quality;
+  d.apply_charge_cut = 1;
+  const int64_t NF = std::max(d.n_fed_slots, 1);
+  int rc = 0;
+#define A(ptr, n) do { rc = dalloc(ctx, &d.ptr, (n)); if (rc) return rc; } while (0)
+  A(ev, E + 1);
+  A(fed_src, E * NF); A(fed_nw, E * NF); A(fed_wo, E * NF); A(fed_nmod, E * NF);
+  A(xx, d.cap_words); A(yy, d.cap_words); A(adc, d.cap_words); A(mid, d.cap_words); A(clus, d.cap_words);
+  A(pdigi, d.cap_words); A(rawid, d.cap_words);
+  A(err, 5 * d.cap_words); A(err_count, 1);
+  A(module_start, E * (kMaxNumModules + 1)); A(clus_in_module, E * kMaxNumModules); A(module_id, E * kMaxNumModules);
+  A(clus_module_start, E * (kMaxNumModules + 1));
+  A(xl, d.cap_hits); A(yl, d.cap_hits); A(xerr, d.cap_hits); A(yerr, d.cap_hits);
+  A(xg, d.cap_hits); A(yg, d.cap_hits); A(zg, d.cap_hits); A(rg, d.cap_hits);
+  A(iphi, d.cap_hits); A(xsize, d.cap_hits); A(ysize, d.cap_hits); A(detind, d.cap_hits); A(charge, d.cap_hits);
+  A(hits_layer_start, E * 11); A(phi_off, E * kPhiTotBins); A(phi_bins, d.cap_hits);
+  A(item_cnt, d.cap_items + 1);
+  A(cell_inner, d.cap_cells); A(cell_outer, d.cap_cells); A(cell_pair, d.cap_cells); A(cell_id, d.cap_cells);
+  A(cell_used, d.cap_cells); A(cell_inner_z, d.cap_cells); A(cell_inner_r, d.cap_cells);
+  A(ohc_cnt, d.cap_hits + 1); A(ohc_cur, d.cap_hits); A(ohc_list, d.cap_cells);
+  A(cn_mask, 4 * d.cap_cells); A(cn_cnt, d.cap_cells + 1); A(cn_cur, d.cap_cells); A(cn_list, d.cap_pairs);
+  A(tstart_cnt, d.cap_cells + 1);
+  A(tuple_off, d.cap_tuples + 1); A(tuple_hits, d.cap_tuple_hits); A(quality, d.cap_tuples);
+  A(tuple_cell, d.cap_tuple_hits);
+  A(ct_cnt, d.cap_cells + 1); A(ct_cur, d.cap_cells); A(ct_list, d.cap_tuple_hits);
+  A(tm_bins, d.cap_tuples);
+  A(t_state, 5 * d.cap_tuples); A(t_cov, 15 * d.cap_tuples); A(t_pt, d.cap_tuples); A(t_eta, d.cap_tuples);
+  A(t_chi2, d.cap_tuples); A(t_fitted, d.cap_tuples);
+  A(htt_cnt, d.cap_hits + 1); A(htt_cur, d.cap_hits); A(htt_list, d.cap_tuple_hits);
+  A(dup_cells, d.cap_cells); A(dup_flag, d.cap_cells + 1);
+  A(idv, d.cap_tuples); A(zv, E * 1024); A(wv, E * 1024); A(vchi2, E * 1024); A(ptv2, E * 1024);
+  A(ndof, d.cap_tuples + E * 1024); A(sort_ind, E * 1024);
+  int64_t st = scan_tmp_elems(std::max({d.cap_words, d.cap_items, d.cap_cells, d.cap_hits, d.cap_tuples}) + 1);
+  A(scan_tmp, st); A(scan_tmp64, st);
+  A(status, 1);
+#undef A
+  // input staging
+  ctx->raw_cap = size_t(d.cap_words) * 4 + size_t(E) * (4 + 16 * 4 + size_t(d.n_fed_slots + 8) * 24) + 4096;
+  rc = dalloc(ctx, &ctx->d_raw, int64_t(ctx->raw_cap));
+  if (rc) return rc;
+  rc = dalloc(ctx, &ctx->d_ev_off, E + 1);
+  if (rc) return rc;
+  CK(cudaMallocHost(&ctx->h_off, size_t(E + 1) * sizeof(uint64_t)));
+  return 0;
+}
+
+int run_chain(PxlCtx* ctx, uint32_t mask, cudaStream_t s) {
+  Dev& d = ctx->d;
+  if (d.E <= 0) return 0;
+  Launch L{s, d.bpe, 256};
+  // stages run in chain order; a producer boundary may stop after any of them and a
+  // later call (pxl_event_continue) resumes from the products already on the device
+  if (mask & PXL_STAGE_DIGIS) {
+    CK(cudaMemsetAsync(d.err_count, 0, sizeof(uint32_t), s));
+    CK(cudaMemsetAsync(d.status, 0, sizeof(uint32_t), s));
+    launch_raw(d, L, ctx->fed_slot_of);
+    launch_cluster(d, L);
+    launch_ev_scan(d, s, int(offsetof(EvInfo, n_hits)), int(offsetof(EvInfo, hit_base)));
+  }
+  if (mask & PXL_STAGE_HITS) launch_rechits(d, L);
+  if (mask & PXL_STAGE_TUPLES) launch_ca(d, L);
+  if (mask & PXL_STAGE_FIT) launch_fit(d, L);
+  if (mask & PXL_STAGE_CLASSIFY) launch_classify(d, L);
+  if (mask & PXL_STAGE_VERTICES) launch_vertices(d, L);
+  CK(cudaGetLastError());
+  ctx->done_mask = (mask & PXL_STAGE_DIGIS) ? mask : (ctx->done_mask | mask);
+  return 0;
+}
+
+int fetch_ev(PxlCtx* ctx) {
+  if (ctx->ev_host_valid) return 0;
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->ev_host.resize(size_t(ctx->last_E) + 1);
+  CK(cudaMemcpy(ctx->ev_host.data(), ctx->d.ev, ctx->ev_host.size() * sizeof(EvInfo), cudaMemcpyDeviceToHost));
+  ctx->ev_host_valid = true;
+  return 0;
+}
+
+template <class T>
+int64_t copy_dev(const T* src, int64_t n, void* dst, int64_t max_bytes) {
+  if (n < 0) return -1;
+  if (dst && max_bytes > 0 && n > 0) {
+    size_t nb = size_t(std::min<int64_t>(n * int64_t(sizeof(T)), max_bytes));
+    if (cudaMemcpy(dst, src, nb, cudaMemcpyDeviceToHost) != cudaSuccess) return PXL_ERR_CUDA;
+  }
+  return n;
+}
+
+template <class T>
+int64_t copy_host(const std::vector<T>& v, void* dst, int64_t max_bytes) {
+  if (dst && max_bytes > 0 && !v.empty())
+    std::memcpy(dst, v.data(), size_t(std::min<int64_t>(int64_t(v.size() * sizeof(T)), max_bytes)));
+  return int64_t(v.size());
+}
+
+template <class T>
+std::vector<T> dvec(const T* src, int64_t n) {
+  std::vector<T> v(size_t(std::max<int64_t>(n, 0)));
+  if (n > 0) cudaMemcpy(v.data(), src, size_t(n) * sizeof(T), cudaMemcpyDeviceToHost);
+  return v;
+}
+
+int stage_input(PxlCtx* ctx, const uint8_t* blob, const uint64_t* offs, int32_t n, bool on_device, cudaStream_t s) {
+  if (n <= 0 || n > ctx->p.max_events) return PXL_ERR_ARG;
+  if (on_device) {
+    ctx->d.raw = blob;
+    ctx->d.ev_off = offs;
+  } else {
+    uint64_t base = offs[0], nbytes = offs[n] - offs[0];
+    if (nbytes > ctx->raw_cap) return PXL_ERR_CAPACITY;
+    for (int32_t e = 0; e <= n; ++e) ctx->h_off[e] = offs[e] - base;
+    CK(cudaMemcpyAsync(ctx->d_raw, blob + base, nbytes, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(ctx->d_ev_off, ctx->h_off, size_t(n + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+    ctx->d.raw = ctx->d_raw;
+    ctx->d.ev_off = ctx->d_ev_off;
+  }
+  ctx->d.E = n;
+  ctx->last_E = n;
+  ctx->ev_host_valid = false;
+  return 0;
+}
+
+int choose_shape(PxlCtx* ctx) {
+  Dev& d = ctx->d;
+  if (ctx->p.blocks_per_event > 0) { d.bpe = ctx->p.blocks_per_event; return 0; }
+  // modules-per-event CTAs: enough CTAs to fill 148 SMs x 8 resident CTAs with few events,
+  // at least one wave of modules per event otherwise
+  int target = 148 * 8;
+  int bpe = std::max(1, std::min(256, target / std::max(1, d.E)));
+  d.bpe = std::max(bpe, 4);
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t pxl_version(void) { return PXL_ABI_VERSION; }
+
+int32_t pxl_params_default(PxlParams* p) {
+  if (!p) return PXL_ERR_ARG;
+  std::memset(p, 0, sizeof(*p));
+  p->device = 0;
+  p->max_events = 1;
+  p->max_words = 300000;  // MAX_FED_WORDS = 150 * 2000 (SiPixelRawToClusterGPUKernel.jl:193)
+  p->max_hits = 48 * 1024;
+  p->max_doublets = 458752;
+  p->max_tuples = 32 * 1024;
+  p->hits_per_event = 48 * 1024;
+  p->doublets_per_event = 458752;
+  p->tuples_per_event = 32 * 1024;
+  p->fits_per_multiplicity = 24 * 1024;
+  p->include_errors = 1;
+  p->use_quality = 1;
+  p->blocks_per_event = 0;
+  p->threads_per_block = 0;
+  return 0;
+}
+
+int32_t pxl_ctx_create(const PxlConditions* cond, const PxlParams* params, PxlCtx** out) {
+  if (!cond || !out) return PXL_ERR_ARG;
+  *out = nullptr;
+  PxlCtx* ctx = new PxlCtx();
+  if (params) ctx->p = *params;
+  else pxl_params_default(&ctx->p);
+  if (ctx->p.max_events <= 0) { delete ctx; return PXL_ERR_ARG; }
+  if (cudaSetDevice(ctx->p.device) != cudaSuccess) { delete ctx; return PXL_ERR_CUDA; }
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return PXL_ERR_CUDA; }
+  int rc = load_conditions(ctx, cond);
+  if (!rc) rc = alloc_batch(ctx);
+  if (rc) { pxl_ctx_destroy(ctx); return rc; }
+  *out = ctx;
+  return 0;
+}
+
+int32_t pxl_ctx_destroy(PxlCtx* ctx) {
+  if (!ctx) return PXL_ERR_ARG;
+  cudaSetDevice(ctx->p.device);
+  if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
+  if (ctx->graph) cudaGraphDestroy(ctx->graph);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (void* q : ctx->allocs) cudaFree(q);
+  if (ctx->h_off) cudaFreeHost(ctx->h_off);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return 0;
+}
+
+int32_t pxl_batch_stage(PxlCtx* ctx, const uint8_t* blob, const uint64_t* offs, int32_t n, void* stream) {
+  if (!ctx || !blob || !offs) return PXL_ERR_ARG;
+  cudaSetDevice(ctx->p.device);
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+  return stage_input(ctx, blob, offs, n, false, s);
+}
+
+int32_t pxl_batch_run(PxlCtx* ctx, const uint8_t* blob, const uint64_t* offs, int32_t n, int32_t on_device,
+                      uint32_t mask, void* stream) {
+  if (!ctx || !blob || !offs) return PXL_ERR_ARG;
+  cudaSetDevice(ctx->p.device);
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+  int rc = stage_input(ctx, blob, offs, n, on_device != 0, s);
+  if (rc) return rc;
+  choose_shape(ctx);
+  ctx->last_mask = mask;
+  rc = run_chain(ctx, mask, s);
+  if (rc) return rc;
+  if (s != ctx->stream) {
+    cudaEvent_t ev;
+    CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    CK(cudaEventRecord(ev, s));
+    CK(cudaStreamWaitEvent(ctx->stream, ev, 0));
+    cudaEventDestroy(ev);
+  }
+  return 0;
+}
+
+int32_t pxl_event_run(PxlCtx* ctx, const uint8_t* raw_event, size_t nbytes, uint32_t mask, void* stream) {
+  if (!ctx || !raw_event) return PXL_ERR_ARG;
+  uint64_t offs[2] = {0, nbytes};
+  return pxl_batch_run(ctx, raw_event, offs, 1, 0, mask | PXL_STAGE_DIGIS, stream);
+}
+
+int32_t pxl_event_continue(PxlCtx* ctx, uint32_t mask, void* stream) {
+  if (!ctx || ctx->d.E <= 0 || (mask & PXL_STAGE_DIGIS)) return PXL_ERR_ARG;
+  if (!(ctx->done_mask & PXL_STAGE_DIGIS)) return PXL_ERR_STATE;
+  // every stage needs the one before it
+  for (uint32_t b = PXL_STAGE_HITS; b <= PXL_STAGE_VERTICES; b <<= 1)
+    if ((mask & b) && !((ctx->done_mask | mask) & (b >> 1))) return PXL_ERR_STATE;
+  cudaSetDevice(ctx->p.device);
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+  ctx->ev_host_valid = false;
+  int rc = run_chain(ctx, mask, s);
+  ctx->last_mask |= mask;
+  return rc;
+}
+
+int32_t pxl_graph_capture(PxlCtx* ctx, uint32_t mask) {
+  if (!ctx || ctx->d.E <= 0) return PXL_ERR_STATE;
+  cudaSetDevice(ctx->p.device);
+  if (ctx->graph_exec) { cudaGraphExecDestroy(ctx->graph_exec); ctx->graph_exec = nullptr; }
+  if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
+  choose_shape(ctx);
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = run_chain(ctx, mask, ctx->stream);
+  cudaGraph_t g = nullptr;
+  cudaError_t err = cudaStreamEndCapture(ctx->stream, &g);
+  if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+  if (err != cudaSuccess) { std::fprintf(stderr, "pxl: capture failed: %s\n", cudaGetErrorString(err)); return PXL_ERR_CUDA; }
+  ctx->graph = g;
+  CK(cudaGraphInstantiate(&ctx->graph_exec, g, 0));
+  ctx->graph_mask = mask;
+  ctx->graph_E = ctx->d.E;
+  ctx->last_mask = mask;
+  return 0;
+}
+
+int32_t pxl_graph_launch(PxlCtx* ctx, void* stream) {
+  if (!ctx || !ctx->graph_exec) return PXL_ERR_STATE;
+  cudaSetDevice(ctx->p.device);
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+  CK(cudaGraphLaunch(ctx->graph_exec, s));
+  ctx->ev_host_valid = false;
+  ctx->last_E = ctx->graph_E;
+  ctx->last_mask = ctx->graph_mask;
+  return 0;
+}
+
+int32_t pxl_sync(PxlCtx* ctx) {
+  if (!ctx) return PXL_ERR_ARG;
+  cudaSetDevice(ctx->p.device);
+  CK(cudaDeviceSynchronize());
+  CK(cudaGetLastError());
+  ctx->ev_host_valid = false;
+  int rc = fetch_ev(ctx);
+  if (rc) return rc;
+  uint32_t w = 0;
+  for (int e = 0; e < ctx->last_E; ++e) w |= ctx->ev_host[e].warnings;
+  uint32_t st = 0;
+  CK(cudaMemcpy(&st, ctx->d.status, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  return int32_t(w | st);
+}
+
+int32_t pxl_event_counts(PxlCtx* ctx, int32_t e, PxlEventCounts* out) {
+  if (!ctx || !out || e < 0 || e >= ctx->last_E) return PXL_ERR_ARG;
+  cudaSetDevice(ctx->p.device);
+  int rc = fetch_ev(ctx);
+  if (rc) return rc;
+  const EvInfo& E = ctx->ev_host[e];
+  out->n_words = E.n_words;
+  out->n_modules = E.n_modules;
+  out->n_clusters = E.n_clusters;
+  out->n_hits = E.n_hits;
+  out->n_doublets = E.n_cells;
+  out->n_tuples = E.n_tuples;
+  out->n_tuple_hits = E.n_tuple_hits;
+  out->n_vertices = E.n_vtx;
+  out->n_vertex_tracks = E.n_vtx_tracks;
+  out->warnings = E.warnings;
+  out->n_errors = E.n_errors;
+  return 0;
+}
+
+int64_t pxl_copy_product(PxlCtx* ctx, int32_t e, int32_t product, void* dst, int64_t max_bytes) {
+  if (!ctx || e < 0 || e >= ctx->last_E) return PXL_ERR_ARG;
+  cudaSetDevice(ctx->p.device);
+  if (fetch_ev(ctx)) return PXL_ERR_CUDA;
+  const Dev& d = ctx->d;
+  const EvInfo& E = ctx->ev_host[e];
+  const uint64_t wb = E.word_base, hb = E.hit_base;
+  const int64_t nw = E.n_words, nh = E.n_hits;
+  const size_t M1 = kMaxNumModules + 1;
+  switch (product) {
+    case PXL_P_XX: return copy_dev(d.xx + wb, nw, dst, max_bytes);
+    case PXL_P_YY: return copy_dev(d.yy + wb, nw, dst, max_bytes);
+    case PXL_P_ADC: return copy_dev(d.adc + wb, nw, dst, max_bytes);
+    case PXL_P_MODULE_IND: return copy_dev(d.mid + wb, nw, dst, max_bytes);
+    case PXL_P_CLUS: return copy_dev(d.clus + wb, nw, dst, max_bytes);
+    case PXL_P_PDIGI: return copy_dev(d.pdigi + wb, nw, dst, max_bytes);
+    case PXL_P_RAW_ID: return copy_dev(d.rawid + wb, nw, dst, max_bytes);
+    case PXL_P_MODULE_START: return copy_dev(d.module_start + size_t(e) * M1, int64_t(M1), dst, max_bytes);
+    case PXL_P_CLUS_IN_MODULE: return copy_dev(d.clus_in_module + size_t(e) * kMaxNumModules, kMaxNumModules, dst, max_bytes);
+    case PXL_P_MODULE_ID: return copy_dev(d.module_id + size_t(e) * kMaxNumModules, kMaxNumModules, dst, max_bytes);
+    case PXL_P_CLUS_MODULE_START: return copy_dev(d.clus_module_start + size_t(e) * M1, int64_t(M1), dst, max_bytes);
+    case PXL_P_XL: return copy_dev(d.xl + hb, nh, dst, max_bytes);
+    case PXL_P_YL: return copy_dev(d.yl + hb, nh, dst, max_bytes);
+    case PXL_P_XERR: return copy_dev(d.xerr + hb, nh, dst, max_bytes);
+    case PXL_P_YERR: return copy_dev(d.yerr + hb, nh, dst, max_bytes);
+    case PXL_P_XG: return copy_dev(d.xg + hb, nh, dst, max_bytes);
+    case PXL_P_YG: return copy_dev(d.yg + hb, nh, dst, max_bytes);
+    case PXL_P_ZG: return copy_dev(d.zg + hb, nh, dst, max_bytes);
+    case PXL_P_RG: return copy_dev(d.rg + hb, nh, dst, max_bytes);
+    case PXL_P_IPHI: return copy_dev(d.iphi + hb, nh, dst, max_bytes);
+    case PXL_P_CHARGE: return copy_dev(d.charge + hb, nh, dst, max_bytes);
+    case PXL_P_XSIZE: return copy_dev(d.xsize + hb, nh, dst, max_bytes);
+    case PXL_P_YSIZE: return copy_dev(d.ysize + hb, nh, dst, max_bytes);
+    case PXL_P_DET_IND: return copy_dev(d.detind + hb, nh, dst, max_bytes);
+    case PXL_P_HITS_LAYER_START: return copy_dev(d.hits_layer_start + size_t(e) * 11, 11, dst, max_bytes);
+    case PXL_P_PHI_OFF: return copy_dev(d.phi_off + size_t(e) * kPhiTotBins, kPhiTotBins, dst, max_bytes);
+    case PXL_P_PHI_BINS: return copy_dev(d.phi_bins + hb, nh, dst, max_bytes);
+    case PXL_P_AVERAGE_GEOMETRY: return copy_host(ctx->avg_geom, dst, max_bytes);
+    case PXL_P_ERRORS: {
+      uint32_t total = 0;
+      cudaMemcpy(&total, d.err_count, sizeof(uint32_t), cudaMemcpyDeviceToHost);
+      total = std::min<uint32_t>(total, uint32_t(d.cap_words));
+      std::vector<uint32_t> all = dvec(d.err, int64_t(total) * 5);
+      std::vector<std::pair<uint32_t, std::array<uint32_t, 4>>> mine;
+      for (uint32_t k = 0; k < total; ++k)
+        if (all[5 * k] == uint32_t(e))
+          mine.push_back({all[5 * k + 1], {all[5 * k + 2], all[5 * k + 3], all[5 * k + 4] & 0xFFu, all[5 * k + 4] >> 8}});
+      std::sort(mine.begin(), mine.end(), [](auto& a, auto& b) { return a.first < b.first; });
+      std::vector<uint32_t> v;
+      for (auto& m : mine) v.insert(v.end(), m.second.begin(), m.second.end());
+      return copy_host(v, dst, max_bytes);
+    }
+    default:
+      break;
+  }
+  return copy_ca_product(ctx, e, product, dst, max_bytes);
+}
+
+int32_t pxl_clusterize_digis(PxlCtx* ctx, const uint16_t* id, const int16_t* x, const int16_t* y, const int32_t* adc,
+                             int32_t n, int32_t apply_charge_cut, uint32_t* module_start, uint32_t* clus_in_module,
+                             uint32_t* module_id, int32_t* clus, uint16_t* id_out) {
+  if (!ctx || !id || !x || !y || !adc || n < 0 || n > ctx->d.cap_words) return PXL_ERR_ARG;
+  cudaSetDevice(ctx->p.device);
+  cudaStream_t s = ctx->stream;
+  Dev d = ctx->d;
+  d.E = 1;
+  d.n_fed_slots = 1;
+  d.apply_charge_cut = apply_charge_cut != 0;
+  d.bpe = 148 * 4;
+  EvInfo ev{};
+  ev.n_words = uint32_t(n);
+  CK(cudaMemcpyAsync(d.ev, &ev, sizeof(EvInfo), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d.mid, id, size_t(n) * 2, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d.xx, x, size_t(n) * 2, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d.yy, y, size_t(n) * 2, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d.adc, adc, size_t(n) * 4, cudaMemcpyHostToDevice, s));
+  std::vector<int32_t> ci(size_t(std::max(n, 1)));
+  for (int32_t i = 0; i < n; ++i) ci[size_t(i)] = i + 1;  // count_modules: clus[i] = i
+  CK(cudaMemcpyAsync(d.clus, ci.data(), size_t(n) * 4, cudaMemcpyHostToDevice, s));
+  uint32_t nw = uint32_t(n), zero = 0;
+  CK(cudaMemcpyAsync(d.fed_nw, &nw, 4, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d.fed_wo, &zero, 4, cudaMemcpyHostToDevice, s));
+  Launch L{s, d.bpe, 256};
+  launch_modstart(d, L);
+  launch_cluster(d, L);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(s));
+  CK(cudaMemcpy(module_start, d.module_start, (kMaxNumModules + 1) * 4, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(clus_in_module, d.clus_in_module, kMaxNumModules * 4, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(module_id, d.module_id, kMaxNumModules * 4, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(clus, d.clus, size_t(n) * 4, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(id_out, d.mid, size_t(n) * 2, cudaMemcpyDeviceToHost));
+  ctx->ev_host_valid = false;
+  ctx->last_E = 0;
+  return 0;
+}
+
+}  // extern "C"

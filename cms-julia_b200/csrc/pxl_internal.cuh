@@ -1,0 +1,238 @@
+// Internal definitions shared by the kernels of libpxl_b200.so.
+//
+// Batched layout: a batch of E events is processed by every kernel at once.
+// Per-event variable-length data (digis, hits, doublets, tuples) are packed
+// back to back; per-event counts and prefix offsets live in EvInfo[E] on the
+// device and are produced by the kernels themselves, so the launch sequence
+// has no host synchronisation and can be captured in one CUDA graph.
+// Per-event work uses 2D grids: blockIdx.y = event, the x dimension strides
+// over that event's work items (launch shape from the autotuner).
+// Every stage writes its output in the order the serial reference produces it
+// (count -> scan -> fill passes, then sorting of short per-key lists), so the
+// integer products match the reference element by element.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace pxl {
+
+constexpr int kMaxNumModules = 2000;
+constexpr uint32_t kMaxLink = 48, kMaxRoc = 8, kMaxFed = 150;
+constexpr uint32_t kCablingSize = kMaxFed * kMaxLink * kMaxRoc;  // 57600
+constexpr uint16_t kInvId = 9999;
+constexpr int kMaxClustersPerModule = 1024;
+constexpr int kMaxPixInModule = 4000;
+constexpr int kLadders = 148;
+constexpr int kPhiTotBins = 1281;
+constexpr int kNPairs = 19;
+constexpr int kTupleStride = 32 * 1024;
+constexpr int kMaxCellsPerHit = 128;
+constexpr int kCellRows = 64;
+constexpr int kMaxActiveColumns = 512 * 1024 / 8;
+constexpr int kMaxFedSlots = 160;
+
+// per-event warning bits (same values as PXL_WARN_* in include/pxl.h)
+enum : uint32_t {
+  kWarnModules = 0x1u, kWarnPixels = 0x2u, kWarnClusters = 0x4u, kWarnHitsClamped = 0x8u,
+  kWarnDoublets = 0x10u, kWarnColumns = 0x20u, kWarnTuples = 0x40u, kWarnFitDomain = 0x80u,
+  kWarnFitsCapped = 0x100u, kWarnVertex = 0x200u, kWarnLists = 0x400u, kWarnBuffer = 0x800u,
+};
+
+struct DetParamsD {
+  float shift_x, shift_y, cw_x, cw_y;
+  float x0, y0, z0;
+  float sx[3], sy[3];
+  float px, py, pz;
+  float R[9];
+  uint8_t is_barrel;
+};
+
+struct Conditions {
+  // cabling, one 64-bit word per (fed, link, roc) entry:
+  // raw_id | module_id << 32 | roc_in_det << 48 | bad_roc << 56 | barrel << 57 | layer << 58 | side(-1) << 62
+  const uint64_t* cab;
+  const uint32_t* fed_ids;
+  int32_t n_fed_ids;
+  // gains
+  const uint32_t* gain_first;  // [2000]
+  const uint32_t* gain_lcd;    // [2000], (last - first) / cols
+  const uint16_t* gain_pairs;  // gain | ped << 8 per entry
+  uint32_t n_gain_pairs;
+  float min_ped, ped_prec, min_gain, gain_prec;
+  uint32_t rows_avg, dead_flag, noisy_flag;
+  // CPE
+  const DetParamsD* det;
+  int32_t n_det;
+  float thick_b, thick_e, pitch_x, pitch_y;
+  uint32_t layer_start[11];
+  const float* avg_geom;  // 6*148 + 2, already shifted by the beam spot
+  float bs_x, bs_y, bs_z;
+  float b_field;  // 1/(pT R) as the CA producer passes it, stored Float32
+};
+
+struct EvInfo {
+  uint64_t raw_off;  // byte offset of the event in the raw blob
+  uint32_t n_words, word_base;
+  uint32_t n_modules, n_clusters;
+  uint32_t n_hits, hit_base;
+  uint32_t n_items, item_base;      // doublet work items (inner hits over the layer pairs)
+  uint32_t n_cells, cell_base;
+  uint32_t n_cells_raw;             // doublets found before the per-event cap
+  uint32_t n_tuples, tuple_base;
+  uint32_t n_tuple_hits, tuple_hit_base;
+  uint32_t n_tuples_raw, n_tuple_hits_raw;
+  uint32_t n_vtx, n_vtx_tracks;
+  uint32_t n_errors, error_base;
+  uint32_t warnings;
+  uint32_t tm_off[9];               // tuple multiplicity offsets (bins 1..8, reference layout)
+  uint32_t n_dup_cells, dup_cell_base;
+};
+
+// Everything a kernel may need, passed by value.
+struct Dev {
+  Conditions c;
+  int32_t E;
+  int32_t n_fed_slots;
+  // limits
+  int64_t cap_words, cap_hits, cap_cells, cap_tuples, cap_tuple_hits, cap_items, cap_pairs;
+  uint32_t hits_per_event, doublets_per_event, tuples_per_event, fits_per_mult;
+  int32_t include_errors, use_quality;
+  int32_t apply_charge_cut;  // 1 in the chain; 0 only for the stand-alone clustering entry
+  // inputs
+  const uint8_t* raw;
+  const uint64_t* ev_off;
+  EvInfo* ev;
+  // FED table, [E][n_fed_slots]
+  uint64_t* fed_src;
+  uint32_t* fed_nw;
+  uint32_t* fed_wo;
+  uint32_t* fed_nmod;  // module starts found per FED slot
+  // digis [cap_words]
+  int16_t* xx; int16_t* yy; int32_t* adc; int16_t* mid; int32_t* clus; uint32_t* pdigi; uint32_t* rawid;
+  // FED error records [cap_words]: raw_id, word, type | fed << 8
+  uint32_t* err;
+  uint32_t* err_count;  // per event
+  // clusters, per event
+  uint32_t* module_start;       // [E][2001]
+  uint32_t* clus_in_module;     // [E][2000]
+  uint32_t* module_id;          // [E][2000]
+  uint32_t* clus_module_start;  // [E][2001]
+  // hits [cap_hits]
+  float* xl; float* yl; float* xerr; float* yerr; float* xg; float* yg; float* zg; float* rg;
+  int16_t* iphi; int16_t* xsize; int16_t* ysize; int16_t* detind; uint32_t* charge;
+  uint32_t* hits_layer_start;  // [E][11]
+  uint32_t* phi_off;           // [E][1281]
+  uint16_t* phi_bins;          // [cap_hits], 1-based hit ids
+  // doublets: work items and cells
+  uint32_t* item_cnt;      // [cap_items] doublets per inner hit item, then exclusive positions
+  uint32_t* cell_inner;    // [cap_cells] event-local 0-based hit index
+  uint32_t* cell_outer;
+  uint8_t* cell_pair;      // 0-based layer pair
+  int32_t* cell_id;        // reference doublet id: 1-based, -1 when killed
+  uint8_t* cell_used;
+  float* cell_inner_z; float* cell_inner_r;
+  // outer-hit-of-cell lists (CSR over hits)
+  uint32_t* ohc_cnt;       // [cap_hits + 1] counts -> offsets
+  uint32_t* ohc_cur;       // [cap_hits] fill cursors
+  uint32_t* ohc_list;      // [cap_cells] global cell indices
+  // cell neighbours (CSR over cells)
+  uint32_t* cn_mask;       // [cap_cells * 4] pass bits over the first 128 candidates
+  uint32_t* cn_cnt;        // [cap_cells + 1]
+  uint32_t* cn_cur;        // [cap_cells]
+  uint32_t* cn_list;       // [cap_pairs] global cell indices
+  // tuples
+  uint64_t* tstart_cnt;    // [cap_cells + 1] (tuples << 32 | hits) per start cell -> exclusive positions
+  uint32_t* tuple_off;     // [cap_tuples + 1] global hit offsets (0-based, packed)
+  uint32_t* tuple_hits;    // [cap_tuple_hits] event-local 0-based hit index
+  uint8_t* quality;        // [cap_tuples] 0 bad 1 dup 2 loose
+  uint32_t* tuple_cell;    // [cap_tuple_hits] (cell of each doublet of a tuple) for the cell -> track lists
+  uint32_t* ct_cnt;        // [cap_cells + 1] tracks per cell -> offsets
+  uint32_t* ct_cur;        // [cap_cells]
+  uint32_t* ct_list;       // [cap_tuple_hits] global tuple indices
+  uint32_t* tm_bins;       // [cap_tuples] tuple multiplicity, global tuple indices, bins ascending by id
+  // fit results [cap_tuples]
+  float* t_state; float* t_cov; float* t_pt; float* t_eta; float* t_chi2; uint8_t* t_fitted;
+  // hit -> tuple lists
+  uint32_t* htt_cnt;       // [cap_hits + 1]
+  uint32_t* htt_cur;
+  uint32_t* htt_list;      // [cap_tuple_hits]
+  // cells with >= 2 tracks, compacted per event
+  uint32_t* dup_cells;     // [cap_cells]
+  uint32_t* dup_flag;      // [cap_cells + 1]
+  // vertices, per event
+  int16_t* idv;            // [cap_tuples] per tuple (global tuple index), -1 when unused
+  float* zv; float* wv; float* vchi2; float* ptv2;  // [E][1024]
+  int32_t* ndof;           // [cap_tuples] per event slot region (same packing as tuples)
+  uint16_t* sort_ind;      // [E][1024]
+  // scratch for scans
+  uint32_t* scan_tmp;      // [scan tile sums]
+  uint64_t* scan_tmp64;
+  uint32_t* status;        // [1] global status bits (buffer overflow)
+  // launch shape
+  int32_t bpe;             // blocks per event for per-event kernels
+};
+
+// ---------------------------------------------------------------- helpers
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v) {
+  const unsigned lane = threadIdx.x & 31u;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= unsigned(o)) v += t;
+  }
+  return v;
+}
+
+// Block-wide exclusive scan of one value per thread (blockDim.x <= 1024, multiple of 32).
+// `sh` needs 33 uint32 of shared memory. Returns the exclusive prefix; *total gets the sum.
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* sh, uint32_t* total) {
+  const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+  const unsigned nw = (blockDim.x + 31) >> 5;
+  uint32_t inc = warp_incl_scan(v);
+  if (lane == 31) sh[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    uint32_t s = lane < nw ? sh[lane] : 0u;
+    uint32_t si = warp_incl_scan(s);
+    if (lane < nw) sh[lane] = si - s;
+    if (lane == nw - 1) sh[32] = si;
+  }
+  __syncthreads();
+  uint32_t r = sh[wid] + inc - v;
+  if (total) *total = sh[32];
+  __syncthreads();
+  return r;
+}
+
+__device__ __forceinline__ void atomic_or_warn(EvInfo* ev, uint32_t bits) { atomicOr(&ev->warnings, bits); }
+
+inline int div_up(int64_t a, int64_t b) { return int((a + b - 1) / b); }
+
+// ---------------------------------------------------------------- launchers (per stage file)
+struct Launch {
+  cudaStream_t s;
+  int bpe;        // blocks per event
+  int tpb;        // threads per block
+};
+
+void launch_raw(const Dev& d, const Launch& L, const int16_t* fed_slot_of);  // a1-a4
+void launch_modstart(const Dev& d, const Launch& L);  // a4 only (digis already in place)
+void launch_ev_scan(const Dev& d, cudaStream_t s, int count_off, int base_off);
+void launch_cluster(const Dev& d, const Launch& L);   // a5-a7
+void launch_rechits(const Dev& d, const Launch& L);   // a8-a9
+void launch_ca(const Dev& d, const Launch& L);        // a10-a14
+void launch_fit(const Dev& d, const Launch& L);       // a15-a16
+void launch_classify(const Dev& d, const Launch& L);  // a17
+void launch_vertices(const Dev& d, const Launch& L);  // a18-a20
+
+// global scans over packed arrays (scan.cu)
+// In place exclusive scan of data[0..n), n = min(ncap, *n_dev) (n_dev may be null); data[n] = total.
+void excl_scan_u32(uint32_t* data, int64_t ncap, const uint32_t* n_dev, uint32_t* tmp, cudaStream_t s);
+void excl_scan_u64(uint64_t* data, int64_t ncap, const uint32_t* n_dev, uint64_t* tmp, cudaStream_t s);
+int64_t scan_tmp_elems(int64_t n);
+
+}  // namespace pxl
+
+struct PxlCtx;
+// copy-out of the CA / fit / vertex products in the reference's layout (k_products.cu)
+int64_t copy_ca_product(PxlCtx* ctx, int32_t e, int32_t product, void* dst, int64_t max_bytes);

@@ -1,0 +1,142 @@
+// Device-wide exclusive scans over packed arrays (three passes: tile sums,
+// scan of the tile sums in one block, tile scan with the tile's offset).
+// In place: data[0..n) becomes the exclusive prefix and data[n] the total.
+#include "pxl_internal.cuh"
+
+namespace pxl {
+
+namespace {
+
+constexpr int kTpb = 256;
+constexpr int kItems = 8;
+constexpr int kTile = kTpb * kItems;
+
+// n_dev (optional) holds the live element count; tiles past it do nothing, so a
+// launch sized for the buffer capacity costs only the live part.
+__device__ __forceinline__ int64_t live_n(int64_t n, const uint32_t* n_dev) {
+  return n_dev ? (int64_t(*n_dev) < n ? int64_t(*n_dev) : n) : n;
+}
+
+template <class T>
+__global__ void k_tile_sums(const T* __restrict__ data, int64_t ncap, const uint32_t* n_dev, T* __restrict__ sums) {
+  int64_t n = live_n(ncap, n_dev);
+  int64_t base = int64_t(blockIdx.x) * kTile;
+  if (base >= n && base > 0) return;
+  T s = 0;
+  for (int k = 0; k < kItems; ++k) {
+    int64_t i = base + int64_t(k) * kTpb + threadIdx.x;
+    if (i < n) s += data[i];
+  }
+  // block reduce
+  __shared__ T sh[kTpb / 32];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    T v = threadIdx.x < kTpb / 32 ? sh[threadIdx.x] : T(0);
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) sums[blockIdx.x] = v;
+  }
+}
+
+template <class T>
+__device__ T warp_incl(T v) {
+  const unsigned lane = threadIdx.x & 31u;
+  for (int o = 1; o < 32; o <<= 1) {
+    T t = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= unsigned(o)) v += t;
+  }
+  return v;
+}
+
+// exclusive scan of the tile sums in one block of 1024 threads
+template <class T>
+__global__ void k_scan_sums(T* __restrict__ sums, int64_t ncap, const uint32_t* n_dev) {
+  int64_t n = live_n(ncap, n_dev);
+  int64_t nt = (n + kTile - 1) / kTile;
+  __shared__ T sh[33];
+  __shared__ T carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+  for (int64_t b = 0; b < nt; b += blockDim.x) {
+    int64_t i = b + threadIdx.x;
+    T v = i < nt ? sums[i] : T(0);
+    T inc = warp_incl(v);
+    if (lane == 31) sh[wid] = inc;
+    __syncthreads();
+    if (wid == 0) {
+      T s = sh[lane];
+      T si = warp_incl(s);
+      sh[lane] = si - s;
+      if (lane == 31) sh[32] = si;
+    }
+    __syncthreads();
+    T r = carry + sh[wid] + inc - v;
+    if (i < nt) sums[i] = r;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += sh[32];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) sums[nt] = carry;
+}
+
+template <class T>
+__global__ void k_tile_scan(T* __restrict__ data, int64_t ncap, const uint32_t* n_dev, const T* __restrict__ sums) {
+  int64_t n = live_n(ncap, n_dev);
+  int64_t nt = (n + kTile - 1) / kTile;
+  int64_t base = int64_t(blockIdx.x) * kTile;
+  if (n == 0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) data[0] = 0;
+    return;
+  }
+  if (int64_t(blockIdx.x) >= nt) return;
+  // each thread owns kItems consecutive elements
+  T v[kItems];
+  T tsum = 0;
+  int64_t i0 = base + int64_t(threadIdx.x) * kItems;
+  for (int k = 0; k < kItems; ++k) {
+    int64_t i = i0 + k;
+    v[k] = i < n ? data[i] : T(0);
+    tsum += v[k];
+  }
+  __shared__ T sh[33];
+  const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+  T inc = warp_incl(tsum);
+  if (lane == 31) sh[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    T s = lane < kTpb / 32 ? sh[lane] : T(0);
+    T si = warp_incl(s);
+    if (lane < kTpb / 32) sh[lane] = si - s;
+  }
+  __syncthreads();
+  T run = sums[blockIdx.x] + sh[wid] + inc - tsum;
+  for (int k = 0; k < kItems; ++k) {
+    int64_t i = i0 + k;
+    if (i < n) data[i] = run;
+    run += v[k];
+  }
+  if (int64_t(blockIdx.x) == nt - 1 && threadIdx.x == 0) data[n] = sums[nt];
+}
+
+template <class T>
+void excl_scan(T* data, int64_t ncap, const uint32_t* n_dev, T* tmp, cudaStream_t s) {
+  int64_t nt = ncap > 0 ? (ncap + kTile - 1) / kTile : 1;
+  k_tile_sums<T><<<unsigned(nt), kTpb, 0, s>>>(data, ncap, n_dev, tmp);
+  k_scan_sums<T><<<1, 1024, 0, s>>>(tmp, ncap, n_dev);
+  k_tile_scan<T><<<unsigned(nt), kTpb, 0, s>>>(data, ncap, n_dev, tmp);
+}
+
+}  // namespace
+
+int64_t scan_tmp_elems(int64_t n) { return (n + kTile - 1) / kTile + 2; }
+
+void excl_scan_u32(uint32_t* data, int64_t ncap, const uint32_t* n_dev, uint32_t* tmp, cudaStream_t s) {
+  excl_scan<uint32_t>(data, ncap, n_dev, tmp, s);
+}
+void excl_scan_u64(uint64_t* data, int64_t ncap, const uint32_t* n_dev, uint64_t* tmp, cudaStream_t s) {
+  excl_scan<uint64_t>(data, ncap, n_dev, tmp, s);
+}
+
+}  // namespace pxl

@@ -1,0 +1,172 @@
+"""Host-side handle of a reconstruction context (one CUDA context object of
+libpxl_b200.so): runs single events or batches and copies products out in the
+reference's layouts."""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _native
+from ._native import PxlConditions, PxlEventCounts, PxlParams, check
+from .formats import CONDITION_FILES
+
+# product ids and element types (enum PxlProduct in include/pxl.h)
+PRODUCTS: dict[str, tuple[int, type]] = {
+    "xx": (1, np.int16), "yy": (2, np.int16), "adc": (3, np.int32), "module_ind": (4, np.int16),
+    "clus": (5, np.int32), "pdigi": (6, np.uint32), "raw_id_arr": (7, np.uint32),
+    "module_start": (10, np.uint32), "clus_in_module": (11, np.uint32), "module_id": (12, np.uint32),
+    "clus_module_start": (13, np.uint32),
+    "xl": (20, np.float32), "yl": (21, np.float32), "xerr": (22, np.float32), "yerr": (23, np.float32),
+    "xg": (24, np.float32), "yg": (25, np.float32), "zg": (26, np.float32), "rg": (27, np.float32),
+    "iphi": (28, np.int16), "charge": (29, np.uint32), "xsize": (30, np.int16), "ysize": (31, np.int16),
+    "det_ind": (32, np.int16), "hits_layer_start": (33, np.uint32), "phi_off": (34, np.uint32),
+    "phi_bins": (35, np.uint16), "agc": (36, np.float32),
+    "cells": (40, np.int32), "cell_neighbors": (41, np.uint32), "cell_tracks": (42, np.uint32),
+    "outer_hit_of_cell": (43, np.uint32), "tuple_multiplicity": (44, np.uint32),
+    "tuple_off": (50, np.uint32), "tuple_hits": (51, np.uint16), "det_hits": (52, np.uint16),
+    "quality": (53, np.uint8), "chi2": (54, np.float32), "eta": (55, np.float32), "pt": (56, np.float32),
+    "state": (57, np.float32), "cov": (58, np.float32), "fitted": (59, np.uint8),
+    "idv": (60, np.int16), "zv": (61, np.float32), "wv": (62, np.float32), "vchi2": (63, np.float32),
+    "ptv2": (64, np.float32), "ndof": (65, np.int32), "sort_ind": (66, np.uint16), "errors": (70, np.uint32),
+}
+
+
+@dataclass
+class EventCounts:
+    n_words: int
+    n_modules: int
+    n_clusters: int
+    n_hits: int
+    n_doublets: int
+    n_tuples: int
+    n_tuple_hits: int
+    n_vertices: int
+    n_vertex_tracks: int
+    warnings: int
+    n_errors: int
+
+
+def default_params(**kw) -> PxlParams:
+    p = PxlParams()
+    check(_native.lib().pxl_params_default(ctypes.byref(p)), "pxl_params_default")
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def batch_params(n_events: int, words_per_event: int = 64_000, hits_per_event_avg: int = 16_000,
+                 doublets_per_event_avg: int = 160_000, tuples_per_event_avg: int = 12_000, **kw) -> PxlParams:
+    """Buffer sizes for a batch of n_events with the given per-event averages; the per-event
+    semantic capacities stay at the reference's values unless overridden."""
+    return default_params(max_events=n_events, max_words=n_events * words_per_event,
+                          max_hits=n_events * hits_per_event_avg, max_doublets=n_events * doublets_per_event_avg,
+                          max_tuples=n_events * tuples_per_event_avg, **kw)
+
+
+class PixelChain:
+    """One reconstruction context on one GPU."""
+
+    def __init__(self, conditions: dict[str, bytes], params: PxlParams | None = None):
+        self._lib = _native.lib()
+        self._cond_bufs = [conditions[n] for n in CONDITION_FILES]
+        c = PxlConditions()
+        for name, buf in zip(("cabling_map", "fed_ids", "gain", "cpe", "beamspot"), self._cond_bufs):
+            setattr(c, name, ctypes.cast(ctypes.c_char_p(buf), ctypes.c_void_p))
+            setattr(c, name + "_bytes", len(buf))
+        self.params = params if params is not None else default_params()
+        h = ctypes.c_void_p()
+        check(self._lib.pxl_ctx_create(ctypes.byref(c), ctypes.byref(self.params), ctypes.byref(h)), "pxl_ctx_create")
+        self._h = h
+        self._keep: list = []
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.pxl_ctx_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):  # pragma: no cover - best effort
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- running
+    def run_event(self, raw_event: bytes | np.ndarray, stages: int = _native.STAGE_ALL) -> int:
+        buf = np.ascontiguousarray(np.frombuffer(raw_event, dtype=np.uint8) if isinstance(raw_event, (bytes, bytearray))
+                                   else raw_event, dtype=np.uint8)
+        self._keep = [buf]
+        check(self._lib.pxl_event_run(self._h, buf.ctypes.data, buf.nbytes, stages, None), "pxl_event_run")
+        return self.sync()
+
+    def continue_stages(self, stages: int) -> int:
+        check(self._lib.pxl_event_continue(self._h, stages, None), "pxl_event_continue")
+        return self.sync()
+
+    def run_batch(self, blob: np.ndarray, offsets: np.ndarray, stages: int = _native.STAGE_ALL,
+                  sync: bool = True) -> int:
+        blob = np.ascontiguousarray(blob, dtype=np.uint8)
+        offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+        self._keep = [blob, offsets]
+        n = len(offsets) - 1
+        check(self._lib.pxl_batch_run(self._h, blob.ctypes.data, offsets.ctypes.data, n, 0, stages, None),
+              "pxl_batch_run")
+        return self.sync() if sync else 0
+
+    def stage_batch(self, blob: np.ndarray, offsets: np.ndarray) -> None:
+        blob = np.ascontiguousarray(blob, dtype=np.uint8)
+        offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+        self._keep = [blob, offsets]
+        check(self._lib.pxl_batch_stage(self._h, blob.ctypes.data, offsets.ctypes.data, len(offsets) - 1, None),
+              "pxl_batch_stage")
+
+    def capture_graph(self, stages: int = _native.STAGE_ALL) -> None:
+        check(self._lib.pxl_graph_capture(self._h, stages), "pxl_graph_capture")
+
+    def launch_graph(self) -> None:
+        check(self._lib.pxl_graph_launch(self._h, None), "pxl_graph_launch")
+
+    def sync(self) -> int:
+        return check(self._lib.pxl_sync(self._h), "pxl_sync")
+
+    # ---- products
+    def counts(self, event: int = 0) -> EventCounts:
+        c = PxlEventCounts()
+        check(self._lib.pxl_event_counts(self._h, event, ctypes.byref(c)), "pxl_event_counts")
+        return EventCounts(**{f: getattr(c, f) for f, _ in PxlEventCounts._fields_})
+
+    def product(self, name: str, event: int = 0) -> np.ndarray:
+        pid, dt = PRODUCTS[name]
+        n = self._lib.pxl_copy_product(self._h, event, pid, None, 0)
+        if n < 0:
+            raise RuntimeError(f"product {name} unavailable ({n})")
+        out = np.empty(int(n), dtype=dt)
+        if n:
+            got = self._lib.pxl_copy_product(self._h, event, pid, out.ctypes.data, out.nbytes)
+            if got < 0:
+                raise RuntimeError(f"product {name} copy failed ({got})")
+        return out
+
+    def clusterize_digis(self, id_: np.ndarray, x: np.ndarray, y: np.ndarray, adc: np.ndarray,
+                         charge_cut: bool = True) -> dict[str, np.ndarray]:
+        n = len(id_)
+        id_ = np.ascontiguousarray(id_, dtype=np.uint16)
+        x = np.ascontiguousarray(x, dtype=np.int16)
+        y = np.ascontiguousarray(y, dtype=np.int16)
+        adc = np.ascontiguousarray(adc, dtype=np.int32)
+        ms = np.zeros(2001, np.uint32)
+        cim = np.zeros(2000, np.uint32)
+        mid = np.zeros(2000, np.uint32)
+        clus = np.zeros(n, np.int32)
+        ido = np.zeros(n, np.uint16)
+        check(self._lib.pxl_clusterize_digis(self._h, id_.ctypes.data, x.ctypes.data, y.ctypes.data, adc.ctypes.data,
+                                             n, int(charge_cut), ms.ctypes.data, cim.ctypes.data, mid.ctypes.data,
+                                             clus.ctypes.data, ido.ctypes.data), "pxl_clusterize_digis")
+        return {"module_start": ms, "clus_in_module": cim, "module_id": mid, "clus": clus, "id": ido}

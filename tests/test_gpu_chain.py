@@ -1,0 +1,97 @@
+"""Parity of the CUDA chain (through the C ABI) with the CPU oracle on the same inputs.
+Integer products and the FP32 rechit arithmetic are compared bit for bit."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+from parity import compare_digis_clusters, compare_hits
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def chain(conditions):
+    from pixeltrack import PixelChain, default_params
+    c = PixelChain(conditions, default_params())
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module")
+def orc(conditions):
+    return oracle.Oracle(conditions)
+
+
+@pytest.mark.parametrize("kn", range(5))
+@pytest.mark.parametrize("cut", [False, True])
+def test_clustering_known_answer_gpu(chain, kn, cut):
+    z = np.load(GOLDEN / f"clustering_kn{kn}.npz")
+    g = chain.clusterize_digis(z["id"], z["x"], z["y"], z["adc"], charge_cut=cut)
+    o = oracle.clusterize_digis(z["id"], z["x"], z["y"], z["adc"], charge_cut=cut)
+    if not cut:
+        assert int(g["clus_in_module"].sum()) == int(z["ncl"])
+    nm = int(o["module_start"][0])
+    assert np.array_equal(g["module_start"][:nm + 1], o["module_start"][:nm + 1])
+    assert np.array_equal(g["module_id"][:nm], o["module_id"][:nm])
+    assert np.array_equal(g["clus_in_module"], o["clus_in_module"])
+    assert np.array_equal(g["clus"], o["clus"])
+    assert np.array_equal(g["id"], o["id"])
+
+
+def test_clustering_diagonal_gpu(chain):
+    z = np.load(GOLDEN / "clustering_diag8.npz")
+    g = chain.clusterize_digis(z["id"], z["x"], z["y"], z["adc"], charge_cut=False)
+    assert int(g["clus_in_module"].sum()) == 6
+
+
+def _run_both(chain, orc, ev, stages):
+    chain.run_event(ev, stages)
+    orc.run_event(ev, stages)
+
+
+def test_single_event_digis_hits(chain, orc, event_single):
+    blob, offs = event_single
+    ev = blob[offs[0]:offs[1]]
+    _run_both(chain, orc, ev, 3)
+    errs = compare_digis_clusters(chain, orc) + compare_hits(chain, orc)
+    assert not errs, errs
+
+
+def test_pu50_events_digis_hits(chain, orc, events_pu50):
+    blob, offs = events_pu50
+    for e in range(len(offs) - 1):
+        ev = blob[offs[e]:offs[e + 1]]
+        _run_both(chain, orc, ev, 3)
+        errs = compare_digis_clusters(chain, orc) + compare_hits(chain, orc)
+        assert not errs, (e, errs)
+
+
+def test_batch_matches_oracle(conditions, orc, events_pu50):
+    from pixeltrack import PixelChain, batch_params
+    blob, offs = events_pu50
+    n = len(offs) - 1
+    with PixelChain(conditions, batch_params(n)) as bc:
+        bc.run_batch(blob, offs, stages=3)
+        for e in range(n):
+            orc.run_event(blob[offs[e]:offs[e + 1]], 3)
+            errs = compare_digis_clusters(bc, orc, e) + compare_hits(bc, orc, e)
+            assert not errs, (e, errs)
+
+
+def test_graph_replay_is_deterministic(conditions, events_pu50):
+    from pixeltrack import PixelChain, batch_params
+    blob, offs = events_pu50
+    n = len(offs) - 1
+    with PixelChain(conditions, batch_params(n)) as bc:
+        bc.stage_batch(blob, offs)
+        bc.capture_graph(3)
+        bc.launch_graph()
+        bc.sync()
+        first = {k: bc.product(k, n - 1) for k in ("clus", "xg", "phi_bins")}
+        bc.launch_graph()
+        bc.sync()
+        for k, v in first.items():
+            assert np.array_equal(v, bc.product(k, n - 1))
