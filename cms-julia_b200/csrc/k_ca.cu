@@ -1,0 +1,691 @@
+// Cellular automaton: doublets, outer-hit lists, cell connection, fishbone,
+// ntuplet search, cell -> track lists, early duplicate removal and tuple
+// multiplicity. Restates gpu_pixel_doublets.jl:19-360 (doublets_from_histo),
+// gpu_ca_cell.jl:130-270, gpu_fishbone.jl:4-63, circle_eq.jl:18-93 and
+// ca_hit_ntuplet_generator_kernels_impl.jl:45-211.
+//
+// Output order equals the serial reference's: doublets are counted per inner
+// hit, scanned and written in the reference's loop order (so doublet ids are
+// the reference's ids); per-key lists (cells ending on a hit, neighbours of a
+// cell, tracks of a cell) are filled with atomics and then sorted, which
+// restores the reference's push order (ascending producer index); tuples are
+// counted per start cell, scanned, and written in the reference's depth-first
+// order, so tuple ids match too.
+#include <cstddef>
+
+#include "pxl_internal.cuh"
+
+namespace pxl {
+
+namespace {
+
+__constant__ uint8_t c_layer_pairs[2 * kNPairs] = {0, 1, 0, 4, 0, 7, 1, 2, 1, 4, 1, 7, 4, 5, 7, 8, 2, 3, 2, 4,
+                                                   2, 7, 5, 6, 8, 9, 0, 2, 1, 3, 0, 5, 0, 8, 4, 6, 7, 9};
+__constant__ int16_t c_phi_cuts[kNPairs] = {522, 730, 730, 522, 626, 626, 522, 522, 626, 626,
+                                            626, 522, 522, 522, 522, 522, 522, 522, 522};
+__constant__ double c_min_z[kNPairs] = {-20., 0., -30., -22., 10., -30., -70., -70., -22., 15.,
+                                        -30., -70., -70., -20., -22., 0., -30., -70., -70.};
+__constant__ double c_max_z[kNPairs] = {20., 30., 0., 22., 30., -10., 70., 70., 22., 30.,
+                                        -15., 70., 70., 20., 22., 30., 0., 70., 70.};
+__constant__ double c_max_r[kNPairs] = {20., 9., 9., 20., 7., 7., 5., 5., 20., 6., 6., 5., 5., 20., 20., 9., 9., 9., 9.};
+
+// CA parameters (ca_hit_ntuplet_generator.jl:9-30), Float32 as Params stores them
+__device__ __forceinline__ float ptmin_f() { return 0.899999976158f; }
+constexpr float kThetaBarrel = 0.00200000009499f;
+constexpr float kThetaForward = 0.00300000002608f;
+constexpr float kHardCurv = 0.0328407224959f;
+constexpr float kDcaInner = 0.15000000596f;
+constexpr float kDcaOuter = 0.25f;
+
+__device__ __forceinline__ uint32_t phi_bin(int16_t t) { return (uint32_t(int32_t(t >> 9)) & 127u) + 1u; }
+
+struct HitView {
+  const float *xg, *yg, *zg, *rg;
+  const int16_t *iphi, *ysize, *detind;
+};
+
+// ---------------------------------------------------------------- doublets
+// per event: cumulative inner-layer sizes over the pairs, number of work items
+__global__ void k_items(Dev d, uint32_t* pair_cum) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= d.E) return;
+  const uint32_t* hls = d.hits_layer_start + size_t(e) * 11;
+  uint32_t acc = 0;
+  for (int p = 0; p < kNPairs; ++p) {
+    const int li = c_layer_pairs[2 * p];
+    acc += hls[li + 1] - hls[li];
+    pair_cum[size_t(e) * kNPairs + p] = acc;
+  }
+  d.ev[e].n_items = d.ev[e].n_hits ? acc : 0u;
+}
+
+template <bool kFill>
+__device__ __forceinline__ uint32_t doublets_of_item(const Dev& d, int e, uint32_t j, const uint32_t* cum,
+                                                     const uint32_t* hls, const HitView& hv, const uint32_t* poff,
+                                                     const uint16_t* pbins, uint64_t cell_pos, uint64_t cell_lo,
+                                                     uint32_t cap) {
+  int pid = 0;
+  while (j >= cum[pid]) ++pid;
+  const int inner = c_layer_pairs[2 * pid], outer = c_layer_pairs[2 * pid + 1];
+  const uint32_t h_off = 128u * uint32_t(outer);
+  uint32_t i = (pid == 0) ? j : j - cum[pid - 1];
+  i += hls[inner];  // event-local 0-based inner hit
+  const int16_t mi = hv.detind[i];
+  if (mi > 2000) return 0;
+  const float me_z = hv.zg[i];
+  if (double(me_z) < c_min_z[pid] || double(me_z) > c_max_z[pid]) return 0;
+  const int32_t me_s = hv.ysize[i];  // idealConditions: every ladder is an outer ladder
+  if ((inner == 0 && outer > 3) && (me_s > 0 && me_s < 36)) return 0;
+  if ((inner == 1 && outer > 3) && (me_s > 0 && me_s < 28)) return 0;
+  const int16_t me_p = hv.iphi[i];
+  const float me_r = hv.rg[i];
+  const int16_t cut = c_phi_cuts[pid];
+  const float z0_cut = 12.f;
+  const float dz_dr_fact = float(8 * 0.0285 / 0.015);
+  const double min_radius = 0.5 * 87.78;
+  const double r2t4 = 4. * min_radius * min_radius;
+  uint32_t kl = phi_bin(int16_t(me_p - cut));
+  uint32_t kh = phi_bin(int16_t(me_p + cut)) + 1;
+  if (kh == 129) kh = 1;
+  uint32_t cnt = 0;
+  for (uint32_t cb = kl; cb != kh;) {
+    const uint32_t p0 = poff[cb + h_off - 1], p1 = poff[cb + h_off];
+    for (uint32_t p = p0; p < p1; ++p) {
+      const uint32_t oi = uint32_t(pbins[p]) - 1u;  // event-local 0-based
+      const int16_t mo = hv.detind[oi];
+      if (mo > 2000) continue;
+      const float zo = hv.zg[oi], ro = hv.rg[oi];
+      {  // z0_cut_off
+        const float dr = __fsub_rn(ro, me_r);
+        if (double(dr) > c_max_r[pid] || dr < 0 ||
+            fabsf(__fsub_rn(__fmul_rn(me_z, ro), __fmul_rn(me_r, zo))) > __fmul_rn(z0_cut, dr))
+          continue;
+      }
+      const int16_t mo_p = hv.iphi[oi];
+      const int16_t dphi = int16_t(mo_p - me_p);
+      const int16_t i_dphi = int16_t(dphi < 0 ? -dphi : dphi);
+      if (i_dphi > cut) continue;
+      {  // z_size_cut
+        bool kill;
+        if (outer < 4) {
+          const int16_t so = hv.ysize[oi];
+          const int dy = inner == 0 ? 28 : 20;
+          const int16_t ds = int16_t(so - int16_t(me_s));
+          kill = me_s > 0 && so > 0 && (ds < 0 ? -int(ds) : int(ds)) > dy;
+        } else {
+          kill = false;
+          if (inner < 4 && me_s > 0) {
+            const float t = __fmul_rn(fabsf(__fdiv_rn(__fsub_rn(me_z, zo), __fsub_rn(me_r, ro))), dz_dr_fact);
+            const double tt = __dadd_rn(double(t), 0.5);
+            if (isfinite(tt)) {
+              const long long pred = (long long)trunc(tt);
+              const long long df = (long long)me_s - pred;
+              kill = (df < 0 ? -df : df) > 20;
+            } else {
+              continue;  // the reference raises (InexactError) here
+            }
+          }
+        }
+        if (kill) continue;
+      }
+      {  // pt_cut
+        const double dphi_f = __dmul_rn(double(i_dphi), (2 * 3.141592653589793) / double(1 << 16));
+        const float rr = __fmul_rn(me_r, ro);
+        const float dd = __fsub_rn(ro, me_r);
+        if (__dmul_rn(__dmul_rn(dphi_f, dphi_f), __dsub_rn(r2t4, double(rr))) > double(__fmul_rn(dd, dd))) continue;
+      }
+      if (kFill) {
+        const uint64_t g = cell_pos + cnt;
+        if (g - cell_lo < cap && g < uint64_t(d.cap_cells)) {
+          d.cell_inner[g] = i;
+          d.cell_outer[g] = oi;
+          d.cell_pair[g] = uint8_t(pid);
+          d.cell_id[g] = int32_t(g - cell_lo + 1);
+          d.cell_used[g] = 0;
+          d.cell_inner_z[g] = me_z;
+          d.cell_inner_r[g] = me_r;
+        }
+      }
+      ++cnt;
+    }
+    cb = cb + 1;
+    if (cb == 129) cb = 1;
+  }
+  return cnt;
+}
+
+template <bool kFill>
+__global__ void __launch_bounds__(256) k_doublets(Dev d, const uint32_t* __restrict__ pair_cum) {
+  const int e = blockIdx.y;
+  const EvInfo& E = d.ev[e];
+  const uint32_t n = E.n_items;
+  if (n == 0) return;
+  __shared__ uint32_t s_cum[kNPairs];
+  __shared__ uint32_t s_hls[11];
+  if (threadIdx.x < kNPairs) s_cum[threadIdx.x] = pair_cum[size_t(e) * kNPairs + threadIdx.x];
+  if (threadIdx.x < 11) s_hls[threadIdx.x] = d.hits_layer_start[size_t(e) * 11 + threadIdx.x];
+  __syncthreads();
+  const uint32_t hb = E.hit_base;
+  HitView hv{d.xg + hb, d.yg + hb, d.zg + hb, d.rg + hb, d.iphi + hb, d.ysize + hb, d.detind + hb};
+  const uint32_t* poff = d.phi_off + size_t(e) * kPhiTotBins;
+  const uint16_t* pbins = d.phi_bins + hb;
+  const uint32_t ib = E.item_base;
+  const uint64_t cell_lo = kFill ? uint64_t(d.item_cnt[ib]) : 0;
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    if (kFill) {
+      doublets_of_item<true>(d, e, j, s_cum, s_hls, hv, poff, pbins, d.item_cnt[ib + j], cell_lo, d.doublets_per_event);
+    } else {
+      d.item_cnt[ib + j] = doublets_of_item<false>(d, e, j, s_cum, s_hls, hv, poff, pbins, 0, 0, 0);
+    }
+  }
+}
+
+// per event: cell base, raw and capped counts
+__global__ void k_cell_bases(Dev d) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e > d.E) return;
+  if (e == d.E) {  // batch total of raw cells (the live length of the per-cell arrays)
+    d.ev[e].n_cells_raw = d.item_cnt[d.ev[d.E].item_base];
+    d.ev[e].cell_base = d.ev[e].n_cells_raw;
+    if (uint64_t(d.ev[e].n_cells_raw) > uint64_t(d.cap_cells)) atomicOr(d.status, kWarnBuffer);
+    return;
+  }
+  EvInfo& E = d.ev[e];
+  const uint32_t lo = d.item_cnt[E.item_base], hi = d.item_cnt[E.item_base + E.n_items];
+  E.n_cols_nb = 0;
+  E.n_cols_tr = 0;
+  E.cell_base = lo;
+  E.n_cells_raw = hi - lo;
+  uint32_t n = hi - lo;
+  if (n > d.doublets_per_event) { n = d.doublets_per_event; E.warnings |= kWarnDoublets; }
+  if (uint64_t(lo) + n > uint64_t(d.cap_cells)) {
+    E.warnings |= kWarnBuffer;
+    n = lo < uint64_t(d.cap_cells) ? uint32_t(d.cap_cells - lo) : 0u;
+  }
+  E.n_cells = n;
+}
+
+// zero the per-cell and per-hit counters of the batch (raw cell ranges, gaps included)
+__global__ void k_zero_counters(Dev d) {
+  const int e = blockIdx.y;
+  const EvInfo& E = d.ev[e];
+  const uint64_t cb = E.cell_base;
+  const uint32_t nraw = E.n_cells_raw;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nraw; k += gridDim.x * blockDim.x) {
+    const uint64_t c = cb + k;
+    if (c >= uint64_t(d.cap_cells)) break;
+    d.cn_cnt[c] = 0; d.cn_cur[c] = 0; d.ct_cnt[c] = 0; d.ct_cur[c] = 0; d.tstart_cnt[c] = 0;
+    d.cn_mask[4 * c] = 0; d.cn_mask[4 * c + 1] = 0; d.cn_mask[4 * c + 2] = 0; d.cn_mask[4 * c + 3] = 0;
+  }
+  const uint32_t hb = E.hit_base, nh = E.n_hits;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nh; k += gridDim.x * blockDim.x) {
+    d.ohc_cnt[hb + k] = 0; d.ohc_cur[hb + k] = 0; d.htt_cnt[hb + k] = 0; d.htt_cur[hb + k] = 0;
+  }
+}
+
+// ---------------------------------------------------------------- outer-hit lists
+template <int kPass>
+__global__ void k_ohc(Dev d) {
+  const int e = blockIdx.y;
+  const EvInfo& E = d.ev[e];
+  const uint64_t cb = E.cell_base;
+  const uint32_t hb = E.hit_base;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < E.n_cells; k += gridDim.x * blockDim.x) {
+    const uint64_t c = cb + k;
+    const uint32_t h = hb + d.cell_outer[c];
+    if (kPass == 0) {
+      atomicAdd(&d.ohc_cnt[h], 1u);
+    } else {
+      const uint32_t pos = d.ohc_cnt[h] + atomicAdd(&d.ohc_cur[h], 1u);
+      d.ohc_list[pos] = uint32_t(c);
+    }
+  }
+}
+
+// sort a short list in place (ascending)
+__device__ __forceinline__ void sort_list(uint32_t* a, uint32_t n) {
+  for (uint32_t p = 1; p < n; ++p) {
+    const uint32_t v = a[p];
+    uint32_t q = p;
+    while (q > 0 && a[q - 1] > v) { a[q] = a[q - 1]; --q; }
+    a[q] = v;
+  }
+}
+
+// per-hit lists (kind 0: cells ending on the hit; 2: tuples through the hit, descending)
+template <int kKind>
+__global__ void k_sort_hit_lists(Dev d) {
+  const int e = blockIdx.y;
+  const EvInfo& E = d.ev[e];
+  const uint32_t hb = E.hit_base;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < E.n_hits; k += gridDim.x * blockDim.x) {
+    const uint32_t h = hb + k;
+    if (kKind == 0) {
+      const uint32_t lo = d.ohc_cnt[h], hi = d.ohc_cnt[h + 1];
+      sort_list(d.ohc_list + lo, hi - lo);
+      if (hi - lo > uint32_t(kMaxCellsPerHit)) atomic_or_warn(&d.ev[e], kWarnLists);
+    }
+  }
+}
+
+// ---------------------------------------------------------------- connect
+struct CircleEq {
+  float xp, yp, c, alpha, beta;
+  __device__ CircleEq(float x1, float y1, float x2, float y2, float x3, float y3) {
+    const bool no_flip = fabsf(__fsub_rn(x3, x1)) < fabsf(__fsub_rn(y3, y1));
+    const float x1p = no_flip ? __fsub_rn(x1, x2) : __fsub_rn(y1, y2);
+    const float y1p = no_flip ? __fsub_rn(y1, y2) : __fsub_rn(x1, x2);
+    const float d12 = __fadd_rn(__fmul_rn(x1p, x1p), __fmul_rn(y1p, y1p));
+    const float x3p = no_flip ? __fsub_rn(x3, x2) : __fsub_rn(y3, y2);
+    const float y3p = no_flip ? __fsub_rn(y3, y2) : __fsub_rn(x3, x2);
+    const float d32 = __fadd_rn(__fmul_rn(x3p, x3p), __fmul_rn(y3p, y3p));
+    const float num = __fsub_rn(__fmul_rn(x1p, y3p), __fmul_rn(y1p, x3p));
+    const float det = __fsub_rn(__fmul_rn(d12, y3p), __fmul_rn(d32, y1p));
+    const float st2 = __fsub_rn(__fmul_rn(d12, x3p), __fmul_rn(d32, x1p));
+    const float seq = __fadd_rn(__fmul_rn(det, det), __fmul_rn(st2, st2));
+    float al2 = __fdiv_rn(1.0f, __fsqrt_rn(seq));
+    const float be2 = __fmul_rn(-st2, al2);
+    const float ct = __fmul_rn(__fmul_rn(2.0f, num), al2);
+    al2 = __fmul_rn(al2, det);
+    xp = x2; yp = y2;
+    c = no_flip ? ct : -ct;
+    alpha = no_flip ? al2 : -be2;
+    beta = no_flip ? be2 : -al2;
+  }
+  __device__ float dca0() const {
+    const float x = __fadd_rn(__fmul_rn(c, xp), alpha);
+    const float y = __fadd_rn(__fmul_rn(c, yp), beta);
+    return __fsub_rn(__fsqrt_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y))), 1.0f);
+  }
+};
+
+__device__ __forceinline__ bool are_aligned(float r1, float z1, float ri, float zi, float ro, float zo, float ptmin,
+                                            float theta_cut) {
+  const float radius_diff = fabsf(__fsub_rn(r1, ro));
+  const float dz = __fsub_rn(z1, zo);
+  const float d13 = __fadd_rn(__fmul_rn(radius_diff, radius_diff), __fmul_rn(dz, dz));
+  const float p_min = __fmul_rn(ptmin, __fsqrt_rn(d13));
+  const float t = fabsf(__fadd_rn(__fadd_rn(__fmul_rn(z1, __fsub_rn(ri, ro)), __fmul_rn(zi, __fsub_rn(ro, r1))),
+                                  __fmul_rn(zo, __fsub_rn(r1, ri))));
+  return __fmul_rn(t, p_min) <= __fmul_rn(__fmul_rn(theta_cut, d13), radius_diff);
+}
+
+template <int kPass>
+__global__ void __launch_bounds__(256) k_connect(Dev d) {
+  const int e = blockIdx.y;
+  const EvInfo& E = d.ev[e];
+  const uint64_t cb = E.cell_base;
+  const uint32_t hb = E.hit_base;
+  const float* xg = d.xg + hb;
+  const float* yg = d.yg + hb;
+  const float* zg = d.zg + hb;
+  const float* rg = d.rg + hb;
+  const int16_t* det = d.detind + hb;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < E.n_cells; k += gridDim.x * blockDim.x) {
+    const uint64_t c = cb + k;
+    const uint32_t ih = d.cell_inner[c], oh = d.cell_outer[c];
+    const uint32_t lo = d.ohc_cnt[hb + ih];
+    uint32_t n = d.ohc_cnt[hb + ih + 1] - lo;
+    if (n > uint32_t(kMaxCellsPerHit)) n = kMaxCellsPerHit;
+    if (kPass == 0) {
+      const float ri = d.cell_inner_r[c], zi = d.cell_inner_z[c];
+      const float ro = rg[oh], zo = zg[oh];
+      const bool is_barrel = det[ih] < 1184;
+      uint32_t mask[4] = {0, 0, 0, 0};
+      bool any = false;
+      for (uint32_t j = 0; j < n; ++j) {
+        const uint32_t o = d.ohc_list[lo + j];
+        const float r1 = d.cell_inner_r[o], z1 = d.cell_inner_z[o];
+        const uint32_t oih = d.cell_inner[o];
+        const bool aligned = are_aligned(r1, z1, ri, zi, ro, zo, ptmin_f(), is_barrel ? kThetaBarrel : kThetaForward);
+        const float region = det[oih] < 96 ? kDcaInner : kDcaOuter;
+        const CircleEq eq(xg[oih], yg[oih], xg[ih], yg[ih], xg[oh], yg[oh]);
+        bool cut;
+        if (eq.c > kHardCurv) cut = false;
+        else cut = fabsf(eq.dca0()) < __fmul_rn(region, fabsf(eq.c));
+        if (aligned && cut) {
+          mask[j >> 5] |= 1u << (j & 31);
+          atomicAdd(&d.cn_cnt[o], 1u);
+          d.cell_used[o] = 1;
+          any = true;
+        }
+      }
+      if (any) d.cell_used[c] = 1;
+      for (int w = 0; w < 4; ++w) d.cn_mask[4 * c + w] = mask[w];
+    } else {
+      for (uint32_t j = 0; j < n; ++j) {
+        if (!((d.cn_mask[4 * c + (j >> 5)] >> (j & 31)) & 1u)) continue;
+        const uint32_t o = d.ohc_list[lo + j];
+        const uint32_t pos = d.cn_cnt[o] + atomicAdd(&d.cn_cur[o], 1u);
+        if (pos < uint64_t(d.cap_pairs)) d.cn_list[pos] = uint32_t(c);
+      }
+    }
+  }
+}
+
+// per-cell lists: neighbours (kind 0) or tracks (kind 1), sorted ascending; flags overflow
+template <int kKind>
+__global__ void k_sort_cell_lists(Dev d) {
+  const int e = blockIdx.y;
+  const EvInfo& E = d.ev[e];
+  const uint64_t cb = E.cell_base;
+  __shared__ uint32_t s_cols;
+  if (threadIdx.x == 0) s_cols = 0;
+  __syncthreads();
+  uint32_t cols = 0;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < E.n_cells; k += gridDim.x * blockDim.x) {
+    const uint64_t c = cb + k;
+    const uint32_t* cnt = kKind == 0 ? d.cn_cnt : d.ct_cnt;
+    uint32_t* list = kKind == 0 ? d.cn_list : d.ct_list;
+    const uint32_t lo = cnt[c], hi = cnt[c + 1];
+    if (hi > lo) {
+      ++cols;
+      sort_list(list + lo, hi - lo);
+      if (hi - lo > uint32_t(kCellRows)) atomic_or_warn(&d.ev[e], kWarnLists);
+    }
+  }
+  if (cols) atomicAdd(&s_cols, cols);
+  __syncthreads();
+  if (threadIdx.x == 0 && s_cols) {
+    // columns of the fixed column store: one per cell with a non-empty list plus the reserved one
+    uint32_t* counter = kKind == 0 ? &d.ev[e].n_cols_nb : &d.ev[e].n_cols_tr;
+    const uint32_t before = atomicAdd(counter, s_cols);
+    if (before + s_cols + 1 > uint32_t(kMaxActiveColumns)) atomic_or_warn(&d.ev[e], kWarnColumns);
+  }
+}
+
+// ---------------------------------------------------------------- fishbone
+__global__ void __launch_bounds__(128) k_fishbone(Dev d) {
+  const int e = blockIdx.y;
+  const EvInfo& E = d.ev[e];
+  if (E.n_hits <= 1) return;
+  const uint32_t hb = E.hit_base;
+  const float* xg = d.xg + hb;
+  const float* yg = d.yg + hb;
+  const float* zg = d.zg + hb;
+  const int16_t* det = d.detind + hb;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < E.n_hits; k += gridDim.x * blockDim.x) {
+    const uint32_t lo = d.ohc_cnt[hb + k];
+    uint32_t n = d.ohc_cnt[hb + k + 1] - lo;
+    if (n < 2) continue;
+    if (n > uint32_t(kMaxCellsPerHit)) n = kMaxCellsPerHit;
+    const uint32_t* L = d.ohc_list + lo;
+    const float xo = xg[k], yo = yg[k], zo = zg[k];
+    // the cells that carry a neighbour relation, in list order
+    float dx[kMaxCellsPerHit], dy[kMaxCellsPerHit], dz[kMaxCellsPerHit], nrm[kMaxCellsPerHit];
+    uint16_t idet[kMaxCellsPerHit];
+    uint8_t idx[kMaxCellsPerHit];
+    uint32_t curr = 0;
+    for (uint32_t j = 0; j < n; ++j) {
+      const uint32_t c = L[j];
+      if (d.cell_used[c] == 0) continue;
+      const uint32_t ih = d.cell_inner[c];
+      idx[curr] = uint8_t(j);
+      idet[curr] = uint16_t(det[ih]);
+      dx[curr] = __fsub_rn(xg[ih], xo);
+      dy[curr] = __fsub_rn(yg[ih], yo);
+      dz[curr] = __fsub_rn(d.cell_inner_z[c], zo);
+      nrm[curr] = __fadd_rn(__fadd_rn(__fmul_rn(dx[curr], dx[curr]), __fmul_rn(dy[curr], dy[curr])),
+                            __fmul_rn(dz[curr], dz[curr]));
+      ++curr;
+    }
+    if (curr < 2) continue;
+    for (uint32_t ic = 0; ic + 1 < curr; ++ic) {
+      for (uint32_t jc = ic + 1; jc < curr; ++jc) {
+        const float cos12 = __fadd_rn(__fadd_rn(__fmul_rn(dx[ic], dx[jc]), __fmul_rn(dy[ic], dy[jc])),
+                                      __fmul_rn(dz[ic], dz[jc]));
+        if (idet[ic] != idet[jc] &&
+            __fmul_rn(cos12, cos12) >= __fmul_rn(__fmul_rn(0.99999f, nrm[ic]), nrm[jc])) {
+          if (nrm[ic] > nrm[jc]) { d.cell_id[L[idx[ic]]] = -1; break; }
+          d.cell_id[L[idx[jc]]] = -1;
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- ntuplets
+constexpr int kMaxDepth = 8;
+
+// Depth-first walk of find_ntuplets from one start cell. kFill == false counts tuples and
+// hits; kFill == true writes them from the given global tuple / hit positions.
+template <bool kFill>
+__device__ void walk(const Dev& d, uint64_t cb, uint64_t start, uint64_t* tuple_pos, uint64_t* hit_pos,
+                     uint32_t* ntup, uint32_t* nhit, uint64_t tuple_lo, uint32_t tcap, int e) {
+  uint32_t stack_c[kMaxDepth];
+  uint32_t stack_k[kMaxDepth];
+  int depth = 0;
+  stack_c[0] = uint32_t(start);
+  stack_k[0] = 0;
+  bool descended = false;  // whether the current top has an alive neighbour
+  bool alive_child[kMaxDepth];
+  alive_child[0] = false;
+  (void)descended;
+  while (depth >= 0) {
+    const uint32_t c = stack_c[depth];
+    const uint32_t lo = d.cn_cnt[c];
+    uint32_t nn = d.cn_cnt[c + 1] - lo;
+    if (nn > uint32_t(kCellRows)) nn = kCellRows;
+    bool pushed = false;
+    while (stack_k[depth] < nn) {
+      const uint32_t o = d.cn_list[lo + stack_k[depth]];
+      stack_k[depth]++;
+      if (d.cell_id[o] < 0) continue;  // killed by the fishbone
+      alive_child[depth] = true;
+      if (depth + 1 >= kMaxDepth) { atomic_or_warn(&d.ev[e], kWarnTuples); continue; }
+      ++depth;
+      stack_c[depth] = o;
+      stack_k[depth] = 0;
+      alive_child[depth] = false;
+      pushed = true;
+      break;
+    }
+    if (pushed) continue;
+    // all neighbours of the top visited
+    if (!alive_child[depth] && depth >= 1) {
+      const uint32_t nh = uint32_t(depth) + 2;  // doublets on the stack + 1
+      if (kFill) {
+        const uint64_t g = *tuple_pos;
+        const uint64_t hp = *hit_pos;
+        if (g < uint64_t(d.cap_tuples) && hp + nh <= uint64_t(d.cap_tuple_hits)) {
+          d.tuple_off[g] = uint32_t(hp);
+          const uint32_t hbase = d.ev[e].hit_base;
+          for (int k = 0; k <= depth; ++k) {
+            const uint32_t ih = d.cell_inner[stack_c[k]];
+            d.tuple_hits[hp + k] = ih;
+            d.tuple_det[hp + k] = uint16_t(d.detind[hbase + ih]);
+          }
+          const uint32_t oh = d.cell_outer[stack_c[depth]];
+          d.tuple_hits[hp + depth + 1] = oh;
+          d.tuple_det[hp + depth + 1] = uint16_t(d.detind[hbase + oh]);
+          d.quality[g] = 0;
+          // cell -> track pairs, only for tuples the reference keeps
+          if (g - tuple_lo < tcap) {
+            const uint64_t pp = hp - g;  // sum over earlier tuples of (hits - 1)
+            for (int k = 0; k <= depth; ++k) {
+              d.tuple_cell[pp + k] = stack_c[k];
+              atomicAdd(&d.ct_cnt[stack_c[k]], 1u);
+            }
+          }
+        }
+        *tuple_pos = g + 1;
+        *hit_pos = hp + nh;
+      } else {
+        *ntup += 1;
+        *nhit += nh;
+      }
+    }
+    --depth;
+  }
+  (void)cb;
+}
+
+__device__ __forceinline__ bool is_start(const Dev& d, uint64_t c) {
+  if (d.cell_id[c] < 0) return false;
+  const int p = d.cell_pair[c];
+  return p < 8 || p > 12;  // minHitsPerNtuplet = 3 (…_impl.jl:125)
+}
+
+template <bool kFill>
+__global__ void __launch_bounds__(128) k_ntuplets(Dev d) {
+  const int e = blockIdx.y;
+  const EvInfo& E = d.ev[e];
+  const uint64_t cb = E.cell_base;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < E.n_cells; k += gridDim.x * blockDim.x) {
+    const uint64_t c = cb + k;
+    if (!kFill) {
+      uint32_t nt = 0, nh = 0;
+      if (is_start(d, c)) walk<false>(d, cb, c, nullptr, nullptr, &nt, &nh, 0, 0, e);
+      d.tstart_cnt[c] = (uint64_t(nt) << 32) | nh;
+    } else {
+      if (!is_start(d, c)) continue;
+      const uint64_t v = d.tstart_cnt[c];
+      uint64_t tp = v >> 32, hp = v & 0xFFFFFFFFull;
+      walk<true>(d, cb, c, &tp, &hp, nullptr, nullptr, d.tstart_cnt[cb] >> 32, d.tuples_per_event, e);
+    }
+  }
+}
+
+__global__ void k_tuple_bases(Dev d) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e > d.E) return;
+  if (e == d.E) {
+    const uint64_t v = d.tstart_cnt[d.ev[d.E].n_cells_raw];
+    d.ev[e].n_tuples_raw = uint32_t(v >> 32);
+    d.ev[e].n_tuple_hits_raw = uint32_t(v);
+    d.ev[e].tuple_base = uint32_t(v >> 32);
+    d.ev[e].tuple_hit_base = uint32_t(v);
+    // the pair list (cell, tuple) holds hits - tuples entries
+    d.ev[e].n_dup_cells = 0;
+    return;
+  }
+  EvInfo& E = d.ev[e];
+  const uint64_t lo = d.tstart_cnt[E.cell_base], hi = d.tstart_cnt[uint64_t(E.cell_base) + E.n_cells_raw];
+  E.tuple_base = uint32_t(lo >> 32);
+  E.tuple_hit_base = uint32_t(lo);
+  E.n_tuples_raw = uint32_t(hi >> 32) - uint32_t(lo >> 32);
+  E.n_tuple_hits_raw = uint32_t(hi) - uint32_t(lo);
+  uint32_t nt = E.n_tuples_raw;
+  if (nt > d.tuples_per_event) { nt = d.tuples_per_event; E.warnings |= kWarnTuples; }
+  if (uint64_t(E.tuple_base) + E.n_tuples_raw > uint64_t(d.cap_tuples) ||
+      uint64_t(E.tuple_hit_base) + E.n_tuple_hits_raw > uint64_t(d.cap_tuple_hits)) {
+    E.warnings |= kWarnBuffer;
+    nt = 0;
+  }
+  E.n_tuples = nt;
+  E.n_dup_cells = 0;
+  E.dup_cell_base = 0;
+}
+
+// tuple hit offsets end markers and the live sizes for the per-tuple loops
+__global__ void k_tuple_ends(Dev d) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= d.E) return;
+  const EvInfo& E = d.ev[e];
+  if (uint64_t(E.tuple_base) + E.n_tuples_raw <= uint64_t(d.cap_tuples))
+    d.tuple_off[uint64_t(E.tuple_base) + E.n_tuples_raw] = E.tuple_hit_base + E.n_tuple_hits_raw;
+}
+
+// cell -> tuple lists: fill from the (cell, tuple) pairs of the kept tuples
+__global__ void k_cell_tracks_fill(Dev d) {
+  const int e = blockIdx.y;
+  const EvInfo& E = d.ev[e];
+  const uint64_t tb = E.tuple_base;
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < E.n_tuples; t += gridDim.x * blockDim.x) {
+    const uint64_t g = tb + t;
+    const uint32_t h0 = d.tuple_off[g], h1 = d.tuple_off[g + 1];
+    const uint64_t pp = uint64_t(h0) - g;
+    for (uint32_t k = 0; k + 1 < h1 - h0; ++k) {
+      const uint32_t c = d.tuple_cell[pp + k];
+      const uint32_t pos = d.ct_cnt[c] + atomicAdd(&d.ct_cur[c], 1u);
+      d.ct_list[pos] = uint32_t(g);
+    }
+  }
+}
+
+// kernel_early_duplicate_remover (…_impl.jl:143-166)
+__global__ void k_early_dup(Dev d) {
+  const int e = blockIdx.y;
+  const EvInfo& E = d.ev[e];
+  const uint64_t cb = E.cell_base;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < E.n_cells; k += gridDim.x * blockDim.x) {
+    const uint64_t c = cb + k;
+    const uint32_t lo = d.ct_cnt[c];
+    uint32_t n = d.ct_cnt[c + 1] - lo;
+    if (n > uint32_t(kCellRows)) n = kCellRows;
+    if (n < 2) continue;
+    uint32_t maxn = 0;
+    for (uint32_t j = 0; j < n; ++j) {
+      const uint32_t t = d.ct_list[lo + j];
+      const uint32_t s = d.tuple_off[t + 1] - d.tuple_off[t];
+      maxn = s > maxn ? s : maxn;
+    }
+    for (uint32_t j = 0; j < n; ++j) {
+      const uint32_t t = d.ct_list[lo + j];
+      if (d.tuple_off[t + 1] - d.tuple_off[t] != maxn) d.quality[t] = 1;
+    }
+  }
+}
+
+// tuple multiplicity counts (kernel_countMultiplicity + finalize!) per event: offsets after
+// kernel_fillMultiplicity are the exclusive prefix over bins 1..8
+__global__ void k_multiplicity(Dev d) {
+  const int e = blockIdx.x;
+  EvInfo& E = d.ev[e];
+  __shared__ uint32_t s_cnt[9];
+  if (threadIdx.x < 9) s_cnt[threadIdx.x] = 0;
+  __syncthreads();
+  const uint64_t tb = E.tuple_base;
+  for (uint32_t t = threadIdx.x; t < E.n_tuples; t += blockDim.x) {
+    const uint64_t g = tb + t;
+    const uint32_t n = d.tuple_off[g + 1] - d.tuple_off[g];
+    if (n < 3 || d.quality[g] == 1) continue;
+    if (n < 9) atomicAdd(&s_cnt[n - 1], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t acc = 0;
+    for (int b = 0; b < 9; ++b) { E.tm_off[b] = acc; acc += s_cnt[b]; }
+    for (int n = 3; n <= 5; ++n)
+      if (s_cnt[n - 1] > d.fits_per_mult) E.warnings |= kWarnFitsCapped;
+  }
+}
+
+}  // namespace
+
+void launch_ca(const Dev& d, const Launch& L) {
+  const dim3 g(L.bpe > 0 ? L.bpe : 64, d.E);
+  const int eb = div_up(d.E + 1, 128);
+  uint32_t* pair_cum = d.pair_cum;
+  k_items<<<div_up(d.E, 128), 128, 0, L.s>>>(d, pair_cum);
+  launch_ev_scan(d, L.s, int(offsetof(EvInfo, n_items)), int(offsetof(EvInfo, item_base)));
+  k_doublets<false><<<g, 256, 0, L.s>>>(d, pair_cum);
+  excl_scan_u32(d.item_cnt, d.cap_items, &d.ev[d.E].n_items, d.scan_tmp, L.s);
+  k_cell_bases<<<eb, 128, 0, L.s>>>(d);
+  k_doublets<true><<<g, 256, 0, L.s>>>(d, pair_cum);
+  k_zero_counters<<<g, 256, 0, L.s>>>(d);
+  // cells ending on each hit
+  k_ohc<0><<<g, 256, 0, L.s>>>(d);
+  excl_scan_u32(d.ohc_cnt, d.cap_hits, &d.ev[d.E].n_hits, d.scan_tmp, L.s);
+  k_ohc<1><<<g, 256, 0, L.s>>>(d);
+  k_sort_hit_lists<0><<<g, 256, 0, L.s>>>(d);
+  // connection and neighbour lists
+  k_connect<0><<<g, 256, 0, L.s>>>(d);
+  excl_scan_u32(d.cn_cnt, d.cap_cells, &d.ev[d.E].n_cells_raw, d.scan_tmp, L.s);
+  k_connect<1><<<g, 256, 0, L.s>>>(d);
+  k_sort_cell_lists<0><<<g, 256, 0, L.s>>>(d);
+  k_fishbone<<<g, 128, 0, L.s>>>(d);
+  // ntuplets
+  k_ntuplets<false><<<g, 128, 0, L.s>>>(d);
+  excl_scan_u64(d.tstart_cnt, d.cap_cells, &d.ev[d.E].n_cells_raw, d.scan_tmp64, L.s);
+  k_tuple_bases<<<eb, 128, 0, L.s>>>(d);
+  k_ntuplets<true><<<g, 128, 0, L.s>>>(d);
+  k_tuple_ends<<<div_up(d.E, 128), 128, 0, L.s>>>(d);
+  excl_scan_u32(d.ct_cnt, d.cap_cells, &d.ev[d.E].n_cells_raw, d.scan_tmp, L.s);
+  k_cell_tracks_fill<<<g, 256, 0, L.s>>>(d);
+  k_sort_cell_lists<1><<<g, 256, 0, L.s>>>(d);
+  k_early_dup<<<g, 256, 0, L.s>>>(d);
+  k_multiplicity<<<d.E, 256, 0, L.s>>>(d);
+}
+
+}  // namespace pxl

@@ -2,11 +2,9 @@
 #include "../../include/pxl.h"
 #include "pxl_internal.cuh"
 namespace pxl {
-void launch_ca(const Dev&, const Launch&) {}
 void launch_fit(const Dev&, const Launch&) {}
 void launch_classify(const Dev&, const Launch&) {}
 void launch_vertices(const Dev&, const Launch&) {}
 }  // namespace pxl
-int64_t copy_ca_product(PxlCtx*, int32_t, int32_t, void*, int64_t) { return PXL_ERR_ARG; }
 extern "C" int32_t pxl_bl_fit(const double*, const float*, const int32_t*, int32_t, double, int32_t, float*, float*,
                               float*, float*, float*, int32_t*, void*) { return PXL_ERR_STATE; }

@@ -10,36 +10,11 @@
 #include <vector>
 
 #include "../../include/pxl.h"
+#include "pxl_ctx.h"
 #include "pxl_internal.cuh"
 
 using namespace pxl;
 
-struct PxlCtx {
-  PxlParams p{};
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  Dev d{};
-  std::vector<void*> allocs;
-  int16_t* fed_slot_of = nullptr;
-  // host copy of the conditions needed at copy-out
-  std::vector<float> avg_geom;
-  // graph
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t graph_exec = nullptr;
-  uint32_t graph_mask = 0;
-  int graph_E = -1;
-  // last run
-  int32_t last_E = 0;
-  uint32_t last_mask = 0;
-  uint32_t done_mask = 0;
-  std::vector<EvInfo> ev_host;
-  bool ev_host_valid = false;
-  // pinned staging for offsets
-  uint64_t* h_off = nullptr;
-  size_t raw_cap = 0;
-  uint64_t* d_ev_off = nullptr;
-  uint8_t* d_raw = nullptr;
-};
 
 namespace {
 
@@ -249,7 +224,9 @@ int alloc_batch(PxlCtx* ctx) {
   A(xg, d.cap_hits); A(yg, d.cap_hits); A(zg, d.cap_hits); A(rg, d.cap_hits);
   A(iphi, d.cap_hits); A(xsize, d.cap_hits); A(ysize, d.cap_hits); A(detind, d.cap_hits); A(charge, d.cap_hits);
   A(hits_layer_start, E * 11); A(phi_off, E * kPhiTotBins); A(phi_bins, d.cap_hits);
+  A(pair_cum, E * kNPairs);
   A(item_cnt, d.cap_items + 1);
+  A(tuple_det, d.cap_tuple_hits);
   A(cell_inner, d.cap_cells); A(cell_outer, d.cap_cells); A(cell_pair, d.cap_cells); A(cell_id, d.cap_cells);
   A(cell_used, d.cap_cells); A(cell_inner_z, d.cap_cells); A(cell_inner_r, d.cap_cells);
   A(ohc_cnt, d.cap_hits + 1); A(ohc_cur, d.cap_hits); A(ohc_list, d.cap_cells);
@@ -302,7 +279,7 @@ int run_chain(PxlCtx* ctx, uint32_t mask, cudaStream_t s) {
   return 0;
 }
 
-int fetch_ev(PxlCtx* ctx) {
+int fetch_ev_impl(PxlCtx* ctx) {
   if (ctx->ev_host_valid) return 0;
   CK(cudaStreamSynchronize(ctx->stream));
   ctx->ev_host.resize(size_t(ctx->last_E) + 1);
@@ -367,6 +344,9 @@ int choose_shape(PxlCtx* ctx) {
 }
 
 }  // namespace
+
+int pxl_fetch_ev(PxlCtx* ctx) { return fetch_ev_impl(ctx); }
+static int fetch_ev(PxlCtx* ctx) { return fetch_ev_impl(ctx); }
 
 extern "C" {
 

@@ -86,6 +86,7 @@ struct EvInfo {
   uint32_t warnings;
   uint32_t tm_off[9];               // tuple multiplicity offsets (bins 1..8, reference layout)
   uint32_t n_dup_cells, dup_cell_base;
+  uint32_t n_cols_nb, n_cols_tr;    // non-empty neighbour / track lists (column store use)
 };
 
 // Everything a kernel may need, passed by value.
@@ -124,6 +125,7 @@ struct Dev {
   uint32_t* phi_off;           // [E][1281]
   uint16_t* phi_bins;          // [cap_hits], 1-based hit ids
   // doublets: work items and cells
+  uint32_t* pair_cum;      // [E][19] cumulative inner-layer sizes over the layer pairs
   uint32_t* item_cnt;      // [cap_items] doublets per inner hit item, then exclusive positions
   uint32_t* cell_inner;    // [cap_cells] event-local 0-based hit index
   uint32_t* cell_outer;
@@ -144,6 +146,7 @@ struct Dev {
   uint64_t* tstart_cnt;    // [cap_cells + 1] (tuples << 32 | hits) per start cell -> exclusive positions
   uint32_t* tuple_off;     // [cap_tuples + 1] global hit offsets (0-based, packed)
   uint32_t* tuple_hits;    // [cap_tuple_hits] event-local 0-based hit index
+  uint16_t* tuple_det;     // [cap_tuple_hits] detector index of each tuple hit (det_indices)
   uint8_t* quality;        // [cap_tuples] 0 bad 1 dup 2 loose
   uint32_t* tuple_cell;    // [cap_tuple_hits] (cell of each doublet of a tuple) for the cell -> track lists
   uint32_t* ct_cnt;        // [cap_cells + 1] tracks per cell -> offsets

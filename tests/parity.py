@@ -48,6 +48,40 @@ def compare_digis_clusters(gpu, orc, event: int = 0) -> list[str]:
     return errs
 
 
+def compare_ca(gpu, orc, event: int = 0) -> list[str]:
+    """Doublets, per-hit / per-cell lists, tuples, duplicate flags and multiplicity."""
+    errs = []
+    c = gpu.counts(event)
+    oc = orc.counts()
+    if c.n_doublets != oc["n_cells"]:
+        errs.append(f"n_doublets: gpu {c.n_doublets} oracle {oc['n_cells']}")
+    if c.n_tuples != oc["n_tuples"]:
+        errs.append(f"n_tuples: gpu {c.n_tuples} oracle {oc['n_tuples']}")
+    if errs:
+        return errs
+    for name in ("cells", "outer_hit_of_cell", "cell_neighbors", "cell_tracks"):
+        g, o = gpu.product(name, event), orc.get(name)
+        if not same_bits(g, o):
+            errs.append(f"{name}: {first_diff(g, o)}")
+    nt, nth = oc["n_tuples"], oc["n_tuple_hits"]
+    g, o = gpu.product("tuple_off", event), orc.get("tuple_off")
+    if not same_bits(g, o):
+        errs.append(f"tuple_off: {first_diff(g, o)}")
+    for name in ("tuple_hits", "det_hits"):
+        g, o = gpu.product(name, event), orc.get(name)[:nth]
+        if not same_bits(g, o):
+            errs.append(f"{name}: {first_diff(g, o)}")
+    g, o = gpu.product("quality", event)[:nt], orc.get("quality")[:nt]
+    if not same_bits(g, o):
+        errs.append(f"quality: {first_diff(g, o)}")
+    tm_off = orc.get("tm_off")
+    tm = np.concatenate([tm_off, orc.get("tm_bins")[:tm_off[-1]].astype(np.uint32)])
+    g = gpu.product("tuple_multiplicity", event)
+    if not same_bits(g, tm):
+        errs.append(f"tuple_multiplicity: {first_diff(g, tm)}")
+    return errs
+
+
 def compare_hits(gpu, orc, event: int = 0) -> list[str]:
     errs = []
     c = gpu.counts(event)

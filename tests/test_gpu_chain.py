@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 from oracle import oracle
-from parity import compare_digis_clusters, compare_hits
+from parity import compare_ca, compare_digis_clusters, compare_hits
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
 pytestmark = pytest.mark.gpu
@@ -67,6 +67,35 @@ def test_pu50_events_digis_hits(chain, orc, events_pu50):
         _run_both(chain, orc, ev, 3)
         errs = compare_digis_clusters(chain, orc) + compare_hits(chain, orc)
         assert not errs, (e, errs)
+
+
+def test_single_event_ca(chain, orc, event_single):
+    blob, offs = event_single
+    ev = blob[offs[0]:offs[1]]
+    _run_both(chain, orc, ev, 7)
+    errs = compare_ca(chain, orc)
+    assert not errs, errs
+
+
+def test_pu50_events_ca(chain, orc, events_pu50):
+    blob, offs = events_pu50
+    for e in range(len(offs) - 1):
+        ev = blob[offs[e]:offs[e + 1]]
+        _run_both(chain, orc, ev, 7)
+        errs = compare_ca(chain, orc)
+        assert not errs, (e, errs)
+
+
+def test_batch_ca_matches_oracle(conditions, orc, events_pu50):
+    from pixeltrack import PixelChain, batch_params
+    blob, offs = events_pu50
+    n = len(offs) - 1
+    with PixelChain(conditions, batch_params(n)) as bc:
+        bc.run_batch(blob, offs, stages=7)
+        for e in range(n):
+            orc.run_event(blob[offs[e]:offs[e + 1]], 7)
+            errs = compare_ca(bc, orc, e)
+            assert not errs, (e, errs)
 
 
 def test_batch_matches_oracle(conditions, orc, events_pu50):
