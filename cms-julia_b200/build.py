@@ -29,7 +29,6 @@ CUDA_SOURCES = [
     "k_fit.cu",
     "k_select.cu",
     "k_products.cu",
-    "k_stub_tail.cu",
     "pipeline.cu",
 ]
 

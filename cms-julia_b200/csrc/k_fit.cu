@@ -1,0 +1,144 @@
+// Broken-line fits of the chain's tuples (launchBrokenLineKernelsOnCPU,
+// broken_line_fit_on_gpu.jl:166-203: 3-hit and 4-hit tuples, 5-hit tuples fitted
+// with their first 4 hits, at most 24576 per multiplicity) and the stand-alone
+// fit entry point pxl_bl_fit (3..8 hits, FP64 or mixed precision).
+#include "../../include/pxl.h"
+#include "bl_fit.cuh"
+#include "pxl_internal.cuh"
+
+namespace pxl {
+
+namespace {
+
+template <int N>
+__device__ void fit_tuple(const Dev& d, uint64_t g, uint32_t hb, const uint32_t* hits_of_tuple, double B) {
+  double h[3][N];
+  float ge[6][N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    const uint32_t hit = hb + hits_of_tuple[i];
+    const int det = d.detind[hit];
+    const DetParamsD& dp = d.c.det[det];
+    float gl[6];
+    bl::to_global_cov(dp.R, d.xerr[hit], 0.0f, d.yerr[hit], gl);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) ge[k][i] = gl[k];
+    h[0][i] = d.xg[hit];
+    h[1][i] = d.yg[hit];
+    h[2][i] = d.zg[hit];
+  }
+  bl::TrackOut o;
+  const bool ok = bl::fit_track<N, double>(h, ge, B, o);
+  float* st = d.t_state + 5 * g;
+  float* cv = d.t_cov + 15 * g;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) st[k] = float(o.state[k]);
+#pragma unroll
+  for (int k = 0; k < 15; ++k) cv[k] = float(o.cov[k]);
+  d.t_pt[g] = float(o.pt);
+  d.t_eta[g] = float(o.eta);
+  d.t_chi2[g] = float((o.chi2_line + o.chi2_circle) / double(2 * N - 5));
+  d.t_fitted[g] = 1;
+  (void)ok;
+}
+
+__global__ void __launch_bounds__(128) k_fit_tuples(Dev d) {
+  const int e = blockIdx.y;
+  const EvInfo& E = d.ev[e];
+  const uint64_t tb = E.tuple_base;
+  const uint32_t hb = E.hit_base;
+  // B = Float64(Float32(bf)) as HelixFitOnGPU stores the field (ca_hit_ntuplet_generator.jl:83)
+  const double B = double(d.c.b_field);
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < E.n_tuples; t += gridDim.x * blockDim.x) {
+    const uint64_t g = tb + t;
+    const uint32_t h0 = d.tuple_off[g], n = d.tuple_off[g + 1] - h0;
+    bool fit = n >= 3 && n <= 5 && d.quality[g] != 1;
+    if (fit) {
+      const uint32_t cnt = E.tm_off[n] - E.tm_off[n - 1];
+      if (cnt > d.fits_per_mult) {
+        // the bin is read in decreasing id: only the largest `fits_per_mult` ids are fitted
+        uint32_t larger = 0;
+        for (uint32_t u = t + 1; u < E.n_tuples; ++u) {
+          const uint64_t gu = tb + u;
+          if (d.tuple_off[gu + 1] - d.tuple_off[gu] == n && d.quality[gu] != 1) ++larger;
+        }
+        fit = larger < d.fits_per_mult;
+      }
+    }
+    if (!fit) {
+      for (int k = 0; k < 5; ++k) d.t_state[5 * g + k] = 0.f;
+      for (int k = 0; k < 15; ++k) d.t_cov[15 * g + k] = 0.f;
+      d.t_pt[g] = 0.f; d.t_eta[g] = 0.f; d.t_chi2[g] = 0.f; d.t_fitted[g] = 0;
+      continue;
+    }
+    const uint32_t* hits = d.tuple_hits + h0;
+    if (n == 3) fit_tuple<3>(d, g, hb, hits, B);
+    else fit_tuple<4>(d, g, hb, hits, B);  // fit5as4
+  }
+}
+
+template <int N, class T>
+__device__ void standalone_fit(const double* hits, const float* hits_ge, int32_t first, double B, float* state,
+                               float* cov, float* chi2, float* pt, float* eta, int32_t* status, int32_t t) {
+  double h[3][N];
+  float ge[6][N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) h[a][i] = hits[3 * (first + i) + a];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) ge[k][i] = hits_ge[6 * (first + i) + k];
+  }
+  bl::TrackOut o;
+  const bool ok = bl::fit_track<N, T>(h, ge, B, o);
+#pragma unroll
+  for (int k = 0; k < 5; ++k) state[5 * t + k] = float(o.state[k]);
+#pragma unroll
+  for (int k = 0; k < 15; ++k) cov[15 * t + k] = float(o.cov[k]);
+  chi2[t] = float((o.chi2_line + o.chi2_circle) / double(2 * N - 5));
+  pt[t] = float(o.pt);
+  eta[t] = float(o.eta);
+  status[t] = ok ? 0 : 1;
+}
+
+template <class T>
+__global__ void __launch_bounds__(128) k_fit_standalone(const double* __restrict__ hits, const float* __restrict__ ge,
+                                                        const int32_t* __restrict__ offs, int32_t n, double B,
+                                                        float* state, float* cov, float* chi2, float* pt, float* eta,
+                                                        int32_t* status) {
+  for (int32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int32_t first = offs[t], nh = offs[t + 1] - offs[t];
+    switch (nh) {
+      case 3: standalone_fit<3, T>(hits, ge, first, B, state, cov, chi2, pt, eta, status, t); break;
+      case 4: standalone_fit<4, T>(hits, ge, first, B, state, cov, chi2, pt, eta, status, t); break;
+      case 5: standalone_fit<5, T>(hits, ge, first, B, state, cov, chi2, pt, eta, status, t); break;
+      case 6: standalone_fit<6, T>(hits, ge, first, B, state, cov, chi2, pt, eta, status, t); break;
+      case 7: standalone_fit<7, T>(hits, ge, first, B, state, cov, chi2, pt, eta, status, t); break;
+      case 8: standalone_fit<8, T>(hits, ge, first, B, state, cov, chi2, pt, eta, status, t); break;
+      default: status[t] = -1; break;
+    }
+  }
+}
+
+}  // namespace
+
+void launch_fit(const Dev& d, const Launch& L) {
+  const dim3 g(L.bpe > 0 ? L.bpe : 64, d.E);
+  k_fit_tuples<<<g, 128, 0, L.s>>>(d);
+}
+
+}  // namespace pxl
+
+extern "C" int32_t pxl_bl_fit(const double* hits, const float* hits_ge, const int32_t* offs, int32_t n, double b_field,
+                              int32_t precision, float* state, float* cov, float* chi2, float* pt, float* eta,
+                              int32_t* status, void* stream) {
+  if (n < 0 || !hits || !hits_ge || !offs || !state || !cov || !chi2 || !pt || !eta || !status) return PXL_ERR_ARG;
+  if (n == 0) return 0;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int blocks = int((n + 127) / 128);
+  if (precision == 0)
+    pxl::k_fit_standalone<double><<<blocks, 128, 0, s>>>(hits, hits_ge, offs, n, b_field, state, cov, chi2, pt, eta, status);
+  else
+    pxl::k_fit_standalone<float><<<blocks, 128, 0, s>>>(hits, hits_ge, offs, n, b_field, state, cov, chi2, pt, eta, status);
+  return cudaGetLastError() == cudaSuccess ? 0 : PXL_ERR_CUDA;
+}

@@ -1,0 +1,449 @@
+// Track classification, duplicate cleaning and vertex finding. Restates
+// ca_hit_ntuplet_generator_kernels_impl.jl:213-362 (kernel_classify_tracks,
+// kernel_fast_duplicate_remover, kernel_count/fill_hit_in_tracks,
+// kernel_triplet_cleaner) with the cuts of ca_hit_ntuplet_generator_kernels.jl:79-87,
+// and plugin-PixelVertexFinding/gpu_vertex_finder.jl:51-436.
+//
+// kernel_fast_duplicate_remover is order dependent (a cell sees the marks of the
+// cells before it), so it runs cell by cell within an event, one warp per event,
+// the lanes sharing the work of each cell. The triplet cleaner only ever writes
+// "dup" and tests "!= bad", so its hits run in parallel. Vertex sums keep the
+// reference's track order (one thread per vertex walks the tracks in order).
+#include <cstddef>
+
+#include "pxl_internal.cuh"
+
+namespace pxl {
+
+namespace {
+
+constexpr float kChi2Coeff[4] = {0.68177776f, 0.74609577f, -0.08035491f, 0.00315399f};
+
+// kernel_classify_tracks
+__global__ void k_classify(Dev d) {
+  const int e = blockIdx.y;
+  const EvInfo& E = d.ev[e];
+  const uint64_t tb = E.tuple_base;
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < E.n_tuples; t += gridDim.x * blockDim.x) {
+    const uint64_t g = tb + t;
+    const uint32_t n = d.tuple_off[g + 1] - d.tuple_off[g];
+    if (d.quality[g] == 1) continue;
+    if (n < 3) continue;
+    const float* st = d.t_state + 5 * g;
+    bool nan = false;
+    for (int k = 0; k < 5; ++k) nan |= isnan(st[k]);
+    if (nan) continue;
+    const float ptv = d.t_pt[g];
+    const float pt = ptv < 10.0f ? ptv : 10.0f;
+    const float cut = __fmul_rn(30.0f, __fadd_rn(kChi2Coeff[0], __fmul_rn(pt, __fadd_rn(kChi2Coeff[1],
+                      __fmul_rn(pt, __fadd_rn(kChi2Coeff[2], __fmul_rn(pt, kChi2Coeff[3])))))));
+    if (__fmul_rn(3.0f, d.t_chi2[g]) >= cut) continue;
+    const bool quad = n > 3;
+    const float max_tip = quad ? 0.5f : 0.3f, min_pt = quad ? 0.3f : 0.5f, max_zip = 12.0f;
+    if (fabsf(st[1]) < max_tip && ptv > min_pt && fabsf(st[4]) < max_zip) d.quality[g] = 2;
+  }
+}
+
+// cells with two or more tracks, compacted in cell order
+template <int kPass>
+__global__ void k_dup_cells(Dev d) {
+  const int e = blockIdx.y;
+  const EvInfo& E = d.ev[e];
+  const uint64_t cb = E.cell_base;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < E.n_cells_raw; k += gridDim.x * blockDim.x) {
+    const uint64_t c = cb + k;
+    if (c >= uint64_t(d.cap_cells)) break;
+    if (kPass == 0) {
+      d.dup_flag[c] = (k < E.n_cells && d.ct_cnt[c + 1] - d.ct_cnt[c] >= 2) ? 1u : 0u;
+    } else if (k < E.n_cells && d.ct_cnt[c + 1] - d.ct_cnt[c] >= 2) {
+      d.dup_cells[d.dup_flag[c]] = uint32_t(c);
+    }
+  }
+}
+
+// kernel_fast_duplicate_remover: one warp per event, cells in order
+__global__ void k_fast_dup(Dev d) {
+  const int e = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  if (e >= d.E) return;
+  const unsigned lane = threadIdx.x & 31u;
+  const EvInfo& E = d.ev[e];
+  const uint32_t lo = d.dup_flag[E.cell_base], hi = d.dup_flag[uint64_t(E.cell_base) + E.n_cells_raw];
+  for (uint32_t q = lo; q < hi; ++q) {
+    const uint32_t c = d.dup_cells[q];
+    const uint32_t l0 = d.ct_cnt[c];
+    uint32_t n = d.ct_cnt[c + 1] - l0;
+    if (n > uint32_t(kCellRows)) n = kCellRows;
+    // argmin |tip| over the loose tracks, first in list order on ties (strict <, mc = 10000)
+    float best = 10000.f;
+    uint32_t best_pos = 0xFFFFFFFFu;
+    for (uint32_t j = lane; j < n; j += 32) {
+      const uint32_t t = d.ct_list[l0 + j];
+      if (d.quality[t] == 2) {
+        const float s = fabsf(d.t_state[5 * size_t(t) + 1]);
+        if (s < best) { best = s; best_pos = j; }
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const float ob = __shfl_down_sync(0xffffffffu, best, o);
+      const uint32_t op = __shfl_down_sync(0xffffffffu, best_pos, o);
+      if (ob < best || (ob == best && op < best_pos)) { best = ob; best_pos = op; }
+    }
+    best_pos = __shfl_sync(0xffffffffu, best_pos, 0);
+    const uint32_t im = best_pos == 0xFFFFFFFFu ? 0xFFFFFFFFu : d.ct_list[l0 + best_pos];
+    __syncwarp();
+    for (uint32_t j = lane; j < n; j += 32) {
+      const uint32_t t = d.ct_list[l0 + j];
+      if (d.quality[t] != 0 && t != im) d.quality[t] = 1;
+    }
+    __syncwarp();
+  }
+}
+
+// hit -> loose tuple lists
+template <int kPass>
+__global__ void k_hit_to_tuple(Dev d) {
+  const int e = blockIdx.y;
+  const EvInfo& E = d.ev[e];
+  const uint64_t tb = E.tuple_base;
+  const uint32_t hb = E.hit_base;
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < E.n_tuples; t += gridDim.x * blockDim.x) {
+    const uint64_t g = tb + t;
+    if (d.quality[g] != 2) continue;
+    const uint32_t h0 = d.tuple_off[g], h1 = d.tuple_off[g + 1];
+    for (uint32_t p = h0; p < h1; ++p) {
+      const uint32_t h = hb + d.tuple_hits[p];
+      if (kPass == 0) atomicAdd(&d.htt_cnt[h], 1u);
+      else d.htt_list[d.htt_cnt[h] + atomicAdd(&d.htt_cur[h], 1u)] = uint32_t(g);
+    }
+  }
+}
+
+// kernel_triplet_cleaner over hits; lists ordered by decreasing tuple id as the reference fills them
+__global__ void k_triplet_cleaner(Dev d) {
+  const int e = blockIdx.y;
+  const EvInfo& E = d.ev[e];
+  const uint32_t hb = E.hit_base;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < E.n_hits; k += gridDim.x * blockDim.x) {
+    const uint32_t lo = d.htt_cnt[hb + k], hi = d.htt_cnt[hb + k + 1];
+    const uint32_t n = hi - lo;
+    uint32_t* L = d.htt_list + lo;
+    for (uint32_t p = 1; p < n; ++p) {  // decreasing id
+      const uint32_t v = L[p];
+      uint32_t q = p;
+      while (q > 0 && L[q - 1] < v) { L[q] = L[q - 1]; --q; }
+      L[q] = v;
+    }
+    if (n < 2) continue;
+    uint32_t maxnh = 0;
+    for (uint32_t j = 0; j < n; ++j) {
+      const uint32_t t = L[j];
+      const uint32_t s = d.tuple_off[t + 1] - d.tuple_off[t];
+      maxnh = s > maxnh ? s : maxnh;
+    }
+    for (uint32_t j = 0; j < n; ++j) {
+      const uint32_t t = L[j];
+      if (d.tuple_off[t + 1] - d.tuple_off[t] != maxnh) d.quality[t] = 1;
+    }
+    if (maxnh > 3) continue;
+    float mc = 10000.f;
+    uint32_t im = 0xFFFFFFFFu;
+    for (uint32_t j = 0; j < n; ++j) {
+      const uint32_t t = L[j];
+      const float s = fabsf(d.t_state[5 * size_t(t) + 1]);
+      if (d.quality[t] != 0 && s < mc) { mc = s; im = t; }
+    }
+    for (uint32_t j = 0; j < n; ++j) {
+      const uint32_t t = L[j];
+      if (d.quality[t] != 0 && t != im) d.quality[t] = 1;
+    }
+  }
+}
+
+// ---------------------------------------------------------------- vertices
+constexpr int kVtxThreads = 256;
+constexpr int kMaxVtx = 1024;
+
+__global__ void __launch_bounds__(kVtxThreads) k_vertices(Dev d) {
+  const int e = blockIdx.x;
+  EvInfo& E = d.ev[e];
+  const uint64_t tb = E.tuple_base;
+  const uint32_t ntu = E.n_tuples;
+  float* zv = d.zv + size_t(e) * kMaxVtx;
+  float* wv = d.wv + size_t(e) * kMaxVtx;
+  float* vchi2 = d.vchi2 + size_t(e) * kMaxVtx;
+  float* ptv2 = d.ptv2 + size_t(e) * kMaxVtx;
+  uint16_t* sort_ind = d.sort_ind + size_t(e) * kMaxVtx;
+  int32_t* nn = d.ndof + tb + size_t(e) * kMaxVtx;  // length n_tuples + 1024
+  float* zt = d.vws_zt + tb;
+  float* ezt2 = d.vws_ezt2 + tb;
+  float* ptt2 = d.vws_ptt2 + tb;
+  int32_t* iv = d.vws_iv + tb;     // 1-based values as the reference stores them
+  uint32_t* itrk = d.vws_itrk + tb;
+  uint8_t* izt = d.vws_izt + tb;
+  __shared__ uint32_t sh[33];
+  __shared__ uint32_t s_off[257];
+  __shared__ uint32_t s_cur[256];
+  __shared__ uint32_t s_nv, s_nvi, s_warn;
+  for (int v = threadIdx.x; v < kMaxVtx; v += blockDim.x) { zv[v] = 0; wv[v] = 0; vchi2[v] = 0; ptv2[v] = 0; sort_ind[v] = 0; }
+  for (uint32_t t = threadIdx.x; t < ntu + kMaxVtx; t += blockDim.x) nn[t] = 0;
+  for (uint32_t t = threadIdx.x; t < ntu; t += blockDim.x) d.idv[tb + t] = -1;
+  if (threadIdx.x == 0) s_warn = 0;
+  // load_tracks (:51-82): >= 4 hits, loose, pt >= 0.5, in tuple order
+  uint32_t nt = 0;
+  for (uint32_t b = 0; b < ntu; b += blockDim.x) {
+    const uint32_t t = b + threadIdx.x;
+    bool sel = false;
+    if (t < ntu) {
+      const uint64_t g = tb + t;
+      const uint32_t n = d.tuple_off[g + 1] - d.tuple_off[g];
+      sel = n >= 4 && d.quality[g] == 2 && !(d.t_pt[g] < 0.5f);
+    }
+    uint32_t tot;
+    const uint32_t ex = block_excl_scan(sel ? 1u : 0u, sh, &tot);
+    if (sel) {
+      const uint64_t g = tb + t;
+      const uint32_t i = nt + ex;
+      const float pt = d.t_pt[g];
+      itrk[i] = t;
+      zt[i] = d.t_state[5 * g + 4];
+      ezt2[i] = d.t_cov[15 * g + 14];
+      ptt2[i] = __fmul_rn(pt, pt);
+    }
+    nt += tot;
+  }
+  if (threadIdx.x == 0) E.n_vtx_tracks = nt;
+  // cluster_tracks_by_density (:84-206), HisToContainer{UInt8,256,16000,8,UInt16}
+  for (int b = threadIdx.x; b < 257; b += blockDim.x) s_off[b] = 0;
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
+    int32_t iz = int32_t(trunc(__dmul_rn(double(zt[i]), 10.)));
+    iz = iz < -128 ? -128 : (iz > 127 ? 127 : iz);
+    izt[i] = uint8_t(iz + 128);
+    atomicAdd(&s_off[izt[i]], 1u);
+    iv[i] = int32_t(i + 1);
+  }
+  __syncthreads();
+  {  // exclusive starts of the 256 bins
+    const uint32_t v = threadIdx.x < 256 ? s_off[threadIdx.x] : 0u;
+    uint32_t tot;
+    const uint32_t ex = block_excl_scan(v, sh, &tot);
+    if (threadIdx.x < 256) { s_off[threadIdx.x] = ex; s_cur[threadIdx.x] = ex; }
+    if (threadIdx.x == 0) s_off[256] = tot;
+  }
+  __syncthreads();
+  uint32_t* B = d.vws_bins + tb;  // histogram contents, 1-based track indices
+  for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
+    const uint32_t pos = atomicAdd(&s_cur[izt[i]], 1u);
+    B[pos] = i + 1;
+  }
+  __syncthreads();
+  for (int b = threadIdx.x; b < 256; b += blockDim.x) {  // decreasing track index within a bin
+    const uint32_t lo = s_off[b], hi = s_off[b + 1];
+    for (uint32_t p = lo + 1; p < hi; ++p) {
+      const uint32_t v = B[p];
+      uint32_t q = p;
+      while (q > lo && B[q - 1] < v) { B[q] = B[q - 1]; --q; }
+      B[q] = v;
+    }
+  }
+  __syncthreads();
+  const float eps = 0.07f, err2_max = __fmul_rn(0.01f, 0.01f), chi2_max = 9.0f;
+  for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
+    if (ezt2[i] > err2_max) continue;
+    const int bs0 = int(izt[i]) + 1;
+    const int be = bs0 + 1 < 256 ? bs0 + 1 : 256;
+    const int bs = bs0 - 1 > 1 ? bs0 - 1 : 1;
+    int32_t cnt = 0;
+    for (uint32_t p = s_off[bs - 1]; p < s_off[be]; ++p) {
+      const uint32_t j = B[p] - 1;
+      if (j == i) continue;
+      const float dist = fabsf(__fsub_rn(zt[i], zt[j]));
+      if (dist > eps) continue;
+      if (__fmul_rn(dist, dist) > __fmul_rn(chi2_max, __fadd_rn(ezt2[i], ezt2[j]))) continue;
+      ++cnt;
+    }
+    nn[i] = cnt;
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
+    float mdist = eps;
+    const int bs0 = int(izt[i]) + 1;
+    const int be = bs0 + 1 < 256 ? bs0 + 1 : 256;
+    const int bs = bs0 - 1 > 1 ? bs0 - 1 : 1;
+    int32_t a = int32_t(i + 1);
+    for (uint32_t p = s_off[bs - 1]; p < s_off[be]; ++p) {
+      const uint32_t j = B[p] - 1;
+      if (nn[j] < nn[i]) continue;
+      if (nn[j] == nn[i] && zt[j] >= zt[i]) continue;
+      const float dist = fabsf(__fsub_rn(zt[i], zt[j]));
+      if (dist > mdist) continue;
+      if (__fmul_rn(dist, dist) > __fmul_rn(chi2_max, __fadd_rn(ezt2[i], ezt2[j]))) continue;
+      mdist = dist;
+      a = int32_t(j + 1);
+    }
+    iv[i] = a;
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
+    int32_t m = iv[i];
+    while (m != iv[m - 1]) m = iv[m - 1];
+    iv[i] = m;
+  }
+  __syncthreads();
+  uint32_t found = 0;
+  for (uint32_t b = 0; b < nt; b += blockDim.x) {
+    const uint32_t i = b + threadIdx.x;
+    const bool root = i < nt && iv[i] == int32_t(i + 1);
+    const bool seed = root && nn[i] >= 2;
+    uint32_t tot;
+    const uint32_t ex = block_excl_scan(seed ? 1u : 0u, sh, &tot);
+    if (root) iv[i] = seed ? -int32_t(found + ex + 1) : -9998;
+    found += tot;
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x)
+    if (iv[i] >= 0) iv[i] = iv[iv[i] - 1];
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) iv[i] = -iv[i];
+  if (threadIdx.x == 0) {
+    if (found >= uint32_t(kMaxVtx)) { s_warn |= kWarnVertex; found = kMaxVtx - 1; }
+    s_nv = found;
+    s_nvi = found;
+  }
+  __syncthreads();
+  // fit_vertices, :228-286 (one thread per vertex keeps the track order of the sums)
+  auto fit = [&](double chi2max) {
+    const uint32_t nvf = s_nvi;
+    for (uint32_t v = threadIdx.x; v < nvf; v += blockDim.x) {
+      float z = 0, w = 0;
+      for (uint32_t i = 0; i < nt; ++i) {
+        if (iv[i] != int32_t(v + 1)) continue;
+        const float wi = __fdiv_rn(1.0f, ezt2[i]);
+        z = __fadd_rn(z, __fmul_rn(zt[i], wi));
+        w = __fadd_rn(w, wi);
+      }
+      if (!(w > 0)) atomicOr(&s_warn, kWarnVertex);
+      z = __fdiv_rn(z, w);
+      float c2s = 0;
+      int32_t cnt = -1;
+      for (uint32_t i = 0; i < nt; ++i) {
+        if (iv[i] != int32_t(v + 1)) continue;
+        float c2 = __fsub_rn(z, zt[i]);
+        c2 = __fmul_rn(c2, __fdiv_rn(c2, ezt2[i]));
+        if (double(c2) > chi2max) { iv[i] = 9999; continue; }
+        c2s = __fadd_rn(c2s, c2);
+        cnt += 1;
+      }
+      if (cnt > 0) w = __fmul_rn(w, __fdiv_rn(float(cnt), c2s));
+      zv[v] = z; wv[v] = w; vchi2[v] = c2s; nn[v] = cnt;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) s_nv = nvf;
+    __syncthreads();
+  };
+  fit(50.);
+  // split_vertices, :288-371: each vertex decides alone; new ids follow the vertex order
+  {
+    const uint32_t nvf = s_nv;
+    for (uint32_t b = 0; b < nvf; b += blockDim.x) {
+      const uint32_t kv = b + threadIdx.x;
+      bool split = false;
+      float znew0 = 0, znew1 = 0;
+      if (kv < nvf && nn[kv] >= 4 && !(vchi2[kv] < __fmul_rn(9.0f, float(nn[kv])))) {
+        if (nn[kv] >= 512) {
+          atomicOr(&s_warn, kWarnVertex);
+        } else {
+          // 2-means in the vertex's tracks (zz = zt - zv, weights 1/ezt2), at most 20 iterations
+          uint32_t nq = 0;
+          const float zc = zv[kv];
+          for (uint32_t i = 0; i < nt; ++i) if (iv[i] == int32_t(kv + 1)) ++nq;
+          if (nq != uint32_t(nn[kv] + 1)) atomicOr(&s_warn, kWarnVertex);
+          // new_v assignment kept in the sign of a scratch copy: recompute per iteration
+          bool more = true;
+          int iter = 20;
+          // first assignment: zz < 0 -> 1 else 2; stored per track in izt's high bit space
+          for (uint32_t i = 0; i < nt; ++i)
+            if (iv[i] == int32_t(kv + 1)) izt[i] = __fsub_rn(zt[i], zc) < 0 ? 1 : 2;
+          float w0 = 0, w1 = 0;
+          while (more) {
+            more = false;
+            znew0 = znew1 = 0; w0 = w1 = 0;
+            for (uint32_t i = 0; i < nt; ++i) {
+              if (iv[i] != int32_t(kv + 1)) continue;
+              const float zz = __fsub_rn(zt[i], zc), ww = __fdiv_rn(1.0f, ezt2[i]);
+              if (izt[i] == 1) { znew0 = __fadd_rn(znew0, __fmul_rn(zz, ww)); w0 = __fadd_rn(w0, ww); }
+              else { znew1 = __fadd_rn(znew1, __fmul_rn(zz, ww)); w1 = __fadd_rn(w1, ww); }
+            }
+            znew0 = __fdiv_rn(znew0, w0);
+            znew1 = __fdiv_rn(znew1, w1);
+            for (uint32_t i = 0; i < nt; ++i) {
+              if (iv[i] != int32_t(kv + 1)) continue;
+              const float zz = __fsub_rn(zt[i], zc);
+              const float d0 = fabsf(__fsub_rn(znew0, zz)), d1 = fabsf(__fsub_rn(znew1, zz));
+              const uint8_t newer = d0 < d1 ? 1 : 2;
+              more |= newer != izt[i];
+              izt[i] = newer;
+            }
+            if (--iter <= 0) more = false;
+          }
+          if (!(w0 == 0 || w1 == 0)) {
+            const float dd = __fsub_rn(znew0, znew1);
+            const float dist2 = __fmul_rn(dd, dd);
+            const float chi2_dist = __fdiv_rn(dist2, __fadd_rn(__fdiv_rn(1.0f, w0), __fdiv_rn(1.0f, w1)));
+            split = !(chi2_dist < 4);
+          }
+        }
+      }
+      uint32_t tot;
+      const uint32_t ex = block_excl_scan(split ? 1u : 0u, sh, &tot);
+      if (split) {
+        const int32_t newv = int32_t(s_nvi + ex + 1);
+        for (uint32_t i = 0; i < nt; ++i)
+          if (iv[i] == int32_t(kv + 1) && izt[i] == 2) iv[i] = newv;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) s_nvi += tot;
+      __syncthreads();
+    }
+    if (threadIdx.x == 0 && s_nvi >= uint32_t(kMaxVtx)) { s_warn |= kWarnVertex; s_nvi = kMaxVtx - 1; }
+    __syncthreads();
+  }
+  fit(5000.);
+  // sort_by_pt2, :391-436 (the sorted order itself is dropped by the reference)
+  const uint32_t nvf = s_nv;
+  if (nvf >= 1) {
+    for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) d.idv[tb + itrk[i]] = int16_t(iv[i]);
+    for (uint32_t v = threadIdx.x; v < nvf; v += blockDim.x) {
+      float s = 0;
+      for (uint32_t i = 0; i < nt; ++i) if (iv[i] == int32_t(v + 1)) s = __fadd_rn(s, ptt2[i]);
+      ptv2[v] = s;
+    }
+    if (threadIdx.x == 0 && nvf == 1) sort_ind[0] = 1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    E.n_vtx = nvf;
+    if (s_warn) E.warnings |= s_warn;
+  }
+}
+
+}  // namespace
+
+void launch_classify(const Dev& d, const Launch& L) {
+  const dim3 g(L.bpe > 0 ? L.bpe : 64, d.E);
+  k_classify<<<g, 256, 0, L.s>>>(d);
+  k_dup_cells<0><<<g, 256, 0, L.s>>>(d);
+  excl_scan_u32(d.dup_flag, d.cap_cells, &d.ev[d.E].n_cells_raw, d.scan_tmp, L.s);
+  k_dup_cells<1><<<g, 256, 0, L.s>>>(d);
+  k_fast_dup<<<div_up(d.E, 4), 128, 0, L.s>>>(d);
+  k_hit_to_tuple<0><<<g, 256, 0, L.s>>>(d);
+  excl_scan_u32(d.htt_cnt, d.cap_hits, &d.ev[d.E].n_hits, d.scan_tmp, L.s);
+  k_hit_to_tuple<1><<<g, 256, 0, L.s>>>(d);
+  k_triplet_cleaner<<<g, 256, 0, L.s>>>(d);
+}
+
+void launch_vertices(const Dev& d, const Launch& L) {
+  k_vertices<<<d.E, kVtxThreads, 0, L.s>>>(d);
+}
+
+}  // namespace pxl

@@ -164,6 +164,8 @@ struct Dev {
   uint32_t* dup_flag;      // [cap_cells + 1]
   // vertices, per event
   int16_t* idv;            // [cap_tuples] per tuple (global tuple index), -1 when unused
+  float* vws_zt; float* vws_ezt2; float* vws_ptt2;  // [cap_tuples] vertex-finder workspace per selected track
+  int32_t* vws_iv; uint32_t* vws_itrk; uint8_t* vws_izt; uint32_t* vws_bins;
   float* zv; float* wv; float* vchi2; float* ptv2;  // [E][1024]
   int32_t* ndof;           // [cap_tuples] per event slot region (same packing as tuples)
   uint16_t* sort_ind;      // [E][1024]

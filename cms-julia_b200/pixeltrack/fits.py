@@ -1,0 +1,38 @@
+"""Stand-alone broken-line fits on device tensors (pxl_bl_fit of include/pxl.h).
+
+Inputs are CUDA tensors: hits [H, 3] float64 (x, y, z), hits_ge [H, 6] float32
+(global covariance per hit, the toGlobal layout of SOARotation.jl:139-147) and
+offsets [n+1] int32 (3..8 hits per track). precision 0 = FP64 throughout,
+1 = FP32 arithmetic with FP64 band-system Cholesky solve and covariance.
+"""
+from __future__ import annotations
+
+import torch
+
+from . import _native
+from ._native import check
+
+
+def bl_fit(hits: torch.Tensor, hits_ge: torch.Tensor, offsets: torch.Tensor, b_field: float,
+           precision: int = 0, stream: torch.cuda.Stream | None = None) -> dict[str, torch.Tensor]:
+    if not (hits.is_cuda and hits_ge.is_cuda and offsets.is_cuda):
+        raise ValueError("bl_fit takes CUDA tensors")
+    hits = hits.contiguous().to(torch.float64)
+    hits_ge = hits_ge.contiguous().to(torch.float32)
+    offsets = offsets.contiguous().to(torch.int32)
+    n = offsets.numel() - 1
+    dev = hits.device
+    out = {
+        "state": torch.empty((n, 5), dtype=torch.float32, device=dev),
+        "cov": torch.empty((n, 15), dtype=torch.float32, device=dev),
+        "chi2": torch.empty(n, dtype=torch.float32, device=dev),
+        "pt": torch.empty(n, dtype=torch.float32, device=dev),
+        "eta": torch.empty(n, dtype=torch.float32, device=dev),
+        "status": torch.empty(n, dtype=torch.int32, device=dev),
+    }
+    s = (stream or torch.cuda.current_stream(dev)).cuda_stream
+    check(_native.lib().pxl_bl_fit(hits.data_ptr(), hits_ge.data_ptr(), offsets.data_ptr(), n, float(b_field),
+                                   int(precision), out["state"].data_ptr(), out["cov"].data_ptr(),
+                                   out["chi2"].data_ptr(), out["pt"].data_ptr(), out["eta"].data_ptr(),
+                                   out["status"].data_ptr(), s), "pxl_bl_fit")
+    return out

@@ -48,8 +48,9 @@ def compare_digis_clusters(gpu, orc, event: int = 0) -> list[str]:
     return errs
 
 
-def compare_ca(gpu, orc, event: int = 0) -> list[str]:
-    """Doublets, per-hit / per-cell lists, tuples, duplicate flags and multiplicity."""
+def compare_ca(gpu, orc, event: int = 0, classified: bool = False) -> list[str]:
+    """Doublets, per-hit / per-cell lists, tuples, duplicate flags and multiplicity
+    (the last two only before classification changes the quality flags)."""
     errs = []
     c = gpu.counts(event)
     oc = orc.counts()
@@ -71,6 +72,8 @@ def compare_ca(gpu, orc, event: int = 0) -> list[str]:
         g, o = gpu.product(name, event), orc.get(name)[:nth]
         if not same_bits(g, o):
             errs.append(f"{name}: {first_diff(g, o)}")
+    if classified:
+        return errs
     g, o = gpu.product("quality", event)[:nt], orc.get("quality")[:nt]
     if not same_bits(g, o):
         errs.append(f"quality: {first_diff(g, o)}")
@@ -79,6 +82,59 @@ def compare_ca(gpu, orc, event: int = 0) -> list[str]:
     g = gpu.product("tuple_multiplicity", event)
     if not same_bits(g, tm):
         errs.append(f"tuple_multiplicity: {first_diff(g, tm)}")
+    return errs
+
+
+# FP64 fits on the GPU and on the CPU use the same operation order; only the
+# transcendentals (atan, log, sin, cos, asinh: CUDA vs the C library, each within
+# 2 ulp in FP64) differ, and the results are stored as FP32.
+FIT_RTOL = 1e-5
+FIT_ATOL = {"state": 1e-6, "cov": 1e-12, "pt": 1e-6, "eta": 1e-6, "chi2": 1e-6}
+
+
+def compare_fits(gpu, orc, event: int = 0) -> list[str]:
+    errs = []
+    nt = orc.counts()["n_tuples"]
+    fg, fo = gpu.product("fitted", event)[:nt], orc.get("fitted")[:nt]
+    if not same_bits(fg, fo):
+        errs.append(f"fitted: {first_diff(fg, fo)}")
+        return errs
+    sel = fo.astype(bool)
+    for name, w in (("state", 5), ("cov", 15), ("pt", 1), ("eta", 1), ("chi2", 1)):
+        g = gpu.product(name, event)[:nt * w].reshape(nt, w)[sel]
+        o = orc.get(name)[:nt * w].reshape(nt, w)[sel]
+        bad = ~np.isclose(g, o, rtol=FIT_RTOL, atol=FIT_ATOL[name], equal_nan=True)
+        if bad.any():
+            i = np.argwhere(bad)[0]
+            errs.append(f"{name}: {int(bad.sum())} values off, first {tuple(i)}: {g[tuple(i)]} vs {o[tuple(i)]}")
+    return errs
+
+
+def compare_quality(gpu, orc, event: int = 0) -> list[str]:
+    nt = orc.counts()["n_tuples"]
+    g, o = gpu.product("quality", event)[:nt], orc.get("quality")[:nt]
+    return [] if same_bits(g, o) else [f"quality: {first_diff(g, o)}"]
+
+
+def compare_vertices(gpu, orc, event: int = 0) -> list[str]:
+    errs = []
+    c = gpu.counts(event)
+    oc = orc.counts()
+    if c.n_vertices != oc["nv_final"] or c.n_vertex_tracks != oc["n_vtx_tracks"]:
+        return [f"vertices: gpu {c.n_vertices}/{c.n_vertex_tracks} oracle {oc['nv_final']}/{oc['n_vtx_tracks']}"]
+    nv = oc["nv_final"]
+    for name in ("idv", "sort_ind"):
+        g, o = gpu.product(name, event), orc.get(name)
+        if not same_bits(g, o):
+            errs.append(f"{name}: {first_diff(g, o)}")
+    n = max(nv, oc["n_vtx_tracks"])
+    g, o = gpu.product("ndof", event)[:n], orc.get("ndof")[:n]
+    if not same_bits(g, o):
+        errs.append(f"ndof: {first_diff(g, o)}")
+    for name in ("zv", "wv", "vchi2", "ptv2"):
+        g, o = gpu.product(name, event)[:nv], orc.get(name)[:nv]
+        if not np.allclose(g, o, rtol=1e-5, atol=1e-7):
+            errs.append(f"{name}: {first_diff(g, o)}")
     return errs
 
 

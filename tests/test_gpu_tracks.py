@@ -1,0 +1,107 @@
+"""Parity of the CUDA fits, track classification and vertexing with the CPU oracle.
+Tolerance for FP64 fit outputs stored as FP32: relative 1e-5 (parity.FIT_RTOL)."""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+from parity import compare_ca, compare_fits, compare_quality, compare_vertices
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def chain(conditions):
+    from pixeltrack import PixelChain, default_params
+    c = PixelChain(conditions, default_params())
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module")
+def orc(conditions):
+    return oracle.Oracle(conditions)
+
+
+def _check_event(chain, orc, ev):
+    chain.run_event(ev, 63)
+    orc.run_event(ev, 63)
+    errs = compare_ca(chain, orc, classified=True) + compare_fits(chain, orc) + compare_quality(chain, orc) + \
+        compare_vertices(chain, orc)
+    return errs
+
+
+def test_single_event_full_chain(chain, orc, event_single):
+    blob, offs = event_single
+    errs = _check_event(chain, orc, blob[offs[0]:offs[1]])
+    assert not errs, errs
+    assert chain.counts().n_vertices == 1
+
+
+def test_pu50_full_chain(chain, orc, events_pu50):
+    blob, offs = events_pu50
+    for e in range(len(offs) - 1):
+        errs = _check_event(chain, orc, blob[offs[e]:offs[e + 1]])
+        assert not errs, (e, errs)
+
+
+def test_batch_full_chain(conditions, orc, events_pu50):
+    from pixeltrack import PixelChain, batch_params
+    blob, offs = events_pu50
+    n = len(offs) - 1
+    with PixelChain(conditions, batch_params(n)) as bc:
+        bc.run_batch(blob, offs, stages=63)
+        for e in range(n):
+            orc.run_event(blob[offs[e]:offs[e + 1]], 63)
+            errs = compare_fits(bc, orc, e) + compare_quality(bc, orc, e) + compare_vertices(bc, orc, e)
+            assert not errs, (e, errs)
+
+
+def test_producer_path_matches_batch(conditions, events_pu50):
+    """The five producers called in turn (stage by stage) give the products of one run."""
+    from pixeltrack import framework, producers
+    from pixeltrack.formats import FedRawDataCollection
+    blob, offs = events_pu50
+    ev_bytes = bytes(blob[offs[0]:offs[1]])
+    reg = framework.ProductRegistry()
+    src = producers.Source(reg)
+    path = producers.make_path(reg)
+    es = producers.eventsetup_from_blobs(conditions)
+    event = framework.Event(0, 1, reg)
+    event.emplace(src.raw_put, FedRawDataCollection.from_bytes(ev_bytes))
+    for p in path:
+        p.produce(event, es)
+    vtx = event.get(reg.consumes(producers.ZVertexSoA))
+    orc = oracle.Oracle(conditions)
+    orc.run_event(ev_bytes, 63)
+    assert vtx.nv_final == orc.counts()["nv_final"]
+    assert np.array_equal(vtx.idv, orc.get("idv"))
+    es.get(producers.GPUContext).chain.close()
+
+
+def _fixture_tracks():
+    data = json.loads((GOLDEN / "brokenline_fixtures.json").read_text())
+    hits, ge, offs = [], [], [0]
+    for n in ("3", "4", "5"):
+        fx = data["fits"][n]
+        hits += fx["hits"]
+        ge += fx["ge"]
+        offs.append(offs[-1] + len(fx["hits"]))
+    return data, np.array(hits, np.float64), np.array(ge, np.float32), np.array(offs, np.int32)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_standalone_fit_fixtures(precision):
+    import torch
+    from pixeltrack.fits import bl_fit
+    data, hits, ge, offs = _fixture_tracks()
+    out = bl_fit(torch.as_tensor(hits).cuda(), torch.as_tensor(ge).cuda(), torch.as_tensor(offs).cuda(), data["B"],
+                 precision=precision)
+    tol = 1e-6 if precision == 0 else 2e-4  # outputs are stored as FP32
+    for k, n in enumerate(("3", "4", "5")):
+        ref = data["fits"][n]["oracle"]
+        np.testing.assert_allclose(out["state"][k].cpu().numpy(), ref["state"], rtol=tol, atol=tol)
+        np.testing.assert_allclose(out["pt"][k].item(), ref["pt"], rtol=max(tol, 1e-6))
