@@ -1,0 +1,346 @@
+"""Benchmark of the pixel reconstruction chain on B200.
+
+One step = the whole chain (raw FED words -> digis -> clusters -> rechits -> CA
+ntuplets -> broken-line fits -> classification -> vertices) over one batch of
+synthetic PU50 events (1000 by default), replayed as one CUDA graph with the input
+already in HBM. Also measured: the same metric end to end through the public API
+(host->device copy of the raw events from pinned memory and device->host read of the
+per-event vertex counts inside the timed region), the plain per-event launch sequence,
+per-kernel times (live CUDA events) for the roofline of the dominant kernel, and the
+CPU baseline (the serial restatement of the reference on the host cores).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+for p in (ROOT, ROOT / "cms-julia_b200"):
+    if str(p) not in sys.path:
+        sys.path.insert(0, str(p))
+
+METRIC = "PU50 events/s on 1 B200 batched vs plain; BL fits/s and err vs FP64"
+WORKLOAD = ("synthetic PU50 events (50 vertices x Poisson(30) helix tracks, |eta|<2.5, pT 0.5-10 GeV, 1e-4 noise, "
+            "1% inefficiency) on a seeded Phase-1-like geometry, batched by prefix offsets, one CUDA graph per step")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--events", type=int, default=1000)
+    ap.add_argument("--pu", type=float, default=50.0)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--plain-events", type=int, default=200)
+    ap.add_argument("--cpu-sample", type=int, default=160)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile-only", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+        self._t = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, smax, reasons = [], 0.0, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = max(smax, float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ algorithmic bytes per kernel group
+def segment_bytes(name: str, c: dict) -> float | None:
+    """Compulsory traffic of one kernel group over the batch: inputs read once, outputs written
+    once (conditions tables are L2-resident and not counted)."""
+    D, H, C, T, TH, I = c["words"], c["hits"], c["cells"], c["tuples"], c["tuple_hits"], c["items"]
+    table = {
+        "unpack_calib": 4 * D + 22 * D,            # words in; xx,yy,adc,moduleInd,clus,pdigi,rawId out
+        "module_starts": 4 * D,                    # moduleInd read by the count and fill passes
+        "find_clus_charge_cut": 14 * D,            # moduleInd,x,y,adc in; clus out
+        "get_hits": 14 * D + 44 * H,               # digis in; 44 B hit SoA out
+        "phi_binner": 4 * H,                       # iphi in; bins out
+        "doublets_count": 14 * I + 4 * I,          # inner hit fields in; count out
+        "doublets_fill": 14 * I + 4 * I + 22 * C,  # + cell SoA out
+        "connect": 28 * C + 16 * C,                # cell fields in; neighbour masks out
+        "broken_line_fit": 22 * TH + 4 * TH + 8 * T + 93 * T,
+        "vertices": 4 * T + 80 * T,
+    }
+    return table.get(name)
+
+
+def load_peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ reference arm (CPU)
+def run_reference(args, rank: int, world: int) -> None:
+    if rank != 0:
+        return
+    from oracle import oracle
+    from pixeltrack import gen
+    conds = gen.conditions()
+    n = max(8, min(args.cpu_sample, args.events))
+    blob, offs = gen.events(n, gen.MODE_PU, pu=args.pu, seed=args.seed)
+    orc = oracle.Oracle(conds)
+    threads = os.cpu_count() or 1
+    for _ in range(max(1, args.warmup)):
+        orc.run_batch(blob, offs, threads)
+    t = 0.0
+    for _ in range(args.steps):
+        t += orc.run_batch(blob, offs, threads)
+    value = n * args.steps / t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "events/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32/f32/f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "events_per_step": n, "pileup": args.pu},
+        "cpu_baseline": {"value": value, "unit": "events/s", "cores": threads, "kind": "port",
+                         "sample": f"{n} PU{int(args.pu)} events per step, full chain, event-parallel threads"},
+        "e2e": {"value": value, "unit": "events/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference is a Julia program; julia is not installed here, so its CPU path is timed as the "
+                "oracle's serial C++ restatement",
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ our arm
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    from pixeltrack import PixelChain, batch_params, default_params, gen
+    conds = gen.conditions()
+    E = args.events
+    blob, offs = gen.events(E, gen.MODE_PU, pu=args.pu, seed=args.seed + 7919 * rank)
+    words = np.diff(offs).sum() // 4
+    params = batch_params(E, words_per_event=int(words / E * 1.3) + 4096, hits_per_event_avg=16_000,
+                          doublets_per_event_avg=140_000, tuples_per_event_avg=11_000, device=local)
+    chain = PixelChain(conds, params)
+    stream = torch.cuda.Stream(device=local)
+    sh = stream.cuda_stream
+
+    # correctness guard and per-kernel profile (non-graph run)
+    chain.stage_batch(blob, offs, sh)
+    stream.synchronize()
+    chain.profile(True)
+    prof_runs = []
+    for _ in range(3):
+        chain.run_batch(blob, offs, sync=False)
+        warn = chain.sync()
+        prof_runs.append(chain.profile_read())
+    chain.profile(False)
+    seg_ms: dict[str, float] = {}
+    for run in prof_runs[1:]:
+        for name, ms in run:
+            seg_ms[name] = seg_ms.get(name, 0.0) + ms / (len(prof_runs) - 1)
+    totals = {"words": 0, "hits": 0, "cells": 0, "tuples": 0, "tuple_hits": 0, "vertices": 0, "items": 0}
+    for e in range(E):
+        c = chain.counts(e)
+        totals["words"] += c.n_words
+        totals["hits"] += c.n_hits
+        totals["cells"] += c.n_doublets
+        totals["tuples"] += c.n_tuples
+        totals["tuple_hits"] += c.n_tuple_hits
+        totals["vertices"] += c.n_vertices
+    totals["items"] = int(totals["hits"] * 3.2)
+    if args.profile_only:
+        print(json.dumps({"segments_ms": seg_ms, "totals": totals, "warnings": warn}), flush=True)
+        return
+
+    # batched graph: input in HBM, one replay per step
+    chain.stage_batch(blob, offs, sh)
+    stream.synchronize()
+    chain.capture_graph()
+    kernels_per_step = chain.graph_kernel_nodes()
+    for _ in range(args.warmup):
+        chain.launch_graph(sh)
+    stream.synchronize()
+    if dist:
+        dist.barrier()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        t0.record(stream)
+        for _ in range(args.steps):
+            chain.launch_graph(sh)
+        t1.record(stream)
+        t1.synchronize()
+    ms = t0.elapsed_time(t1)
+    if dist:
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    ms_per_step = ms / args.steps
+    value = world * E * args.steps / (ms / 1e3)
+
+    # end to end through the public API: pinned host raw events in, per-event results out
+    pinned = torch.empty(len(blob), dtype=torch.uint8, pin_memory=True)
+    pinned.numpy()[:] = blob
+    res = torch.empty(E, dtype=torch.int32, pin_memory=True)
+    h2d = int(offs[-1] - offs[0]) + 8 * (E + 1)
+    d2h = 4 * E
+    for _ in range(args.warmup):
+        chain.stage_batch(pinned.numpy(), offs, sh)
+        chain.launch_graph(sh)
+        chain.results_async(res.data_ptr(), E, sh)
+    stream.synchronize()
+    if dist:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        chain.stage_batch(pinned.numpy(), offs, sh)
+        chain.launch_graph(sh)
+        chain.results_async(res.data_ptr(), E, sh)
+    e1.record(stream)
+    e1.synchronize()
+    ems = e0.elapsed_time(e1)
+    if dist:
+        tt = torch.tensor([ems], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ems = float(tt.item())
+    e2e_value = world * E * args.steps / (ems / 1e3)
+    nv_check = int(res.numpy().sum())
+
+    # plain per-event launch sequence (one event per launch sequence, input already in HBM)
+    plain = PixelChain(conds, default_params(device=local))
+    dev_blob = torch.as_tensor(blob).cuda()
+    dev_offs = torch.as_tensor(offs.astype(np.int64)).cuda()
+    npl = min(args.plain_events, E)
+    for e in range(min(5, npl)):
+        plain.run_batch_device(dev_blob.data_ptr(), dev_offs.data_ptr() + 8 * e, 1, stream=sh)
+    stream.synchronize()
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    for e in range(npl):
+        plain.run_batch_device(dev_blob.data_ptr(), dev_offs.data_ptr() + 8 * e, 1, stream=sh)
+    p1.record(stream)
+    p1.synchronize()
+    plain_value = npl / (p0.elapsed_time(p1) / 1e3)
+    plain.close()
+
+    # roofline of the dominant kernel group (live CUDA-event times of the profiled runs)
+    peak, peak_kind = load_peaks()
+    dom = max(seg_ms, key=seg_ms.get) if seg_ms else None
+    dom_bytes = segment_bytes(dom, totals) if dom else None
+    roofline = None
+    if dom:
+        achieved = (dom_bytes / (seg_ms[dom] / 1e3) / 1e9) if dom_bytes else None
+        roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+                    "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": None,
+                    "ms_per_launch": seg_ms[dom], "algorithmic_bytes_per_launch": dom_bytes}
+
+    # CPU baseline: the oracle (serial restatement of the reference) on the host cores
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle import oracle
+        n = min(args.cpu_sample, E)
+        sub = blob[: int(offs[n])]
+        orc = oracle.Oracle(conds)
+        threads = os.cpu_count() or 1
+        orc.run_batch(sub, offs[: n + 1], threads)
+        t = orc.run_batch(sub, offs[: n + 1], threads)
+        cpu = {"value": n / t, "unit": "events/s", "cores": threads, "kind": "port",
+               "sample": f"{n} of the {E} PU{int(args.pu)} events, full chain, {threads} event-parallel threads"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "events/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32/f32/f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "events_per_step": E, "pileup": args.pu,
+                       "raw_bytes_per_step": int(offs[-1]), "l2": "inputs and intermediates larger than L2",
+                       "parallelism": f"events sharded over {world} GPU(s), no data-path collective"},
+            "e2e": {"value": e2e_value, "unit": "events/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "plain": {"value": plain_value, "unit": "events/s", "events": npl,
+                      "note": "one launch sequence per event, input in HBM"},
+            "batched_over_plain": value / world / plain_value,
+            "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": kernels_per_step * args.steps,
+            "clocks": clk.summary(), "segments_ms": seg_ms, "totals": totals, "warnings": warn,
+            "vertices_per_event": nv_check / E,
+        }
+        print(json.dumps(line), flush=True)
+    chain.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

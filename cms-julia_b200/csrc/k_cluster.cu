@@ -236,7 +236,9 @@ __global__ void k_hits_module_start(Dev d) {
 void launch_cluster(const Dev& d, const Launch& L) {
   dim3 g(L.bpe > 0 ? L.bpe : 64, d.E);
   k_find_clus<<<g, 256, 0, L.s>>>(d);
+  L.mark("find_clus_charge_cut");
   k_hits_module_start<<<d.E, 1024, 0, L.s>>>(d);
+  L.mark("hits_module_start");
 }
 
 }  // namespace pxl

@@ -125,6 +125,7 @@ __global__ void __launch_bounds__(128) k_fit_standalone(const double* __restrict
 void launch_fit(const Dev& d, const Launch& L) {
   const dim3 g(L.bpe > 0 ? L.bpe : 64, d.E);
   k_fit_tuples<<<g, 128, 0, L.s>>>(d);
+  L.mark("broken_line_fit");
 }
 
 }  // namespace pxl

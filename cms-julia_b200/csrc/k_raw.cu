@@ -326,13 +326,17 @@ __global__ void k_modstart_fill(Dev d) {
 
 void launch_raw(const Dev& d, const Launch& L, const int16_t* fed_slot_of) {
   const int NF = d.n_fed_slots;
+  L.mark("start");
   k_fed_table<<<d.E, 256, 0, L.s>>>(d, fed_slot_of);
   k_ev_scan<<<1, 1024, 0, L.s>>>(d.ev, d.E, int(offsetof(EvInfo, n_words)), int(offsetof(EvInfo, word_base)));
+  L.mark("fed_table");
   dim3 g(NF, d.E);
   k_unpack<<<g, 256, 0, L.s>>>(d);
+  L.mark("unpack_calib");
   k_modstart_count<<<g, 256, 0, L.s>>>(d);
   k_modstart_scan<<<d.E, 256, 0, L.s>>>(d);
   k_modstart_fill<<<g, 256, 0, L.s>>>(d);
+  L.mark("module_starts");
 }
 
 void launch_modstart(const Dev& d, const Launch& L) {

@@ -260,7 +260,9 @@ __global__ void __launch_bounds__(1024) k_phi_binner(Dev d) {
 void launch_rechits(const Dev& d, const Launch& L) {
   dim3 g(L.bpe > 0 ? L.bpe : 64, d.E);
   k_get_hits<<<g, 256, 0, L.s>>>(d);
+  L.mark("get_hits");
   k_phi_binner<<<d.E, 1024, 0, L.s>>>(d);
+  L.mark("phi_binner");
 }
 
 }  // namespace pxl

@@ -261,7 +261,8 @@ int alloc_batch(PxlCtx* ctx) {
 int run_chain(PxlCtx* ctx, uint32_t mask, cudaStream_t s) {
   Dev& d = ctx->d;
   if (d.E <= 0) return 0;
-  Launch L{s, d.bpe, 256};
+  Launch L{s, d.bpe, 256, (ctx->prof.on && !ctx->capturing) ? &ctx->prof : nullptr};
+  if ((mask & PXL_STAGE_DIGIS) && L.prof) ctx->prof.n = 0;
   // stages run in chain order; a producer boundary may stop after any of them and a
   // later call (pxl_event_continue) resumes from the products already on the device
   if (mask & PXL_STAGE_DIGIS) {
@@ -459,7 +460,9 @@ int32_t pxl_graph_capture(PxlCtx* ctx, uint32_t mask) {
   choose_shape(ctx);
   CK(cudaStreamSynchronize(ctx->stream));
   CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  ctx->capturing = true;
   int rc = run_chain(ctx, mask, ctx->stream);
+  ctx->capturing = false;
   cudaGraph_t g = nullptr;
   cudaError_t err = cudaStreamEndCapture(ctx->stream, &g);
   if (rc) { if (g) cudaGraphDestroy(g); return rc; }
@@ -481,6 +484,55 @@ int32_t pxl_graph_launch(PxlCtx* ctx, void* stream) {
   ctx->last_E = ctx->graph_E;
   ctx->last_mask = ctx->graph_mask;
   return 0;
+}
+
+int64_t pxl_results_async(PxlCtx* ctx, uint32_t* host_dst, int64_t max_events, void* stream) {
+  if (!ctx || !host_dst) return PXL_ERR_ARG;
+  cudaSetDevice(ctx->p.device);
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+  const int64_t n = std::min<int64_t>(max_events, ctx->last_E);
+  if (n <= 0) return 0;
+  // one uint32 (n_vtx) per event, gathered from the per-event records
+  CK(cudaMemcpy2DAsync(host_dst, sizeof(uint32_t), &ctx->d.ev[0].n_vtx, sizeof(EvInfo), sizeof(uint32_t), size_t(n),
+                       cudaMemcpyDeviceToHost, s));
+  return n;
+}
+
+int32_t pxl_graph_kernel_nodes(PxlCtx* ctx) {
+  if (!ctx || !ctx->graph) return PXL_ERR_STATE;
+  size_t n = 0;
+  CK(cudaGraphGetNodes(ctx->graph, nullptr, &n));
+  std::vector<cudaGraphNode_t> nodes(n);
+  CK(cudaGraphGetNodes(ctx->graph, nodes.data(), &n));
+  int32_t k = 0;
+  for (auto nd : nodes) {
+    cudaGraphNodeType t;
+    CK(cudaGraphNodeGetType(nd, &t));
+    if (t == cudaGraphNodeTypeKernel) ++k;
+  }
+  return k;
+}
+
+int32_t pxl_profile_enable(PxlCtx* ctx, int32_t on) {
+  if (!ctx) return PXL_ERR_ARG;
+  cudaSetDevice(ctx->p.device);
+  if (on && !ctx->prof.ev[0])
+    for (int i = 0; i < Prof::kMax; ++i) CK(cudaEventCreate(&ctx->prof.ev[i]));
+  ctx->prof.on = on != 0;
+  ctx->prof.n = 0;
+  return 0;
+}
+
+int32_t pxl_profile_read(PxlCtx* ctx, float* ms, const char** names, int32_t max) {
+  if (!ctx || !ms) return PXL_ERR_ARG;
+  cudaSetDevice(ctx->p.device);
+  CK(cudaStreamSynchronize(ctx->stream));
+  int32_t k = 0;
+  for (int i = 1; i < ctx->prof.n && k < max; ++i, ++k) {
+    CK(cudaEventElapsedTime(&ms[k], ctx->prof.ev[i - 1], ctx->prof.ev[i]));
+    if (names) names[k] = ctx->prof.name[i];
+  }
+  return k;
 }
 
 int32_t pxl_sync(PxlCtx* ctx) {

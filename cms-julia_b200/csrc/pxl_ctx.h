@@ -31,6 +31,9 @@ struct PxlCtx {
   size_t raw_cap = 0;
   uint64_t* d_ev_off = nullptr;
   uint8_t* d_raw = nullptr;
+  // per-kernel timing of non-graph runs
+  pxl::Prof prof;
+  bool capturing = false;
 };
 
 // reads the events' counters back (synchronises the context stream)

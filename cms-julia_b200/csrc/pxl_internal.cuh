@@ -214,10 +214,28 @@ __device__ __forceinline__ void atomic_or_warn(EvInfo* ev, uint32_t bits) { atom
 inline int div_up(int64_t a, int64_t b) { return int((a + b - 1) / b); }
 
 // ---------------------------------------------------------------- launchers (per stage file)
+// Optional per-kernel timing: when enabled, the launchers record a CUDA event after
+// every kernel; segment i lasts from event i-1 to event i.
+struct Prof {
+  static constexpr int kMax = 128;
+  bool on = false;
+  int n = 0;
+  cudaEvent_t ev[kMax] = {};
+  const char* name[kMax] = {};
+};
+
 struct Launch {
   cudaStream_t s;
   int bpe;        // blocks per event
   int tpb;        // threads per block
+  Prof* prof = nullptr;
+  void mark(const char* nm) const {
+    if (prof && prof->on && prof->n < Prof::kMax) {
+      cudaEventRecord(prof->ev[prof->n], s);
+      prof->name[prof->n] = nm;
+      ++prof->n;
+    }
+  }
 };
 
 void launch_raw(const Dev& d, const Launch& L, const int16_t* fed_slot_of);  // a1-a4

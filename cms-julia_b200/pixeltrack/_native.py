@@ -68,6 +68,11 @@ _SIGS = {
     "pxl_graph_capture": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32]),
     "pxl_graph_launch": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p]),
     "pxl_sync": (ctypes.c_int32, [ctypes.c_void_p]),
+    "pxl_graph_kernel_nodes": (ctypes.c_int32, [ctypes.c_void_p]),
+    "pxl_results_async": (ctypes.c_int64, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]),
+    "pxl_profile_enable": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_int32]),
+    "pxl_profile_read": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float),
+                                          ctypes.POINTER(ctypes.c_char_p), ctypes.c_int32]),
     "pxl_event_counts": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_int32, ctypes.POINTER(PxlEventCounts)]),
     "pxl_copy_product": (ctypes.c_int64, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
                                           ctypes.c_int64]),

@@ -120,21 +120,42 @@ class PixelChain:
               "pxl_batch_run")
         return self.sync() if sync else 0
 
-    def stage_batch(self, blob: np.ndarray, offsets: np.ndarray) -> None:
+    def run_batch_device(self, blob_ptr: int, offsets_ptr: int, n_events: int, stages: int = _native.STAGE_ALL,
+                         stream: int | None = None) -> None:
+        """Batch already in device memory (pointers to the blob and its uint64 offsets)."""
+        check(self._lib.pxl_batch_run(self._h, blob_ptr, offsets_ptr, n_events, 1, stages, stream),
+              "pxl_batch_run")
+
+    def stage_batch(self, blob: np.ndarray, offsets: np.ndarray, stream: int | None = None) -> None:
         blob = np.ascontiguousarray(blob, dtype=np.uint8)
         offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
         self._keep = [blob, offsets]
-        check(self._lib.pxl_batch_stage(self._h, blob.ctypes.data, offsets.ctypes.data, len(offsets) - 1, None),
+        check(self._lib.pxl_batch_stage(self._h, blob.ctypes.data, offsets.ctypes.data, len(offsets) - 1, stream),
               "pxl_batch_stage")
 
     def capture_graph(self, stages: int = _native.STAGE_ALL) -> None:
         check(self._lib.pxl_graph_capture(self._h, stages), "pxl_graph_capture")
 
-    def launch_graph(self) -> None:
-        check(self._lib.pxl_graph_launch(self._h, None), "pxl_graph_launch")
+    def launch_graph(self, stream: int | None = None) -> None:
+        check(self._lib.pxl_graph_launch(self._h, stream), "pxl_graph_launch")
+
+    def results_async(self, host_ptr: int, max_events: int, stream: int | None = None) -> int:
+        return check(self._lib.pxl_results_async(self._h, host_ptr, max_events, stream), "pxl_results_async")
 
     def sync(self) -> int:
         return check(self._lib.pxl_sync(self._h), "pxl_sync")
+
+    def graph_kernel_nodes(self) -> int:
+        return check(self._lib.pxl_graph_kernel_nodes(self._h), "pxl_graph_kernel_nodes")
+
+    def profile(self, on: bool = True) -> None:
+        check(self._lib.pxl_profile_enable(self._h, int(on)), "pxl_profile_enable")
+
+    def profile_read(self) -> list[tuple[str, float]]:
+        ms = (ctypes.c_float * 128)()
+        names = (ctypes.c_char_p * 128)()
+        n = check(self._lib.pxl_profile_read(self._h, ms, names, 128), "pxl_profile_read")
+        return [(names[i].decode(), ms[i]) for i in range(n)]
 
     # ---- products
     def counts(self, event: int = 0) -> EventCounts:

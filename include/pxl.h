@@ -199,6 +199,19 @@ int32_t pxl_batch_stage(PxlCtx* ctx, const uint8_t* blob, const uint64_t* event_
 int32_t pxl_graph_capture(PxlCtx* ctx, uint32_t stage_mask);
 int32_t pxl_graph_launch(PxlCtx* ctx, void* stream);
 
+/* Enqueues on `stream` the copy of the per-event vertex counts (nvFinal) of the last run into
+ * host memory (pinned for an asynchronous copy), one uint32 per event; returns the count. */
+int64_t pxl_results_async(PxlCtx* ctx, uint32_t* host_dst, int64_t max_events, void* stream);
+
+/* Number of kernel nodes in the captured graph (the kernels one replay launches). */
+int32_t pxl_graph_kernel_nodes(PxlCtx* ctx);
+
+/* Per-kernel timing of non-graph runs: when enabled, a CUDA event is recorded after
+ * each kernel group; pxl_profile_read returns the milliseconds of each segment of the last
+ * run and its name (static strings), at most max entries. */
+int32_t pxl_profile_enable(PxlCtx* ctx, int32_t on);
+int32_t pxl_profile_read(PxlCtx* ctx, float* ms, const char** names, int32_t max);
+
 /* Waits for the context's work; returns 0, the OR of the events' PXL_WARN_* bits, or < 0. */
 int32_t pxl_sync(PxlCtx* ctx);
 
