@@ -29,6 +29,7 @@ CUDA_SOURCES = [
     "k_fit.cu",
     "k_select.cu",
     "k_products.cu",
+    "noalloc.cu",
     "pipeline.cu",
 ]
 

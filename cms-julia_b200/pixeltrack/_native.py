@@ -78,6 +78,8 @@ _SIGS = {
                                           ctypes.c_int64]),
     "pxl_clusterize_digis": (ctypes.c_int32, [ctypes.c_void_p] + [ctypes.c_void_p] * 4 + [ctypes.c_int32,
                              ctypes.c_int32] + [ctypes.c_void_p] * 5),
+    "pxl_clusterize_digis_noalloc": (ctypes.c_int32, [ctypes.c_void_p] * 4 + [ctypes.c_int32, ctypes.c_int32]
+                                     + [ctypes.c_void_p] * 6),
     "pxl_bl_fit": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
                                     ctypes.c_double, ctypes.c_int32] + [ctypes.c_void_p] * 6 + [ctypes.c_void_p]),
 }

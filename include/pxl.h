@@ -230,6 +230,22 @@ int32_t pxl_clusterize_digis(PxlCtx* ctx, const uint16_t* id, const int16_t* x, 
                              int32_t n, int32_t apply_charge_cut, uint32_t* module_start, uint32_t* clus_in_module,
                              uint32_t* module_id, int32_t* clus, uint16_t* id_out);
 
+/* Same clustering as pxl_clusterize_digis, on DEVICE arrays, for callers that cannot
+ * allocate device memory (an event loop whose device memory belongs to another allocator,
+ * or a path that must not block on cudaMalloc/cudaFree). It allocates nothing: inputs
+ * (id, x, y, adc; n digis) and outputs (module_start[2001], clus_in_module[2000],
+ * module_id[2000], clus[n], id_out[n]) are the caller's device buffers, and the scratch
+ * is a fixed file-scope device array of the library (about 52 KB on every GPU that loads
+ * it, held until exit). At most 1,048,576 digis per call; larger n returns
+ * PXL_ERR_CAPACITY. The first call on a device looks the array up on that device, so make
+ * it before any stream capture. Calls share the array: calls that overlap on the GPU race.
+ * Enqueued on `stream` (a cudaStream_t or NULL); the caller synchronises.
+ * No counterpart in the reference: it adds an allocation-free form of the clustering. */
+int32_t pxl_clusterize_digis_noalloc(const uint16_t* id, const int16_t* x, const int16_t* y, const int32_t* adc,
+                                     int32_t n, int32_t apply_charge_cut, uint32_t* module_start,
+                                     uint32_t* clus_in_module, uint32_t* module_id, int32_t* clus, uint16_t* id_out,
+                                     void* stream);
+
 /* Standalone broken-line fits of n_tracks tracks (broken_line.jl:275-696, driven as
  * broken_line_fit_on_gpu.jl:24-163 does). Device pointers: hits[3*H] (x,y,z per hit,
  * float64), hits_ge[6*H] (global covariance per hit, float32), hit_offsets[n_tracks+1]
