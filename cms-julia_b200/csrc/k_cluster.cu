@@ -5,11 +5,21 @@
 //
 // find_clus labels 8-connected pixel components by iterated min-propagation,
 // which makes every pixel's root the smallest digi index of its component and
-// numbers clusters by ascending root. Here each module is one CTA: pixels are
-// binned by column in shared memory, components are merged with a lock-free
-// union-find that always hooks the larger root under the smaller one (so the
-// final root is again the smallest index), and roots are numbered with a
-// block scan in index order: the same cluster ids as the reference.
+// numbers clusters by ascending root. Here components are merged with a
+// lock-free union-find that always hooks the larger root under the smaller one
+// (so the final root is again the smallest index), and roots are numbered by a
+// scan in index order: the same cluster ids as the reference.
+//
+// Two paths share that scheme:
+//  * one warp per module for modules of at most kWarpPix digis (nearly all of
+//    them: a PU50 module holds about 22). The warp keeps its digis in
+//    registers, finds neighbour pairs by broadcasting every digi of the module
+//    through shuffles, and scans with ballots; it never waits on a CTA barrier.
+//  * one CTA per module for larger modules, which the warp path appends to a
+//    device work list: pixels are binned by column in shared memory and only
+//    the same and the next column are searched.
+#include <algorithm>
+
 #include "pxl_internal.cuh"
 
 namespace pxl {
@@ -18,6 +28,9 @@ namespace {
 
 constexpr int kNPix = 4096;  // >= 4001, the largest range find_clus processes
 constexpr int kNBins = 418;
+constexpr int kWarpPix = kWarpModulePix;  // digis per module handled by one warp
+constexpr int kWarpSlots = kWarpPix / 32;
+constexpr int kWarpsPerBlock = 8;
 
 __device__ __forceinline__ int cc_find(volatile int32_t* lab, int x) {
   int p = lab[x];
@@ -38,165 +51,333 @@ __device__ __forceinline__ void cc_union(int32_t* lab, int a, int b) {
   }
 }
 
-__global__ void __launch_bounds__(256) k_find_clus(Dev d) {
-  const int e = blockIdx.y;
-  __shared__ int16_t s_x[kNPix];
-  __shared__ int16_t s_y[kNPix];
-  __shared__ int32_t s_lab[kNPix];
-  __shared__ uint16_t s_sorted[kNPix];
-  __shared__ uint32_t s_start[kNBins + 2];
-  __shared__ uint32_t s_cur[kNBins + 2];
-  __shared__ uint32_t sh[33];
-  __shared__ int32_t s_crun;
-  __shared__ uint32_t s_warn;
-  int32_t* s_charge = reinterpret_cast<int32_t*>(s_x);   // after labelling: [1024]
-  uint16_t* s_newc = reinterpret_cast<uint16_t*>(s_y);   // after labelling: [1024]
+// The digi range find_clus assigns to module position m of event e, with the
+// reference's msize arithmetic (1-based exclusive end + 1, truncation to
+// kMaxPixInModule, +1 for the last module). Returns false for a malformed list.
+struct ModRange {
+  uint64_t g0;      // first digi (global index)
+  int n;            // digis in the range
+  int16_t this_id;  // module id of the first digi
+  bool truncated;
+};
 
+__device__ __forceinline__ bool module_range(const Dev& d, int e, uint32_t m, ModRange& r) {
+  const EvInfo& E = d.ev[e];
+  const uint32_t nmod = E.n_modules, n_el = E.n_words;
+  const uint64_t eb = E.word_base;
+  const uint32_t* ms = d.module_start + size_t(e) * (kMaxNumModules + 1);
+  const uint32_t first1 = ms[m + 1];  // 1-based
+  uint32_t msize = (m + 1 < nmod) ? ms[m + 2] : n_el;
+  if (first1 < 1 || first1 > n_el || msize < first1 || msize > n_el) return false;
+  r.this_id = d.mid[eb + first1 - 1];
+  r.truncated = false;
+  if (msize - first1 > uint32_t(kMaxPixInModule)) {
+    msize = uint32_t(kMaxPixInModule) + first1;
+    r.truncated = true;
+  }
+  if (msize == n_el && d.mid[eb + msize - 1] == r.this_id) msize += 1;
+  r.n = int(msize - first1);  // range [first1-1, first1-1+n)
+  r.g0 = eb + first1 - 1;
+  return true;
+}
+
+__device__ __forceinline__ void write_module_record(const Dev& d, int e, uint32_t m, int16_t this_id, uint32_t nclus,
+                                                    uint32_t warn) {
+  d.module_id[size_t(e) * kMaxNumModules + m] = uint32_t(uint16_t(this_id));
+  if (uint16_t(this_id) < uint16_t(kMaxNumModules))
+    d.clus_in_module[size_t(e) * kMaxNumModules + uint16_t(this_id)] = nclus;
+  if (warn) atomic_or_warn(&d.ev[e], warn);
+}
+
+// ------------------------------------------------------------ warp per module
+struct WarpSmem {
+  int32_t lab[kWarpPix];
+  int32_t charge[kWarpPix];
+  uint16_t cid[kWarpPix];   // cluster number (1-based) of each root
+  uint16_t newc[kWarpPix];  // cluster number after the charge cut
+};
+
+__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_find_clus_warp(Dev d) {
+  __shared__ WarpSmem smem[kWarpsPerBlock];
+  const int e = blockIdx.y;
+  const unsigned lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  WarpSmem& S = smem[wib];
   const EvInfo& E = d.ev[e];
   const uint32_t nmod = E.n_modules;
-  const uint32_t n_el = E.n_words;
-  const uint64_t eb = E.word_base;
-  if (eb + n_el > uint64_t(d.cap_words)) return;
-  const uint32_t* ms = d.module_start + size_t(e) * (kMaxNumModules + 1);
-
-  for (uint32_t m = blockIdx.x; m < nmod; m += gridDim.x) {
-    const uint32_t first1 = ms[m + 1];  // 1-based
-    const int16_t this_id = d.mid[eb + first1 - 1];
-    // msize as the reference derives it (1-based, exclusive end + 1)
-    uint32_t msize = (m + 1 < nmod) ? ms[m + 2] : n_el;
-    if (first1 < 1 || first1 > n_el || msize < first1 || msize > n_el) continue;  // malformed module list
-    if (threadIdx.x == 0) { s_warn = 0; s_crun = 0x7fffffff; }
-    if (msize - first1 > uint32_t(kMaxPixInModule)) {
-      msize = uint32_t(kMaxPixInModule) + first1;
-      if (threadIdx.x == 0) s_warn |= kWarnPixels;
+  if (E.word_base + uint64_t(E.n_words) > uint64_t(d.cap_words)) return;
+  for (uint32_t m = blockIdx.x * kWarpsPerBlock + wib; m < nmod; m += gridDim.x * kWarpsPerBlock) {
+    ModRange r;
+    if (!module_range(d, e, m, r)) continue;
+    const int n = r.n;
+    if (n > kWarpPix) {
+      if (lane == 0) {
+        const uint32_t slot = atomicAdd(&d.big_list[0], 1u);
+        if (slot < uint32_t(d.cap_big)) d.big_list[2 + slot] = (uint32_t(e) << 11) | m;
+      }
+      continue;
     }
-    if (msize == n_el && d.mid[eb + msize - 1] == this_id) msize += 1;
-    const int n = int(msize - first1);  // range [first1-1, first1-1+n)
-    const uint64_t g0 = eb + first1 - 1;
-    for (int b = threadIdx.x; b < kNBins + 2; b += blockDim.x) s_start[b] = 0;
-    __syncthreads();
-    // load and count by column (bin = (y & 511) + 1)
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-      const int16_t id = d.mid[g0 + k];
-      const int16_t x = d.xx[g0 + k], y = d.yy[g0 + k];
-      // a column past the 418-bin histogram makes the reference's histogram assert fail;
-      // such a digi is flagged and kept out of the clustering
-      const bool in_hist = (uint32_t(uint16_t(y)) & 511u) + 2u <= uint32_t(kNBins);
-      if (id != int16_t(kInvId) && !in_hist) atomicOr(&s_warn, kWarnPixels);
-      const bool valid = id != int16_t(kInvId) && in_hist;
-      s_x[k] = x; s_y[k] = y;
-      s_lab[k] = valid ? k : -1;
-      if (valid) atomicAdd(&s_start[(uint32_t(uint16_t(y)) & 511u) + 1u], 1u);
-      else atomicMin(&s_crun, k);
-    }
-    __syncthreads();
-    // exclusive scan of the bin counts (420 entries, two per thread)
-    {
-      uint32_t a = 0, b2 = 0;
-      int i0 = 2 * threadIdx.x;
-      if (i0 < kNBins + 2) a = s_start[i0];
-      if (i0 + 1 < kNBins + 2) b2 = s_start[i0 + 1];
-      uint32_t tot;
-      uint32_t ex = block_excl_scan(a + b2, sh, &tot);
-      if (i0 < kNBins + 2) { s_start[i0] = ex; s_cur[i0] = ex; }
-      if (i0 + 1 < kNBins + 2) { s_start[i0 + 1] = ex + a; s_cur[i0 + 1] = ex + a; }
-    }
-    __syncthreads();
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-      if (s_lab[k] < 0) continue;
-      uint32_t bn = (uint32_t(uint16_t(s_y[k])) & 511u) + 1u;
-      uint32_t pos = atomicAdd(&s_cur[bn], 1u);
-      s_sorted[pos] = uint16_t(k);
-    }
-    __syncthreads();
-    // neighbours: same column (later index) and next column, |dx| <= 1
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-      if (s_lab[k] < 0) continue;
-      const int16_t xk = s_x[k], yk = s_y[k];
-      const uint32_t bn = (uint32_t(uint16_t(yk)) & 511u) + 1u;
-      const uint32_t p1 = s_start[bn + 2 <= kNBins + 1 ? bn + 2 : kNBins + 1];
-      for (uint32_t p = s_start[bn]; p < p1; ++p) {
-        const int mm = s_sorted[p];
-        if (mm == k) continue;
-        const int16_t ym = s_y[mm];
-        if (ym == yk && mm < k) continue;  // each same-column pair once
-        const int dx = int(s_x[mm]) - int(xk);
-        if (dx > 1 || dx < -1) continue;
-        cc_union(s_lab, k, mm);
+    // load: each lane keeps digis k = lane + 32 j in registers
+    uint32_t xy[kWarpSlots];  // x (16 bits) | column bin << 16; 0xffffffff when not clustered
+    int32_t q[kWarpSlots];
+    uint32_t warn = 0;
+    int crun = n;
+#pragma unroll
+    for (int j = 0; j < kWarpSlots; ++j) {
+      const int k = int(lane) + 32 * j;
+      xy[j] = 0xffffffffu;
+      q[j] = 0;
+      if (k < n) {
+        const uint64_t g = r.g0 + k;
+        const int16_t id = d.mid[g];
+        const int16_t x = d.xx[g], y = d.yy[g];
+        q[j] = d.adc[g];
+        const uint32_t yb = uint32_t(uint16_t(y)) & 511u;
+        // a column past the 418-bin histogram makes the reference's histogram assert
+        // fail; such a digi is flagged and kept out of the clustering
+        const bool in_hist = yb + 2u <= uint32_t(kNBins);
+        if (id != int16_t(kInvId) && !in_hist) warn |= kWarnPixels;
+        const bool valid = id != int16_t(kInvId) && in_hist;
+        if (valid) xy[j] = uint32_t(uint16_t(x)) | (yb << 16);
+        else crun = crun < k ? crun : k;
+        S.lab[k] = valid ? k : -1;
       }
     }
-    __syncthreads();
-    for (int k = threadIdx.x; k < n; k += blockDim.x)
-      if (s_lab[k] >= 0) s_lab[k] = cc_find(s_lab, k);
-    __syncthreads();
-    // number roots in index order
-    uint32_t carry = 0;
-    for (int b = 0; b < n; b += blockDim.x) {
-      int k = b + threadIdx.x;
-      bool root = k < n && s_lab[k] == k;
-      uint32_t tot;
-      uint32_t ex = block_excl_scan(root ? 1u : 0u, sh, &tot);
-      if (root) s_sorted[k] = uint16_t(carry + ex + 1);
-      carry += tot;
-    }
-    __syncthreads();
-    const uint32_t nclus = carry;
-    const int crun = s_crun < n ? s_crun : n;  // charge sums stop at the first invalid digi
-    // cluster_charge_cut
-    uint32_t nclus_eff = nclus;
-    if (nclus > uint32_t(kMaxClustersPerModule)) {
-      nclus_eff = kMaxClustersPerModule;
-      if (threadIdx.x == 0) s_warn |= kWarnClusters;
-    }
-    for (int c = threadIdx.x; c < kMaxClustersPerModule; c += blockDim.x) s_charge[c] = 0;
-    __syncthreads();
-    if (nclus > 0) {
-      for (int k = threadIdx.x; k < crun; k += blockDim.x) {
-        uint32_t cl = s_sorted[s_lab[k]];
-        if (cl <= nclus_eff) atomicAdd(&s_charge[cl - 1], d.adc[g0 + k]);
+    crun = int(__reduce_min_sync(0xffffffffu, uint32_t(crun)));
+    warn = __reduce_or_sync(0xffffffffu, warn);
+    __syncwarp();
+    // neighbour pairs (|dx| <= 1, |dcolumn| <= 1), each pair once from its smaller index
+    for (int base = 0; base < n; base += 32) {
+      uint32_t v = 0xffffffffu;
+#pragma unroll
+      for (int j = 0; j < kWarpSlots; ++j)
+        if (j == (base >> 5)) v = xy[j];
+      const int tmax = n - base < 32 ? n - base : 32;
+      for (int t = 0; t < tmax; ++t) {
+        const uint32_t vm = __shfl_sync(0xffffffffu, v, t);
+        if (vm == 0xffffffffu) continue;
+        const int mm = base + t;
+        const int xm = int(int16_t(vm & 0xffffu)), ym = int(vm >> 16);
+#pragma unroll
+        for (int j = 0; j < kWarpSlots; ++j) {
+          const int k = int(lane) + 32 * j;
+          if (32 * j >= n) break;
+          if (k >= mm || xy[j] == 0xffffffffu) continue;
+          const int dx = int(int16_t(xy[j] & 0xffffu)) - xm;
+          const int dy = int(xy[j] >> 16) - ym;
+          if (dx <= 1 && dx >= -1 && dy <= 1 && dy >= -1) cc_union(S.lab, k, mm);
+        }
       }
     }
-    __syncthreads();
-    const int32_t cut = this_id < 96 ? 2000 : 4000;
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < kWarpSlots; ++j) {
+      const int k = int(lane) + 32 * j;
+      if (k < n && xy[j] != 0xffffffffu) S.lab[k] = cc_find(S.lab, k);
+    }
+    __syncwarp();
+    // number the roots in index order
+    uint32_t nclus = 0;
+    for (int base = 0; base < n; base += 32) {
+      const int k = base + int(lane);
+      const bool root = k < n && S.lab[k] == k;
+      const unsigned b = __ballot_sync(0xffffffffu, root);
+      if (root) S.cid[k] = uint16_t(nclus + __popc(b & lt) + 1);
+      nclus += __popc(b);
+    }
+    for (uint32_t c = lane; c < nclus; c += 32) S.charge[c] = 0;
+    __syncwarp();
+    // cluster_charge_cut: charge sums stop at the first invalid digi
+#pragma unroll
+    for (int j = 0; j < kWarpSlots; ++j) {
+      const int k = int(lane) + 32 * j;
+      if (k < crun) atomicAdd(&S.charge[S.cid[S.lab[k]] - 1], q[j]);
+    }
+    __syncwarp();
+    const int32_t cut = r.this_id < 96 ? 2000 : 4000;
     uint32_t last_new = 0;
-    {
-      uint32_t c2 = 0;
-      for (int b = 0; b < int(nclus_eff); b += blockDim.x) {
-        int c = b + threadIdx.x;
-        uint32_t ok = (c < int(nclus_eff) && s_charge[c] > cut) ? 1u : 0u;
-        uint32_t tot;
-        uint32_t ex = block_excl_scan(ok, sh, &tot);
-        if (c < int(nclus_eff)) s_newc[c] = ok ? uint16_t(c2 + ex + 1) : uint16_t(kInvId);
-        c2 += tot;
-      }
-      last_new = c2;
+    for (uint32_t base = 0; base < nclus; base += 32) {
+      const uint32_t c = base + lane;
+      const bool ok = c < nclus && S.charge[c] > cut;
+      const unsigned b = __ballot_sync(0xffffffffu, ok);
+      if (c < nclus) S.newc[c] = ok ? uint16_t(last_new + __popc(b & lt) + 1) : uint16_t(kInvId);
+      last_new += __popc(b);
     }
-    __syncthreads();
-    const bool changed = d.apply_charge_cut && nclus_eff > 0 && last_new != nclus_eff;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-      const uint64_t g = g0 + k;
-      if (s_lab[k] < 0) { d.clus[g] = -9999; continue; }
-      uint32_t cl = s_sorted[s_lab[k]];
-      if (d.apply_charge_cut && nclus > uint32_t(kMaxClustersPerModule) && k < crun && cl > uint32_t(kMaxClustersPerModule)) {
-        d.clus[g] = int32_t(kInvId);
-        d.mid[g] = int16_t(kInvId);
-        continue;
-      }
-      if (changed && cl <= nclus_eff) {
-        uint16_t nc = s_newc[cl - 1];
+    __syncwarp();
+    const bool changed = d.apply_charge_cut && nclus > 0 && last_new != nclus;
+#pragma unroll
+    for (int j = 0; j < kWarpSlots; ++j) {
+      const int k = int(lane) + 32 * j;
+      if (k >= n) continue;
+      const uint64_t g = r.g0 + k;
+      if (xy[j] == 0xffffffffu) { d.clus[g] = -9999; continue; }
+      const uint32_t cl = S.cid[S.lab[k]];
+      if (changed) {
+        const uint16_t nc = S.newc[cl - 1];
         d.clus[g] = int32_t(nc);
         if (nc == kInvId) d.mid[g] = int16_t(kInvId);
       } else {
         d.clus[g] = int32_t(cl);
       }
     }
-    if (threadIdx.x == 0) {
-      d.module_id[size_t(e) * kMaxNumModules + m] = uint32_t(uint16_t(this_id));
-      if (uint16_t(this_id) < uint16_t(kMaxNumModules))
-        d.clus_in_module[size_t(e) * kMaxNumModules + uint16_t(this_id)] = changed ? last_new : nclus;
-      if (s_warn) atomic_or_warn(&d.ev[e], s_warn);
+    if (lane == 0) write_module_record(d, e, m, r.this_id, changed ? last_new : nclus, warn);
+    __syncwarp();
+  }
+}
+
+// ------------------------------------------------------------ CTA per module
+struct BlockSmem {
+  int16_t x[kNPix];
+  int16_t y[kNPix];
+  int32_t lab[kNPix];
+  uint16_t sorted[kNPix];
+  uint32_t start[kNBins + 2];
+  uint32_t cur[kNBins + 2];
+  uint32_t sh[33];
+  int32_t crun;
+  uint32_t warn;
+};
+
+__device__ void cluster_module_block(const Dev& d, int e, uint32_t m, BlockSmem& S) {
+  int32_t* s_charge = reinterpret_cast<int32_t*>(S.x);  // after labelling: [1024]
+  uint16_t* s_newc = reinterpret_cast<uint16_t*>(S.y);  // after labelling: [1024]
+  ModRange r;
+  if (!module_range(d, e, m, r)) return;
+  const int n = r.n;
+  const uint64_t g0 = r.g0;
+  const int16_t this_id = r.this_id;
+  if (threadIdx.x == 0) { S.warn = r.truncated ? kWarnPixels : 0u; S.crun = 0x7fffffff; }
+  for (int b = threadIdx.x; b < kNBins + 2; b += blockDim.x) S.start[b] = 0;
+  __syncthreads();
+  // load and count by column (bin = (y & 511) + 1)
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    const int16_t id = d.mid[g0 + k];
+    const int16_t x = d.xx[g0 + k], y = d.yy[g0 + k];
+    const bool in_hist = (uint32_t(uint16_t(y)) & 511u) + 2u <= uint32_t(kNBins);
+    if (id != int16_t(kInvId) && !in_hist) atomicOr(&S.warn, kWarnPixels);
+    const bool valid = id != int16_t(kInvId) && in_hist;
+    S.x[k] = x; S.y[k] = y;
+    S.lab[k] = valid ? k : -1;
+    if (valid) atomicAdd(&S.start[(uint32_t(uint16_t(y)) & 511u) + 1u], 1u);
+    else atomicMin(&S.crun, k);
+  }
+  __syncthreads();
+  // exclusive scan of the bin counts (420 entries, two per thread)
+  {
+    uint32_t a = 0, b2 = 0;
+    int i0 = 2 * threadIdx.x;
+    if (i0 < kNBins + 2) a = S.start[i0];
+    if (i0 + 1 < kNBins + 2) b2 = S.start[i0 + 1];
+    uint32_t tot;
+    uint32_t ex = block_excl_scan(a + b2, S.sh, &tot);
+    if (i0 < kNBins + 2) { S.start[i0] = ex; S.cur[i0] = ex; }
+    if (i0 + 1 < kNBins + 2) { S.start[i0 + 1] = ex + a; S.cur[i0 + 1] = ex + a; }
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    if (S.lab[k] < 0) continue;
+    uint32_t bn = (uint32_t(uint16_t(S.y[k])) & 511u) + 1u;
+    uint32_t pos = atomicAdd(&S.cur[bn], 1u);
+    S.sorted[pos] = uint16_t(k);
+  }
+  __syncthreads();
+  // neighbours: same column (later index) and next column, |dx| <= 1
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    if (S.lab[k] < 0) continue;
+    const int16_t xk = S.x[k], yk = S.y[k];
+    const uint32_t bn = (uint32_t(uint16_t(yk)) & 511u) + 1u;
+    const uint32_t p1 = S.start[bn + 2 <= kNBins + 1 ? bn + 2 : kNBins + 1];
+    for (uint32_t p = S.start[bn]; p < p1; ++p) {
+      const int mm = S.sorted[p];
+      if (mm == k) continue;
+      const int16_t ym = S.y[mm];
+      if (ym == yk && mm < k) continue;  // each same-column pair once
+      const int dx = int(S.x[mm]) - int(xk);
+      if (dx > 1 || dx < -1) continue;
+      cc_union(S.lab, k, mm);
     }
-    __syncthreads();
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < n; k += blockDim.x)
+    if (S.lab[k] >= 0) S.lab[k] = cc_find(S.lab, k);
+  __syncthreads();
+  // number roots in index order
+  uint32_t carry = 0;
+  for (int b = 0; b < n; b += blockDim.x) {
+    int k = b + threadIdx.x;
+    bool root = k < n && S.lab[k] == k;
+    uint32_t tot;
+    uint32_t ex = block_excl_scan(root ? 1u : 0u, S.sh, &tot);
+    if (root) S.sorted[k] = uint16_t(carry + ex + 1);
+    carry += tot;
+  }
+  __syncthreads();
+  const uint32_t nclus = carry;
+  const int crun = S.crun < n ? S.crun : n;  // charge sums stop at the first invalid digi
+  // cluster_charge_cut
+  uint32_t nclus_eff = nclus;
+  if (nclus > uint32_t(kMaxClustersPerModule)) {
+    nclus_eff = kMaxClustersPerModule;
+    if (threadIdx.x == 0) S.warn |= kWarnClusters;
+  }
+  for (int c = threadIdx.x; c < kMaxClustersPerModule; c += blockDim.x) s_charge[c] = 0;
+  __syncthreads();
+  if (nclus > 0) {
+    for (int k = threadIdx.x; k < crun; k += blockDim.x) {
+      uint32_t cl = S.sorted[S.lab[k]];
+      if (cl <= nclus_eff) atomicAdd(&s_charge[cl - 1], d.adc[g0 + k]);
+    }
+  }
+  __syncthreads();
+  const int32_t cut = this_id < 96 ? 2000 : 4000;
+  uint32_t last_new = 0;
+  {
+    uint32_t c2 = 0;
+    for (int b = 0; b < int(nclus_eff); b += blockDim.x) {
+      int c = b + threadIdx.x;
+      uint32_t ok = (c < int(nclus_eff) && s_charge[c] > cut) ? 1u : 0u;
+      uint32_t tot;
+      uint32_t ex = block_excl_scan(ok, S.sh, &tot);
+      if (c < int(nclus_eff)) s_newc[c] = ok ? uint16_t(c2 + ex + 1) : uint16_t(kInvId);
+      c2 += tot;
+    }
+    last_new = c2;
+  }
+  __syncthreads();
+  const bool changed = d.apply_charge_cut && nclus_eff > 0 && last_new != nclus_eff;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    const uint64_t g = g0 + k;
+    if (S.lab[k] < 0) { d.clus[g] = -9999; continue; }
+    uint32_t cl = S.sorted[S.lab[k]];
+    if (d.apply_charge_cut && nclus > uint32_t(kMaxClustersPerModule) && k < crun && cl > uint32_t(kMaxClustersPerModule)) {
+      d.clus[g] = int32_t(kInvId);
+      d.mid[g] = int16_t(kInvId);
+      continue;
+    }
+    if (changed && cl <= nclus_eff) {
+      uint16_t nc = s_newc[cl - 1];
+      d.clus[g] = int32_t(nc);
+      if (nc == kInvId) d.mid[g] = int16_t(kInvId);
+    } else {
+      d.clus[g] = int32_t(cl);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) write_module_record(d, e, m, this_id, changed ? last_new : nclus, S.warn);
+  __syncthreads();
+}
+
+// the modules the warp path handed over: (event << 11 | module position) entries
+__global__ void __launch_bounds__(256) k_find_clus_block(Dev d) {
+  __shared__ BlockSmem S;
+  const uint32_t cnt = d.big_list[0];
+  const uint32_t n = cnt < uint32_t(d.cap_big) ? cnt : uint32_t(d.cap_big);
+  for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+    const uint32_t v = d.big_list[2 + i];
+    const int e = int(v >> 11);
+    const EvInfo& E = d.ev[e];
+    if (E.word_base + uint64_t(E.n_words) > uint64_t(d.cap_words)) continue;
+    cluster_module_block(d, e, v & 2047u, S);
   }
 }
 
@@ -234,9 +415,13 @@ __global__ void k_hits_module_start(Dev d) {
 }  // namespace
 
 void launch_cluster(const Dev& d, const Launch& L) {
-  dim3 g(L.bpe > 0 ? L.bpe : 64, d.E);
-  k_find_clus<<<g, 256, 0, L.s>>>(d);
-  L.mark("find_clus_charge_cut");
+  cudaMemsetAsync(d.big_list, 0, 2 * sizeof(uint32_t), L.s);
+  // enough warps that a few events fill the GPU, at least 8 modules per warp otherwise
+  const int bx = std::max(4, std::min(250, (148 * 8 * 4) / std::max(1, int(d.E))));
+  k_find_clus_warp<<<dim3(bx, d.E), 32 * kWarpsPerBlock, 0, L.s>>>(d);
+  L.mark("find_clus_warp");
+  k_find_clus_block<<<148 * 2, 256, 0, L.s>>>(d);
+  L.mark("find_clus_block");
   k_hits_module_start<<<d.E, 1024, 0, L.s>>>(d);
   L.mark("hits_module_start");
 }

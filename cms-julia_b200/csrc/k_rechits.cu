@@ -3,9 +3,13 @@
 // errorFromDB), phase1PixelTopology.jl:249-296, SOARotation.jl:126-136,
 // approx_atan2.jl:159-184 (unsafe_atan2s), PixelRecHits.jl:20-82 and
 // hist_to_container.jl:217-270 (fill_many_from_vector).
-// One CTA per module; per-cluster reductions use shared-memory integer
-// atomics (order independent), then one thread per cluster evaluates the CPE
-// in FP32 with round-to-nearest and no contraction, as the reference does.
+// One warp per module (a CTA for the few modules above 256 digis or 128
+// clusters, handed over through a device work list); per-cluster reductions
+// use shared-memory integer atomics (order independent), then one thread per
+// cluster evaluates the CPE in FP32 with round-to-nearest and no contraction,
+// as the reference does.
+#include <algorithm>
+
 #include "pxl_internal.cuh"
 
 namespace pxl {
@@ -65,124 +69,234 @@ __device__ float correction(uint32_t sizeM1, int32_t q_f, int32_t q_l, uint16_t 
 }
 
 constexpr int kMaxClus = 1024;
+constexpr int kWarpClus = 128;  // clusters per module handled by one warp
+constexpr int kWarpSlots = kWarpModulePix / 32;
+constexpr int kWarpsPerBlock = 8;
 
-__global__ void __launch_bounds__(256) k_get_hits(Dev d) {
-  const int e = blockIdx.y;
-  __shared__ uint32_t s_minr[kMaxClus], s_maxr[kMaxClus], s_minc[kMaxClus], s_maxc[kMaxClus];
-  __shared__ int32_t s_q[kMaxClus], s_qfx[kMaxClus], s_qlx[kMaxClus], s_qfy[kMaxClus], s_qly[kMaxClus];
+// per-cluster reductions of getHits: bounding box and charges (total, first/last row and column)
+struct ClusSum {
+  uint32_t minr, maxr, minc, maxc;
+  int32_t q, qfx, qlx, qfy, qly;
+};
+
+// CPE of one cluster and its hit record at event-local hit index h (gpuPixelRecHits.jl:266-333)
+__device__ void write_hit(const Dev& d, int e, uint32_t me, uint32_t h, const ClusSum& s) {
+  const Conditions& c = d.c;
+  const uint32_t hb = d.ev[e].hit_base;
+  if (h >= d.hits_per_event) return;
+  if (uint64_t(hb) + h >= uint64_t(d.cap_hits)) { atomic_or_warn(&d.ev[e], kWarnBuffer); return; }
+  const DetParamsD& dp = c.det[me];
+  const uint32_t min_row = s.minr, max_row = s.maxr, min_col = s.minc, max_col = s.maxc;
+  const int32_t qfx = s.qfx, qlx = s.qlx, qfy = s.qfy, qly = s.qly;
+  // position_corr
+  const uint16_t llx = uint16_t(min_row + 1), lly = uint16_t(min_col + 1), urx = uint16_t(max_row), ury = uint16_t(max_col);
+  const uint16_t llxl = local_x(llx), llyl = local_y(lly), urxl = local_x(urx), uryl = local_y(ury);
+  const uint16_t mx = uint16_t(llxl + urxl), my = uint16_t(llyl + uryl);
+  int32_t xsize = int32_t(urxl) + 2 - int32_t(llxl);
+  int32_t ysize = int32_t(uryl) + 2 - int32_t(llyl);
+  if (big_x(min_row)) xsize += 1;
+  if (big_x(max_row)) xsize += 1;
+  if (big_y(min_col)) ysize += 1;
+  if (big_y(max_col)) ysize += 1;
+  const int32_t unb_x = int32_t(trunc(__ddiv_rn(__dmul_rn(8.0, double(fabsf(float(qfx - qlx)))), double(float(qfx + qlx)))));
+  const int32_t unb_y = int32_t(trunc(__ddiv_rn(__dmul_rn(8.0, double(fabsf(float(qfy - qly)))), double(float(qfy + qly)))));
+  xsize = 8 * xsize - unb_x;
+  ysize = 8 * ysize - unb_y;
+  int16_t sxs = int16_t(xsize < 1023 ? xsize : 1023);
+  int16_t sys = int16_t(ysize < 1023 ? ysize : 1023);
+  if (min_row == 0 || max_row == 159) sxs = int16_t(-sxs);
+  if (min_col == 0 || max_col == 415) sys = int16_t(-sys);
+  float xpos = __fadd_rn(dp.shift_x, __fmul_rn(c.pitch_x, __fadd_rn(__fmul_rn(0.5f, float(mx)), -81.0f)));
+  float ypos = __fadd_rn(dp.shift_y, __fmul_rn(c.pitch_y, __fadd_rn(__fmul_rn(0.5f, float(my)), -216.0f)));
+  const float gvz = __fdiv_rn(-1.0f, dp.z0);
+  const float cota = __fmul_rn(__fsub_rn(xpos, dp.x0), gvz);
+  const float cotb = __fmul_rn(__fsub_rn(ypos, dp.y0), gvz);
+  const float thick = dp.is_barrel ? c.thick_b : c.thick_e;
+  const float xcorr = correction(max_row - min_row, qfx, qlx, llxl, urxl, dp.cw_x, thick, cota, c.pitch_x, big_x(min_row), big_x(max_row));
+  const float ycorr = correction(max_col - min_col, qfy, qly, llyl, uryl, dp.cw_y, thick, cotb, c.pitch_y, big_y(min_col), big_y(max_col));
+  xpos = __fadd_rn(xpos, xcorr);
+  ypos = __fadd_rn(ypos, ycorr);
+  // errorFromDB
+  float xerr = 0.0050f, yerr = 0.0085f;
+  {
+    const uint32_t sx = max_row - min_row, sy = max_col - min_col;
+    const bool edge_x = min_row == 0 || max_row == 159, edge_y = min_col == 0 || max_col == 415;
+    int ix = sx == 0 ? 1 : 0, iy = sy == 0 ? 1 : 0;
+    ix += (sx == 0 && big_x(min_row)) ? 1 : 0;
+    iy += (sy == 0 && big_y(min_col)) ? 1 : 0;
+    if (!edge_x) xerr = dp.sx[ix];
+    if (!edge_y) yerr = dp.sy[iy];
+  }
+  // toGlobal_Special and beam spot
+  float ux = __fadd_rn(__fmul_rn(dp.R[0], xpos), __fmul_rn(dp.R[3], ypos));
+  float uy = __fadd_rn(__fmul_rn(dp.R[1], xpos), __fmul_rn(dp.R[4], ypos));
+  float uz = __fadd_rn(__fmul_rn(dp.R[2], xpos), __fmul_rn(dp.R[5], ypos));
+  ux = __fadd_rn(ux, dp.px); uy = __fadd_rn(uy, dp.py); uz = __fadd_rn(uz, dp.pz);
+  const float xg = __fsub_rn(ux, c.bs_x), yg = __fsub_rn(uy, c.bs_y), zg = __fsub_rn(uz, c.bs_z);
+  const size_t o = size_t(hb) + h;
+  d.charge[o] = uint32_t(s.q);
+  d.detind[o] = int16_t(me);
+  d.xl[o] = xpos; d.yl[o] = ypos;
+  d.xsize[o] = sxs; d.ysize[o] = sys;
+  d.xerr[o] = __fmul_rn(xerr, xerr); d.yerr[o] = __fmul_rn(yerr, yerr);
+  d.xg[o] = xg; d.yg[o] = yg; d.zg[o] = zg;
+  d.rg[o] = __fsqrt_rn(__fadd_rn(__fmul_rn(xg, xg), __fmul_rn(yg, yg)));
+  d.iphi[o] = atan2s(yg, xg);
+}
+
+// The module at position m of event e as getHits reads it: detector index, cluster count
+// (capped at kMaxClus) and digi range [first0, end0). Returns false when there is nothing to do.
+struct HitModule {
+  uint32_t me, nclus, first0, end0;
+};
+
+__device__ __forceinline__ bool hit_module(const Dev& d, int e, uint32_t m, HitModule& hm) {
   const EvInfo& E = d.ev[e];
   const uint32_t nmod = E.n_modules, n_el = E.n_words;
-  const uint64_t eb = E.word_base;
-  if (eb + n_el > uint64_t(d.cap_words)) return;
-  const uint32_t hb = E.hit_base;
   const uint32_t* ms = d.module_start + size_t(e) * (kMaxNumModules + 1);
-  const uint32_t* cim = d.clus_in_module + size_t(e) * kMaxNumModules;
+  hm.me = d.module_id[size_t(e) * kMaxNumModules + m];
+  if (hm.me >= uint32_t(kMaxNumModules) || int32_t(hm.me) >= d.c.n_det) return false;
+  hm.nclus = d.clus_in_module[size_t(e) * kMaxNumModules + hm.me];
+  if (hm.nclus == 0) return false;
+  if (hm.nclus > uint32_t(kMaxClus)) hm.nclus = kMaxClus;
+  hm.first0 = ms[m + 1] - 1;
+  hm.end0 = (m + 1 < nmod) ? ms[m + 2] - 1 : n_el;
+  if (ms[m + 1] < 1 || hm.end0 < hm.first0 || hm.end0 > n_el) return false;
+  return true;
+}
+
+// ------------------------------------------------------------ warp per module
+struct WarpHitSmem {
+  uint32_t minr[kWarpClus], maxr[kWarpClus], minc[kWarpClus], maxc[kWarpClus];
+  int32_t q[kWarpClus], qfx[kWarpClus], qlx[kWarpClus], qfy[kWarpClus], qly[kWarpClus];
+};
+
+__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_get_hits_warp(Dev d) {
+  __shared__ WarpHitSmem smem[kWarpsPerBlock];
+  const int e = blockIdx.y;
+  const unsigned lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+  WarpHitSmem& S = smem[wib];
+  const EvInfo& E = d.ev[e];
+  const uint32_t nmod = E.n_modules;
+  if (E.word_base + uint64_t(E.n_words) > uint64_t(d.cap_words)) return;
+  const uint64_t eb = E.word_base;
   const uint32_t* cms = d.clus_module_start + size_t(e) * (kMaxNumModules + 1);
-  const uint32_t hcap = d.hits_per_event;
-  const Conditions& c = d.c;
-  for (uint32_t m = blockIdx.x; m < nmod; m += gridDim.x) {
-    const uint32_t me = d.module_id[size_t(e) * kMaxNumModules + m];
-    if (me >= uint32_t(kMaxNumModules) || int32_t(me) >= c.n_det) continue;
-    uint32_t nclus = cim[me];
-    if (nclus == 0) continue;
-    if (nclus > uint32_t(kMaxClus)) nclus = kMaxClus;
-    const uint32_t first0 = ms[m + 1] - 1;
-    const uint32_t end0 = (m + 1 < nmod) ? ms[m + 2] - 1 : n_el;
-    if (ms[m + 1] < 1 || end0 < first0 || end0 > n_el) continue;
+  for (uint32_t m = blockIdx.x * kWarpsPerBlock + wib; m < nmod; m += gridDim.x * kWarpsPerBlock) {
+    HitModule hm;
+    if (!hit_module(d, e, m, hm)) continue;
+    const uint32_t nd = hm.end0 - hm.first0;
+    if (nd > uint32_t(kWarpModulePix) || hm.nclus > uint32_t(kWarpClus)) {
+      if (lane == 0) {
+        const uint32_t slot = atomicAdd(&d.big_list[1], 1u);
+        if (slot < uint32_t(d.cap_big)) d.big_list[2 + d.cap_big + slot] = (uint32_t(e) << 11) | m;
+      }
+      continue;
+    }
+    const uint32_t nclus = hm.nclus;
+    for (uint32_t k = lane; k < nclus; k += 32) {
+      S.minr[k] = 0xFFFFFFFFu; S.maxr[k] = 0; S.minc[k] = 0xFFFFFFFFu; S.maxc[k] = 0;
+      S.q[k] = 0; S.qfx[k] = 0; S.qlx[k] = 0; S.qfy[k] = 0; S.qly[k] = 0;
+    }
+    __syncwarp();
+    // digis of this module's range that belong to it, kept in registers
+    uint32_t xs[kWarpSlots], ys[kWarpSlots];
+    int32_t cls[kWarpSlots], chs[kWarpSlots];
+#pragma unroll
+    for (int j = 0; j < kWarpSlots; ++j) {
+      const uint32_t i = hm.first0 + lane + 32u * j;
+      cls[j] = 0;
+      if (i < hm.end0) {
+        const uint64_t g = eb + i;
+        const int16_t id = d.mid[g];
+        const int32_t cl = d.clus[g];
+        if (id != int16_t(kInvId) && uint32_t(int32_t(id)) == hm.me && cl >= 1 && uint32_t(cl) <= nclus) {
+          cls[j] = cl;
+          xs[j] = uint32_t(int32_t(d.xx[g]));
+          ys[j] = uint32_t(int32_t(d.yy[g]));
+          const int32_t a = d.adc[g];
+          chs[j] = a < 65535 ? a : 65535;
+          atomicMin(&S.minr[cl - 1], xs[j]); atomicMax(&S.maxr[cl - 1], xs[j]);
+          atomicMin(&S.minc[cl - 1], ys[j]); atomicMax(&S.maxc[cl - 1], ys[j]);
+        }
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < kWarpSlots; ++j) {
+      if (cls[j] == 0) continue;
+      const int k = cls[j] - 1;
+      atomicAdd(&S.q[k], chs[j]);
+      if (S.minr[k] == xs[j]) atomicAdd(&S.qfx[k], chs[j]);
+      if (S.maxr[k] == xs[j]) atomicAdd(&S.qlx[k], chs[j]);
+      if (S.minc[k] == ys[j]) atomicAdd(&S.qfy[k], chs[j]);
+      if (S.maxc[k] == ys[j]) atomicAdd(&S.qly[k], chs[j]);
+    }
+    __syncwarp();
+    for (uint32_t k = lane; k < nclus; k += 32) {
+      const ClusSum s{S.minr[k], S.maxr[k], S.minc[k], S.maxc[k], S.q[k], S.qfx[k], S.qlx[k], S.qfy[k], S.qly[k]};
+      write_hit(d, e, hm.me, cms[hm.me] + k, s);
+    }
+    __syncwarp();
+  }
+}
+
+// ------------------------------------------------------------ CTA per module
+struct BlockHitSmem {
+  uint32_t minr[kMaxClus], maxr[kMaxClus], minc[kMaxClus], maxc[kMaxClus];
+  int32_t q[kMaxClus], qfx[kMaxClus], qlx[kMaxClus], qfy[kMaxClus], qly[kMaxClus];
+};
+
+__global__ void __launch_bounds__(256) k_get_hits_block(Dev d) {
+  __shared__ BlockHitSmem S;
+  const uint32_t cnt = d.big_list[1];
+  const uint32_t nbig = cnt < uint32_t(d.cap_big) ? cnt : uint32_t(d.cap_big);
+  for (uint32_t bi = blockIdx.x; bi < nbig; bi += gridDim.x) {
+    const uint32_t v = d.big_list[2 + d.cap_big + bi];
+    const int e = int(v >> 11);
+    const uint32_t m = v & 2047u;
+    const EvInfo& E = d.ev[e];
+    if (E.word_base + uint64_t(E.n_words) > uint64_t(d.cap_words)) continue;
+    const uint64_t eb = E.word_base;
+    const uint32_t* cms = d.clus_module_start + size_t(e) * (kMaxNumModules + 1);
+    HitModule hm;
+    if (!hit_module(d, e, m, hm)) continue;
+    const uint32_t nclus = hm.nclus;
     for (uint32_t k = threadIdx.x; k < nclus; k += blockDim.x) {
-      s_minr[k] = 0xFFFFFFFFu; s_maxr[k] = 0; s_minc[k] = 0xFFFFFFFFu; s_maxc[k] = 0;
-      s_q[k] = 0; s_qfx[k] = 0; s_qlx[k] = 0; s_qfy[k] = 0; s_qly[k] = 0;
+      S.minr[k] = 0xFFFFFFFFu; S.maxr[k] = 0; S.minc[k] = 0xFFFFFFFFu; S.maxc[k] = 0;
+      S.q[k] = 0; S.qfx[k] = 0; S.qlx[k] = 0; S.qfy[k] = 0; S.qly[k] = 0;
     }
     __syncthreads();
-    for (uint32_t i = first0 + threadIdx.x; i < end0; i += blockDim.x) {
+    for (uint32_t i = hm.first0 + threadIdx.x; i < hm.end0; i += blockDim.x) {
       const uint64_t g = eb + i;
       const int16_t id = d.mid[g];
-      if (id == int16_t(kInvId) || uint32_t(int32_t(id)) != me) continue;
+      if (id == int16_t(kInvId) || uint32_t(int32_t(id)) != hm.me) continue;
       const int32_t cl = d.clus[g];
       if (cl < 1 || uint32_t(cl) > nclus) continue;
       const uint32_t x = uint32_t(int32_t(d.xx[g])), y = uint32_t(int32_t(d.yy[g]));
-      atomicMin(&s_minr[cl - 1], x); atomicMax(&s_maxr[cl - 1], x);
-      atomicMin(&s_minc[cl - 1], y); atomicMax(&s_maxc[cl - 1], y);
+      atomicMin(&S.minr[cl - 1], x); atomicMax(&S.maxr[cl - 1], x);
+      atomicMin(&S.minc[cl - 1], y); atomicMax(&S.maxc[cl - 1], y);
     }
     __syncthreads();
-    for (uint32_t i = first0 + threadIdx.x; i < end0; i += blockDim.x) {
+    for (uint32_t i = hm.first0 + threadIdx.x; i < hm.end0; i += blockDim.x) {
       const uint64_t g = eb + i;
       const int16_t id = d.mid[g];
-      if (id == int16_t(kInvId) || uint32_t(int32_t(id)) != me) continue;
+      if (id == int16_t(kInvId) || uint32_t(int32_t(id)) != hm.me) continue;
       const int32_t cl = d.clus[g];
       if (cl < 1 || uint32_t(cl) > nclus) continue;
       const uint32_t x = uint32_t(int32_t(d.xx[g])), y = uint32_t(int32_t(d.yy[g]));
       const int32_t a = d.adc[g];
       const int32_t ch = a < 65535 ? a : 65535;
       const int k = cl - 1;
-      atomicAdd(&s_q[k], ch);
-      if (s_minr[k] == x) atomicAdd(&s_qfx[k], ch);
-      if (s_maxr[k] == x) atomicAdd(&s_qlx[k], ch);
-      if (s_minc[k] == y) atomicAdd(&s_qfy[k], ch);
-      if (s_maxc[k] == y) atomicAdd(&s_qly[k], ch);
+      atomicAdd(&S.q[k], ch);
+      if (S.minr[k] == x) atomicAdd(&S.qfx[k], ch);
+      if (S.maxr[k] == x) atomicAdd(&S.qlx[k], ch);
+      if (S.minc[k] == y) atomicAdd(&S.qfy[k], ch);
+      if (S.maxc[k] == y) atomicAdd(&S.qly[k], ch);
     }
     __syncthreads();
-    const DetParamsD& dp = c.det[me];
     for (uint32_t k = threadIdx.x; k < nclus; k += blockDim.x) {
-      const uint32_t h = cms[me] + k;  // 0-based event-local hit index
-      if (h >= hcap) continue;
-      if (uint64_t(hb) + h >= uint64_t(d.cap_hits)) { atomic_or_warn(&d.ev[e], kWarnBuffer); continue; }
-      const uint32_t min_row = s_minr[k], max_row = s_maxr[k], min_col = s_minc[k], max_col = s_maxc[k];
-      const int32_t qfx = s_qfx[k], qlx = s_qlx[k], qfy = s_qfy[k], qly = s_qly[k];
-      // position_corr
-      const uint16_t llx = uint16_t(min_row + 1), lly = uint16_t(min_col + 1), urx = uint16_t(max_row), ury = uint16_t(max_col);
-      const uint16_t llxl = local_x(llx), llyl = local_y(lly), urxl = local_x(urx), uryl = local_y(ury);
-      const uint16_t mx = uint16_t(llxl + urxl), my = uint16_t(llyl + uryl);
-      int32_t xsize = int32_t(urxl) + 2 - int32_t(llxl);
-      int32_t ysize = int32_t(uryl) + 2 - int32_t(llyl);
-      if (big_x(min_row)) xsize += 1;
-      if (big_x(max_row)) xsize += 1;
-      if (big_y(min_col)) ysize += 1;
-      if (big_y(max_col)) ysize += 1;
-      const int32_t unb_x = int32_t(trunc(__ddiv_rn(__dmul_rn(8.0, double(fabsf(float(qfx - qlx)))), double(float(qfx + qlx)))));
-      const int32_t unb_y = int32_t(trunc(__ddiv_rn(__dmul_rn(8.0, double(fabsf(float(qfy - qly)))), double(float(qfy + qly)))));
-      xsize = 8 * xsize - unb_x;
-      ysize = 8 * ysize - unb_y;
-      int16_t sxs = int16_t(xsize < 1023 ? xsize : 1023);
-      int16_t sys = int16_t(ysize < 1023 ? ysize : 1023);
-      if (min_row == 0 || max_row == 159) sxs = int16_t(-sxs);
-      if (min_col == 0 || max_col == 415) sys = int16_t(-sys);
-      float xpos = __fadd_rn(dp.shift_x, __fmul_rn(c.pitch_x, __fadd_rn(__fmul_rn(0.5f, float(mx)), -81.0f)));
-      float ypos = __fadd_rn(dp.shift_y, __fmul_rn(c.pitch_y, __fadd_rn(__fmul_rn(0.5f, float(my)), -216.0f)));
-      const float gvz = __fdiv_rn(-1.0f, dp.z0);
-      const float cota = __fmul_rn(__fsub_rn(xpos, dp.x0), gvz);
-      const float cotb = __fmul_rn(__fsub_rn(ypos, dp.y0), gvz);
-      const float thick = dp.is_barrel ? c.thick_b : c.thick_e;
-      const float xcorr = correction(max_row - min_row, qfx, qlx, llxl, urxl, dp.cw_x, thick, cota, c.pitch_x, big_x(min_row), big_x(max_row));
-      const float ycorr = correction(max_col - min_col, qfy, qly, llyl, uryl, dp.cw_y, thick, cotb, c.pitch_y, big_y(min_col), big_y(max_col));
-      xpos = __fadd_rn(xpos, xcorr);
-      ypos = __fadd_rn(ypos, ycorr);
-      // errorFromDB
-      float xerr = 0.0050f, yerr = 0.0085f;
-      {
-        const uint32_t sx = max_row - min_row, sy = max_col - min_col;
-        const bool edge_x = min_row == 0 || max_row == 159, edge_y = min_col == 0 || max_col == 415;
-        int ix = sx == 0 ? 1 : 0, iy = sy == 0 ? 1 : 0;
-        ix += (sx == 0 && big_x(min_row)) ? 1 : 0;
-        iy += (sy == 0 && big_y(min_col)) ? 1 : 0;
-        if (!edge_x) xerr = dp.sx[ix];
-        if (!edge_y) yerr = dp.sy[iy];
-      }
-      // toGlobal_Special and beam spot
-      float ux = __fadd_rn(__fmul_rn(dp.R[0], xpos), __fmul_rn(dp.R[3], ypos));
-      float uy = __fadd_rn(__fmul_rn(dp.R[1], xpos), __fmul_rn(dp.R[4], ypos));
-      float uz = __fadd_rn(__fmul_rn(dp.R[2], xpos), __fmul_rn(dp.R[5], ypos));
-      ux = __fadd_rn(ux, dp.px); uy = __fadd_rn(uy, dp.py); uz = __fadd_rn(uz, dp.pz);
-      const float xg = __fsub_rn(ux, c.bs_x), yg = __fsub_rn(uy, c.bs_y), zg = __fsub_rn(uz, c.bs_z);
-      const size_t o = size_t(hb) + h;
-      d.charge[o] = uint32_t(s_q[k]);
-      d.detind[o] = int16_t(me);
-      d.xl[o] = xpos; d.yl[o] = ypos;
-      d.xsize[o] = sxs; d.ysize[o] = sys;
-      d.xerr[o] = __fmul_rn(xerr, xerr); d.yerr[o] = __fmul_rn(yerr, yerr);
-      d.xg[o] = xg; d.yg[o] = yg; d.zg[o] = zg;
-      d.rg[o] = __fsqrt_rn(__fadd_rn(__fmul_rn(xg, xg), __fmul_rn(yg, yg)));
-      d.iphi[o] = atan2s(yg, xg);
+      const ClusSum s{S.minr[k], S.maxr[k], S.minc[k], S.maxc[k], S.q[k], S.qfx[k], S.qlx[k], S.qfy[k], S.qly[k]};
+      write_hit(d, e, hm.me, cms[hm.me] + k, s);
     }
     __syncthreads();
   }
@@ -258,9 +372,11 @@ __global__ void __launch_bounds__(1024) k_phi_binner(Dev d) {
 }  // namespace
 
 void launch_rechits(const Dev& d, const Launch& L) {
-  dim3 g(L.bpe > 0 ? L.bpe : 64, d.E);
-  k_get_hits<<<g, 256, 0, L.s>>>(d);
-  L.mark("get_hits");
+  const int bx = std::max(4, std::min(250, (148 * 8 * 4) / std::max(1, int(d.E))));
+  k_get_hits_warp<<<dim3(bx, d.E), 32 * kWarpsPerBlock, 0, L.s>>>(d);
+  L.mark("get_hits_warp");
+  k_get_hits_block<<<148 * 2, 256, 0, L.s>>>(d);
+  L.mark("get_hits_block");
   k_phi_binner<<<d.E, 1024, 0, L.s>>>(d);
   L.mark("phi_binner");
 }

@@ -4,7 +4,8 @@
 // is wholly owned by another allocator, or a trigger path that must not block on
 // cudaMalloc/cudaFree (both can synchronise the device). This entry point takes
 // device inputs and outputs from the caller and keeps its scratch (per-event
-// record, per-chunk module-start counts, cluster module starts) in one
+// record, per-chunk module-start counts, cluster module starts, the list of
+// modules too large for one warp) in one
 // file-scope device array of fixed size, so it calls no cudaMalloc, cudaFree
 // or allocating library routine.
 //
@@ -36,6 +37,7 @@ struct NoAllocScratch {
   uint32_t chunk_wo[kMaxChunks];
   uint32_t chunk_nmod[kMaxChunks];
   uint32_t clus_module_start[kMaxNumModules + 1];
+  uint32_t big_list[2 + 2 * kMaxNumModules];
   uint32_t status;
 };
 
@@ -121,6 +123,8 @@ extern "C" int32_t pxl_clusterize_digis_noalloc(const uint16_t* id, const int16_
   d.clus_in_module = clus_in_module;
   d.module_id = module_id;
   d.clus_module_start = s->clus_module_start;
+  d.big_list = s->big_list;
+  d.cap_big = kMaxNumModules;
   d.bpe = 148 * 4;
   Launch L{st, d.bpe, 256};
   launch_modstart(d, L);

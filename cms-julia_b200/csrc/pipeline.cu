@@ -247,6 +247,8 @@ int alloc_batch(PxlCtx* ctx) {
   int64_t st = scan_tmp_elems(std::max({d.cap_words, d.cap_items, d.cap_cells, d.cap_hits, d.cap_tuples}) + 1);
   A(scan_tmp, st); A(scan_tmp64, st);
   A(status, 1);
+  d.cap_big = E * kMaxNumModules;
+  A(big_list, 2 + 2 * d.cap_big);
 #undef A
   // input staging
   ctx->raw_cap = size_t(d.cap_words) * 4 + size_t(E) * (4 + 16 * 4 + size_t(d.n_fed_slots + 8) * 24) + 4096;

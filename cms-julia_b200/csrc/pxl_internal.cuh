@@ -30,6 +30,7 @@ constexpr int kMaxCellsPerHit = 128;
 constexpr int kCellRows = 64;
 constexpr int kMaxActiveColumns = 512 * 1024 / 8;
 constexpr int kMaxFedSlots = 160;
+constexpr int kWarpModulePix = 256;  // modules up to this many digis are clustered by one warp
 
 // per-event warning bits (same values as PXL_WARN_* in include/pxl.h)
 enum : uint32_t {
@@ -173,6 +174,10 @@ struct Dev {
   uint32_t* scan_tmp;      // [scan tile sums]
   uint64_t* scan_tmp64;
   uint32_t* status;        // [1] global status bits (buffer overflow)
+  // modules too large for the warp-per-module kernels: [0] clustering count, [1] rechit
+  // count, then cap_big entries (event << 11 | module position) for each
+  uint32_t* big_list;
+  int64_t cap_big;
   // launch shape
   int32_t bpe;             // blocks per event for per-event kernels
 };
