@@ -1,206 +1,305 @@
-// Broken-line helix fit, one thread per track with every matrix in registers.
-// Restates plugin-PixelTriplets/broken_line.jl:46-528 (BL_Fast_fit,
+// Broken-line helix fit, one thread per track with every array in registers.
+// Restates plugin-PixelTriplets/broken_line.jl:46-696 (BL_Fast_fit,
 // prepare_broken_line_data, mult_scatt, matrixc_u, BL_Line_fit, BL_Circle_fit,
-// translate_karimaki) and cholesky_inversion.jl (symmetric inverse).
+// translate_karimaki); the reference inverts the band systems with the dense
+// Cholesky of cholesky_inversion.jl.
 //
-// Scalar policy: T is the working type of the bulk arithmetic. The symmetric
-// band-system inverse, the solve u = C^-1 r and every covariance propagation
-// are always FP64. T = double gives the reference's all-FP64 fit; T = float
-// gives the mixed-precision fit (FP32 arithmetic, FP64 Cholesky and covariance).
+// B200 formulation (same mathematics, different evaluation):
+//  * Band solve. The line system is pentadiagonal (matrixc_u) and the circle
+//    system adds one dense border row for the curvature correction. Both are
+//    factorised as L D L^T in O(N), eliminating the hits in reverse order and
+//    the border last, so that the covariance entries the fit needs (hits 0, 1
+//    and the border) come from the trailing 3x3 block of the inverse alone.
+//    The factorisation, the solve and everything downstream of the solution
+//    (parameters, Jacobians, Karimaki translations, covariances) are FP64.
+//  * Local frame. Hit coordinates are taken relative to hit 0 (subtracted in
+//    FP64 on load). Arc lengths and radial residuals are formed from
+//    cancellation-free identities: the angle between two radius vectors
+//    r0 and r0 + p is atan2(r0 x p, |r0|^2 + r0.p), and |r0 + p| - |r0| =
+//    (2 r0.p + |p|^2) / (|r0 + p| + |r0|), with the fast-fit radius taken as
+//    |r0| so that the linearisation circle passes exactly through hit 0.
+//    The line fit works on (S, Z) relative to hit 0 and moves the intercept
+//    back in FP64.
+// T is the working type of the hit geometry, the weights, the multiple-
+// scattering variances, the band-matrix entries and the chi2: T = double is the
+// FP64 fit, T = float the mixed-precision fit.
 #pragma once
+#include <cmath>
 #include <cstdint>
+
+// the fit is host-callable too, so that the formulation can be checked on the CPU
+#define BL_HD __host__ __device__ __forceinline__
 
 namespace pxl {
 namespace bl {
 
-template <class T> __device__ __forceinline__ T s_sqrt(T x);
-template <> __device__ __forceinline__ double s_sqrt<double>(double x) { return sqrt(x); }
-template <> __device__ __forceinline__ float s_sqrt<float>(float x) { return sqrtf(x); }
-template <class T> __device__ __forceinline__ T s_atan(T x);
-template <> __device__ __forceinline__ double s_atan<double>(double x) { return atan(x); }
-template <> __device__ __forceinline__ float s_atan<float>(float x) { return atanf(x); }
-template <class T> __device__ __forceinline__ T s_log(T x);
-template <> __device__ __forceinline__ double s_log<double>(double x) { return log(x); }
-template <> __device__ __forceinline__ float s_log<float>(float x) { return logf(x); }
-template <class T> __device__ __forceinline__ T s_sin(T x);
-template <> __device__ __forceinline__ double s_sin<double>(double x) { return sin(x); }
-template <> __device__ __forceinline__ float s_sin<float>(float x) { return sinf(x); }
-template <class T> __device__ __forceinline__ T s_cos(T x);
-template <> __device__ __forceinline__ double s_cos<double>(double x) { return cos(x); }
-template <> __device__ __forceinline__ float s_cos<float>(float x) { return cosf(x); }
-template <class T> __device__ __forceinline__ T s_abs(T x) { return x < T(0) ? -x : x; }
+template <class T> BL_HD T s_sqrt(T x);
+template <> BL_HD double s_sqrt<double>(double x) { return sqrt(x); }
+template <> BL_HD float s_sqrt<float>(float x) { return sqrtf(x); }
+template <class T> BL_HD T s_atan(T x);
+template <> BL_HD double s_atan<double>(double x) { return atan(x); }
+template <> BL_HD float s_atan<float>(float x) { return atanf(x); }
+template <class T> BL_HD T s_log(T x);
+template <> BL_HD double s_log<double>(double x) { return log(x); }
+template <> BL_HD float s_log<float>(float x) { return logf(x); }
+template <class T> BL_HD T s_abs(T x) { return x < T(0) ? -x : x; }
 
 constexpr double kPi = 3.141592653589793;
 
 // custom atan2 of broken_line.jl:256-268: range (-pi/2, 3pi/2)
 template <class T>
-__device__ __forceinline__ T bl_atan2(T y, T x) {
+BL_HD T bl_atan2(T y, T x) {
   if (x > T(0)) return s_atan<T>(y / x);
   if (x < T(0)) return s_atan<T>(y / x) + T(kPi);
   if (y > T(0) && x == T(0)) return T(kPi / 2);
   if (y < T(0) && x == T(0)) return T(-kPi / 2);
-  return T(__longlong_as_double(0x7ff8000000000000ll));
+  return T(NAN);
 }
 
+// multiple-scattering variance of one segment (broken_line.jl:46-57)
 template <class T>
-__device__ __forceinline__ T mult_scatt(T length, T B, T R, T slope) {
+BL_HD T mult_scatt(T length, T B, T R, T slope) {
   T pt2 = B * R;
   pt2 = pt2 < T(20.0) ? pt2 : T(20.0);
   pt2 = pt2 * pt2;
   const T XXI_0 = T(0.06 / 16.0);
   const T fact = T(0.7 * ((13.6 / 1000) * (13.6 / 1000)));
-  const T slope_term = T(1) + slope * slope;
   const T abs_len = s_abs(length) * XXI_0;
-  const T lt = s_log<T>(abs_len);
-  const T sq = (T(1) + T(0.038) * lt) * (T(1) + T(0.038) * lt);
-  return fact / (pt2 * slope_term) * abs_len * sq;
+  const T lt = T(1) + T(0.038) * s_log<T>(abs_len);
+  return fact / (pt2 * (T(1) + slope * slope)) * abs_len * (lt * lt);
 }
 
 template <class T>
-__device__ __forceinline__ void rotation_matrix(T slope, T R[2][2]) {
+BL_HD void rotation_matrix(T slope, T R[2][2]) {
   const T a = T(1) / s_sqrt<T>(T(1) + slope * slope);
   const T b = slope * a;
   R[0][0] = a; R[0][1] = b; R[1][0] = -b; R[1][1] = a;
 }
 
-// symmetric positive-definite inverse by LDL^T, FP64, reading the lower triangle
-template <int M>
-__device__ __forceinline__ void invert_sym(const double A[M][M], double Inv[M][M]) {
-  double L[M][M], D[M], Li[M][M];
-#pragma unroll
-  for (int j = 0; j < M; ++j) {
-    double dd = A[j][j];
-#pragma unroll
-    for (int k = 0; k < j; ++k) dd -= L[j][k] * L[j][k] * D[k];
-    D[j] = dd;
-    L[j][j] = 1.0;
-#pragma unroll
-    for (int i = j + 1; i < M; ++i) {
-      double v = A[i][j];
-#pragma unroll
-      for (int k = 0; k < j; ++k) v -= L[i][k] * L[j][k] * D[k];
-      L[i][j] = v / dd;
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < M; ++i) {
-    Li[i][i] = 1.0;
-#pragma unroll
-    for (int j = 0; j < i; ++j) {
-      double v = 0;
-#pragma unroll
-      for (int k = j; k < i; ++k) v -= L[i][k] * Li[k][j];
-      Li[i][j] = v;
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < M; ++i)
-#pragma unroll
-    for (int j = 0; j <= i; ++j) {
-      double v = 0;
-#pragma unroll
-      for (int k = i; k < M; ++k) v += Li[k][i] * Li[k][j] / D[k];
-      Inv[i][j] = v;
-      Inv[j][i] = v;
-    }
-}
-
-template <int N, class T>
-struct Prepared {
-  int q;
-  T radii[2][N];
-  T s[N], S[N], Z[N], VarBeta[N];
+// --------------------------------------------------------------- band solver
+// Symmetric positive-definite system of N hit unknowns (pentadiagonal block)
+// and, when Border, one extra unknown coupled to every hit. Arrays are in
+// elimination order k = 0..N-1, which is hit N-1-k; the border is eliminated last.
+template <int N, bool Border>
+struct Band {
+  static constexpr int M = N + (Border ? 1 : 0);
+  double D[M];   // pivots
+  double l1[N];  // L[k][k-1]
+  double l2[N];  // L[k][k-2]
+  double g[N];   // L[border][k]
 };
 
-// BL_Fast_fit; h[3][N] hit coordinates (columns are hits)
-template <int N, class T>
-__device__ __forceinline__ void fast_fit(const T h[3][N], T r[4]) {
-  constexpr int mid = N >> 1;
-  const T h11 = h[0][0], h21 = h[1][0], h1m = h[0][mid], h2m = h[1][mid], h1n = h[0][N - 1], h2n = h[1][N - 1];
-  const T a1 = h1m - h11, a2 = h2m - h21, b1 = h1n - h1m, b2 = h2n - h2m, c1 = h11 - h1n, c2 = h21 - h2n;
-  const T ca = c1 * a2 - c2 * a1, ba = b1 * a2 - b2 * a1;
-  const T nc = c1 * c1 + c2 * c2, na = a1 * a1 + a2 * a2, nb = b1 * b1 + b2 * b2;
-  const T tmp = T(0.5) / ca;
-  r[0] = h11 - (a2 * nc + c2 * na) * tmp;
-  r[1] = h21 + (a1 * nc + c1 * na) * tmp;
-  r[2] = s_sqrt<T>(na * nb * nc) / (T(2.0) * s_abs(ba));
-  const T cx = r[0], cy = r[1];
-  const T d1 = h11 - cx, d2 = h21 - cy, e1 = h1n - cx, e2 = h2n - cy;
-  const T de = d1 * e2 - d2 * e1, dotde = d1 * e1 + d2 * e2;
-  const T dz = h[2][N - 1] - h[2][0];
-  r[3] = r[2] * bl_atan2<T>(de, dotde) / dz;
+// d: diagonal, e1[k]: entry (k, k+1), e2[k]: entry (k, k+2), b[k]: (border, k), c: (border, border)
+template <int N, bool Border>
+BL_HD void band_factor(const double d[N], const double e1[N], const double e2[N],
+                                            const double b[N], double c, Band<N, Border>& f) {
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    double l2 = 0.0, l1 = 0.0;
+    if (k >= 2) l2 = e2[k - 2] / f.D[k - 2];
+    if (k >= 1) l1 = (e1[k - 1] - (k >= 2 ? l2 * f.D[k - 2] * f.l1[k - 1] : 0.0)) / f.D[k - 1];
+    f.l1[k] = l1;
+    f.l2[k] = l2;
+    double dk = d[k];
+    if (k >= 1) dk -= l1 * l1 * f.D[k - 1];
+    if (k >= 2) dk -= l2 * l2 * f.D[k - 2];
+    f.D[k] = dk;
+    if constexpr (Border) {
+      double gk = b[k];
+      if (k >= 1) gk -= f.g[k - 1] * f.D[k - 1] * l1;
+      if (k >= 2) gk -= f.g[k - 2] * f.D[k - 2] * l2;
+      f.g[k] = gk / dk;
+    }
+  }
+  if constexpr (Border) {
+    double dn = c;
+#pragma unroll
+    for (int k = 0; k < N; ++k) dn -= f.g[k] * f.g[k] * f.D[k];
+    f.D[N] = dn;
+  }
 }
 
+// solves the system for a right-hand side that is zero on the border; x[M]
+template <int N, bool Border>
+BL_HD void band_solve(const Band<N, Border>& f, const double r[N], double x[Band<N, Border>::M]) {
+  constexpr int M = Band<N, Border>::M;
+  double y[M];
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    double v = r[k];
+    if (k >= 1) v -= f.l1[k] * y[k - 1];
+    if (k >= 2) v -= f.l2[k] * y[k - 2];
+    y[k] = v;
+  }
+  if constexpr (Border) {
+    double v = 0.0;
+#pragma unroll
+    for (int k = 0; k < N; ++k) v -= f.g[k] * y[k];
+    y[N] = v;
+  }
+#pragma unroll
+  for (int k = 0; k < M; ++k) y[k] /= f.D[k];
+  if constexpr (Border) x[N] = y[N];
+#pragma unroll
+  for (int k = N - 1; k >= 0; --k) {
+    double v = y[k];
+    if (k + 1 < N) v -= f.l1[k + 1] * x[k + 1];
+    if (k + 2 < N) v -= f.l2[k + 2] * x[k + 2];
+    if constexpr (Border) v -= f.g[k] * x[N];
+    x[k] = v;
+  }
+}
+
+// trailing block of the inverse: entries among hit 1 (elimination N-2), hit 0
+// (elimination N-1) and the border. Inv[a][b] with a, b in {hit0, hit1, border} = {0, 1, 2}.
+template <int N, bool Border>
+BL_HD void band_trailing_inverse(const Band<N, Border>& f, double inv[3][3]) {
+  // L block rows (hit1, hit0, border): [[1,0,0],[a,1,0],[gb,gc,1]]; its inverse is
+  // [[1,0,0],[-a,1,0],[a*gc-gb,-gc,1]]
+  const double a = f.l1[N - 1];
+  double gb = 0.0, gc = 0.0, idn = 0.0;
+  if constexpr (Border) {
+    gb = f.g[N - 2];
+    gc = f.g[N - 1];
+    idn = 1.0 / f.D[N];
+  }
+  const double Mi[3][3] = {{1.0, 0.0, 0.0}, {-a, 1.0, 0.0}, {a * gc - gb, -gc, 1.0}};
+  const double iD[3] = {1.0 / f.D[N - 2], 1.0 / f.D[N - 1], idn};
+  double blk[3][3];
+#pragma unroll
+  for (int p = 0; p < 3; ++p)
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      double v = 0.0;
+#pragma unroll
+      for (int m = 0; m < 3; ++m) v += Mi[m][p] * Mi[m][q] * iD[m];
+      blk[p][q] = v;
+    }
+  // reorder (hit1, hit0, border) -> (hit0, hit1, border)
+  const int o[3] = {1, 0, 2};
+#pragma unroll
+  for (int p = 0; p < 3; ++p)
+#pragma unroll
+    for (int q = 0; q < 3; ++q) inv[p][q] = blk[o[p]][o[q]];
+}
+
+// band entries of matrixc_u (broken_line.jl:217-250) for weights w, abscissae S and
+// scattering variances VB, in elimination order (k = hit N-1-k)
 template <int N, class T>
-__device__ __forceinline__ void prepare(const T h[3][N], const T f[4], T B, Prepared<N, T>& d) {
-  const T x1 = h[0][1] - h[0][0], y1 = h[1][1] - h[1][0];
-  const T xn = h[0][N - 1] - h[0][N - 2], yn = h[1][N - 1] - h[1][N - 2];
-  d.q = (x1 * yn - y1 * xn) > T(0) ? -1 : 1;
-  const T slope = -T(d.q) / f[3];
-  T R[2][2];
-  rotation_matrix<T>(slope, R);
+BL_HD void band_entries(const T w[N], const T S[N], const T VB[N], double d[N], double e1[N],
+                                             double e2[N]) {
+  T dS[N];  // dS[i] = S[i+1] - S[i]
 #pragma unroll
-  for (int j = 0; j < N; ++j) { d.radii[0][j] = h[0][j] - f[0]; d.radii[1][j] = h[1][j] - f[1]; }
-  const T rr = s_sqrt<T>(f[0] * f[0] + f[1] * f[1]);
-  const T sc = -f[2] / rr;
-  const T e1 = sc * f[0], e2 = sc * f[1];
-  const T fac = T(d.q) * f[2];
+  for (int i = 0; i + 1 < N; ++i) dS[i] = S[i + 1] - S[i];
+  dS[N - 1] = T(1);
+  T iv[N];  // 1 / VB at the interior hits
+#pragma unroll
+  for (int i = 0; i < N; ++i) iv[i] = (i > 0 && i < N - 1) ? T(1) / VB[i] : T(0);
 #pragma unroll
   for (int i = 0; i < N; ++i) {
-    const T xi = d.radii[0][i], yi = d.radii[1][i];
-    d.s[i] = fac * bl_atan2<T>(xi * e2 - yi * e1, xi * e1 + yi * e2);
+    T dg = w[i];
+    if (i > 1) dg += iv[i - 1] / (dS[i - 1] * dS[i - 1]);
+    if (i > 0 && i < N - 1) {
+      const T q = (dS[i] + dS[i - 1]) / (dS[i] * dS[i - 1]);
+      dg += iv[i] * (q * q);
+    }
+    if (i < N - 2) dg += iv[i + 1] / (dS[i] * dS[i]);
+    T o1 = T(0), o2 = T(0);
+    if (i > 0 && i < N - 1) o1 = -iv[i] / dS[i] * ((dS[i] + dS[i - 1]) / (dS[i] * dS[i - 1]));
+    if (i < N - 2) {
+      o1 += -iv[i + 1] / dS[i] * ((dS[i + 1] + dS[i]) / (dS[i + 1] * dS[i]));
+      o2 = iv[i + 1] / (dS[i + 1] * dS[i]);
+    }
+    const int k = N - 1 - i;
+    d[k] = double(dg);
+    // entry (i, i+1) is (k-1, k) in elimination order, (i, i+2) is (k-2, k)
+    if (i + 1 < N) e1[k - 1] = double(o1);
+    if (i + 2 < N) e2[k - 2] = double(o2);
   }
+  e1[N - 1] = 0.0;
+  e2[N - 2] = 0.0;
+  e2[N - 1] = 0.0;
+}
+
+// --------------------------------------------------------------- fit state
+template <int N, class T>
+struct Geo {
+  T p[3][N];     // hit - hit 0
+  double h0[3];  // hit 0
+};
+
+template <int N, class T>
+struct Prep {
+  int q;
+  T R, f3, slope;
+  T cx, cy;       // fast-fit centre relative to hit 0
+  T rx[N], ry[N]; // hit - centre
+  T s[N];         // arc length relative to hit 0
+  double s0;      // arc length of hit 0
+  T S[N], Z[N];   // line-fit coordinates relative to hit 0
+  T VB[N];
+  T Rl[2][2];     // line-fit rotation
+};
+
+// BL_Fast_fit (broken_line.jl:275-313) in the frame of hit 0
+template <int N, class T>
+BL_HD void fast_fit(const Geo<N, T>& G, Prep<N, T>& P) {
+  constexpr int mid = N >> 1;
+  const T a1 = G.p[0][mid], a2 = G.p[1][mid];
+  const T b1 = G.p[0][N - 1] - G.p[0][mid], b2 = G.p[1][N - 1] - G.p[1][mid];
+  const T c1 = -G.p[0][N - 1], c2 = -G.p[1][N - 1];
+  const T ca = c1 * a2 - c2 * a1;
+  const T nc = c1 * c1 + c2 * c2, na = a1 * a1 + a2 * a2;
+  const T tmp = T(0.5) / ca;
+  P.cx = -(a2 * nc + c2 * na) * tmp;
+  P.cy = (a1 * nc + c1 * na) * tmp;
+  P.R = s_sqrt<T>(P.cx * P.cx + P.cy * P.cy);
+  // angle from (hit0 - centre) to (hit N-1 - centre)
+  const T d1 = -P.cx, d2 = -P.cy;
+  const T de = d1 * G.p[1][N - 1] - d2 * G.p[0][N - 1];
+  const T dotde = d1 * d1 + d2 * d2 + d1 * G.p[0][N - 1] + d2 * G.p[1][N - 1];
+  P.f3 = P.R * bl_atan2<T>(de, dotde) / G.p[2][N - 1];
+}
+
+// prepare_broken_line_data (broken_line.jl:150-207)
+template <int N, class T>
+BL_HD void prepare(const Geo<N, T>& G, T B, Prep<N, T>& P) {
+  const T x1 = G.p[0][1], y1 = G.p[1][1];
+  const T xn = G.p[0][N - 1] - G.p[0][N - 2], yn = G.p[1][N - 1] - G.p[1][N - 2];
+  P.q = (x1 * yn - y1 * xn) > T(0) ? -1 : 1;
+  P.slope = -T(P.q) / P.f3;
+  rotation_matrix<T>(P.slope, P.Rl);
+#pragma unroll
+  for (int i = 0; i < N; ++i) { P.rx[i] = G.p[0][i] - P.cx; P.ry[i] = G.p[1][i] - P.cy; }
+  const T ux = -P.cx, uy = -P.cy, uu = ux * ux + uy * uy;
+  const T fac = T(P.q) * P.R;
+  // the reference measures s from the direction centre -> origin: e ~ u - hit0
+  const T hx = T(G.h0[0]), hy = T(G.h0[1]);
+  P.s0 = double(fac * bl_atan2<T>(-(ux * hy - uy * hx), uu - (ux * hx + uy * hy)));
+  P.s[0] = T(0);
+#pragma unroll
+  for (int i = 1; i < N; ++i)
+    P.s[i] = -fac * bl_atan2<T>(ux * G.p[1][i] - uy * G.p[0][i], uu + ux * G.p[0][i] + uy * G.p[1][i]);
 #pragma unroll
   for (int i = 0; i < N; ++i) {
-    const T xi = d.s[i], yi = h[2][i];
-    d.S[i] = R[0][0] * xi + R[0][1] * yi;
-    d.Z[i] = R[1][0] * xi + R[1][1] * yi;
+    P.S[i] = P.Rl[0][0] * P.s[i] + P.Rl[0][1] * G.p[2][i];
+    P.Z[i] = P.Rl[1][0] * P.s[i] + P.Rl[1][1] * G.p[2][i];
   }
-  d.VarBeta[0] = 0;
-  d.VarBeta[N - 1] = 0;
+  P.VB[0] = T(0);
+  P.VB[N - 1] = T(0);
 #pragma unroll
   for (int i = 1; i < N - 1; ++i)
-    d.VarBeta[i] = mult_scatt<T>(d.S[i + 1] - d.S[i], B, f[2], slope) + mult_scatt<T>(d.S[i] - d.S[i - 1], B, f[2], slope);
+    P.VB[i] = mult_scatt<T>(P.S[i + 1] - P.S[i], B, P.R, P.slope) + mult_scatt<T>(P.S[i] - P.S[i - 1], B, P.R, P.slope);
 }
 
-// matrixc_u (broken_line.jl:217-250) into the top-left N x N block of C (M >= N)
-template <int N, int M, class T>
-__device__ __forceinline__ void matrixc_u(const T w[N], const T S[N], const T VB[N], double C[M][M]) {
-  T Tm[N][N + 2];
-#pragma unroll
-  for (int i = 0; i < N; ++i)
-#pragma unroll
-    for (int j = 0; j < N + 2; ++j) Tm[i][j] = T(0);
-#pragma unroll
-  for (int i = 0; i < N; ++i) {
-    Tm[i][i] = w[i];
-    if (i > 1) Tm[i][i] += T(1) / (VB[i - 1] * ((S[i] - S[i - 1]) * (S[i] - S[i - 1])));
-    if (i > 0 && i < N - 1) {
-      const T q = (S[i + 1] - S[i - 1]) / ((S[i + 1] - S[i]) * (S[i] - S[i - 1]));
-      Tm[i][i] += (T(1) / VB[i]) * (q * q);
-    }
-    if (i < N - 2) Tm[i][i] += T(1) / (VB[i + 1] * ((S[i + 1] - S[i]) * (S[i + 1] - S[i])));
-    if (i > 0 && i < N - 1)
-      Tm[i][i + 1] = T(1) / (VB[i] * (S[i + 1] - S[i])) * (-(S[i + 1] - S[i - 1]) / ((S[i + 1] - S[i]) * (S[i] - S[i - 1])));
-    if (i < N - 2)
-      Tm[i][i + 1] += T(1) / (VB[i + 1] * (S[i + 1] - S[i])) * (-(S[i + 2] - S[i]) / ((S[i + 2] - S[i + 1]) * (S[i + 1] - S[i])));
-    if (i < N - 2) Tm[i][i + 2] = T(1) / (VB[i + 1] * (S[i + 2] - S[i + 1]) * (S[i + 1] - S[i]));
-    Tm[i][i] *= T(0.5);
-  }
-#pragma unroll
-  for (int i = 0; i < N; ++i)
-#pragma unroll
-    for (int j = 0; j < N; ++j) C[i][j] = double(Tm[i][j] + Tm[j][i]);
-}
-
-__device__ __forceinline__ void sandwich2(const double J[2][2], double C[2][2]) {
+BL_HD void sandwich2(const double J[2][2], double C[2][2]) {
   double Tm[2][2], O[2][2];
   for (int a = 0; a < 2; ++a) for (int b = 0; b < 2; ++b) Tm[a][b] = J[a][0] * C[0][b] + J[a][1] * C[1][b];
   for (int a = 0; a < 2; ++a) for (int b = 0; b < 2; ++b) O[a][b] = Tm[a][0] * J[b][0] + Tm[a][1] * J[b][1];
   for (int a = 0; a < 2; ++a) for (int b = 0; b < 2; ++b) C[a][b] = O[a][b];
 }
 
-__device__ __forceinline__ void sandwich3(const double J[3][3], double C[3][3]) {
+BL_HD void sandwich3(const double J[3][3], double C[3][3]) {
   double Tm[3][3], O[3][3];
   for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) Tm[a][b] = J[a][0] * C[0][b] + J[a][1] * C[1][b] + J[a][2] * C[2][b];
   for (int a = 0; a < 3; ++a) for (int b = 0; b < 3; ++b) O[a][b] = Tm[a][0] * J[b][0] + Tm[a][1] * J[b][1] + Tm[a][2] * J[b][2];
@@ -210,110 +309,134 @@ __device__ __forceinline__ void sandwich3(const double J[3][3], double C[3][3]) 
 struct LineOut { double par[2]; double cov[2][2]; double chi2; };
 struct CircleOut { double par[3]; double cov[3][3]; int q; double chi2; };
 
-// BL_Line_fit, broken_line.jl:546-696; ge[6][N] as Float32
+// line-fit weights: 1 / variance of the hit along Z after the rotation (broken_line.jl:560-590)
 template <int N, class T>
-__device__ __forceinline__ void line_fit(const float ge[6][N], const T f[4], T B, const Prepared<N, T>& d, LineOut& L) {
-  const T slope = -T(d.q) / f[3];
-  T R[2][2];
-  rotation_matrix<T>(slope, R);
+BL_HD void line_weights(const float ge[6][N], const Prep<N, T>& P, T w[N]) {
   const double tol = 1e-12;
-  T w[N];
 #pragma unroll
   for (int i = 0; i < N; ++i) {
     auto z = [&](float v) { return fabs(double(v)) < tol ? T(0) : T(v); };
     const T V[3][3] = {{T(ge[0][i]), z(ge[1][i]), z(ge[3][i])}, {z(ge[1][i]), T(ge[2][i]), z(ge[4][i])},
                        {z(ge[3][i]), z(ge[4][i]), T(ge[5][i])}};
-    const T tmp = T(1) / s_sqrt<T>(d.radii[0][i] * d.radii[0][i] + d.radii[1][i] * d.radii[1][i]);
-    const T J[2][3] = {{d.radii[1][i] * tmp, -d.radii[0][i] * tmp, T(0)}, {T(0), T(0), T(1)}};
-    T M1[2][3], M2[2][3], M3[2][2];
-    for (int a = 0; a < 2; ++a) for (int b = 0; b < 3; ++b) M1[a][b] = R[a][0] * J[0][b] + R[a][1] * J[1][b];
-    for (int a = 0; a < 2; ++a) for (int b = 0; b < 3; ++b) M2[a][b] = M1[a][0] * V[0][b] + M1[a][1] * V[1][b] + M1[a][2] * V[2][b];
-    for (int a = 0; a < 2; ++a) for (int b = 0; b < 2; ++b) M3[a][b] = M2[a][0] * J[b][0] + M2[a][1] * J[b][1] + M2[a][2] * J[b][2];
-    const T m22 = M3[1][0] * R[1][0] + M3[1][1] * R[1][1];
+    const T tmp = T(1) / s_sqrt<T>(P.rx[i] * P.rx[i] + P.ry[i] * P.ry[i]);
+    const T J[2][3] = {{P.ry[i] * tmp, -P.rx[i] * tmp, T(0)}, {T(0), T(0), T(1)}};
+    // second row of R J V J^T R^T
+    T rj[3];
+#pragma unroll
+    for (int b = 0; b < 3; ++b) rj[b] = P.Rl[1][0] * J[0][b] + P.Rl[1][1] * J[1][b];
+    T m22 = T(0);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      T v = T(0);
+#pragma unroll
+      for (int b = 0; b < 3; ++b) v += V[a][b] * rj[b];
+      m22 += rj[a] * v;
+    }
     w[i] = T(1) / m22;
   }
-  double C[N][N], I[N][N];
-  matrixc_u<N, N, T>(w, d.S, d.VarBeta, C);
-  invert_sym<N>(C, I);
+}
+
+// BL_Line_fit (broken_line.jl:546-696)
+template <int N, class T>
+BL_HD void line_fit(const float ge[6][N], const Geo<N, T>& G, T B, const Prep<N, T>& P, LineOut& L) {
+  T w[N];
+  line_weights<N, T>(ge, P, w);
+  double d[N], e1[N], e2[N], r[N];
+  band_entries<N, T>(w, P.S, P.VB, d, e1, e2);
+#pragma unroll
+  for (int i = 0; i < N; ++i) r[N - 1 - i] = double(w[i] * P.Z[i]);
+  Band<N, false> f;
+  band_factor<N, false>(d, e1, e2, nullptr, 0.0, f);
+  double ue[N];
+  band_solve<N, false>(f, r, ue);
   double u[N];
 #pragma unroll
-  for (int i = 0; i < N; ++i) {
-    double v = 0;
-#pragma unroll
-    for (int k = 0; k < N; ++k) v += I[i][k] * double(w[k] * d.Z[k]);
-    u[i] = v;
-  }
-  T par0 = (T(u[1]) - T(u[0])) / (d.S[1] - d.S[0]);
-  T par1 = T(u[0]);
-  const double idiff = 1.0 / double(d.S[1] - d.S[0]);
-  double cov[2][2] = {{(I[0][0] - 2 * I[0][1] + I[1][1]) * (idiff * idiff) + double(mult_scatt<T>(d.S[1] - d.S[0], B, f[2], slope)),
+  for (int i = 0; i < N; ++i) u[i] = ue[N - 1 - i];
+  double I[3][3];
+  band_trailing_inverse<N, false>(f, I);
+  // absolute position of hit 0 in the rotated (S, Z) frame
+  const double Sc = double(P.Rl[0][0]) * P.s0 + double(P.Rl[0][1]) * G.h0[2];
+  const double Zc = double(P.Rl[1][0]) * P.s0 + double(P.Rl[1][1]) * G.h0[2];
+  const double dS0 = double(P.S[1]) - double(P.S[0]);
+  double par0 = (u[1] - u[0]) / dS0;
+  double par1 = (u[0] + Zc) - par0 * (double(P.S[0]) + Sc);
+  const double idiff = 1.0 / dS0;
+  double cov[2][2] = {{(I[0][0] - 2 * I[0][1] + I[1][1]) * (idiff * idiff) +
+                           double(mult_scatt<T>(P.S[1] - P.S[0], B, P.R, P.slope)),
                        (I[0][1] - I[0][0]) * idiff},
                       {(I[0][1] - I[0][0]) * idiff, I[0][0]}};
-  double jac[2][2] = {{1, 0}, {-double(d.S[0]), 1}};
-  par1 = par1 - par0 * d.S[0];
+  double jac[2][2] = {{1, 0}, {-(double(P.S[0]) + Sc), 1}};
   sandwich2(jac, cov);
-  const T tmp = R[0][0] - par0 * R[0][1];
-  const T j22 = T(1) / tmp;
-  jac[1][1] = double(j22);
-  jac[0][0] = double(j22 * j22);
+  const double R00 = double(P.Rl[0][0]), R01 = double(P.Rl[0][1]);
+  const double j22 = 1.0 / (R00 - par0 * R01);
+  jac[0][0] = j22 * j22;
   jac[0][1] = 0;
-  jac[1][0] = double(par1 * R[0][1] * (j22 * j22));
+  jac[1][0] = par1 * R01 * (j22 * j22);
+  jac[1][1] = j22;
   par1 = par1 * j22;
-  par0 = (R[0][1] + par0 * R[0][0]) * j22;
+  par0 = (R01 + par0 * R00) * j22;
   sandwich2(jac, cov);
-  L.par[0] = double(par0);
-  L.par[1] = double(par1);
+  L.par[0] = par0;
+  L.par[1] = par1;
   for (int a = 0; a < 2; ++a) for (int b = 0; b < 2; ++b) L.cov[a][b] = cov[a][b];
   T chi2 = 0;
 #pragma unroll
   for (int i = 0; i < N; ++i) {
-    const T diff = d.Z[i] - T(u[i]);
+    const T diff = P.Z[i] - T(u[i]);
     chi2 += w[i] * (diff * diff);
     if (i > 0 && i < N - 1) {
-      const T den1 = d.S[i] - d.S[i - 1], den2 = d.S[i + 1] - d.S[i], den3 = d.S[i] - d.S[i - 1], den4 = d.S[i + 1] - d.S[i - 1];
-      const T t = (T(u[i - 1]) / den1) - (T(u[i]) * (den4 / (den2 * den3))) + (T(u[i + 1]) / (d.S[i + 1] - d.S[i]));
-      chi2 += (t * t) / d.VarBeta[i];
+      const T d1 = P.S[i] - P.S[i - 1], d2 = P.S[i + 1] - P.S[i];
+      const T t = T(u[i - 1]) / d1 - T(u[i]) * ((d1 + d2) / (d2 * d1)) + T(u[i + 1]) / d2;
+      chi2 += (t * t) / P.VB[i];
     }
   }
   L.chi2 = double(chi2);
 }
 
-template <class T>
-__device__ __forceinline__ void translate_karimaki(CircleOut& c, T x0, T y0) {
-  const T p1 = T(c.par[0]), p2 = T(c.par[1]), p3 = T(c.par[2]);
-  const T cs = s_cos<T>(p1), sn = s_sin<T>(p1);
-  const T DP = x0 * cs + y0 * sn;
-  const T DO = x0 * sn - y0 * cs + p2;
-  const T uu = T(1) + p3 * p2;
-  const T C = -p3 * y0 + uu * cs;
-  const T BB = p3 * x0 + uu * sn;
-  const T A = T(2.0) * DO + p3 * (DO * DO + DP * DP);
-  const T U = s_sqrt<T>(T(1.0) + p3 * A);
-  const T xi = T(1.0) / (BB * BB + C * C);
-  const T v = T(1.0) + p3 * DO;
-  const T lambda = (T(0.5) * A) / (U * ((T(1.0) + U) * (T(1.0) + U)));
-  const T mu = T(1.0) / (U * (T(1.0) + U)) + p3 * lambda;
-  const T zeta = DO * DO + DP * DP;
-  const double J[3][3] = {{double(xi * uu * v), double(-xi * (p3 * p3) * DP), double(xi * DP)},
-                          {double(T(2.0) * mu * uu * DP), double(T(2.0) * mu * v), double(mu * zeta - lambda * A)},
+// Karimaki translation of (phi, d, rho) and its covariance to a point (x0, y0) (broken_line.jl:85-127)
+BL_HD void translate_karimaki(CircleOut& c, double x0, double y0) {
+  const double p1 = c.par[0], p2 = c.par[1], p3 = c.par[2];
+  double sn, cs;
+  sincos(p1, &sn, &cs);
+  const double DP = x0 * cs + y0 * sn;
+  const double DO = x0 * sn - y0 * cs + p2;
+  const double uu = 1.0 + p3 * p2;
+  const double C = -p3 * y0 + uu * cs;
+  const double BB = p3 * x0 + uu * sn;
+  const double A = 2.0 * DO + p3 * (DO * DO + DP * DP);
+  const double U = sqrt(1.0 + p3 * A);
+  const double xi = 1.0 / (BB * BB + C * C);
+  const double v = 1.0 + p3 * DO;
+  const double lambda = (0.5 * A) / (U * ((1.0 + U) * (1.0 + U)));
+  const double mu = 1.0 / (U * (1.0 + U)) + p3 * lambda;
+  const double zeta = DO * DO + DP * DP;
+  const double J[3][3] = {{xi * uu * v, -xi * (p3 * p3) * DP, xi * DP},
+                          {2.0 * mu * uu * DP, 2.0 * mu * v, mu * zeta - lambda * A},
                           {0.0, 0.0, 1.0}};
-  c.par[0] = double(bl_atan2<T>(BB, C));
-  c.par[1] = double(A / (T(1.0) + U));
+  c.par[0] = bl_atan2<double>(BB, C);
+  c.par[1] = A / (1.0 + U);
   sandwich3(J, c.cov);
 }
 
-// BL_Circle_fit, broken_line.jl:330-528; returns false where the reference raises
+// BL_Circle_fit (broken_line.jl:330-528); returns false where the reference raises
 template <int N, class T>
-__device__ __forceinline__ bool circle_fit(const T h[3][N], const float ge[6][N], const T f[4], T B, Prepared<N, T>& d,
+BL_HD bool circle_fit(const float ge[6][N], const Geo<N, T>& G, T B, const Prep<N, T>& P,
                                            CircleOut& c) {
   bool ok = true;
-  c.q = d.q;
-  const T slope = -T(c.q) / f[3];
+  c.q = P.q;
+  const T ms_scale = T(1.0) + P.slope * P.slope;
   T VB[N];
 #pragma unroll
-  for (int i = 0; i < N; ++i) VB[i] = d.VarBeta[i] * (T(1.0) + slope * slope);
+  for (int i = 0; i < N; ++i) VB[i] = P.VB[i] * ms_scale;
+  // radial residuals of the hits to the fast-fit circle, which passes through hit 0
+  const T ux = -P.cx, uy = -P.cy;
+  T Z[N], rn[N];
 #pragma unroll
-  for (int i = 0; i < N; ++i) d.Z[i] = s_sqrt<T>(d.radii[0][i] * d.radii[0][i] + d.radii[1][i] * d.radii[1][i]) - f[2];
+  for (int i = 0; i < N; ++i) {
+    rn[i] = s_sqrt<T>(P.rx[i] * P.rx[i] + P.ry[i] * P.ry[i]);
+    const T px = G.p[0][i], py = G.p[1][i];
+    Z[i] = (T(2) * (ux * px + uy * py) + (px * px + py * py)) / (rn[i] + P.R);
+  }
   const double tol = 1e-12;
   T w[N];
 #pragma unroll
@@ -321,19 +444,14 @@ __device__ __forceinline__ bool circle_fit(const T h[3][N], const float ge[6][N]
     auto z = [&](float v) { return fabs(double(v)) < tol ? T(0) : T(v); };
     const T V[2][2] = {{z(ge[0][i]), z(ge[1][i])}, {z(ge[1][i]), z(ge[2][i])}};
     T RR[2][2];
-    rotation_matrix<T>(-d.radii[0][i] / d.radii[1][i], RR);
+    rotation_matrix<T>(-P.rx[i] / P.ry[i], RR);
     const T t0 = RR[1][0] * V[0][0] + RR[1][1] * V[1][0];
     const T t1 = RR[1][0] * V[0][1] + RR[1][1] * V[1][1];
     w[i] = T(1.0) / (t0 * RR[1][0] + t1 * RR[1][1]);
   }
-  constexpr int M = N + 1;
-  double C[M][M];
-#pragma unroll
-  for (int i = 0; i < M; ++i)
-#pragma unroll
-    for (int j = 0; j < M; ++j) C[i][j] = 0.0;
-  matrixc_u<N, M, T>(w, d.s, VB, C);
-  const T* s = d.s;
+  double d[N], e1[N], e2[N], b[N], r[N];
+  band_entries<N, T>(w, P.s, VB, d, e1, e2);
+  const T* s = P.s;
   T cnn = 0;
 #pragma unroll
   for (int i = 0; i < N; ++i) {
@@ -341,57 +459,54 @@ __device__ __forceinline__ bool circle_fit(const T h[3][N], const float ge[6][N]
     if (i > 0 && i < N - 1) v += -(s[i + 1] - s[i - 1]) * (s[i + 1] - s[i - 1]) / (T(2.0) * VB[i] * (s[i + 1] - s[i]) * (s[i] - s[i - 1]));
     if (i > 1) v += (s[i] - s[i - 2]) / (T(2.0) * VB[i - 1] * (s[i] - s[i - 1]));
     if (i < N - 2) v += (s[i + 2] - s[i]) / (T(2.0) * VB[i + 1] * (s[i + 1] - s[i]));
-    C[i][N] = double(v);
-    C[N][i] = double(v);
+    b[N - 1 - i] = double(v);
+    r[N - 1 - i] = double(w[i] * Z[i]);
     if (i > 0 && i < N - 1) cnn += ((s[i + 1] - s[i - 1]) * (s[i + 1] - s[i - 1])) / (T(4.0) * VB[i]);
   }
-  C[N][N] = double(cnn);
-  double I[M][M];
-  invert_sym<M>(C, I);
-  double u[M];
+  Band<N, true> f;
+  band_factor<N, true>(d, e1, e2, b, double(cnn), f);
+  double ue[N + 1];
+  band_solve<N, true>(f, r, ue);
+  double u[N + 1];
 #pragma unroll
-  for (int i = 0; i < M; ++i) {
-    double v = 0;
-#pragma unroll
-    for (int k = 0; k < N; ++k) v += I[i][k] * double(w[k] * d.Z[k]);
-    u[i] = v;
-  }
-#pragma unroll
-  for (int col = 0; col < 2; ++col) {
-    const T t = s_sqrt<T>(d.radii[0][col] * d.radii[0][col] + d.radii[1][col] * d.radii[1][col]);
-    d.radii[0][col] /= t;
-    d.radii[1][col] /= t;
-  }
-  const T tmp1 = -d.Z[0] + T(u[0]);
-  const T dv0 = h[0][0] + tmp1 * d.radii[0][0], dv1 = h[1][0] + tmp1 * d.radii[1][0];
-  const T tmp2 = -d.Z[1] + T(u[1]);
-  const T ev0 = h[0][1] + tmp2 * d.radii[0][1], ev1 = h[1][1] + tmp2 * d.radii[1][1];
-  const T emd0 = ev0 - dv0, emd1 = ev1 - dv1;
-  const T nrm = s_sqrt<T>(emd0 * emd0 + emd1 * emd1);
-  c.par[0] = double(bl_atan2<T>(emd1, emd0));
-  const T inner = f[2] * f[2] - T(0.25) * (nrm * nrm);
-  if (inner < T(0)) ok = false;
-  c.par[1] = double(-T(c.q) * (f[2] - s_sqrt<T>(inner)));
-  c.par[2] = double(T(c.q) * (T(1.0) / f[2] + T(u[N])));
+  for (int i = 0; i < N; ++i) u[i] = ue[N - 1 - i];
+  u[N] = ue[N];
+  double I[3][3];
+  band_trailing_inverse<N, true>(f, I);
+  // fitted points 0 and 1 (hit-0 frame), FP64 from here on
+  const double R = double(P.R);
+  const double n0 = double(rn[0]), n1 = double(rn[1]);
+  const double r0x = double(P.rx[0]) / n0, r0y = double(P.ry[0]) / n0;
+  const double r1x = double(P.rx[1]) / n1, r1y = double(P.ry[1]) / n1;
+  const double tmp1 = u[0] - double(Z[0]);
+  const double dv0 = tmp1 * r0x, dv1 = tmp1 * r0y;
+  const double tmp2 = u[1] - double(Z[1]);
+  const double ev0 = double(G.p[0][1]) + tmp2 * r1x, ev1 = double(G.p[1][1]) + tmp2 * r1y;
+  const double emd0 = ev0 - dv0, emd1 = ev1 - dv1;
+  const double t1 = emd0 * emd0 + emd1 * emd1;
+  c.par[0] = bl_atan2<double>(emd1, emd0);
+  const double inner = R * R - 0.25 * t1;
+  if (inner < 0) ok = false;
+  c.par[1] = -double(c.q) * (0.25 * t1) / (R + sqrt(inner));
+  c.par[2] = double(c.q) * (1.0 / R + u[N]);
   if (!(double(c.q) * c.par[1] <= 0)) ok = false;
-  const T t1 = nrm * nrm;
-  const T fl = T(floor(double(c.q) / 2));
-  const T den = s_sqrt<T>((T(2) * f[2]) * (T(2) * f[2]) - t1);
+  const double fl = floor(double(c.q) / 2);
+  const double den = sqrt((2 * R) * (2 * R) - t1);
   const double J[3][3] = {
-      {double((d.radii[1][0] * emd0 - emd1 * d.radii[0][0]) / t1), double((d.radii[1][1] * emd0 - emd1 * d.radii[0][1]) / t1), 0},
-      {double(fl * (emd0 * d.radii[0][0] + emd1 * d.radii[1][0]) / den), double(fl * (emd0 * d.radii[0][1] + emd1 * d.radii[1][1]) / den), 0},
+      {(r0y * emd0 - emd1 * r0x) / t1, (r1y * emd0 - emd1 * r1x) / t1, 0},
+      {fl * (emd0 * r0x + emd1 * r0y) / den, fl * (emd0 * r1x + emd1 * r1y) / den, 0},
       {0, 0, double(c.q)}};
-  c.cov[0][0] = I[0][0]; c.cov[0][1] = I[0][1]; c.cov[0][2] = I[0][N];
-  c.cov[1][0] = I[1][0]; c.cov[1][1] = I[1][1]; c.cov[1][2] = I[1][N];
-  c.cov[2][0] = I[N][0]; c.cov[2][1] = I[N][1]; c.cov[2][2] = I[N][N];
+  c.cov[0][0] = I[0][0]; c.cov[0][1] = I[0][1]; c.cov[0][2] = I[0][2];
+  c.cov[1][0] = I[1][0]; c.cov[1][1] = I[1][1]; c.cov[1][2] = I[1][2];
+  c.cov[2][0] = I[2][0]; c.cov[2][1] = I[2][1]; c.cov[2][2] = I[2][2];
   sandwich3(J, c.cov);
-  translate_karimaki<T>(c, T(0.5) * emd0, T(0.5) * emd1);
-  c.cov[0][0] += double((T(1) + slope * slope) * mult_scatt<T>(d.S[1] - d.S[0], B, f[2], slope));
-  translate_karimaki<T>(c, dv0, dv1);
+  translate_karimaki(c, 0.5 * emd0, 0.5 * emd1);
+  c.cov[0][0] += double(ms_scale * mult_scatt<T>(P.S[1] - P.S[0], B, P.R, P.slope));
+  translate_karimaki(c, G.h0[0] + dv0, G.h0[1] + dv1);
   T chi2 = 0;
 #pragma unroll
   for (int i = 0; i < N; ++i) {
-    const T diff = d.Z[i] - T(u[i]);
+    const T diff = Z[i] - T(u[i]);
     chi2 += w[i] * (diff * diff);
     if (i > 0 && i < N - 1) {
       const T d1 = s[i] - s[i - 1], d2 = s[i + 1] - s[i], d3 = s[i + 1] - s[i - 1];
@@ -411,21 +526,22 @@ struct TrackOut {
 
 // full fit of one track of N hits: hits[3][N] (FP64 inputs), ge[6][N] (Float32)
 template <int N, class T>
-__device__ __forceinline__ bool fit_track(const double hits[3][N], const float ge[6][N], double Bd, TrackOut& o) {
-  T h[3][N];
+BL_HD bool fit_track(const double hits[3][N], const float ge[6][N], double Bd, TrackOut& o) {
+  Geo<N, T> G;
 #pragma unroll
-  for (int a = 0; a < 3; ++a)
+  for (int a = 0; a < 3; ++a) {
+    G.h0[a] = hits[a][0];
 #pragma unroll
-    for (int i = 0; i < N; ++i) h[a][i] = T(hits[a][i]);
+    for (int i = 0; i < N; ++i) G.p[a][i] = T(hits[a][i] - hits[a][0]);
+  }
   const T B = T(Bd);
-  T f[4];
-  fast_fit<N, T>(h, f);
-  Prepared<N, T> d;
-  prepare<N, T>(h, f, B, d);
+  Prep<N, T> P;
+  fast_fit<N, T>(G, P);
+  prepare<N, T>(G, B, P);
   LineOut L;
-  line_fit<N, T>(ge, f, B, d, L);
+  line_fit<N, T>(ge, G, B, P, L);
   CircleOut C;
-  const bool ok = circle_fit<N, T>(h, ge, f, B, d, C);
+  const bool ok = circle_fit<N, T>(ge, G, B, P, C);
   const double b = 1.0 / Bd;
   o.state[0] = C.par[0]; o.state[1] = C.par[1]; o.state[2] = C.par[2] * b; o.state[3] = L.par[0]; o.state[4] = L.par[1];
   const double cv[15] = {C.cov[0][0], C.cov[0][1], b * C.cov[0][2], 0.0, 0.0, C.cov[1][1], b * C.cov[1][2], 0.0, 0.0,

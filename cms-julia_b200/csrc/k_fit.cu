@@ -2,6 +2,8 @@
 // broken_line_fit_on_gpu.jl:166-203: 3-hit and 4-hit tuples, 5-hit tuples fitted
 // with their first 4 hits, at most 24576 per multiplicity) and the stand-alone
 // fit entry point pxl_bl_fit (3..8 hits, FP64 or mixed precision).
+#include <algorithm>
+
 #include "../../include/pxl.h"
 #include "bl_fit.cuh"
 #include "pxl_internal.cuh"
@@ -42,38 +44,61 @@ __device__ void fit_tuple(const Dev& d, uint64_t g, uint32_t hb, const uint32_t*
   (void)ok;
 }
 
-__global__ void __launch_bounds__(128) k_fit_tuples(Dev d) {
-  const int e = blockIdx.y;
-  const EvInfo& E = d.ev[e];
+// Which tuples are fitted, and with how many hits: 3-hit tuples with 3, 4- and
+// 5-hit tuples with 4 (fit5as4), none flagged duplicate, at most fits_per_mult
+// per multiplicity (the bin is read in decreasing id, so the largest ids win).
+// One block per event: the fitted tuples go to the event's region of fit_list
+// (3-hit from the front, 4-hit from the back) so that every warp of the fit
+// kernel runs one hit count; the others get zero outputs here.
+__global__ void __launch_bounds__(256) k_fit_list(Dev d) {
+  const int e = blockIdx.x;
+  EvInfo& E = d.ev[e];
+  __shared__ uint32_t s_n3, s_n4;
+  if (threadIdx.x == 0) { s_n3 = 0; s_n4 = 0; }
+  __syncthreads();
   const uint64_t tb = E.tuple_base;
-  const uint32_t hb = E.hit_base;
-  // B = Float64(Float32(bf)) as HelixFitOnGPU stores the field (ca_hit_ntuplet_generator.jl:83)
-  const double B = double(d.c.b_field);
-  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < E.n_tuples; t += gridDim.x * blockDim.x) {
+  const uint32_t nt = E.n_tuples;
+  for (uint32_t t = threadIdx.x; t < nt; t += blockDim.x) {
     const uint64_t g = tb + t;
-    const uint32_t h0 = d.tuple_off[g], n = d.tuple_off[g + 1] - h0;
+    const uint32_t n = d.tuple_off[g + 1] - d.tuple_off[g];
     bool fit = n >= 3 && n <= 5 && d.quality[g] != 1;
     if (fit) {
       const uint32_t cnt = E.tm_off[n] - E.tm_off[n - 1];
       if (cnt > d.fits_per_mult) {
-        // the bin is read in decreasing id: only the largest `fits_per_mult` ids are fitted
         uint32_t larger = 0;
-        for (uint32_t u = t + 1; u < E.n_tuples; ++u) {
+        for (uint32_t u = t + 1; u < nt; ++u) {
           const uint64_t gu = tb + u;
           if (d.tuple_off[gu + 1] - d.tuple_off[gu] == n && d.quality[gu] != 1) ++larger;
         }
         fit = larger < d.fits_per_mult;
       }
     }
-    if (!fit) {
-      for (int k = 0; k < 5; ++k) d.t_state[5 * g + k] = 0.f;
-      for (int k = 0; k < 15; ++k) d.t_cov[15 * g + k] = 0.f;
-      d.t_pt[g] = 0.f; d.t_eta[g] = 0.f; d.t_chi2[g] = 0.f; d.t_fitted[g] = 0;
+    if (fit) {
+      if (n == 3) d.fit_list[tb + atomicAdd(&s_n3, 1u)] = t;
+      else d.fit_list[tb + nt - 1 - atomicAdd(&s_n4, 1u)] = t;
       continue;
     }
-    const uint32_t* hits = d.tuple_hits + h0;
-    if (n == 3) fit_tuple<3>(d, g, hb, hits, B);
-    else fit_tuple<4>(d, g, hb, hits, B);  // fit5as4
+    for (int k = 0; k < 5; ++k) d.t_state[5 * g + k] = 0.f;
+    for (int k = 0; k < 15; ++k) d.t_cov[15 * g + k] = 0.f;
+    d.t_pt[g] = 0.f; d.t_eta[g] = 0.f; d.t_chi2[g] = 0.f; d.t_fitted[g] = 0;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) { E.n_fit3 = s_n3; E.n_fit4 = s_n4; }
+}
+
+// one hit count per launch, so that each instantiation keeps only its own registers
+template <int N>
+__global__ void __launch_bounds__(128) k_fit_tuples(Dev d) {
+  const int e = blockIdx.y;
+  const EvInfo& E = d.ev[e];
+  const uint64_t tb = E.tuple_base;
+  const uint32_t hb = E.hit_base;
+  const uint32_t nt = E.n_tuples, nfit = N == 3 ? E.n_fit3 : E.n_fit4;
+  // B = Float64(Float32(bf)) as HelixFitOnGPU stores the field (ca_hit_ntuplet_generator.jl:83)
+  const double B = double(d.c.b_field);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nfit; i += gridDim.x * blockDim.x) {
+    const uint64_t g = tb + d.fit_list[N == 3 ? tb + i : tb + nt - 1 - i];
+    fit_tuple<N>(d, g, hb, d.tuple_hits + d.tuple_off[g], B);
   }
 }
 
@@ -123,9 +148,14 @@ __global__ void __launch_bounds__(128) k_fit_standalone(const double* __restrict
 }  // namespace
 
 void launch_fit(const Dev& d, const Launch& L) {
-  const dim3 g(L.bpe > 0 ? L.bpe : 64, d.E);
-  k_fit_tuples<<<g, 128, 0, L.s>>>(d);
-  L.mark("broken_line_fit");
+  k_fit_list<<<d.E, 256, 0, L.s>>>(d);
+  L.mark("fit_list");
+  // about 7000 fits per PU50 event: enough CTAs for every SM with few events
+  const int bx = std::max(2, std::min(64, (148 * 16) / std::max(1, int(d.E))));
+  k_fit_tuples<3><<<dim3(bx, d.E), 128, 0, L.s>>>(d);
+  L.mark("broken_line_fit_3");
+  k_fit_tuples<4><<<dim3(bx, d.E), 128, 0, L.s>>>(d);
+  L.mark("broken_line_fit_4");
 }
 
 }  // namespace pxl

@@ -238,6 +238,7 @@ int alloc_batch(PxlCtx* ctx) {
   A(tm_bins, d.cap_tuples);
   A(t_state, 5 * d.cap_tuples); A(t_cov, 15 * d.cap_tuples); A(t_pt, d.cap_tuples); A(t_eta, d.cap_tuples);
   A(t_chi2, d.cap_tuples); A(t_fitted, d.cap_tuples);
+  A(fit_list, d.cap_tuples);
   A(htt_cnt, d.cap_hits + 1); A(htt_cur, d.cap_hits); A(htt_list, d.cap_tuple_hits);
   A(dup_cells, d.cap_cells); A(dup_flag, d.cap_cells + 1);
   A(vws_zt, d.cap_tuples); A(vws_ezt2, d.cap_tuples); A(vws_ptt2, d.cap_tuples); A(vws_iv, d.cap_tuples);

@@ -88,6 +88,7 @@ struct EvInfo {
   uint32_t tm_off[9];               // tuple multiplicity offsets (bins 1..8, reference layout)
   uint32_t n_dup_cells, dup_cell_base;
   uint32_t n_cols_nb, n_cols_tr;    // non-empty neighbour / track lists (column store use)
+  uint32_t n_fit3, n_fit4;          // tuples fitted with 3 and with 4 hits (fit5as4 included)
 };
 
 // Everything a kernel may need, passed by value.
@@ -156,6 +157,7 @@ struct Dev {
   uint32_t* tm_bins;       // [cap_tuples] tuple multiplicity, global tuple indices, bins ascending by id
   // fit results [cap_tuples]
   float* t_state; float* t_cov; float* t_pt; float* t_eta; float* t_chi2; uint8_t* t_fitted;
+  uint32_t* fit_list;      // [cap_tuples] per event: 3-hit fits from the front, 4-hit fits from the back
   // hit -> tuple lists
   uint32_t* htt_cnt;       // [cap_hits + 1]
   uint32_t* htt_cur;
