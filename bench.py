@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=160)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile-only", action="store_true")
+    ap.add_argument("--bpe", type=int, default=0, help="blocks per event for the per-event kernels (0: automatic)")
     return ap.parse_args()
 
 
@@ -189,12 +190,18 @@ def main():
     blob, offs = gen.events(E, gen.MODE_PU, pu=args.pu, seed=args.seed + 7919 * rank)
     words = np.diff(offs).sum() // 4
     params = batch_params(E, words_per_event=int(words / E * 1.3) + 4096, hits_per_event_avg=16_000,
-                          doublets_per_event_avg=140_000, tuples_per_event_avg=11_000, device=local)
+                          doublets_per_event_avg=140_000, tuples_per_event_avg=11_000, device=local,
+                          blocks_per_event=args.bpe)
     chain = PixelChain(conds, params)
     stream = torch.cuda.Stream(device=local)
     sh = stream.cuda_stream
 
-    # correctness guard and per-kernel profile (non-graph run)
+    # launch shapes chosen by the autotuner on this batch (outside the timed region)
+    chain.stage_batch(blob, offs, sh)
+    stream.synchronize()
+    tuned = chain.autotune() if args.bpe == 0 else {}
+
+    # correctness guard and per-kernel profile (non-graph run, tuned shapes)
     chain.stage_batch(blob, offs, sh)
     stream.synchronize()
     chain.profile(True)
@@ -326,7 +333,8 @@ def main():
             "vs_baseline": None, "dtype": "int32/f32/f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "events_per_step": E, "pileup": args.pu,
                        "raw_bytes_per_step": int(offs[-1]), "l2": "inputs and intermediates larger than L2",
-                       "parallelism": f"events sharded over {world} GPU(s), no data-path collective"},
+                       "parallelism": f"events sharded over {world} GPU(s), no data-path collective",
+                       "blocks_per_event": tuned or args.bpe},
             "e2e": {"value": e2e_value, "unit": "events/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "plain": {"value": plain_value, "unit": "events/s", "events": npl,
                       "note": "one launch sequence per event, input in HBM"},

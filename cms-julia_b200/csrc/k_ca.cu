@@ -654,48 +654,48 @@ __global__ void k_multiplicity(Dev d) {
 }  // namespace
 
 void launch_ca(const Dev& d, const Launch& L) {
-  const dim3 g(L.bpe > 0 ? L.bpe : 64, d.E);
+  auto g = [&](int seg) { return dim3(L.bpe_of(seg), d.E); };
   const int eb = div_up(d.E + 1, 128);
   uint32_t* pair_cum = d.pair_cum;
   k_items<<<div_up(d.E, 128), 128, 0, L.s>>>(d, pair_cum);
   launch_ev_scan(d, L.s, int(offsetof(EvInfo, n_items)), int(offsetof(EvInfo, item_base)));
   L.mark("doublet_items");
-  k_doublets<false><<<g, 256, 0, L.s>>>(d, pair_cum);
+  k_doublets<false><<<g(kTuneDoublets), 256, 0, L.s>>>(d, pair_cum);
   L.mark("doublets_count");
   excl_scan_u32(d.item_cnt, d.cap_items, &d.ev[d.E].n_items, d.scan_tmp, L.s);
   k_cell_bases<<<eb, 128, 0, L.s>>>(d);
   L.mark("doublets_scan");
-  k_doublets<true><<<g, 256, 0, L.s>>>(d, pair_cum);
+  k_doublets<true><<<g(kTuneDoublets), 256, 0, L.s>>>(d, pair_cum);
   L.mark("doublets_fill");
-  k_zero_counters<<<g, 256, 0, L.s>>>(d);
+  k_zero_counters<<<g(kTuneHitLists), 256, 0, L.s>>>(d);
   // cells ending on each hit
-  k_ohc<0><<<g, 256, 0, L.s>>>(d);
+  k_ohc<0><<<g(kTuneHitLists), 256, 0, L.s>>>(d);
   excl_scan_u32(d.ohc_cnt, d.cap_hits, &d.ev[d.E].n_hits, d.scan_tmp, L.s);
-  k_ohc<1><<<g, 256, 0, L.s>>>(d);
-  k_sort_hit_lists<0><<<g, 256, 0, L.s>>>(d);
+  k_ohc<1><<<g(kTuneHitLists), 256, 0, L.s>>>(d);
+  k_sort_hit_lists<0><<<g(kTuneHitLists), 256, 0, L.s>>>(d);
   L.mark("outer_hit_lists");
   // connection and neighbour lists
-  k_connect<0><<<g, 256, 0, L.s>>>(d);
+  k_connect<0><<<g(kTuneConnect), 256, 0, L.s>>>(d);
   L.mark("connect");
   excl_scan_u32(d.cn_cnt, d.cap_cells, &d.ev[d.E].n_cells_raw, d.scan_tmp, L.s);
-  k_connect<1><<<g, 256, 0, L.s>>>(d);
-  k_sort_cell_lists<0><<<g, 256, 0, L.s>>>(d);
+  k_connect<1><<<g(kTuneCellLists), 256, 0, L.s>>>(d);
+  k_sort_cell_lists<0><<<g(kTuneCellLists), 256, 0, L.s>>>(d);
   L.mark("neighbour_lists");
-  k_fishbone<<<g, 128, 0, L.s>>>(d);
+  k_fishbone<<<g(kTuneFishbone), 128, 0, L.s>>>(d);
   L.mark("fishbone");
   // ntuplets
-  k_ntuplets<false><<<g, 128, 0, L.s>>>(d);
+  k_ntuplets<false><<<g(kTuneNtuplets), 128, 0, L.s>>>(d);
   L.mark("ntuplets_count");
   excl_scan_u64(d.tstart_cnt, d.cap_cells, &d.ev[d.E].n_cells_raw, d.scan_tmp64, L.s);
   k_tuple_bases<<<eb, 128, 0, L.s>>>(d);
-  k_ntuplets<true><<<g, 128, 0, L.s>>>(d);
+  k_ntuplets<true><<<g(kTuneNtuplets), 128, 0, L.s>>>(d);
   k_tuple_ends<<<div_up(d.E, 128), 128, 0, L.s>>>(d);
   L.mark("ntuplets_fill");
   excl_scan_u32(d.ct_cnt, d.cap_cells, &d.ev[d.E].n_cells_raw, d.scan_tmp, L.s);
-  k_cell_tracks_fill<<<g, 256, 0, L.s>>>(d);
-  k_sort_cell_lists<1><<<g, 256, 0, L.s>>>(d);
+  k_cell_tracks_fill<<<g(kTuneCellTracks), 256, 0, L.s>>>(d);
+  k_sort_cell_lists<1><<<g(kTuneCellTracks), 256, 0, L.s>>>(d);
   L.mark("cell_tracks");
-  k_early_dup<<<g, 256, 0, L.s>>>(d);
+  k_early_dup<<<g(kTuneEarlyDup), 256, 0, L.s>>>(d);
   k_multiplicity<<<d.E, 256, 0, L.s>>>(d);
   L.mark("dup_multiplicity");
 }

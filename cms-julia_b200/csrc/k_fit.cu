@@ -151,7 +151,8 @@ void launch_fit(const Dev& d, const Launch& L) {
   k_fit_list<<<d.E, 256, 0, L.s>>>(d);
   L.mark("fit_list");
   // about 7000 fits per PU50 event: enough CTAs for every SM with few events
-  const int bx = std::max(2, std::min(64, (148 * 16) / std::max(1, int(d.E))));
+  const int bx = (L.tune && L.tune[kTuneFitTuples] > 0) ? L.tune[kTuneFitTuples]
+                                                         : std::max(2, std::min(64, (148 * 16) / std::max(1, int(d.E))));
   k_fit_tuples<3><<<dim3(bx, d.E), 128, 0, L.s>>>(d);
   L.mark("broken_line_fit_3");
   k_fit_tuples<4><<<dim3(bx, d.E), 128, 0, L.s>>>(d);

@@ -430,20 +430,20 @@ __global__ void __launch_bounds__(kVtxThreads) k_vertices(Dev d) {
 }  // namespace
 
 void launch_classify(const Dev& d, const Launch& L) {
-  const dim3 g(L.bpe > 0 ? L.bpe : 64, d.E);
-  k_classify<<<g, 256, 0, L.s>>>(d);
+  auto g = [&](int seg) { return dim3(L.bpe_of(seg), d.E); };
+  k_classify<<<g(kTuneClassify), 256, 0, L.s>>>(d);
   L.mark("classify");
-  k_dup_cells<0><<<g, 256, 0, L.s>>>(d);
+  k_dup_cells<0><<<g(kTuneClassify), 256, 0, L.s>>>(d);
   excl_scan_u32(d.dup_flag, d.cap_cells, &d.ev[d.E].n_cells_raw, d.scan_tmp, L.s);
-  k_dup_cells<1><<<g, 256, 0, L.s>>>(d);
+  k_dup_cells<1><<<g(kTuneClassify), 256, 0, L.s>>>(d);
   L.mark("dup_cell_list");
   k_fast_dup<<<div_up(d.E, 4), 128, 0, L.s>>>(d);
   L.mark("fast_duplicate_remover");
-  k_hit_to_tuple<0><<<g, 256, 0, L.s>>>(d);
+  k_hit_to_tuple<0><<<g(kTuneHitToTuple), 256, 0, L.s>>>(d);
   excl_scan_u32(d.htt_cnt, d.cap_hits, &d.ev[d.E].n_hits, d.scan_tmp, L.s);
-  k_hit_to_tuple<1><<<g, 256, 0, L.s>>>(d);
+  k_hit_to_tuple<1><<<g(kTuneHitToTuple), 256, 0, L.s>>>(d);
   L.mark("hit_to_tuple");
-  k_triplet_cleaner<<<g, 256, 0, L.s>>>(d);
+  k_triplet_cleaner<<<g(kTuneHitToTuple), 256, 0, L.s>>>(d);
   L.mark("triplet_cleaner");
 }
 

@@ -265,6 +265,7 @@ int run_chain(PxlCtx* ctx, uint32_t mask, cudaStream_t s) {
   Dev& d = ctx->d;
   if (d.E <= 0) return 0;
   Launch L{s, d.bpe, 256, (ctx->prof.on && !ctx->capturing) ? &ctx->prof : nullptr};
+  L.tune = ctx->tune;
   if ((mask & PXL_STAGE_DIGIS) && L.prof) ctx->prof.n = 0;
   // stages run in chain order; a producer boundary may stop after any of them and a
   // later call (pxl_event_continue) resumes from the products already on the device
@@ -536,6 +537,57 @@ int32_t pxl_profile_read(PxlCtx* ctx, float* ms, const char** names, int32_t max
     if (names) names[k] = ctx->prof.name[i];
   }
   return k;
+}
+
+int32_t pxl_autotune(PxlCtx* ctx, const int32_t* candidates, int32_t n_candidates, int32_t reps, int32_t* chosen) {
+  if (!ctx || !candidates || n_candidates <= 0 || n_candidates > 32 || reps <= 0) return PXL_ERR_ARG;
+  if (ctx->d.E <= 0) return PXL_ERR_STATE;
+  for (int i = 0; i < n_candidates; ++i)
+    if (candidates[i] <= 0 || candidates[i] > 4096) return PXL_ERR_ARG;
+  // timed segments (names given by the launchers) and the stage each one tunes
+  static const struct { const char* name; int seg; } kMap[] = {
+      {"doublets_count", kTuneDoublets}, {"doublets_fill", kTuneDoublets}, {"outer_hit_lists", kTuneHitLists},
+      {"connect", kTuneConnect}, {"neighbour_lists", kTuneCellLists}, {"fishbone", kTuneFishbone},
+      {"ntuplets_count", kTuneNtuplets}, {"ntuplets_fill", kTuneNtuplets}, {"cell_tracks", kTuneCellTracks},
+      {"dup_multiplicity", kTuneEarlyDup}, {"classify", kTuneClassify}, {"dup_cell_list", kTuneClassify},
+      {"hit_to_tuple", kTuneHitToTuple}, {"triplet_cleaner", kTuneHitToTuple},
+      {"broken_line_fit_3", kTuneFitTuples}, {"broken_line_fit_4", kTuneFitTuples}};
+  cudaSetDevice(ctx->p.device);
+  const bool prof_was = ctx->prof.on;
+  int rc = pxl_profile_enable(ctx, 1);
+  if (rc) return rc;
+  double best_t[kTuneCount];
+  int best_b[kTuneCount];
+  for (int s = 0; s < kTuneCount; ++s) { best_t[s] = 1e300; best_b[s] = 0; }
+  for (int c = 0; c < n_candidates; ++c) {
+    for (int s = 0; s < kTuneCount; ++s) ctx->tune[s] = candidates[c];
+    double acc[kTuneCount] = {};
+    for (int r = 0; r <= reps; ++r) {  // the first run of each shape is a warm-up
+      rc = run_chain(ctx, 0x3F, ctx->stream);
+      if (rc) break;
+      CK(cudaStreamSynchronize(ctx->stream));
+      CK(cudaGetLastError());
+      if (r == 0) continue;
+      for (int i = 1; i < ctx->prof.n; ++i) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ctx->prof.ev[i - 1], ctx->prof.ev[i]));
+        for (const auto& m : kMap)
+          if (std::strcmp(m.name, ctx->prof.name[i]) == 0) acc[m.seg] += ms;
+      }
+    }
+    if (rc) break;
+    for (int s = 0; s < kTuneCount; ++s)
+      if (acc[s] < best_t[s]) { best_t[s] = acc[s]; best_b[s] = candidates[c]; }
+  }
+  for (int s = 0; s < kTuneCount; ++s) {
+    ctx->tune[s] = rc ? 0 : best_b[s];
+    if (chosen) chosen[s] = ctx->tune[s];
+  }
+  ctx->last_mask = 0x3F;
+  ctx->done_mask = 0x3F;
+  ctx->ev_host_valid = false;
+  pxl_profile_enable(ctx, prof_was ? 1 : 0);
+  return rc;
 }
 
 int32_t pxl_sync(PxlCtx* ctx) {

@@ -34,6 +34,8 @@ struct PxlCtx {
   // per-kernel timing of non-graph runs
   pxl::Prof prof;
   bool capturing = false;
+  // blocks per event of the tunable stages (0 = the default shape), set by pxl_autotune
+  int tune[pxl::kTuneCount] = {};
 };
 
 // reads the events' counters back (synchronises the context stream)

@@ -231,11 +231,22 @@ struct Prof {
   const char* name[kMax] = {};
 };
 
+// Stages whose launch shape (blocks per event) the autotuner chooses.
+enum TuneSeg : int {
+  kTuneDoublets, kTuneHitLists, kTuneConnect, kTuneCellLists, kTuneFishbone, kTuneNtuplets, kTuneCellTracks,
+  kTuneEarlyDup, kTuneClassify, kTuneHitToTuple, kTuneFitTuples, kTuneCount
+};
+
 struct Launch {
   cudaStream_t s;
   int bpe;        // blocks per event
   int tpb;        // threads per block
   Prof* prof = nullptr;
+  const int* tune = nullptr;  // [kTuneCount] blocks per event per stage, 0 = bpe
+  int bpe_of(int seg) const {
+    const int b = (tune && tune[seg] > 0) ? tune[seg] : bpe;
+    return b > 0 ? b : 64;
+  }
   void mark(const char* nm) const {
     if (prof && prof->on && prof->n < Prof::kMax) {
       cudaEventRecord(prof->ev[prof->n], s);

@@ -13,6 +13,9 @@ PXL_ERR = {-1: "bad argument", -2: "CUDA error", -3: "bad conditions", -4: "capa
 STAGE_DIGIS, STAGE_HITS, STAGE_TUPLES, STAGE_FIT, STAGE_CLASSIFY, STAGE_VERTICES = 1, 2, 4, 8, 16, 32
 STAGE_ALL = 0x3F
 
+TUNE_STAGES = ("doublets", "hit_lists", "connect", "cell_lists", "fishbone", "ntuplets", "cell_tracks",
+               "early_dup", "classify", "hit_to_tuple", "fits")
+
 WARN_BITS = {
     0x1: "modules", 0x2: "pixels_per_module", 0x4: "clusters_per_module", 0x8: "hits_clamped",
     0x10: "doublets", 0x20: "columns", 0x40: "tuples", 0x80: "fit_domain", 0x100: "fits_capped",
@@ -68,6 +71,8 @@ _SIGS = {
     "pxl_graph_capture": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32]),
     "pxl_graph_launch": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p]),
     "pxl_sync": (ctypes.c_int32, [ctypes.c_void_p]),
+    "pxl_autotune": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                      ctypes.c_void_p]),
     "pxl_graph_kernel_nodes": (ctypes.c_int32, [ctypes.c_void_p]),
     "pxl_results_async": (ctypes.c_int64, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]),
     "pxl_profile_enable": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_int32]),

@@ -212,6 +212,17 @@ int32_t pxl_graph_kernel_nodes(PxlCtx* ctx);
 int32_t pxl_profile_enable(PxlCtx* ctx, int32_t on);
 int32_t pxl_profile_read(PxlCtx* ctx, float* ms, const char** names, int32_t max);
 
+/* Launch-shape autotuner. Runs the whole chain on the batch staged last (pxl_batch_stage or
+ * pxl_batch_run) once per candidate blocks-per-event value (each shape warmed up once, then
+ * timed reps times with per-stage CUDA events) and keeps, for each tunable stage (doublets,
+ * hit lists, connect, cell lists, fishbone, ntuplets, cell tracks, early duplicates,
+ * classification, hit-to-tuple, fits), the fastest value. The choice holds for later runs
+ * and graph captures of this context. chosen[PXL_TUNE_STAGES] (may be NULL) receives it.
+ * Products of the staged batch are recomputed. No counterpart in the reference, whose
+ * serial loops have no launch shape. */
+#define PXL_TUNE_STAGES 11
+int32_t pxl_autotune(PxlCtx* ctx, const int32_t* candidates, int32_t n_candidates, int32_t reps, int32_t* chosen);
+
 /* Waits for the context's work; returns 0, the OR of the events' PXL_WARN_* bits, or < 0. */
 int32_t pxl_sync(PxlCtx* ctx);
 
