@@ -99,6 +99,90 @@ __global__ void k_fast_dup(Dev d) {
   }
 }
 
+// The same remover with the event's qualities in shared memory: one warp per event
+// stages the static part of 32 dup cells at a time (track lists and |tip|) into
+// shared memory, then walks the cells in order with shared-memory reads only. The
+// argmin takes the smallest |tip| bit pattern (|tip| >= 0 orders as its bits) and,
+// among equal ones, the first position: the reference's strict < in list order.
+constexpr int kDupMaxTuples = 32768;  // qualities of one event in shared memory
+constexpr int kDupStage = 1024;       // staged track entries per batch of cells
+
+__global__ void __launch_bounds__(32) k_fast_dup_smem(Dev d) {
+  __shared__ uint8_t s_q[kDupMaxTuples];
+  __shared__ uint16_t s_t[kDupStage];
+  __shared__ uint32_t s_tip[kDupStage];
+  __shared__ uint32_t s_off[33];
+  __shared__ uint32_t s_l0[32];
+  const int e = blockIdx.x;
+  const unsigned lane = threadIdx.x;
+  const EvInfo& E = d.ev[e];
+  const uint64_t tb = E.tuple_base;
+  const uint32_t nt = E.n_tuples;
+  if (nt > uint32_t(kDupMaxTuples)) return;  // k_fast_dup handles such events
+  const uint32_t lo = d.dup_flag[E.cell_base], hi = d.dup_flag[uint64_t(E.cell_base) + E.n_cells_raw];
+  if (lo == hi) return;
+  for (uint32_t t = lane; t < nt; t += 32) s_q[t] = d.quality[tb + t];
+  for (uint32_t q0 = lo; q0 < hi;) {
+    // stage up to 32 cells: list start and length (capped at kCellRows)
+    const uint32_t q = q0 + lane;
+    uint32_t n = 0, l0 = 0;
+    if (q < hi) {
+      const uint32_t c = d.dup_cells[q];
+      l0 = d.ct_cnt[c];
+      n = d.ct_cnt[c + 1] - l0;
+      if (n > uint32_t(kCellRows)) n = kCellRows;
+    }
+    const uint32_t inc = warp_incl_scan(n);
+    const bool fits = q < hi && inc <= uint32_t(kDupStage);
+    const uint32_t ncell = __popc(__ballot_sync(0xffffffffu, fits));
+    if (fits) { s_off[lane] = inc - n; s_l0[lane] = l0; }
+    const uint32_t total = __shfl_sync(0xffffffffu, inc, ncell - 1);
+    if (lane == 0) s_off[ncell] = total;
+    __syncwarp();
+    for (uint32_t x = lane; x < total; x += 32) {
+      uint32_t a = 0, b = ncell;  // last cell whose offset <= x
+      while (b - a > 1) {
+        const uint32_t m = (a + b) >> 1;
+        if (s_off[m] <= x) a = m; else b = m;
+      }
+      const uint32_t t = d.ct_list[s_l0[a] + (x - s_off[a])];
+      s_t[x] = uint16_t(t - tb);
+      s_tip[x] = __float_as_uint(fabsf(d.t_state[5 * size_t(t) + 1]));
+    }
+    __syncwarp();
+    for (uint32_t k = 0; k < ncell; ++k) {
+      const uint32_t o = s_off[k], nk = s_off[k + 1] - o;
+      uint32_t key0 = 0xffffffffu, key1 = 0xffffffffu;
+      uint16_t t0 = 0, t1 = 0;
+      if (lane < nk) {
+        t0 = s_t[o + lane];
+        if (s_q[t0] == 2) key0 = s_tip[o + lane];
+      }
+      if (lane + 32 < nk) {
+        t1 = s_t[o + lane + 32];
+        if (s_q[t1] == 2) key1 = s_tip[o + lane + 32];
+      }
+      // |tip| < 10000 as the reference's initial best (mc = 10000, strict <)
+      const uint32_t lim = __float_as_uint(10000.f);
+      if (key0 >= lim) key0 = 0xffffffffu;
+      if (key1 >= lim) key1 = 0xffffffffu;
+      const uint32_t kmin = __reduce_min_sync(0xffffffffu, key0 < key1 ? key0 : key1);
+      uint32_t im = 0xffffffffu;
+      if (kmin != 0xffffffffu) {
+        const uint32_t pos = __reduce_min_sync(0xffffffffu, key0 == kmin ? lane : (key1 == kmin ? lane + 32 : 0xffffffffu));
+        im = s_t[o + pos];
+      }
+      __syncwarp();
+      if (lane < nk && s_q[t0] != 0 && t0 != im) s_q[t0] = 1;
+      if (lane + 32 < nk && s_q[t1] != 0 && t1 != im) s_q[t1] = 1;
+      __syncwarp();
+    }
+    q0 += ncell;
+  }
+  __syncwarp();
+  for (uint32_t t = lane; t < nt; t += 32) d.quality[tb + t] = s_q[t];
+}
+
 // hit -> loose tuple lists
 template <int kPass>
 __global__ void k_hit_to_tuple(Dev d) {
@@ -437,7 +521,8 @@ void launch_classify(const Dev& d, const Launch& L) {
   excl_scan_u32(d.dup_flag, d.cap_cells, &d.ev[d.E].n_cells_raw, d.scan_tmp, L.s);
   k_dup_cells<1><<<g(kTuneClassify), 256, 0, L.s>>>(d);
   L.mark("dup_cell_list");
-  k_fast_dup<<<div_up(d.E, 4), 128, 0, L.s>>>(d);
+  if (d.tuples_per_event > uint32_t(kDupMaxTuples)) k_fast_dup<<<div_up(d.E, 4), 128, 0, L.s>>>(d);
+  else k_fast_dup_smem<<<d.E, 32, 0, L.s>>>(d);
   L.mark("fast_duplicate_remover");
   k_hit_to_tuple<0><<<g(kTuneHitToTuple), 256, 0, L.s>>>(d);
   excl_scan_u32(d.htt_cnt, d.cap_hits, &d.ev[d.E].n_hits, d.scan_tmp, L.s);
