@@ -48,6 +48,9 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=160)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile-only", action="store_true")
+    ap.add_argument("--fit-tracks", type=int, default=1 << 20)
+    ap.add_argument("--fit-oracle-sample", type=int, default=4000)
+    ap.add_argument("--no-fits", action="store_true")
     ap.add_argument("--bpe", type=int, default=0, help="blocks per event for the per-event kernels (0: automatic)")
     return ap.parse_args()
 
@@ -116,16 +119,100 @@ def segment_bytes(name: str, c: dict) -> float | None:
     table = {
         "unpack_calib": 4 * D + 22 * D,            # words in; xx,yy,adc,moduleInd,clus,pdigi,rawId out
         "module_starts": 4 * D,                    # moduleInd read by the count and fill passes
-        "find_clus_charge_cut": 14 * D,            # moduleInd,x,y,adc in; clus out
-        "get_hits": 14 * D + 44 * H,               # digis in; 44 B hit SoA out
+        "find_clus_warp": 14 * D,                  # moduleInd,x,y,adc in; clus (and moduleInd) out
+        "get_hits_warp": 14 * D + 44 * H,          # digis in; 44 B hit SoA out
         "phi_binner": 4 * H,                       # iphi in; bins out
         "doublets_count": 14 * I + 4 * I,          # inner hit fields in; count out
         "doublets_fill": 14 * I + 4 * I + 22 * C,  # + cell SoA out
         "connect": 28 * C + 16 * C,                # cell fields in; neighbour masks out
-        "broken_line_fit": 22 * TH + 4 * TH + 8 * T + 93 * T,
+        "broken_line_fit_4": 22 * TH + 4 * TH + 8 * T + 93 * T,
         "vertices": 4 * T + 80 * T,
     }
     return table.get(name)
+
+
+# dram__bytes_read.sum + dram__bytes_write.sum per unit of work, from ncu captures of the
+# 300-event case (profiles/), scaled to a launch by the units it processes
+TRAFFIC_PER_UNIT = {
+    "find_clus_warp": ("words", (125.75e6 + 38.76e6) / 12_349_460),
+    "get_hits_warp": ("words", (182.15e6 + 103.86e6) / 12_349_460),
+    "doublets_fill": ("cells", (374.91e6 + 786.06e6) / 25_257_080),
+    "vertices": ("tuples", (79.25e6 + 18.84e6) / 2_062_854),
+}
+
+FIT_B = 0.0114256972711507  # 1/(pT R) at 3.8 T, GeV^-1 cm^-1
+
+
+def bench_fits(args, local: int, rank: int, world: int) -> dict:
+    """Stand-alone broken-line fits of 2^20 synthetic tracks of 3..8 hits (mix 30/40/20/10 %
+    for 3/4/5/6-8): fits/s in mixed precision and in FP64, per-parameter error of the mixed
+    mode against the FP64 mode on every track, and of the FP64 mode against the CPU oracle on
+    a sample. Inputs resident in HBM (about 210 MB, larger than L2)."""
+    import torch
+    from pixeltrack import gen
+    from pixeltrack.fits import bl_fit, workspace
+    n = args.fit_tracks
+    w = gen.fit_tracks(n, seed=args.seed + 104729 * rank)
+    dev = torch.device("cuda", local)
+    hits = torch.as_tensor(w["hits"]).to(dev)
+    ge = torch.as_tensor(w["ge"]).to(dev)
+    offs = torch.as_tensor(w["offsets"]).to(dev)
+    ws = workspace(n, dev)
+    stream = torch.cuda.Stream(device=dev)
+    out = {}
+    res = {}
+    with torch.cuda.stream(stream):
+        for prec, name in ((1, "mixed"), (0, "fp64")):
+            for _ in range(args.warmup):
+                r = bl_fit(hits, ge, offs, FIT_B, precision=prec, stream=stream, ws=ws)
+            stream.synchronize()
+            t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0.record(stream)
+            for _ in range(args.steps):
+                r = bl_fit(hits, ge, offs, FIT_B, precision=prec, stream=stream, ws=ws)
+            t1.record(stream)
+            t1.synchronize()
+            ms = t0.elapsed_time(t1) / args.steps
+            res[name] = {k: v.double().cpu().numpy() for k, v in r.items() if k in ("state", "pt", "status")}
+            out[name] = {"fits_per_s": world * n / (ms / 1e3), "ms_per_step": ms}
+    nh = np.diff(w["offsets"]).astype(np.int64)
+    bytes_per_step = 48 * int(nh.sum()) + 4 * (n + 1) + (5 + 15 + 3) * 4 * n + 4 * n
+    peak, peak_kind = load_peaks()
+    for name in out:
+        gbs = bytes_per_step / (out[name]["ms_per_step"] / 1e3) / 1e9
+        out[name]["hbm"] = {"achieved": gbs, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": gbs / peak,
+                            "algorithmic_bytes_per_step": bytes_per_step}
+    # per-parameter error of the mixed mode against the FP64 mode (all tracks)
+    a, b = res["mixed"]["state"], res["fp64"]["state"]
+    ok = np.all(np.isfinite(b), axis=1) & (res["fp64"]["status"] == 0)
+    d = np.abs(a[ok] - b[ok])
+    stats = lambda v: {"median": float(np.median(v)), "p99": float(np.percentile(v, 99)), "max": float(v.max())}
+    err = {"q_over_pt_rel": stats(d[:, 2] / np.abs(b[ok, 2])), "phi_abs_rad": stats(d[:, 0]),
+           "cot_theta_rel": stats(d[:, 3] / np.maximum(np.abs(b[ok, 3]), 1e-3)),
+           "d0_abs_cm": stats(d[:, 1]), "z0_abs_cm": stats(d[:, 4]), "tracks": int(ok.sum())}
+    # FP64 mode against the CPU oracle on a sample (the oracle stores FP64, the GPU FP32)
+    m = min(args.fit_oracle_sample, n)
+    st, _, _ = oracle_fit_sample(w, m)
+    okm = np.all(np.isfinite(st), axis=1)
+    rel = np.abs(res["fp64"]["state"][:m][okm] - st[okm]) / np.maximum(np.abs(st[okm]), 1e-6)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle import oracle
+        k = min(n, 200_000)
+        _, _, dt = oracle.bl_fit_batch(w["hits"][: w["offsets"][k]], w["ge"][: w["offsets"][k]], w["offsets"][: k + 1],
+                                       FIT_B, 1)
+        cpu = {"value": k / dt, "unit": "fits/s", "cores": 1, "kind": "port",
+               "sample": f"{k} of the {n} tracks, FP64 oracle fit, one thread"}
+    return {"workload": f"2^{int(np.log2(n))} synthetic tracks, 3-8 hits (30/40/20/10 % for 3/4/5/6-8), helices with "
+                        "0.02 X0 scattering kinks, 10 um r-phi / 20 um z smearing",
+            "tracks": n, "mixed": out["mixed"], "fp64": out["fp64"], "err_mixed_vs_fp64": err,
+            "fp64_vs_oracle": {"max_rel": float(rel.max()), "tracks": int(okm.sum())},
+            "cpu_baseline": cpu}
+
+
+def oracle_fit_sample(w: dict, m: int):
+    from oracle import oracle
+    return oracle.bl_fit_batch(w["hits"][: w["offsets"][m]], w["ge"][: w["offsets"][m]], w["offsets"][: m + 1], FIT_B, 1)
 
 
 def load_peaks() -> tuple[float, str]:
@@ -309,8 +396,10 @@ def main():
     roofline = None
     if dom:
         achieved = (dom_bytes / (seg_ms[dom] / 1e3) / 1e9) if dom_bytes else None
+        tu = TRAFFIC_PER_UNIT.get(dom)
+        traffic = tu[1] * totals[tu[0]] if tu else None
         roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
-                    "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": None,
+                    "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                     "ms_per_launch": seg_ms[dom], "algorithmic_bytes_per_launch": dom_bytes}
 
     # CPU baseline: the oracle (serial restatement of the reference) on the host cores
@@ -326,6 +415,8 @@ def main():
         cpu = {"value": n / t, "unit": "events/s", "cores": threads, "kind": "port",
                "sample": f"{n} of the {E} PU{int(args.pu)} events, full chain, {threads} event-parallel threads"}
 
+    fits = None if args.no_fits else bench_fits(args, local, rank, world)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "events/s", "n_gpus": world, "steps": args.steps,
@@ -340,7 +431,7 @@ def main():
                       "note": "one launch sequence per event, input in HBM"},
             "batched_over_plain": value / world / plain_value,
             "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": kernels_per_step * args.steps,
-            "clocks": clk.summary(), "segments_ms": seg_ms, "totals": totals, "warnings": warn,
+            "clocks": clk.summary(), "segments_ms": seg_ms, "totals": totals, "warnings": warn, "fits": fits,
             "vertices_per_event": nv_check / E,
         }
         print(json.dumps(line), flush=True)

@@ -76,6 +76,43 @@ BL_HD void rotation_matrix(T slope, T R[2][2]) {
   R[0][0] = a; R[0][1] = b; R[1][0] = -b; R[1][1] = a;
 }
 
+// Power of the point p with respect to the circle through the local origin whose
+// centre is -u: |u + p|^2 - |u|^2 = 2 u.p + |p|^2. For a hit near the circle the two
+// terms cancel (u is a radius long, p a chord), so in FP32 the products and sums are
+// carried with their exact rounding errors (fma two-product and two-sum, the Dot2
+// scheme of Ogita, Rump and Oishi): the result is as accurate as the inputs allow.
+template <class T>
+BL_HD T power_of_point(T ux, T uy, T px, T py) {
+  if constexpr (sizeof(T) == 8) {
+    return T(2) * (ux * px + uy * py) + (px * px + py * py);
+  } else {
+    auto two_sum = [](T a, T b, T& e) { const T s = a + b; const T z = s - a; e = (a - (s - z)) + (b - z); return s; };
+    const T p1 = ux * px, e1 = fmaf(ux, px, -p1);
+    const T p2 = uy * py, e2 = fmaf(uy, py, -p2);
+    const T q1 = px * px, f1 = fmaf(px, px, -q1);
+    const T q2 = py * py, f2 = fmaf(py, py, -q2);
+    T es, et, eh;
+    const T sp = two_sum(p1, p2, es);
+    const T sq = two_sum(q1, q2, et);
+    const T h = two_sum(T(2) * sp, sq, eh);
+    return h + (eh + T(2) * (e1 + e2 + es) + (f1 + f2 + et));
+  }
+}
+
+// a*d - b*c with the rounding of both products compensated in FP32 (Kahan's
+// fma-based difference of products); exact enough for nearly parallel chords
+template <class T>
+BL_HD T diff_of_products(T a, T d, T b, T c) {
+  if constexpr (sizeof(T) == 8) {
+    return a * d - b * c;
+  } else {
+    const T w = b * c;
+    const T e = fmaf(-b, c, w);
+    const T f = fmaf(a, d, -w);
+    return f + e;
+  }
+}
+
 // --------------------------------------------------------------- band solver
 // Symmetric positive-definite system of N hit unknowns (pentadiagonal block)
 // and, when Border, one extra unknown coupled to every hit. Arrays are in
@@ -248,7 +285,7 @@ BL_HD void fast_fit(const Geo<N, T>& G, Prep<N, T>& P) {
   const T a1 = G.p[0][mid], a2 = G.p[1][mid];
   const T b1 = G.p[0][N - 1] - G.p[0][mid], b2 = G.p[1][N - 1] - G.p[1][mid];
   const T c1 = -G.p[0][N - 1], c2 = -G.p[1][N - 1];
-  const T ca = c1 * a2 - c2 * a1;
+  const T ca = diff_of_products<T>(c1, a2, c2, a1);
   const T nc = c1 * c1 + c2 * c2, na = a1 * a1 + a2 * a2;
   const T tmp = T(0.5) / ca;
   P.cx = -(a2 * nc + c2 * na) * tmp;
@@ -435,7 +472,7 @@ BL_HD bool circle_fit(const float ge[6][N], const Geo<N, T>& G, T B, const Prep<
   for (int i = 0; i < N; ++i) {
     rn[i] = s_sqrt<T>(P.rx[i] * P.rx[i] + P.ry[i] * P.ry[i]);
     const T px = G.p[0][i], py = G.p[1][i];
-    Z[i] = (T(2) * (ux * px + uy * py) + (px * px + py * py)) / (rn[i] + P.R);
+    Z[i] = power_of_point<T>(ux, uy, px, py) / (rn[i] + P.R);
   }
   const double tol = 1e-12;
   T w[N];

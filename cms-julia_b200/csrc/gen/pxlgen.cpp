@@ -599,4 +599,129 @@ int pxlgen_events(uint64_t seed, int32_t n_events, int32_t mode, double pu, int3
 
 void pxlgen_free(void* p) { std::free(p); }
 
+// ---------------------------------------------------------------- fit workload
+// Helices for the stand-alone fits: an 8-layer barrel telescope made of the four
+// pixel layers above (hits there carry the module id, for alignment) and four
+// outer cylinders at 20/24/28/32 cm, so that tracks of 6 to 8 hits exist.
+// Hit count mix 30/40/20/10 % for 3/4/5/6-8 hits; 1/pT uniform in [0.1, 2] GeV^-1,
+// |eta| < 1, z0 ~ N(0, 5 cm), transverse origin ~ N(0, 10 um); at every layer a
+// multiple-scattering kink of 0.02 X0 (Highland), then the measured point is
+// smeared by N(0, 10 um) along r-phi and N(0, 20 um) along z. Each track draws
+// from its own counter-based random stream, so results do not depend on threads.
+int32_t pxlgen_module_positions(double* out) {  // [1856][3] module centres (cm)
+  const Geometry& g = geom();
+  for (int m = 0; m < kModules; ++m)
+    for (int j = 0; j < 3; ++j) out[3 * m + j] = g.mods[m].p[j];
+  return kModules;
+}
+
+int32_t pxlgen_fit_tracks(uint64_t seed, int32_t n_tracks, int32_t n_threads, double* hits, float* ge,
+                          int32_t* offsets, int16_t* module, double* truth) {
+  if (n_tracks < 0 || !hits || !ge || !offsets || !module) return -1;
+  static const double kR[8] = {2.9, 6.8, 10.9, 16.0, 20.0, 24.0, 28.0, 32.0};
+  static const double kHalf[8] = {26.0, 26.0, 26.0, 26.0, 60.0, 60.0, 60.0, 60.0};
+  const double s_rphi = 10e-4, s_z = 20e-4;
+  struct Rng {  // splitmix64 stream
+    uint64_t x;
+    uint64_t next() { uint64_t z = (x += 0x9e3779b97f4a7c15ull); z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+                      z = (z ^ (z >> 27)) * 0x94d049bb133111ebull; return z ^ (z >> 31); }
+    double uni() { return (next() >> 11) * (1.0 / 9007199254740992.0); }
+    double gaus() { double u = uni(), v = uni(); return std::sqrt(-2.0 * std::log(u + 1e-300)) * std::cos(2 * M_PI * v); }
+  };
+  auto n_hits_of = [&](int64_t t) {
+    Rng r{seed * 0x2545f4914f6cdd1dull + uint64_t(t) * 0x9e3779b97f4a7c15ull + 1};
+    const double u = r.uni();
+    if (u < 0.3) return 3;
+    if (u < 0.7) return 4;
+    if (u < 0.9) return 5;
+    return 6 + int(r.uni() * 3.0);
+  };
+  offsets[0] = 0;
+  for (int64_t t = 0; t < n_tracks; ++t) offsets[t + 1] = offsets[t] + n_hits_of(t);
+  const Geometry& g = geom();
+  (void)g;
+  auto one = [&](int64_t t) {
+    const int n = offsets[t + 1] - offsets[t];
+    Rng r{seed * 0x94d049bb133111ebull + uint64_t(t) * 0xbf58476d1ce4e5b9ull + 7};
+    double hx[8], hy[8], hz[8];
+    double tr[5] = {0, 0, 0, 0, 0};
+    for (int attempt = 0; attempt < 1000; ++attempt) {
+      const double invpt = 0.1 + 1.9 * r.uni();
+      const double eta = attempt < 900 ? -1.0 + 2.0 * r.uni() : 0.0;
+      const double phi0 = -M_PI + 2 * M_PI * r.uni();
+      const int q = r.uni() < 0.5 ? -1 : 1;
+      const double z0 = 5.0 * r.gaus();
+      double px = 0.001 * r.gaus(), py = 0.001 * r.gaus(), pz = z0;
+      const double p = std::cosh(eta) / invpt;  // |p| in GeV
+      double theta = 2.0 * std::atan(std::exp(-eta));
+      double phid = phi0;                        // direction of motion in the transverse plane
+      tr[0] = phi0; tr[1] = 0.0; tr[2] = q * invpt; tr[3] = std::sinh(eta); tr[4] = z0;
+      bool ok = true;
+      for (int L = 0; L < n && ok; ++L) {
+        const double pt = p * std::sin(theta);
+        const double R = pt / kInvRadiusPerGeV;  // cm
+        const double cot = std::cos(theta) / std::sin(theta);
+        const double cx = px + q * R * (-std::sin(phid)), cy = py + q * R * std::cos(phid);
+        const double dc = std::hypot(cx, cy), rl = kR[L];
+        if (dc + R < rl || std::fabs(dc - R) > rl || dc == 0) { ok = false; break; }
+        const double a = (rl * rl - R * R + dc * dc) / (2 * dc);
+        const double h = std::sqrt(std::max(rl * rl - a * a, 0.0));
+        const double ux = cx / dc, uy = cy / dc;
+        const double psi0 = std::atan2(py - cy, px - cx);
+        double best = 1e300, bx = 0, by = 0;
+        for (int sg = -1; sg <= 1; sg += 2) {
+          const double ix = a * ux - sg * h * uy, iy = a * uy + sg * h * ux;
+          double dpsi = q * (std::atan2(iy - cy, ix - cx) - psi0);
+          while (dpsi <= 1e-12) dpsi += 2 * M_PI;
+          while (dpsi > 2 * M_PI) dpsi -= 2 * M_PI;
+          if (dpsi < best) { best = dpsi; bx = ix; by = iy; }
+        }
+        if (best > M_PI) { ok = false; break; }  // would have to loop back
+        const double sT = R * best;
+        px = bx; py = by; pz += cot * sT;
+        if (std::fabs(pz) > kHalf[L]) { ok = false; break; }
+        phid += q * best;
+        hx[L] = px; hy[L] = py; hz[L] = pz;
+        // Highland kink for 0.02 X0 crossed at the track's polar angle
+        const double x0 = 0.02 / std::sin(theta);
+        const double th0 = 0.0136 / p * std::sqrt(x0) * (1.0 + 0.038 * std::log(x0));
+        phid += th0 * r.gaus() / std::sin(theta);
+        theta += th0 * r.gaus();
+        if (theta <= 0.05 || theta >= M_PI - 0.05) { ok = false; break; }
+      }
+      if (ok) break;
+    }
+    const int64_t b = offsets[t];
+    for (int L = 0; L < n; ++L) {
+      const double ph = std::atan2(hy[L], hx[L]);
+      const double sn = std::sin(ph), cs = std::cos(ph);
+      const double d1 = s_rphi * r.gaus(), d2 = s_z * r.gaus();
+      double* H = hits + 3 * (b + L);
+      H[0] = hx[L] - sn * d1; H[1] = hy[L] + cs * d1; H[2] = hz[L] + d2;
+      float* G = ge + 6 * (b + L);
+      G[0] = float(s_rphi * s_rphi * sn * sn); G[1] = float(-s_rphi * s_rphi * sn * cs);
+      G[2] = float(s_rphi * s_rphi * cs * cs); G[3] = 0.f; G[4] = 0.f; G[5] = float(s_z * s_z);
+      int16_t mid = -1;
+      if (L < 4) {
+        const int nl = kLaddersPerLayer[L];
+        const double kf = ph / (2 * M_PI) * nl - 0.25 * L;
+        const int k = ((int(std::lround(kf))) % nl + nl) % nl;
+        int mz = int(std::floor((hz[L] + 26.0) / 6.5));
+        mz = mz < 0 ? 0 : (mz > 7 ? 7 : mz);
+        mid = int16_t(kLayerStart[L] + k * 8 + mz);
+      }
+      module[b + L] = mid;
+    }
+    if (truth)
+      for (int k = 0; k < 5; ++k) truth[5 * t + k] = tr[k];
+  };
+  int nt = n_threads > 0 ? n_threads : int(std::max(1u, std::thread::hardware_concurrency()));
+  nt = std::max(1, std::min<int>(nt, n_tracks > 0 ? n_tracks : 1));
+  std::vector<std::thread> th;
+  for (int w = 0; w < nt; ++w)
+    th.emplace_back([&, w] { for (int64_t t = w; t < n_tracks; t += nt) one(t); });
+  for (auto& x : th) x.join();
+  return offsets[n_tracks];
+}
+
 }  // extern "C"

@@ -581,9 +581,13 @@ __global__ void k_tuple_bases(Dev d) {
 __global__ void k_tuple_ends(Dev d) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= d.E) return;
-  const EvInfo& E = d.ev[e];
-  if (uint64_t(E.tuple_base) + E.n_tuples_raw <= uint64_t(d.cap_tuples))
+  EvInfo& E = d.ev[e];
+  E.n_tuple_hits = 0;
+  if (uint64_t(E.tuple_base) + E.n_tuples_raw <= uint64_t(d.cap_tuples)) {
     d.tuple_off[uint64_t(E.tuple_base) + E.n_tuples_raw] = E.tuple_hit_base + E.n_tuple_hits_raw;
+    // hits of the tuples kept (the first n_tuples)
+    E.n_tuple_hits = d.tuple_off[uint64_t(E.tuple_base) + E.n_tuples] - E.tuple_hit_base;
+  }
 }
 
 // cell -> tuple lists: fill from the (cell, tuple) pairs of the kept tuples

@@ -126,23 +126,66 @@ __device__ void standalone_fit(const double* hits, const float* hits_ge, int32_t
   status[t] = ok ? 0 : 1;
 }
 
-template <class T>
-__global__ void __launch_bounds__(128) k_fit_standalone(const double* __restrict__ hits, const float* __restrict__ ge,
-                                                        const int32_t* __restrict__ offs, int32_t n, double B,
-                                                        float* state, float* cov, float* chi2, float* pt, float* eta,
-                                                        int32_t* status) {
+}  // namespace
+
+// ------------------------------------------------------------ hit-count buckets
+// Stand-alone fits take tracks of 3..8 hits in any order. A count and a scatter
+// pass sort the track indices into one list per hit count in the caller's
+// workspace, so that each per-N kernel holds only its own registers and every
+// warp runs one N. Workspace: FitPlan header, then the lists.
+__global__ void k_fit_plan_count(const int32_t* __restrict__ offs, int32_t n, FitPlan* plan, int32_t* status) {
+  __shared__ uint32_t s_cnt[kFitMaxN + 1];
+  if (threadIdx.x <= kFitMaxN) s_cnt[threadIdx.x] = 0;
+  __syncthreads();
   for (int32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-    const int32_t first = offs[t], nh = offs[t + 1] - offs[t];
-    switch (nh) {
-      case 3: standalone_fit<3, T>(hits, ge, first, B, state, cov, chi2, pt, eta, status, t); break;
-      case 4: standalone_fit<4, T>(hits, ge, first, B, state, cov, chi2, pt, eta, status, t); break;
-      case 5: standalone_fit<5, T>(hits, ge, first, B, state, cov, chi2, pt, eta, status, t); break;
-      case 6: standalone_fit<6, T>(hits, ge, first, B, state, cov, chi2, pt, eta, status, t); break;
-      case 7: standalone_fit<7, T>(hits, ge, first, B, state, cov, chi2, pt, eta, status, t); break;
-      case 8: standalone_fit<8, T>(hits, ge, first, B, state, cov, chi2, pt, eta, status, t); break;
-      default: status[t] = -1; break;
-    }
+    const int32_t nh = offs[t + 1] - offs[t];
+    if (nh >= 3 && nh <= kFitMaxN) atomicAdd(&s_cnt[nh], 1u);
+    else if (status) status[t] = -1;
   }
+  __syncthreads();
+  if (threadIdx.x <= kFitMaxN && s_cnt[threadIdx.x]) atomicAdd(&plan->count[threadIdx.x], s_cnt[threadIdx.x]);
+}
+
+__global__ void k_fit_plan_fill(const int32_t* __restrict__ offs, int32_t n, FitPlan* plan) {
+  __shared__ uint32_t s_base[kFitMaxN + 1];
+  if (threadIdx.x == 0) {
+    uint32_t acc = 0;
+    for (int k = 0; k <= kFitMaxN; ++k) { s_base[k] = acc; acc += (k >= 3) ? plan->count[k] : 0u; }
+  }
+  __syncthreads();
+  if (blockIdx.x == 0 && threadIdx.x <= kFitMaxN) plan->base[threadIdx.x] = s_base[threadIdx.x];
+  for (int32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    const int32_t nh = offs[t + 1] - offs[t];
+    if (nh < 3 || nh > kFitMaxN) continue;
+    plan->list[s_base[nh] + atomicAdd(&plan->cursor[nh], 1u)] = t;
+  }
+}
+
+namespace {
+
+template <int N, class T>
+__global__ void __launch_bounds__(128) k_fit_bucket(const double* __restrict__ hits, const float* __restrict__ ge,
+                                                    const int32_t* __restrict__ offs, const FitPlan* __restrict__ plan,
+                                                    double B, float* state, float* cov, float* chi2, float* pt,
+                                                    float* eta, int32_t* status) {
+  const uint32_t cnt = plan->count[N];
+  const int32_t* list = plan->list + plan->base_of(N);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+    const int32_t t = list[i];
+    standalone_fit<N, T>(hits, ge, offs[t], B, state, cov, chi2, pt, eta, status, t);
+  }
+}
+
+template <class T>
+void launch_bucket_fits(const double* hits, const float* ge, const int32_t* offs, const FitPlan* plan, double B,
+                        float* state, float* cov, float* chi2, float* pt, float* eta, int32_t* status, cudaStream_t s) {
+  const int g = 148 * 4;
+  k_fit_bucket<3, T><<<g, 128, 0, s>>>(hits, ge, offs, plan, B, state, cov, chi2, pt, eta, status);
+  k_fit_bucket<4, T><<<g, 128, 0, s>>>(hits, ge, offs, plan, B, state, cov, chi2, pt, eta, status);
+  k_fit_bucket<5, T><<<g, 128, 0, s>>>(hits, ge, offs, plan, B, state, cov, chi2, pt, eta, status);
+  k_fit_bucket<6, T><<<g, 128, 0, s>>>(hits, ge, offs, plan, B, state, cov, chi2, pt, eta, status);
+  k_fit_bucket<7, T><<<g, 128, 0, s>>>(hits, ge, offs, plan, B, state, cov, chi2, pt, eta, status);
+  k_fit_bucket<8, T><<<g, 128, 0, s>>>(hits, ge, offs, plan, B, state, cov, chi2, pt, eta, status);
 }
 
 }  // namespace
@@ -159,18 +202,37 @@ void launch_fit(const Dev& d, const Launch& L) {
   L.mark("broken_line_fit_4");
 }
 
+int64_t fit_plan_bytes(int32_t n_tracks) {
+  return (int64_t(sizeof(FitPlan)) + 4 * int64_t(n_tracks > 0 ? n_tracks : 0) + 255) / 256 * 256;
+}
+
+int fit_plan_build(const int32_t* offs, int32_t n, FitPlan* plan, int32_t* status, cudaStream_t s) {
+  if (cudaMemsetAsync(plan, 0, sizeof(FitPlan) - sizeof(plan->list), s) != cudaSuccess) return PXL_ERR_CUDA;
+  const int blocks = std::max(1, std::min(148 * 8, int((n + 255) / 256)));
+  k_fit_plan_count<<<blocks, 256, 0, s>>>(offs, n, plan, status);
+  k_fit_plan_fill<<<blocks, 256, 0, s>>>(offs, n, plan);
+  return cudaGetLastError() == cudaSuccess ? 0 : PXL_ERR_CUDA;
+}
+
 }  // namespace pxl
+
+extern "C" int64_t pxl_fit_workspace_bytes(int32_t n_tracks) { return pxl::fit_plan_bytes(n_tracks); }
 
 extern "C" int32_t pxl_bl_fit(const double* hits, const float* hits_ge, const int32_t* offs, int32_t n, double b_field,
                               int32_t precision, float* state, float* cov, float* chi2, float* pt, float* eta,
-                              int32_t* status, void* stream) {
-  if (n < 0 || !hits || !hits_ge || !offs || !state || !cov || !chi2 || !pt || !eta || !status) return PXL_ERR_ARG;
+                              int32_t* status, void* workspace, int64_t workspace_bytes, void* stream) {
+  if (n < 0 || !hits || !hits_ge || !offs || !state || !cov || !chi2 || !pt || !eta || !status || !workspace)
+    return PXL_ERR_ARG;
+  if (precision != 0 && precision != 1) return PXL_ERR_ARG;
+  if (workspace_bytes < pxl::fit_plan_bytes(n)) return PXL_ERR_CAPACITY;
   if (n == 0) return 0;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const int blocks = int((n + 127) / 128);
+  auto* plan = static_cast<pxl::FitPlan*>(workspace);
+  int rc = pxl::fit_plan_build(offs, n, plan, status, s);
+  if (rc) return rc;
   if (precision == 0)
-    pxl::k_fit_standalone<double><<<blocks, 128, 0, s>>>(hits, hits_ge, offs, n, b_field, state, cov, chi2, pt, eta, status);
+    pxl::launch_bucket_fits<double>(hits, hits_ge, offs, plan, b_field, state, cov, chi2, pt, eta, status, s);
   else
-    pxl::k_fit_standalone<float><<<blocks, 128, 0, s>>>(hits, hits_ge, offs, n, b_field, state, cov, chi2, pt, eta, status);
+    pxl::launch_bucket_fits<float>(hits, hits_ge, offs, plan, b_field, state, cov, chi2, pt, eta, status, s);
   return cudaGetLastError() == cudaSuccess ? 0 : PXL_ERR_CUDA;
 }

@@ -184,6 +184,19 @@ struct Dev {
   int32_t bpe;             // blocks per event for per-event kernels
 };
 
+// Track lists by hit count for the stand-alone fits (workspace layout).
+constexpr int kFitMaxN = 8;
+struct FitPlan {
+  uint32_t count[kFitMaxN + 1];   // tracks with n hits, n = 3..8
+  uint32_t cursor[kFitMaxN + 1];
+  uint32_t base[kFitMaxN + 1];    // first list entry of each hit count
+  uint32_t pad;
+  int32_t list[1];                // track indices grouped by hit count (n_tracks entries)
+  __host__ __device__ uint32_t base_of(int n) const { return base[n]; }
+};
+int64_t fit_plan_bytes(int32_t n_tracks);
+int fit_plan_build(const int32_t* offs, int32_t n, FitPlan* plan, int32_t* status, cudaStream_t s);
+
 // ---------------------------------------------------------------- helpers
 __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v) {
   const unsigned lane = threadIdx.x & 31u;

@@ -85,8 +85,10 @@ _SIGS = {
                              ctypes.c_int32] + [ctypes.c_void_p] * 5),
     "pxl_clusterize_digis_noalloc": (ctypes.c_int32, [ctypes.c_void_p] * 4 + [ctypes.c_int32, ctypes.c_int32]
                                      + [ctypes.c_void_p] * 6),
+    "pxl_fit_workspace_bytes": (ctypes.c_int64, [ctypes.c_int32]),
     "pxl_bl_fit": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
-                                    ctypes.c_double, ctypes.c_int32] + [ctypes.c_void_p] * 6 + [ctypes.c_void_p]),
+                                    ctypes.c_double, ctypes.c_int32] + [ctypes.c_void_p] * 6 +
+                   [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]),
 }
 
 
@@ -123,6 +125,10 @@ def gen() -> ctypes.CDLL:
         _gen.pxlgen_events.restype = ctypes.c_int
         _gen.pxlgen_events.argtypes = [ctypes.c_uint64, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
                                        ctypes.c_int32, ctypes.c_int32, P, S, ctypes.c_void_p]
+        _gen.pxlgen_fit_tracks.restype = ctypes.c_int32
+        _gen.pxlgen_fit_tracks.argtypes = [ctypes.c_uint64, ctypes.c_int32, ctypes.c_int32] + [ctypes.c_void_p] * 5
+        _gen.pxlgen_module_positions.restype = ctypes.c_int32
+        _gen.pxlgen_module_positions.argtypes = [ctypes.c_void_p]
         _gen.pxlgen_free.restype = None
         _gen.pxlgen_free.argtypes = [ctypes.c_void_p]
     return _gen

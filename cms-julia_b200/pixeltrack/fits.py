@@ -3,7 +3,8 @@
 Inputs are CUDA tensors: hits [H, 3] float64 (x, y, z), hits_ge [H, 6] float32
 (global covariance per hit, the toGlobal layout of SOARotation.jl:139-147) and
 offsets [n+1] int32 (3..8 hits per track). precision 0 = FP64 throughout,
-1 = FP32 arithmetic with FP64 band-system Cholesky solve and covariance.
+1 = FP32 arithmetic with the band-system LDL^T solve, the parameter transport and the
+covariance in FP64.
 """
 from __future__ import annotations
 
@@ -13,8 +14,14 @@ from . import _native
 from ._native import check
 
 
+def workspace(n_tracks: int, device) -> torch.Tensor:
+    """Device scratch for the stand-alone fits of n_tracks tracks (reusable across calls)."""
+    return torch.empty(int(_native.lib().pxl_fit_workspace_bytes(n_tracks)), dtype=torch.uint8, device=device)
+
+
 def bl_fit(hits: torch.Tensor, hits_ge: torch.Tensor, offsets: torch.Tensor, b_field: float,
-           precision: int = 0, stream: torch.cuda.Stream | None = None) -> dict[str, torch.Tensor]:
+           precision: int = 0, stream: torch.cuda.Stream | None = None,
+           ws: torch.Tensor | None = None) -> dict[str, torch.Tensor]:
     if not (hits.is_cuda and hits_ge.is_cuda and offsets.is_cuda):
         raise ValueError("bl_fit takes CUDA tensors")
     hits = hits.contiguous().to(torch.float64)
@@ -31,8 +38,9 @@ def bl_fit(hits: torch.Tensor, hits_ge: torch.Tensor, offsets: torch.Tensor, b_f
         "status": torch.empty(n, dtype=torch.int32, device=dev),
     }
     s = (stream or torch.cuda.current_stream(dev)).cuda_stream
+    ws = workspace(n, dev) if ws is None else ws
     check(_native.lib().pxl_bl_fit(hits.data_ptr(), hits_ge.data_ptr(), offsets.data_ptr(), n, float(b_field),
                                    int(precision), out["state"].data_ptr(), out["cov"].data_ptr(),
                                    out["chi2"].data_ptr(), out["pt"].data_ptr(), out["eta"].data_ptr(),
-                                   out["status"].data_ptr(), s), "pxl_bl_fit")
+                                   out["status"].data_ptr(), ws.data_ptr(), ws.numel(), s), "pxl_bl_fit")
     return out

@@ -48,3 +48,28 @@ def events(n_events: int, mode: int = MODE_PU, pu: float = 50.0, ntracks: int = 
     arr = np.frombuffer(ctypes.string_at(blob.value, nb.value), dtype=np.uint8).copy()
     g.pxlgen_free(blob)
     return arr, offs
+
+
+def fit_tracks(n_tracks: int, seed: int = 1, threads: int = 0) -> dict[str, np.ndarray]:
+    """Seeded fit workload: hits (H, 3) float64, ge (H, 6) float32 global covariances,
+    offsets (n+1,) int32, module (H,) int16 (-1 off the pixel layers), truth (n, 5)
+    float64 = (phi0, d0, q/pT, cot(theta), z0) at generation."""
+    g = _native.gen()
+    cap = 8 * n_tracks
+    hits = np.zeros((cap, 3), np.float64)
+    ge = np.zeros((cap, 6), np.float32)
+    offs = np.zeros(n_tracks + 1, np.int32)
+    mod = np.zeros(cap, np.int16)
+    truth = np.zeros((n_tracks, 5), np.float64)
+    vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+    nh = g.pxlgen_fit_tracks(seed, n_tracks, threads, vp(hits), vp(ge), vp(offs), vp(mod), vp(truth))
+    if nh < 0:
+        raise RuntimeError("pxlgen_fit_tracks failed")
+    return {"hits": hits[:nh], "ge": ge[:nh], "offsets": offs, "module": mod[:nh], "truth": truth}
+
+
+def module_positions() -> np.ndarray:
+    """Centres (1856, 3) of the synthetic geometry's modules, in cm."""
+    out = np.zeros((1856, 3), np.float64)
+    _native.gen().pxlgen_module_positions(out.ctypes.data_as(ctypes.c_void_p))
+    return out

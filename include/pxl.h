@@ -260,13 +260,16 @@ int32_t pxl_clusterize_digis_noalloc(const uint16_t* id, const int16_t* x, const
 /* Standalone broken-line fits of n_tracks tracks (broken_line.jl:275-696, driven as
  * broken_line_fit_on_gpu.jl:24-163 does). Device pointers: hits[3*H] (x,y,z per hit,
  * float64), hits_ge[6*H] (global covariance per hit, float32), hit_offsets[n_tracks+1]
- * (3..8 hits per track). precision: 0 = FP64 throughout, 1 = FP32 arithmetic with the
- * band-matrix Cholesky solve and the final covariance in FP64.
+ * (3..8 hits per track, any order). precision: 0 = FP64 throughout, 1 = FP32 arithmetic
+ * with the band-matrix LDL^T solve, the parameter transport and the covariance in FP64.
+ * workspace: device scratch of at least pxl_fit_workspace_bytes(n_tracks) bytes, used
+ * to group the tracks by hit count (contents need not be initialised).
  * Outputs (device): state[5*n] (phi, tip, q/pt, cot(theta), zip as copyFromCircle! stores
- * them), cov[15*n], chi2[n], pt[n], eta[n], status[n] (0 ok, 1 domain). */
+ * them), cov[15*n], chi2[n], pt[n], eta[n], status[n] (0 ok, 1 domain, -1 bad hit count). */
+int64_t pxl_fit_workspace_bytes(int32_t n_tracks);
 int32_t pxl_bl_fit(const double* hits, const float* hits_ge, const int32_t* hit_offsets, int32_t n_tracks, double b_field,
                    int32_t precision, float* state, float* cov, float* chi2, float* pt, float* eta, int32_t* status,
-                   void* stream);
+                   void* workspace, int64_t workspace_bytes, void* stream);
 
 #ifdef __cplusplus
 }

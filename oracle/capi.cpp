@@ -226,4 +226,26 @@ double orc_run_batch(OrcCtx* c, const uint8_t* blob, const uint64_t* offsets, in
   return std::chrono::duration<double>(t1 - t0).count();
 }
 
+// FP64 broken-line fits of n tracks (hits row-major per hit, offsets[n+1]) with n_threads
+// host threads; state5[5n] and pt[n] (may be null) receive the results. Returns seconds.
+double orc_bl_fit_batch(const double* hits, const float* ge, const int32_t* offsets, int32_t n, double B,
+                        int32_t n_threads, double* state5, double* pt) {
+  int nt = n_threads > 0 ? n_threads : 1;
+  auto t0 = std::chrono::steady_clock::now();
+  std::vector<std::thread> th;
+  for (int t = 0; t < nt; ++t) {
+    th.emplace_back([&, t] {
+      for (int32_t k = t; k < n; k += nt) {
+        const int32_t a = offsets[k], m = offsets[k + 1] - offsets[k];
+        double st[5], cv[15], cl, cc, p, eta;
+        bl_fit_track(hits + 3 * size_t(a), ge + 6 * size_t(a), m, B, st, cv, &cl, &cc, &p, &eta, nullptr);
+        if (state5) for (int j = 0; j < 5; ++j) state5[5 * size_t(k) + j] = st[j];
+        if (pt) pt[k] = p;
+      }
+    });
+  }
+  for (auto& x : th) x.join();
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
 }  // extern "C"

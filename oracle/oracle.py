@@ -59,6 +59,8 @@ def lib() -> ctypes.CDLL:
         _lib.orc_clusterize_digis.argtypes = [V, V, V, V, ctypes.c_int32, V, V, V, V, V, ctypes.c_int32]
         _lib.orc_bl_fit.restype = ctypes.c_int32
         _lib.orc_bl_fit.argtypes = [V, V, ctypes.c_int32, ctypes.c_double, V, V, V, V, V, V]
+        _lib.orc_bl_fit_batch.restype = ctypes.c_double
+        _lib.orc_bl_fit_batch.argtypes = [V, V, V, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, V, V]
         _lib.orc_run_batch.restype = ctypes.c_double
         _lib.orc_run_batch.argtypes = [V, V, V, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, V]
     return _lib
@@ -150,3 +152,17 @@ def bl_fit(hits: np.ndarray, ge: np.ndarray, B: float) -> dict:
                       pt.ctypes.data, eta.ctypes.data, ff.ctypes.data)
     return {"rc": rc, "state": st, "cov": cv, "chi2_line": c2[0], "chi2_circle": c2[1], "pt": pt[0], "eta": eta[0],
             "fast_fit": ff}
+
+
+def bl_fit_batch(hits: np.ndarray, ge: np.ndarray, offsets: np.ndarray, B: float, threads: int = 1):
+    """FP64 fits of a track collection: hits (H, 3) float64, ge (H, 6) float32, offsets
+    (n+1,) int32. Returns (state (n, 5), pt (n,), elapsed seconds)."""
+    l = lib()
+    h = np.ascontiguousarray(hits, np.float64)
+    g = np.ascontiguousarray(ge, np.float32)
+    o = np.ascontiguousarray(offsets, np.int32)
+    n = len(o) - 1
+    st = np.zeros((n, 5))
+    pt = np.zeros(n)
+    dt = l.orc_bl_fit_batch(h.ctypes.data, g.ctypes.data, o.ctypes.data, n, B, threads, st.ctypes.data, pt.ctypes.data)
+    return st, pt, dt

@@ -129,3 +129,54 @@ def test_autotuned_shapes_keep_results(conditions, events_pu50):
             errs = compare_ca(bc, orc, e, classified=True) + compare_fits(bc, orc, e) + compare_quality(bc, orc, e) \
                 + compare_vertices(bc, orc, e)
             assert not errs, (e, errs)
+
+
+def _fit_workload(n, seed):
+    from pixeltrack import gen
+    return gen.fit_tracks(n, seed=seed)
+
+
+def test_standalone_fits_all_hit_counts_match_oracle():
+    """Tracks of 3..8 hits in mixed order (the fit workload generator) through the bucketed
+    FP64 fit: state, pt and chi2 equal the oracle's within FP32 storage precision."""
+    import torch
+    from pixeltrack.fits import bl_fit
+    B = 0.0114256972711507
+    w = _fit_workload(600, seed=21)
+    out = bl_fit(torch.as_tensor(w["hits"]).cuda(), torch.as_tensor(w["ge"]).cuda(),
+                 torch.as_tensor(w["offsets"]).cuda(), B, precision=0)
+    st = out["state"].cpu().numpy()
+    pt = out["pt"].cpu().numpy()
+    status = out["status"].cpu().numpy()
+    seen = set()
+    for t in range(600):
+        a, b = w["offsets"][t], w["offsets"][t + 1]
+        ref = oracle.bl_fit(w["hits"][a:b].T, w["ge"][a:b].T, B)
+        assert status[t] == ref["rc"]
+        if ref["rc"]:
+            continue
+        seen.add(b - a)
+        np.testing.assert_allclose(st[t], ref["state"], rtol=2e-6, atol=1e-7)
+        np.testing.assert_allclose(pt[t], ref["pt"], rtol=2e-6)
+    assert seen == {3, 4, 5, 6, 7, 8}
+
+
+def test_mixed_precision_fit_error_bounds():
+    """FP32 mode against the FP64 mode on 20k workload tracks: the stated error bounds
+    (relative for q/pT and cot(theta), absolute for phi, d0 and z0)."""
+    import torch
+    from pixeltrack.fits import bl_fit
+    B = 0.0114256972711507
+    w = _fit_workload(20000, seed=22)
+    args = (torch.as_tensor(w["hits"]).cuda(), torch.as_tensor(w["ge"]).cuda(), torch.as_tensor(w["offsets"]).cuda(), B)
+    f64 = bl_fit(*args, precision=0)["state"].double().cpu().numpy()
+    f32 = bl_fit(*args, precision=1)["state"].double().cpu().numpy()
+    ok = np.all(np.isfinite(f64), axis=1)
+    d = np.abs(f32[ok] - f64[ok])
+    qpt = d[:, 2] / np.abs(f64[ok, 2])
+    cot = d[:, 3] / np.maximum(np.abs(f64[ok, 3]), 1e-3)
+    assert np.percentile(qpt, 99) < 1e-5 and qpt.max() < 1e-4
+    assert cot.max() < 5e-6
+    assert d[:, 0].max() < 2e-6       # phi, rad
+    assert d[:, 1].max() < 5e-6       # d0, cm
+    assert d[:, 4].max() < 1e-5       # z0, cm
