@@ -27,6 +27,7 @@ CUDA_SOURCES = [
     "k_rechits.cu",
     "k_ca.cu",
     "k_fit.cu",
+    "k_adjoint.cu",
     "k_select.cu",
     "k_products.cu",
     "noalloc.cu",

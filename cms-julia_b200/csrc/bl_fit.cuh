@@ -373,22 +373,28 @@ BL_HD void line_weights(const float ge[6][N], const Prep<N, T>& P, T w[N]) {
   }
 }
 
-// BL_Line_fit (broken_line.jl:546-696)
+// line-fit system: weights, band factorisation and solution u (hit order)
 template <int N, class T>
-BL_HD void line_fit(const float ge[6][N], const Geo<N, T>& G, T B, const Prep<N, T>& P, LineOut& L) {
-  T w[N];
+BL_HD void line_system(const float ge[6][N], const Prep<N, T>& P, T w[N], Band<N, false>& f, double u[N]) {
   line_weights<N, T>(ge, P, w);
   double d[N], e1[N], e2[N], r[N];
   band_entries<N, T>(w, P.S, P.VB, d, e1, e2);
 #pragma unroll
   for (int i = 0; i < N; ++i) r[N - 1 - i] = double(w[i] * P.Z[i]);
-  Band<N, false> f;
   band_factor<N, false>(d, e1, e2, nullptr, 0.0, f);
   double ue[N];
   band_solve<N, false>(f, r, ue);
-  double u[N];
 #pragma unroll
   for (int i = 0; i < N; ++i) u[i] = ue[N - 1 - i];
+}
+
+// BL_Line_fit (broken_line.jl:546-696)
+template <int N, class T>
+BL_HD void line_fit(const float ge[6][N], const Geo<N, T>& G, T B, const Prep<N, T>& P, LineOut& L) {
+  T w[N];
+  Band<N, false> f;
+  double u[N];
+  line_system<N, T>(ge, P, w, f, u);
   double I[3][3];
   band_trailing_inverse<N, false>(f, I);
   // absolute position of hit 0 in the rotated (S, Z) frame
@@ -455,19 +461,16 @@ BL_HD void translate_karimaki(CircleOut& c, double x0, double y0) {
   sandwich3(J, c.cov);
 }
 
-// BL_Circle_fit (broken_line.jl:330-528); returns false where the reference raises
+// circle-fit system: scaled scattering variances, radial residuals, weights, band
+// factorisation (border = curvature correction) and solution u[N+1] (hit order)
 template <int N, class T>
-BL_HD bool circle_fit(const float ge[6][N], const Geo<N, T>& G, T B, const Prep<N, T>& P,
-                                           CircleOut& c) {
-  bool ok = true;
-  c.q = P.q;
+BL_HD void circle_system(const float ge[6][N], const Geo<N, T>& G, const Prep<N, T>& P, T VB[N], T Z[N], T rn[N],
+                         T w[N], Band<N, true>& f, double u[N + 1]) {
   const T ms_scale = T(1.0) + P.slope * P.slope;
-  T VB[N];
 #pragma unroll
   for (int i = 0; i < N; ++i) VB[i] = P.VB[i] * ms_scale;
   // radial residuals of the hits to the fast-fit circle, which passes through hit 0
   const T ux = -P.cx, uy = -P.cy;
-  T Z[N], rn[N];
 #pragma unroll
   for (int i = 0; i < N; ++i) {
     rn[i] = s_sqrt<T>(P.rx[i] * P.rx[i] + P.ry[i] * P.ry[i]);
@@ -475,7 +478,6 @@ BL_HD bool circle_fit(const float ge[6][N], const Geo<N, T>& G, T B, const Prep<
     Z[i] = power_of_point<T>(ux, uy, px, py) / (rn[i] + P.R);
   }
   const double tol = 1e-12;
-  T w[N];
 #pragma unroll
   for (int i = 0; i < N; ++i) {
     auto z = [&](float v) { return fabs(double(v)) < tol ? T(0) : T(v); };
@@ -500,14 +502,26 @@ BL_HD bool circle_fit(const float ge[6][N], const Geo<N, T>& G, T B, const Prep<
     r[N - 1 - i] = double(w[i] * Z[i]);
     if (i > 0 && i < N - 1) cnn += ((s[i + 1] - s[i - 1]) * (s[i + 1] - s[i - 1])) / (T(4.0) * VB[i]);
   }
-  Band<N, true> f;
   band_factor<N, true>(d, e1, e2, b, double(cnn), f);
   double ue[N + 1];
   band_solve<N, true>(f, r, ue);
-  double u[N + 1];
 #pragma unroll
   for (int i = 0; i < N; ++i) u[i] = ue[N - 1 - i];
   u[N] = ue[N];
+}
+
+// BL_Circle_fit (broken_line.jl:330-528); returns false where the reference raises
+template <int N, class T>
+BL_HD bool circle_fit(const float ge[6][N], const Geo<N, T>& G, T B, const Prep<N, T>& P,
+                                           CircleOut& c) {
+  bool ok = true;
+  c.q = P.q;
+  const T ms_scale = T(1.0) + P.slope * P.slope;
+  T VB[N], Z[N], rn[N], w[N];
+  Band<N, true> f;
+  double u[N + 1];
+  circle_system<N, T>(ge, G, P, VB, Z, rn, w, f, u);
+  const T* s = P.s;
   double I[3][3];
   band_trailing_inverse<N, true>(f, I);
   // fitted points 0 and 1 (hit-0 frame), FP64 from here on

@@ -271,6 +271,23 @@ int32_t pxl_bl_fit(const double* hits, const float* hits_ge, const int32_t* hit_
                    int32_t precision, float* state, float* cov, float* chi2, float* pt, float* eta, int32_t* status,
                    void* workspace, int64_t workspace_bytes, void* stream);
 
+/* Adjoint of the broken-line fit: per track the FP64 chi2 = chi2_line + chi2_circle and
+ * its gradient with respect to the hit coordinates, the fit being recomputed in the
+ * backward pass (nothing stored between passes). Same track inputs as pxl_bl_fit.
+ * Alignment (optional, all of hit_module[H], module_pos[3*n_modules] (module centres,
+ * FP64) and n_modules > 0): when align[6*n_modules] (tx, ty, tz, wx, wy, wz per module;
+ * float) is given, each hit h on module m (hit_module >= 0) is first moved to
+ * h + t_m + w_m x (h - c_m). Outputs (device, each may be NULL): chi2[n] (float),
+ * grad_hits[3*H] (float, gradient w.r.t. the moved hits), grad_align[6*n_modules]
+ * (float) and grad_align64[6*n_modules] (FP64) = d(sum chi2)/d(alignment), accumulated
+ * in FP64. workspace: pxl_adjoint_workspace_bytes(n_tracks, n_modules) bytes.
+ * The reference has no gradient path: this extends the fit of broken_line.jl. */
+int64_t pxl_adjoint_workspace_bytes(int32_t n_tracks, int32_t n_modules);
+int32_t pxl_bl_fit_adjoint(const double* hits, const float* hits_ge, const int32_t* hit_offsets, int32_t n_tracks,
+                           double b_field, const int16_t* hit_module, const double* module_pos, const float* align,
+                           int32_t n_modules, float* chi2, float* grad_hits, float* grad_align, double* grad_align64,
+                           void* workspace, int64_t workspace_bytes, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -226,6 +226,11 @@ double orc_run_batch(OrcCtx* c, const uint8_t* blob, const uint64_t* offsets, in
   return std::chrono::duration<double>(t1 - t0).count();
 }
 
+// forward-mode gradient of one track's chi2 (chi2_line + chi2_circle) w.r.t. its hits
+double orc_bl_chi2_grad_fwd(const double* hits, const float* ge, int32_t n, double B, double* grad) {
+  return bl_chi2_grad_fwd(hits, ge, n, B, grad);
+}
+
 // FP64 broken-line fits of n tracks (hits row-major per hit, offsets[n+1]) with n_threads
 // host threads; state5[5n] and pt[n] (may be null) receive the results. Returns seconds.
 double orc_bl_fit_batch(const double* hits, const float* ge, const int32_t* offsets, int32_t n, double B,

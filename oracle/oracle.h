@@ -211,5 +211,8 @@ void make_vertices(const Conditions& c, EventOut& ev);
 // when the reference would raise.
 int bl_fit_track(const double* hits, const float* ge, int n, double B, double* state5, double* cov15,
                  double* chi2_line, double* chi2_circle, double* pt, double* eta, double* fast_fit4);
+// chi2_line + chi2_circle of one track and its gradient with respect to the hit
+// coordinates (grad[3n], hit-major) by forward-mode dual numbers (brokenline_fwd.cpp)
+double bl_chi2_grad_fwd(const double* hits, const float* ge, int n, double B, double* grad);
 
 }  // namespace orc

@@ -59,6 +59,8 @@ def lib() -> ctypes.CDLL:
         _lib.orc_clusterize_digis.argtypes = [V, V, V, V, ctypes.c_int32, V, V, V, V, V, ctypes.c_int32]
         _lib.orc_bl_fit.restype = ctypes.c_int32
         _lib.orc_bl_fit.argtypes = [V, V, ctypes.c_int32, ctypes.c_double, V, V, V, V, V, V]
+        _lib.orc_bl_chi2_grad_fwd.restype = ctypes.c_double
+        _lib.orc_bl_chi2_grad_fwd.argtypes = [V, V, ctypes.c_int32, ctypes.c_double, V]
         _lib.orc_bl_fit_batch.restype = ctypes.c_double
         _lib.orc_bl_fit_batch.argtypes = [V, V, V, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, V, V]
         _lib.orc_run_batch.restype = ctypes.c_double
@@ -166,3 +168,13 @@ def bl_fit_batch(hits: np.ndarray, ge: np.ndarray, offsets: np.ndarray, B: float
     pt = np.zeros(n)
     dt = l.orc_bl_fit_batch(h.ctypes.data, g.ctypes.data, o.ctypes.data, n, B, threads, st.ctypes.data, pt.ctypes.data)
     return st, pt, dt
+
+
+def bl_chi2_grad_fwd(hits: np.ndarray, ge: np.ndarray, B: float):
+    """chi2_line + chi2_circle of one track and its gradient (N, 3) with respect to the hits
+    (forward-mode dual numbers through the reference formulation). hits (N, 3), ge (N, 6)."""
+    h = np.ascontiguousarray(hits, np.float64)
+    g = np.ascontiguousarray(ge, np.float32)
+    grad = np.zeros_like(h)
+    c = lib().orc_bl_chi2_grad_fwd(h.ctypes.data, g.ctypes.data, h.shape[0], B, grad.ctypes.data)
+    return c, grad

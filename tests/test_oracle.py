@@ -102,3 +102,27 @@ def test_chain_counts_plausible(conditions, event_single, events_pu50):
     c = orc.counts()
     assert c["flags"] == 0
     assert 35 <= c["nv_final"] <= 60
+
+
+def test_forward_mode_gradient_matches_central_differences():
+    """The oracle's dual-number gradient of chi2_line + chi2_circle agrees with central
+    finite differences (h = 1e-6 cm) of the oracle's own FP64 fit."""
+    import sys
+    sys.path.insert(0, str(Path(__file__).resolve().parents[1] / "cms-julia_b200"))
+    from pixeltrack import gen
+    B = 0.0114256972711507
+    w = gen.fit_tracks(40, seed=41)
+    chi = lambda hh, ge: (lambda r: r["chi2_line"] + r["chi2_circle"])(oracle.bl_fit(hh.T, ge.T, B))
+    for t in range(40):
+        a, b = w["offsets"][t], w["offsets"][t + 1]
+        hits, ge = w["hits"][a:b], w["ge"][a:b]
+        c, g = oracle.bl_chi2_grad_fwd(hits, ge, B)
+        assert abs(c - chi(hits, ge)) <= 1e-12 * abs(c)
+        fd = np.zeros_like(hits)
+        for i in range(b - a):
+            for k in range(3):
+                hp, hm = hits.copy(), hits.copy()
+                hp[i, k] += 1e-6
+                hm[i, k] -= 1e-6
+                fd[i, k] = (chi(hp, ge) - chi(hm, ge)) / 2e-6
+        assert np.abs(g - fd).max() <= 1e-6 * np.abs(fd).max()
