@@ -176,6 +176,23 @@ def bench_fits(args, local: int, rank: int, world: int) -> dict:
             ms = t0.elapsed_time(t1) / args.steps
             res[name] = {k: v.double().cpu().numpy() for k, v in r.items() if k in ("state", "pt", "status")}
             out[name] = {"fits_per_s": world * n / (ms / 1e3), "ms_per_step": ms}
+    # Riemann fits of the same tracks
+    from pixeltrack.fits import riemann_fit
+    rres = {}
+    with torch.cuda.stream(stream):
+        for prec, name in ((1, "riemann_mixed"), (0, "riemann_fp64")):
+            for _ in range(args.warmup):
+                r = riemann_fit(hits, ge, offs, FIT_B, precision=prec, stream=stream, ws=ws)
+            stream.synchronize()
+            t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0.record(stream)
+            for _ in range(args.steps):
+                r = riemann_fit(hits, ge, offs, FIT_B, precision=prec, stream=stream, ws=ws)
+            t1.record(stream)
+            t1.synchronize()
+            ms = t0.elapsed_time(t1) / args.steps
+            rres[name] = {k: v.double().cpu().numpy() for k, v in r.items() if k in ("state", "status")}
+            out[name] = {"fits_per_s": world * n / (ms / 1e3), "ms_per_step": ms}
     nh = np.diff(w["offsets"]).astype(np.int64)
     bytes_per_step = 48 * int(nh.sum()) + 4 * (n + 1) + (5 + 15 + 3) * 4 * n + 4 * n
     peak, peak_kind = load_peaks()
@@ -188,9 +205,15 @@ def bench_fits(args, local: int, rank: int, world: int) -> dict:
     ok = np.all(np.isfinite(b), axis=1) & (res["fp64"]["status"] == 0)
     d = np.abs(a[ok] - b[ok])
     stats = lambda v: {"median": float(np.median(v)), "p99": float(np.percentile(v, 99)), "max": float(v.max())}
-    err = {"q_over_pt_rel": stats(d[:, 2] / np.abs(b[ok, 2])), "phi_abs_rad": stats(d[:, 0]),
-           "cot_theta_rel": stats(d[:, 3] / np.maximum(np.abs(b[ok, 3]), 1e-3)),
-           "d0_abs_cm": stats(d[:, 1]), "z0_abs_cm": stats(d[:, 4]), "tracks": int(ok.sum())}
+    def param_err(a, b, ok):
+        d = np.abs(a[ok] - b[ok])
+        return {"q_over_pt_rel": stats(d[:, 2] / np.abs(b[ok, 2])), "phi_abs_rad": stats(d[:, 0]),
+                "cot_theta_rel": stats(d[:, 3] / np.maximum(np.abs(b[ok, 3]), 1e-3)),
+                "d0_abs_cm": stats(d[:, 1]), "z0_abs_cm": stats(d[:, 4]), "tracks": int(ok.sum())}
+    err = param_err(a, b, ok)
+    rb = rres["riemann_fp64"]["state"]
+    rok = np.all(np.isfinite(rb), axis=1) & (rres["riemann_fp64"]["status"] == 0)
+    err_riemann = param_err(rres["riemann_mixed"]["state"], rb, rok)
     # FP64 mode against the CPU oracle on a sample (the oracle stores FP64, the GPU FP32)
     m = min(args.fit_oracle_sample, n)
     st, _, _ = oracle_fit_sample(w, m)
@@ -207,6 +230,8 @@ def bench_fits(args, local: int, rank: int, world: int) -> dict:
     return {"workload": f"2^{int(np.log2(n))} synthetic tracks, 3-8 hits (30/40/20/10 % for 3/4/5/6-8), helices with "
                         "0.02 X0 scattering kinks, 10 um r-phi / 20 um z smearing",
             "tracks": n, "mixed": out["mixed"], "fp64": out["fp64"], "err_mixed_vs_fp64": err,
+            "riemann_mixed": out["riemann_mixed"], "riemann_fp64": out["riemann_fp64"],
+            "riemann_err_mixed_vs_fp64": err_riemann,
             "fp64_vs_oracle": {"max_rel": float(rel.max()), "tracks": int(okm.sum())},
             "cpu_baseline": cpu}
 

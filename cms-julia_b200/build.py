@@ -28,6 +28,7 @@ CUDA_SOURCES = [
     "k_ca.cu",
     "k_fit.cu",
     "k_adjoint.cu",
+    "k_riemann.cu",
     "k_select.cu",
     "k_products.cu",
     "noalloc.cu",

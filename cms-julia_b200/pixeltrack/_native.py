@@ -87,6 +87,8 @@ _SIGS = {
                                      + [ctypes.c_void_p] * 6),
     "pxl_fit_workspace_bytes": (ctypes.c_int64, [ctypes.c_int32]),
     "pxl_adjoint_workspace_bytes": (ctypes.c_int64, [ctypes.c_int32, ctypes.c_int32]),
+    "pxl_riemann_fit": (ctypes.c_int32, [ctypes.c_void_p] * 3 + [ctypes.c_int32, ctypes.c_double, ctypes.c_int32] +
+                        [ctypes.c_void_p] * 5 + [ctypes.c_int64, ctypes.c_void_p]),
     "pxl_bl_fit_adjoint": (ctypes.c_int32, [ctypes.c_void_p] * 3 + [ctypes.c_int32, ctypes.c_double] +
                            [ctypes.c_void_p] * 3 + [ctypes.c_int32] + [ctypes.c_void_p] * 5 +
                            [ctypes.c_int64, ctypes.c_void_p]),

@@ -81,3 +81,28 @@ def bl_fit_adjoint(hits: torch.Tensor, hits_ge: torch.Tensor, offsets: torch.Ten
                                            ptr(out.get("grad_align64")), ws.data_ptr(), ws.numel(), s),
           "pxl_bl_fit_adjoint")
     return out
+
+
+def riemann_fit(hits: torch.Tensor, hits_ge: torch.Tensor, offsets: torch.Tensor, b_field: float,
+                precision: int = 0, stream: torch.cuda.Stream | None = None,
+                ws: torch.Tensor | None = None) -> dict[str, torch.Tensor]:
+    """Riemann helix fits (pxl_riemann_fit): state (n, 5) = (phi, d0, q/pT, cot(theta), zip),
+    chi2 (n, 2) = (circle, line), pt, status."""
+    if not (hits.is_cuda and hits_ge.is_cuda and offsets.is_cuda):
+        raise ValueError("riemann_fit takes CUDA tensors")
+    hits = hits.contiguous().to(torch.float64)
+    hits_ge = hits_ge.contiguous().to(torch.float32)
+    offsets = offsets.contiguous().to(torch.int32)
+    n = offsets.numel() - 1
+    dev = hits.device
+    out = {"state": torch.empty((n, 5), dtype=torch.float32, device=dev),
+           "chi2": torch.empty((n, 2), dtype=torch.float32, device=dev),
+           "pt": torch.empty(n, dtype=torch.float32, device=dev),
+           "status": torch.empty(n, dtype=torch.int32, device=dev)}
+    ws = workspace(n, dev) if ws is None else ws
+    s = (stream or torch.cuda.current_stream(dev)).cuda_stream
+    check(_native.lib().pxl_riemann_fit(hits.data_ptr(), hits_ge.data_ptr(), offsets.data_ptr(), n, float(b_field),
+                                        int(precision), out["state"].data_ptr(), out["chi2"].data_ptr(),
+                                        out["pt"].data_ptr(), out["status"].data_ptr(), ws.data_ptr(), ws.numel(), s),
+          "pxl_riemann_fit")
+    return out

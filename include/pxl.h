@@ -271,6 +271,17 @@ int32_t pxl_bl_fit(const double* hits, const float* hits_ge, const int32_t* hit_
                    int32_t precision, float* state, float* cov, float* chi2, float* pt, float* eta, int32_t* status,
                    void* workspace, int64_t workspace_bytes, void* stream);
 
+/* Stand-alone Riemann helix fits (plugin-PixelTriplets/riemann_fit.jl: fast_fit, the
+ * Riemann-Chernov circle_fit with multiple scattering, line_fit in the rotated s-z plane),
+ * parameters and chi2 (no covariance propagation). Same track inputs and workspace as
+ * pxl_bl_fit; precision 0 = FP64, 1 = FP32 per-hit geometry and covariance models with
+ * FP64 Cholesky inverses, scatter matrix, 3x3 eigenproblem and final parameters.
+ * Outputs (device): state[5*n] (phi, d0, q/pT, cot(theta), zip), chi2[2*n] (circle, line),
+ * pt[n], status[n] (0 ok, 1 non-finite result, -1 bad hit count). */
+int32_t pxl_riemann_fit(const double* hits, const float* hits_ge, const int32_t* hit_offsets, int32_t n_tracks,
+                        double b_field, int32_t precision, float* state, float* chi2, float* pt, int32_t* status,
+                        void* workspace, int64_t workspace_bytes, void* stream);
+
 /* Adjoint of the broken-line fit: per track the FP64 chi2 = chi2_line + chi2_circle and
  * its gradient with respect to the hit coordinates, the fit being recomputed in the
  * backward pass (nothing stored between passes). Same track inputs as pxl_bl_fit.

@@ -226,6 +226,12 @@ double orc_run_batch(OrcCtx* c, const uint8_t* blob, const uint64_t* offsets, in
   return std::chrono::duration<double>(t1 - t0).count();
 }
 
+// Riemann fit of one track
+int32_t orc_riemann_fit(const double* hits, const float* ge, int32_t n, double B, double* state5, double* chi2,
+                        double* pt) {
+  return riemann_fit_track(hits, ge, n, B, state5, chi2, chi2 + 1, pt);
+}
+
 // forward-mode gradient of one track's chi2 (chi2_line + chi2_circle) w.r.t. its hits
 double orc_bl_chi2_grad_fwd(const double* hits, const float* ge, int32_t n, double B, double* grad) {
   return bl_chi2_grad_fwd(hits, ge, n, B, grad);

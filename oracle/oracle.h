@@ -215,4 +215,10 @@ int bl_fit_track(const double* hits, const float* ge, int n, double B, double* s
 // coordinates (grad[3n], hit-major) by forward-mode dual numbers (brokenline_fwd.cpp)
 double bl_chi2_grad_fwd(const double* hits, const float* ge, int n, double B, double* grad);
 
+// Riemann helix fit of one track (riemann.cpp): state5 = (phi, d0, q/pT, cot(theta), zip),
+// the circle and line chi2 and pT; hits row-major per hit, ge 6 per hit. Returns 0 or 1
+// (non-finite result), -1 for a hit count outside 3..8.
+int riemann_fit_track(const double* hits, const float* ge, int n, double B, double* state5, double* chi2_circle,
+                      double* chi2_line, double* pt);
+
 }  // namespace orc

@@ -61,6 +61,8 @@ def lib() -> ctypes.CDLL:
         _lib.orc_bl_fit.argtypes = [V, V, ctypes.c_int32, ctypes.c_double, V, V, V, V, V, V]
         _lib.orc_bl_chi2_grad_fwd.restype = ctypes.c_double
         _lib.orc_bl_chi2_grad_fwd.argtypes = [V, V, ctypes.c_int32, ctypes.c_double, V]
+        _lib.orc_riemann_fit.restype = ctypes.c_int32
+        _lib.orc_riemann_fit.argtypes = [V, V, ctypes.c_int32, ctypes.c_double, V, V, V]
         _lib.orc_bl_fit_batch.restype = ctypes.c_double
         _lib.orc_bl_fit_batch.argtypes = [V, V, V, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, V, V]
         _lib.orc_run_batch.restype = ctypes.c_double
@@ -178,3 +180,15 @@ def bl_chi2_grad_fwd(hits: np.ndarray, ge: np.ndarray, B: float):
     grad = np.zeros_like(h)
     c = lib().orc_bl_chi2_grad_fwd(h.ctypes.data, g.ctypes.data, h.shape[0], B, grad.ctypes.data)
     return c, grad
+
+
+def riemann_fit(hits: np.ndarray, ge: np.ndarray, B: float) -> dict:
+    """Riemann helix fit of one track: hits (N, 3) float64, ge (N, 6) float32. state =
+    (phi, d0, q/pT, cot(theta), zip)."""
+    h = np.ascontiguousarray(hits, np.float64)
+    g = np.ascontiguousarray(ge, np.float32)
+    st = np.zeros(5)
+    c2 = np.zeros(2)
+    pt = np.zeros(1)
+    rc = lib().orc_riemann_fit(h.ctypes.data, g.ctypes.data, h.shape[0], B, st.ctypes.data, c2.ctypes.data, pt.ctypes.data)
+    return {"rc": rc, "state": st, "chi2_circle": c2[0], "chi2_line": c2[1], "pt": pt[0]}
