@@ -206,10 +206,13 @@ def bench_fits(args, local: int, rank: int, world: int) -> dict:
     d = np.abs(a[ok] - b[ok])
     stats = lambda v: {"median": float(np.median(v)), "p99": float(np.percentile(v, 99)), "max": float(v.max())}
     def param_err(a, b, ok):
+        bad = ok & ~np.all(np.isfinite(a), axis=1)  # finite in FP64, not in the mixed mode
+        ok = ok & ~bad
         d = np.abs(a[ok] - b[ok])
         return {"q_over_pt_rel": stats(d[:, 2] / np.abs(b[ok, 2])), "phi_abs_rad": stats(d[:, 0]),
                 "cot_theta_rel": stats(d[:, 3] / np.maximum(np.abs(b[ok, 3]), 1e-3)),
-                "d0_abs_cm": stats(d[:, 1]), "z0_abs_cm": stats(d[:, 4]), "tracks": int(ok.sum())}
+                "d0_abs_cm": stats(d[:, 1]), "z0_abs_cm": stats(d[:, 4]), "tracks": int(ok.sum()),
+                "nonfinite_mixed": int(bad.sum())}
     err = param_err(a, b, ok)
     rb = rres["riemann_fp64"]["state"]
     rok = np.all(np.isfinite(rb), axis=1) & (rres["riemann_fp64"]["status"] == 0)

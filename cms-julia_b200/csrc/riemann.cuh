@@ -10,9 +10,10 @@
 // and tan(theta) in the line's scattering term, and (phi, d0, pT) from the circle
 // geometry (pT = R B).
 //
-// Precision: T is the type of the per-hit geometry and the covariance models;
-// the inverses of the N x N covariance matrices (Cholesky), the scatter matrix,
-// its 3x3 eigenproblem and the final parameters are FP64.
+// Precision: T is the type of the per-hit geometry and the scattering models;
+// the per-hit projected variances, the inverses of the N x N covariance matrices
+// (Cholesky), the scatter matrix, its 3x3 eigenproblem and the final parameters
+// are FP64.
 #pragma once
 #include "bl_fit.cuh"
 
@@ -167,7 +168,8 @@ BL_HD bool riemann_fit(const double hits[3][N], const float ge[6][N], double Bd,
 #pragma unroll
     for (int i = 0; i < N; ++i) {
       const T rl = (i == 0 ? sv[0] * k3 : s_abs(sv[i] * k3 - sv[i - 1] * k3)) * x0inv;
-      const T l = T(1) + T(0.038) * s_log<T>(rl);
+      // (1 + 0.038 ln x)^2 x -> 0 as x -> 0: the continuous value where a length rounds to 0
+      const T l = rl > T(0) ? T(1) + T(0.038) * s_log<T>(rl) : T(0);
       sig2[i] = l * l * rl * T(0.000225) / (p_2 * st * st);
     }
 #pragma unroll
@@ -182,18 +184,20 @@ BL_HD bool riemann_fit(const double hits[3][N], const float ge[6][N], double Bd,
       }
 #pragma unroll
     for (int i = 0; i < N; ++i) {
-      const T vxx = T(ge[0][i]), vxy = T(ge[1][i]), vyy = T(ge[2][i]);
-      T d;
+      // projected variance (cov_carttorad_prefit): its three terms cancel almost exactly
+      // for hits near the coordinate axes, so it is evaluated in FP64 in both modes
+      const double vxx = ge[0][i], vxy = ge[1][i], vyy = ge[2][i];
+      double d;
       if (rad[i] < T(1e-4)) {
         d = vxx;
       } else {
-        const T ax = T(hits[0][i]), ay = T(hits[1][i]);
-        const T bx = ax - gcx, by = ay - gcy;
-        const T x2 = ax * bx + ay * by, y2 = ax * by - ay * bx;
-        const T tc = -y2 / x2, tc2 = tc * tc;
-        d = T(1) / (T(1) + tc2) * (vxx + vyy * tc2 + T(2) * vxy * tc);
+        const double ax = hits[0][i], ay = hits[1][i];
+        const double bx = ax - double(gcx), by = ay - double(gcy);
+        const double x2 = ax * bx + ay * by, y2 = ax * by - ay * bx;
+        const double tc = -y2 / x2, tc2 = tc * tc;
+        d = 1.0 / (1.0 + tc2) * (vxx + vyy * tc2 + 2.0 * vxy * tc);
       }
-      Cr[i][i] += double(d);
+      Cr[i][i] += d;
     }
   }
   double G[N][N];
@@ -311,7 +315,7 @@ BL_HD bool riemann_fit(const double hits[3][N], const float ge[6][N], double Bd,
 #pragma unroll
     for (int i = 0; i < N; ++i) {
       const T rl = (i == 0 ? S3[0] : s_abs(S3[i] - S3[i - 1])) * x0inv;
-      const T l = T(1) + T(0.038) * s_log<T>(rl);
+      const T l = rl > T(0) ? T(1) + T(0.038) * s_log<T>(rl) : T(0);
       sig2[i] = T(0.000225) / p_2 * (l * l) * rl;
     }
 #pragma unroll
