@@ -135,12 +135,14 @@ __device__ __forceinline__ uint32_t doublets_of_item(const Dev& d, int e, uint32
         if (__dmul_rn(__dmul_rn(dphi_f, dphi_f), __dsub_rn(r2t4, double(rr))) > double(__fmul_rn(dd, dd))) continue;
       }
       if (kFill) {
-        const uint64_t g = cell_pos + cnt;
-        if (g - cell_lo < cap && g < uint64_t(d.cap_cells)) {
+        // cell_pos: the item's first position within the event, cell_lo: the event's region
+        const uint64_t local = cell_pos + cnt;
+        if (local < cap) {
+          const uint64_t g = cell_lo + local;
           d.cell_inner[g] = i;
           d.cell_outer[g] = oi;
           d.cell_pair[g] = uint8_t(pid);
-          d.cell_id[g] = int32_t(g - cell_lo + 1);
+          d.cell_id[g] = int32_t(local + 1);
           d.cell_used[g] = 0;
           d.cell_inner_z[g] = me_z;
           d.cell_inner_r[g] = me_r;
@@ -170,10 +172,14 @@ __global__ void __launch_bounds__(256) k_doublets(Dev d, const uint32_t* __restr
   const uint32_t* poff = d.phi_off + size_t(e) * kPhiTotBins;
   const uint16_t* pbins = d.phi_bins + hb;
   const uint32_t ib = E.item_base;
-  const uint64_t cell_lo = kFill ? uint64_t(d.item_cnt[ib]) : 0;
+  // raw positions of the count scan are made local to the event; the event keeps its
+  // first n_cells doublets, stored from cell_base on
+  const uint32_t raw_lo = kFill ? d.item_cnt[ib] : 0u;
+  const uint64_t cell_lo = E.cell_base;
+  const uint32_t keep = E.n_cells;
   for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
     if (kFill) {
-      doublets_of_item<true>(d, e, j, s_cum, s_hls, hv, poff, pbins, d.item_cnt[ib + j], cell_lo, d.doublets_per_event);
+      doublets_of_item<true>(d, e, j, s_cum, s_hls, hv, poff, pbins, d.item_cnt[ib + j] - raw_lo, cell_lo, keep);
     } else {
       d.item_cnt[ib + j] = doublets_of_item<false>(d, e, j, s_cum, s_hls, hv, poff, pbins, 0, 0, 0);
     }
@@ -183,26 +189,21 @@ __global__ void __launch_bounds__(256) k_doublets(Dev d, const uint32_t* __restr
 // per event: cell base, raw and capped counts
 __global__ void k_cell_bases(Dev d) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e > d.E) return;
-  if (e == d.E) {  // batch total of raw cells (the live length of the per-cell arrays)
-    d.ev[e].n_cells_raw = d.item_cnt[d.ev[d.E].item_base];
-    d.ev[e].cell_base = d.ev[e].n_cells_raw;
-    if (uint64_t(d.ev[e].n_cells_raw) > uint64_t(d.cap_cells)) atomicOr(d.status, kWarnBuffer);
-    return;
-  }
+  if (e >= d.E) return;
   EvInfo& E = d.ev[e];
   const uint32_t lo = d.item_cnt[E.item_base], hi = d.item_cnt[E.item_base + E.n_items];
   E.n_cols_nb = 0;
   E.n_cols_tr = 0;
-  E.cell_base = lo;
-  E.n_cells_raw = hi - lo;
-  uint32_t n = hi - lo;
+  uint32_t n = hi - lo;  // doublets found; the reference keeps the first doublets_per_event
   if (n > d.doublets_per_event) { n = d.doublets_per_event; E.warnings |= kWarnDoublets; }
-  if (uint64_t(lo) + n > uint64_t(d.cap_cells)) {
-    E.warnings |= kWarnBuffer;
-    n = lo < uint64_t(d.cap_cells) ? uint32_t(d.cap_cells - lo) : 0u;
-  }
   E.n_cells = n;
+}
+
+// after the event scan of n_cells: events past the buffer are emptied, regions fixed
+__global__ void k_cell_regions(Dev d) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e > d.E) return;
+  d.ev[e].n_cells_raw = d.ev[e].n_cells;
 }
 
 // zero the per-cell and per-hit counters of the batch (raw cell ranges, gaps included)
@@ -358,6 +359,7 @@ __global__ void __launch_bounds__(256) k_connect(Dev d) {
         const uint32_t o = d.ohc_list[lo + j];
         const uint32_t pos = d.cn_cnt[o] + atomicAdd(&d.cn_cur[o], 1u);
         if (pos < uint64_t(d.cap_pairs)) d.cn_list[pos] = uint32_t(c);
+        else atomicOr(d.status, kWarnBuffer);
       }
     }
   }
@@ -377,7 +379,10 @@ __global__ void k_sort_cell_lists(Dev d) {
     const uint64_t c = cb + k;
     const uint32_t* cnt = kKind == 0 ? d.cn_cnt : d.ct_cnt;
     uint32_t* list = kKind == 0 ? d.cn_list : d.ct_list;
-    const uint32_t lo = cnt[c], hi = cnt[c + 1];
+    const uint32_t lo = cnt[c];
+    uint32_t hi = cnt[c + 1];
+    const uint64_t lcap = uint64_t(kKind == 0 ? d.cap_pairs : d.cap_tuple_hits);
+    if (uint64_t(hi) > lcap) hi = uint32_t(lcap);
     if (hi > lo) {
       ++cols;
       sort_list(list + lo, hi - lo);
@@ -466,6 +471,8 @@ __device__ void walk(const Dev& d, uint64_t cb, uint64_t start, uint64_t* tuple_
     const uint32_t lo = d.cn_cnt[c];
     uint32_t nn = d.cn_cnt[c + 1] - lo;
     if (nn > uint32_t(kCellRows)) nn = kCellRows;
+    // entries past the pair buffer were not stored (buffer warning raised by the fill)
+    if (uint64_t(lo) + nn > uint64_t(d.cap_pairs)) nn = uint64_t(lo) < uint64_t(d.cap_pairs) ? uint32_t(d.cap_pairs - lo) : 0u;
     bool pushed = false;
     while (stack_k[depth] < nn) {
       const uint32_t o = d.cn_list[lo + stack_k[depth]];
@@ -668,6 +675,9 @@ void launch_ca(const Dev& d, const Launch& L) {
   L.mark("doublets_count");
   excl_scan_u32(d.item_cnt, d.cap_items, &d.ev[d.E].n_items, d.scan_tmp, L.s);
   k_cell_bases<<<eb, 128, 0, L.s>>>(d);
+  launch_ev_scan(d, L.s, int(offsetof(EvInfo, n_cells)), int(offsetof(EvInfo, cell_base)));
+  launch_ev_clamp(d, L.s, int(offsetof(EvInfo, n_cells)), int(offsetof(EvInfo, cell_base)), d.cap_cells);
+  k_cell_regions<<<eb, 128, 0, L.s>>>(d);
   L.mark("doublets_scan");
   k_doublets<true><<<g(kTuneDoublets), 256, 0, L.s>>>(d, pair_cum);
   L.mark("doublets_fill");

@@ -350,4 +350,28 @@ void launch_ev_scan(const Dev& d, cudaStream_t s, int count_off, int base_off) {
   k_ev_scan<<<1, 1024, 0, s>>>(d.ev, d.E, count_off, base_off);
 }
 
+// Events whose region [base, base + count) would pass the buffer capacity are
+// emptied (count = 0, buffer warning) and the batch total is capped, so that no
+// later kernel indexes past the buffer.
+__global__ void k_ev_clamp(EvInfo* ev, int E, int count_off, int base_off, int64_t cap, uint32_t* status) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e > E) return;
+  char* b = reinterpret_cast<char*>(ev) + size_t(e) * sizeof(EvInfo);
+  uint32_t& cnt = *reinterpret_cast<uint32_t*>(b + count_off);
+  const uint32_t base = *reinterpret_cast<const uint32_t*>(b + base_off);
+  if (e == E) {
+    if (int64_t(cnt) > cap) cnt = uint32_t(cap);
+    return;
+  }
+  if (int64_t(base) + int64_t(cnt) > cap) {
+    cnt = 0;
+    atomicOr(&ev[e].warnings, kWarnBuffer);
+    atomicOr(status, kWarnBuffer);
+  }
+}
+
+void launch_ev_clamp(const Dev& d, cudaStream_t s, int count_off, int base_off, int64_t cap) {
+  k_ev_clamp<<<div_up(d.E + 1, 128), 128, 0, s>>>(d.ev, d.E, count_off, base_off, cap, d.status);
+}
+
 }  // namespace pxl

@@ -275,6 +275,7 @@ int run_chain(PxlCtx* ctx, uint32_t mask, cudaStream_t s) {
     launch_raw(d, L, ctx->fed_slot_of);
     launch_cluster(d, L);
     launch_ev_scan(d, s, int(offsetof(EvInfo, n_hits)), int(offsetof(EvInfo, hit_base)));
+    launch_ev_clamp(d, s, int(offsetof(EvInfo, n_hits)), int(offsetof(EvInfo, hit_base)), d.cap_hits);
   }
   if (mask & PXL_STAGE_HITS) launch_rechits(d, L);
   if (mask & PXL_STAGE_TUPLES) launch_ca(d, L);

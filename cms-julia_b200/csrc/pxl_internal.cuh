@@ -78,7 +78,7 @@ struct EvInfo {
   uint32_t n_hits, hit_base;
   uint32_t n_items, item_base;      // doublet work items (inner hits over the layer pairs)
   uint32_t n_cells, cell_base;
-  uint32_t n_cells_raw;             // doublets found before the per-event cap
+  uint32_t n_cells_raw;             // length of the event's cell region (= n_cells)
   uint32_t n_tuples, tuple_base;
   uint32_t n_tuple_hits, tuple_hit_base;
   uint32_t n_tuples_raw, n_tuple_hits_raw;
@@ -272,6 +272,7 @@ struct Launch {
 void launch_raw(const Dev& d, const Launch& L, const int16_t* fed_slot_of);  // a1-a4
 void launch_modstart(const Dev& d, const Launch& L);  // a4 only (digis already in place)
 void launch_ev_scan(const Dev& d, cudaStream_t s, int count_off, int base_off);
+void launch_ev_clamp(const Dev& d, cudaStream_t s, int count_off, int base_off, int64_t cap);
 void launch_cluster(const Dev& d, const Launch& L);   // a5-a7
 void launch_rechits(const Dev& d, const Launch& L);   // a8-a9
 void launch_ca(const Dev& d, const Launch& L);        // a10-a14
