@@ -153,6 +153,7 @@ def bench_uneven(args, local: int, rank: int, world: int, plain_value: float) ->
     autotuner, one captured CUDA graph per step. Events above PU ~140 reach the reference's
     per-event doublet and tuple capacities, which truncate them as the reference does."""
     import torch
+    from pixeltrack import dist as pdist
     from pixeltrack import PixelChain, batch_params, gen
     E = args.uneven_events
     conds = gen.conditions()
@@ -178,7 +179,7 @@ def bench_uneven(args, local: int, rank: int, world: int, plain_value: float) ->
         chain.launch_graph(sh)
     t1.record(stream)
     t1.synchronize()
-    ms = t0.elapsed_time(t1) / args.uneven_steps
+    ms = pdist.max_over_ranks(t0.elapsed_time(t1), device=torch.device("cuda", local)) / args.uneven_steps
     tot = {"digis_min": 10 ** 9, "digis_max": 0, "hits": 0, "cells": 0, "tuples": 0, "vertices": 0,
            "capped_events": 0, "buffer_overflow_events": 0}
     from pixeltrack._native import WARN_BITS
@@ -207,6 +208,7 @@ def bench_fits(args, local: int, rank: int, world: int) -> dict:
     mode against the FP64 mode on every track, and of the FP64 mode against the CPU oracle on
     a sample. Inputs resident in HBM (about 210 MB, larger than L2)."""
     import torch
+    from pixeltrack import dist as pdist
     from pixeltrack import gen
     from pixeltrack.fits import bl_fit, workspace
     n = args.fit_tracks
@@ -230,7 +232,7 @@ def bench_fits(args, local: int, rank: int, world: int) -> dict:
                 r = bl_fit(hits, ge, offs, FIT_B, precision=prec, stream=stream, ws=ws)
             t1.record(stream)
             t1.synchronize()
-            ms = t0.elapsed_time(t1) / args.steps
+            ms = pdist.max_over_ranks(t0.elapsed_time(t1), device=dev) / args.steps
             res[name] = {k: v.double().cpu().numpy() for k, v in r.items() if k in ("state", "pt", "status")}
             out[name] = {"fits_per_s": world * n / (ms / 1e3), "ms_per_step": ms}
     # Riemann fits of the same tracks
@@ -247,7 +249,7 @@ def bench_fits(args, local: int, rank: int, world: int) -> dict:
                 r = riemann_fit(hits, ge, offs, FIT_B, precision=prec, stream=stream, ws=ws)
             t1.record(stream)
             t1.synchronize()
-            ms = t0.elapsed_time(t1) / args.steps
+            ms = pdist.max_over_ranks(t0.elapsed_time(t1), device=dev) / args.steps
             rres[name] = {k: v.double().cpu().numpy() for k, v in r.items() if k in ("state", "status")}
             out[name] = {"fits_per_s": world * n / (ms / 1e3), "ms_per_step": ms}
     nh = np.diff(w["offsets"]).astype(np.int64)
@@ -303,6 +305,7 @@ def bench_adjoint(args, local: int, rank: int, world: int) -> dict:
     intermediates); the gradient is checked against the oracle's forward-mode derivative and
     central finite differences (h = 1e-6 cm) on a sample."""
     import torch
+    from pixeltrack import dist as pdist
     from pixeltrack import gen
     from pixeltrack.fits import bl_fit_adjoint
     n = args.fit_tracks
@@ -328,7 +331,7 @@ def bench_adjoint(args, local: int, rank: int, world: int) -> dict:
             out = bl_fit_adjoint(hits, ge, offs, FIT_B, mod, mpos, al, True, stream=stream)
         t1.record(stream)
         t1.synchronize()
-    ms = t0.elapsed_time(t1) / args.steps
+    ms = pdist.max_over_ranks(t0.elapsed_time(t1), device=dev) / args.steps
     peak_extra = torch.cuda.max_memory_allocated(dev) - base_mem
     g = out["grad_hits"].double().cpu().numpy()
     # moved hits (as the kernel sees them) for the oracle checks
@@ -421,17 +424,15 @@ def main():
         run_reference(args, rank, world)
         return
     import torch
+    from pixeltrack import dist as pdist
     dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     torch.cuda.set_device(local)
+    if pdist.init("nccl"):
+        import torch.distributed as dist
     from pixeltrack import PixelChain, batch_params, default_params, gen
     conds = gen.conditions()
     E = args.events
-    blob, offs = gen.events(E, gen.MODE_PU, pu=args.pu, seed=args.seed + 7919 * rank)
+    blob, offs = gen.events(E, gen.MODE_PU, pu=args.pu, seed=pdist.rank_seed(args.seed, rank))
     words = np.diff(offs).sum() // 4
     params = batch_params(E, words_per_event=int(words / E * 1.3) + 4096, hits_per_event_avg=16_000,
                           doublets_per_event_avg=140_000, tuples_per_event_avg=11_000, device=local,
@@ -491,11 +492,7 @@ def main():
             chain.launch_graph(sh)
         t1.record(stream)
         t1.synchronize()
-    ms = t0.elapsed_time(t1)
-    if dist:
-        tt = torch.tensor([ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = pdist.max_over_ranks(t0.elapsed_time(t1), device="cuda")
     ms_per_step = ms / args.steps
     value = world * E * args.steps / (ms / 1e3)
 
@@ -521,11 +518,7 @@ def main():
         chain.results_async(res.data_ptr(), E, sh)
     e1.record(stream)
     e1.synchronize()
-    ems = e0.elapsed_time(e1)
-    if dist:
-        tt = torch.tensor([ems], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ems = float(tt.item())
+    ems = pdist.max_over_ranks(e0.elapsed_time(e1), device="cuda")
     e2e_value = world * E * args.steps / (ems / 1e3)
     nv_check = int(res.numpy().sum())
 

@@ -329,6 +329,7 @@ void launch_raw(const Dev& d, const Launch& L, const int16_t* fed_slot_of) {
   L.mark("start");
   k_fed_table<<<d.E, 256, 0, L.s>>>(d, fed_slot_of);
   k_ev_scan<<<1, 1024, 0, L.s>>>(d.ev, d.E, int(offsetof(EvInfo, n_words)), int(offsetof(EvInfo, word_base)));
+  launch_ev_clamp(d, L.s, int(offsetof(EvInfo, n_words)), int(offsetof(EvInfo, word_base)), d.cap_words);
   L.mark("fed_table");
   dim3 g(NF, d.E);
   k_unpack<<<g, 256, 0, L.s>>>(d);

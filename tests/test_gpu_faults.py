@@ -1,0 +1,89 @@
+"""Failure injection on the host (no device fault is ever provoked): corrupted FED
+payload words, a FED directory that announces more FEDs than the event holds, and batch
+buffers too small for the batch. The chain must flag what the reference flags, keep the
+results of everything that fits identical to the oracle's, and never fault."""
+import numpy as np
+import pytest
+
+from oracle import oracle
+from parity import compare_digis_clusters, compare_hits
+
+pytestmark = pytest.mark.gpu
+
+
+def _corrupt_words(ev: bytes, rng, frac: float) -> bytes:
+    from pixeltrack.formats import FedRawData, FedRawDataCollection
+    c = FedRawDataCollection.from_bytes(ev)
+    for fid, fd in list(c.feds.items()):
+        if len(fd.data) < 24:
+            continue
+        w = np.frombuffer(fd.data, dtype=np.uint32).copy()
+        payload = np.arange(2, len(w) - 2)  # 8-byte header and trailer kept
+        pick = payload[rng.random(len(payload)) < frac]
+        w[pick] ^= (rng.integers(1, 1 << 31, len(pick), dtype=np.uint64)).astype(np.uint32)
+        c.feds[fid] = FedRawData(fid, w.tobytes())
+    return c.to_bytes()
+
+
+def _errors(chain, e):
+    g = chain.product("errors", e)
+    return g.reshape(-1, 4) if g.size else g.reshape(0, 4)
+
+
+def test_corrupted_words_match_oracle(conditions, events_pu50):
+    from pixeltrack import PixelChain, default_params
+    blob, offs = events_pu50
+    rng = np.random.default_rng(3)
+    orc = oracle.Oracle(conditions)
+    with PixelChain(conditions, default_params()) as chain:
+        for e in range(2):
+            ev = _corrupt_words(bytes(blob[offs[e]:offs[e + 1]]), rng, 0.02)
+            chain.run_event(ev, 3)
+            orc.run_event(ev, 3)
+            errs = compare_digis_clusters(chain, orc, 0) + compare_hits(chain, orc, 0)
+            assert not errs, errs
+            ge, oe = _errors(chain, 0), orc.get("errors").reshape(-1, 4)
+            assert len(ge) == len(oe) > 0
+            # records are appended in parallel: compare as sets of (rawId, word, type, fed)
+            assert sorted(map(tuple, ge.tolist())) == sorted(map(tuple, oe.tolist()))
+
+
+def test_directory_announcing_missing_feds(conditions, events_pu50):
+    from pixeltrack import PixelChain, default_params
+    blob, offs = events_pu50
+    ev = bytearray(blob[offs[0]:offs[1]])
+    n = int.from_bytes(ev[:4], "little")
+    ev[:4] = (n + 3).to_bytes(4, "little")  # three FEDs more than the event holds
+    orc = oracle.Oracle(conditions)
+    with PixelChain(conditions, default_params()) as chain:
+        chain.run_event(bytes(ev), 3)
+        orc.run_event(bytes(ev), 3)
+        errs = compare_digis_clusters(chain, orc, 0) + compare_hits(chain, orc, 0)
+        assert not errs, errs
+        assert chain.counts(0).warnings & 0x800  # the truncated directory is flagged
+
+
+def test_batch_buffers_too_small(conditions, events_pu50):
+    """Hit buffer for about two of the four events: the events that fit are exact through
+    the whole chain, the others are emptied with the buffer warning, and the run completes."""
+    from pixeltrack import PixelChain, batch_params
+    from parity import compare_ca
+    blob, offs = events_pu50
+    orc = oracle.Oracle(conditions)
+    nh = []
+    for e in range(4):
+        orc.run_event(blob[offs[e]:offs[e + 1]], 3)
+        nh.append(orc.counts()["n_hits"])
+    cap = nh[0] + nh[1] + nh[2] // 2
+    params = batch_params(4, hits_per_event_avg=cap // 4 + 1)
+    with PixelChain(conditions, params) as bc:
+        bc.run_batch(blob, offs, stages=7)
+        warn = bc.sync()
+        assert warn & 0x800
+        for e in range(2):
+            orc.run_event(blob[offs[e]:offs[e + 1]], 7)
+            errs = compare_digis_clusters(bc, orc, e) + compare_hits(bc, orc, e) + compare_ca(bc, orc, e)
+            assert not errs, (e, errs)
+        for e in (2, 3):
+            c = bc.counts(e)
+            assert c.warnings & 0x800 and c.n_hits == 0 and c.n_doublets == 0 and c.n_tuples == 0
