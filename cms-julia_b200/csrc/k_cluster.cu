@@ -67,9 +67,10 @@ __device__ __forceinline__ bool module_range(const Dev& d, int e, uint32_t m, Mo
   const uint64_t eb = E.word_base;
   const uint32_t* ms = d.module_start + size_t(e) * (kMaxNumModules + 1);
   const uint32_t first1 = ms[m + 1];  // 1-based
-  uint32_t msize = (m + 1 < nmod) ? ms[m + 2] : n_el;
-  if (first1 < 1 || first1 > n_el || msize < first1 || msize > n_el) return false;
+  if (first1 < 1 || first1 > n_el) return false;
   r.this_id = d.mid[eb + first1 - 1];
+  uint32_t msize = module_end1(d.mid, eb, ms, m, nmod, n_el, first1, r.this_id);
+  if (msize < first1 || msize > n_el) return false;
   r.truncated = false;
   if (msize - first1 > uint32_t(kMaxPixInModule)) {
     msize = uint32_t(kMaxPixInModule) + first1;
@@ -81,11 +82,15 @@ __device__ __forceinline__ bool module_range(const Dev& d, int e, uint32_t m, Mo
   return true;
 }
 
+// Module positions are clustered in parallel; a module id seen in several runs of one
+// event (only malformed data does that) keeps the count of its last run, as the serial
+// loop leaves it: the count is stored with its position as the key of an atomicMax
+// ((position + 1) << 11 | count, count <= 1024) and k_hits_module_start strips the key.
 __device__ __forceinline__ void write_module_record(const Dev& d, int e, uint32_t m, int16_t this_id, uint32_t nclus,
                                                     uint32_t warn) {
   d.module_id[size_t(e) * kMaxNumModules + m] = uint32_t(uint16_t(this_id));
   if (uint16_t(this_id) < uint16_t(kMaxNumModules))
-    d.clus_in_module[size_t(e) * kMaxNumModules + uint16_t(this_id)] = nclus;
+    atomicMax(&d.clus_in_module[size_t(e) * kMaxNumModules + uint16_t(this_id)], ((m + 1u) << 11) | nclus);
   if (warn) atomic_or_warn(&d.ev[e], warn);
 }
 
@@ -385,7 +390,9 @@ __global__ void __launch_bounds__(256) k_find_clus_block(Dev d) {
 __global__ void k_hits_module_start(Dev d) {
   const int e = blockIdx.x;
   __shared__ uint32_t sh[33];
-  const uint32_t* cim = d.clus_in_module + size_t(e) * kMaxNumModules;
+  uint32_t* cim = d.clus_in_module + size_t(e) * kMaxNumModules;
+  for (int i = threadIdx.x; i < kMaxNumModules; i += blockDim.x) cim[i] &= 0x7FFu;  // strip the position key
+  __syncthreads();
   uint32_t* cms = d.clus_module_start + size_t(e) * (kMaxNumModules + 1);
   const uint32_t cap = d.hits_per_event;
   uint32_t carry = 0;

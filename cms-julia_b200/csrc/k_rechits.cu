@@ -159,9 +159,13 @@ __device__ __forceinline__ bool hit_module(const Dev& d, int e, uint32_t m, HitM
   hm.nclus = d.clus_in_module[size_t(e) * kMaxNumModules + hm.me];
   if (hm.nclus == 0) return false;
   if (hm.nclus > uint32_t(kMaxClus)) hm.nclus = kMaxClus;
+  if (ms[m + 1] < 1 || ms[m + 1] > n_el) return false;
   hm.first0 = ms[m + 1] - 1;
-  hm.end0 = (m + 1 < nmod) ? ms[m + 2] - 1 : n_el;
-  if (ms[m + 1] < 1 || hm.end0 < hm.first0 || hm.end0 > n_el) return false;
+  const uint64_t eb = E.word_base;
+  // the module's first digi may have been invalidated by the charge cut: compare with its id
+  const uint32_t e1 = module_end1(d.mid, eb, ms, m, nmod, n_el, ms[m + 1], int16_t(hm.me));
+  hm.end0 = (m + 1 < nmod) ? e1 - 1 : n_el;
+  if (hm.end0 < hm.first0 || hm.end0 > n_el) return false;
   return true;
 }
 

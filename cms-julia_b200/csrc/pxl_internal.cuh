@@ -231,6 +231,22 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* sh, ui
 
 __device__ __forceinline__ void atomic_or_warn(EvInfo* ev, uint32_t bits) { atomicOr(&ev->warnings, bits); }
 
+// End of a module's digi range as find_clus and getHits bound it: the 1-based index of the
+// first valid digi with another module id after first1, or n_el if none. The next entry
+// of the module-start list holds exactly this, except when more than 2000 module runs
+// overflowed the list: its last slot then holds the last run, and the module before it
+// must scan (gpu_clustering.jl:106-114, gpuPixelRecHits.jl:149-156).
+__device__ __forceinline__ uint32_t module_end1(const int16_t* mid, uint64_t eb, const uint32_t* ms, uint32_t m,
+                                                uint32_t nmod, uint32_t n_el, uint32_t first1, int16_t this_id) {
+  if (m + 1 >= nmod) return n_el;
+  if (!(nmod == uint32_t(kMaxNumModules) && m + 2 == nmod)) return ms[m + 2];
+  for (uint32_t i1 = first1; i1 <= n_el; ++i1) {
+    const int16_t id = mid[eb + i1 - 1];
+    if (id != int16_t(kInvId) && id != this_id) return i1;
+  }
+  return n_el;
+}
+
 inline int div_up(int64_t a, int64_t b) { return int((a + b - 1) / b); }
 
 // ---------------------------------------------------------------- launchers (per stage file)

@@ -19,8 +19,12 @@ def _corrupt_words(ev: bytes, rng, frac: float) -> bytes:
             continue
         w = np.frombuffer(fd.data, dtype=np.uint32).copy()
         payload = np.arange(2, len(w) - 2)  # 8-byte header and trailer kept
+        # pixel address and ADC bits (invalid rows/columns give code 37), and a few words
+        # moved to ROC 25 (code 25); link and ROC stay otherwise, so module runs stay whole
         pick = payload[rng.random(len(payload)) < frac]
-        w[pick] ^= (rng.integers(1, 1 << 31, len(pick), dtype=np.uint64)).astype(np.uint32)
+        w[pick] ^= (rng.integers(1, 1 << 21, len(pick), dtype=np.uint64)).astype(np.uint32)
+        roc25 = payload[rng.random(len(payload)) < frac / 4]
+        w[roc25] = (w[roc25] & ~np.uint32(0x1F << 21)) | np.uint32(25 << 21)
         c.feds[fid] = FedRawData(fid, w.tobytes())
     return c.to_bytes()
 
