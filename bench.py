@@ -123,12 +123,17 @@ def segment_bytes(name: str, c: dict) -> float | None:
     table = {
         "unpack_calib": 4 * D + 22 * D,            # words in; xx,yy,adc,moduleInd,clus,pdigi,rawId out
         "module_starts": 4 * D,                    # moduleInd read by the count and fill passes
-        "find_clus_warp": 14 * D,                  # moduleInd,x,y,adc in; clus (and moduleInd) out
+        "find_clus_small": 14 * D,                 # moduleInd,x,y,adc in; clus (and moduleInd) out (modules <= 32 digis;
+                                                   # the larger ones only read their range bounds here)
         "get_hits_warp": 14 * D + 44 * H,          # digis in; 44 B hit SoA out
         "phi_binner": 4 * H,                       # iphi in; bins out
         "doublets_count": 14 * I + 4 * I,          # inner hit fields in; count out
         "doublets_fill": 14 * I + 4 * I + 22 * C,  # + cell SoA out
         "connect": 28 * C + 16 * C,                # cell fields in; neighbour masks out
+        "outer_hit_lists": 37 * C,                 # cell outer/inner/r/z in; lists and candidate records out
+        "neighbour_lists": 16 * C,                 # masks and list entries
+        "ntuplets_fill": 5 * T + 6 * TH,           # tuple offsets, hits, detector indices out
+        "fast_duplicate_remover": 12 * T,          # qualities in and out, cell track lists in
         "broken_line_fit_4": 22 * TH + 4 * TH + 8 * T + 93 * T,
         "vertices": 4 * T + 80 * T,
     }
@@ -138,7 +143,6 @@ def segment_bytes(name: str, c: dict) -> float | None:
 # dram__bytes_read.sum + dram__bytes_write.sum per unit of work, from ncu captures of the
 # 300-event case (profiles/), scaled to a launch by the units it processes
 TRAFFIC_PER_UNIT = {
-    "find_clus_warp": ("words", (125.75e6 + 38.76e6) / 12_349_460),
     "get_hits_warp": ("words", (182.15e6 + 103.86e6) / 12_349_460),
     "doublets_fill": ("cells", (374.91e6 + 786.06e6) / 25_257_080),
     "vertices": ("tuples", (79.25e6 + 18.84e6) / 2_062_854),

@@ -62,7 +62,7 @@ __global__ void k_items(Dev d, uint32_t* pair_cum) {
 template <bool kFill>
 __device__ __forceinline__ uint32_t doublets_of_item(const Dev& d, int e, uint32_t j, const uint32_t* cum,
                                                      const uint32_t* hls, const HitView& hv, const uint32_t* poff,
-                                                     const uint16_t* pbins, uint64_t cell_pos, uint64_t cell_lo,
+                                                     const HitRec* __restrict__ hrec, uint64_t cell_pos, uint64_t cell_lo,
                                                      uint32_t cap) {
   int pid = 0;
   while (j >= cum[pid]) ++pid;
@@ -91,24 +91,25 @@ __device__ __forceinline__ uint32_t doublets_of_item(const Dev& d, int e, uint32
   for (uint32_t cb = kl; cb != kh;) {
     const uint32_t p0 = poff[cb + h_off - 1], p1 = poff[cb + h_off];
     for (uint32_t p = p0; p < p1; ++p) {
-      const uint32_t oi = uint32_t(pbins[p]) - 1u;  // event-local 0-based
-      const int16_t mo = hv.detind[oi];
+      const HitRec hr = hrec[p];
+      const uint32_t oi = hr.id;  // event-local 0-based
+      const int16_t mo = hr.det;
       if (mo > 2000) continue;
-      const float zo = hv.zg[oi], ro = hv.rg[oi];
+      const float zo = hr.z, ro = hr.r;
       {  // z0_cut_off
         const float dr = __fsub_rn(ro, me_r);
         if (double(dr) > c_max_r[pid] || dr < 0 ||
             fabsf(__fsub_rn(__fmul_rn(me_z, ro), __fmul_rn(me_r, zo))) > __fmul_rn(z0_cut, dr))
           continue;
       }
-      const int16_t mo_p = hv.iphi[oi];
+      const int16_t mo_p = hr.iphi;
       const int16_t dphi = int16_t(mo_p - me_p);
       const int16_t i_dphi = int16_t(dphi < 0 ? -dphi : dphi);
       if (i_dphi > cut) continue;
       {  // z_size_cut
         bool kill;
         if (outer < 4) {
-          const int16_t so = hv.ysize[oi];
+          const int16_t so = hr.ysize;
           const int dy = inner == 0 ? 28 : 20;
           const int16_t ds = int16_t(so - int16_t(me_s));
           kill = me_s > 0 && so > 0 && (ds < 0 ? -int(ds) : int(ds)) > dy;
@@ -170,7 +171,7 @@ __global__ void __launch_bounds__(256) k_doublets(Dev d, const uint32_t* __restr
   const uint32_t hb = E.hit_base;
   HitView hv{d.xg + hb, d.yg + hb, d.zg + hb, d.rg + hb, d.iphi + hb, d.ysize + hb, d.detind + hb};
   const uint32_t* poff = d.phi_off + size_t(e) * kPhiTotBins;
-  const uint16_t* pbins = d.phi_bins + hb;
+  const HitRec* hrec = d.hit_rec + hb;
   const uint32_t ib = E.item_base;
   // raw positions of the count scan are made local to the event; the event keeps its
   // first n_cells doublets, stored from cell_base on
@@ -179,9 +180,9 @@ __global__ void __launch_bounds__(256) k_doublets(Dev d, const uint32_t* __restr
   const uint32_t keep = E.n_cells;
   for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
     if (kFill) {
-      doublets_of_item<true>(d, e, j, s_cum, s_hls, hv, poff, pbins, d.item_cnt[ib + j] - raw_lo, cell_lo, keep);
+      doublets_of_item<true>(d, e, j, s_cum, s_hls, hv, poff, hrec, d.item_cnt[ib + j] - raw_lo, cell_lo, keep);
     } else {
-      d.item_cnt[ib + j] = doublets_of_item<false>(d, e, j, s_cum, s_hls, hv, poff, pbins, 0, 0, 0);
+      d.item_cnt[ib + j] = doublets_of_item<false>(d, e, j, s_cum, s_hls, hv, poff, hrec, 0, 0, 0);
     }
   }
 }
@@ -311,6 +312,20 @@ __device__ __forceinline__ bool are_aligned(float r1, float z1, float ri, float 
   return __fmul_rn(t, p_min) <= __fmul_rn(__fmul_rn(theta_cut, d13), radius_diff);
 }
 
+// connect's candidates of each outer-hit list entry, gathered once per entry
+__global__ void __launch_bounds__(256) k_ohc_records(Dev d) {
+  const int e = blockIdx.y;
+  const EvInfo& E = d.ev[e];
+  const uint32_t hb = E.hit_base;
+  const uint32_t lo = d.ohc_cnt[hb], hi = d.ohc_cnt[uint64_t(hb) + E.n_hits];
+  for (uint32_t p = lo + blockIdx.x * blockDim.x + threadIdx.x; p < hi; p += gridDim.x * blockDim.x) {
+    const uint32_t o = d.ohc_list[p];
+    const uint32_t oih = d.cell_inner[o];
+    d.ohc_rec[p] = make_float4(d.cell_inner_r[o], d.cell_inner_z[o], d.xg[hb + oih], d.yg[hb + oih]);
+    d.ohc_inner[p] = d.detind[hb + oih] < 96 ? 1 : 0;
+  }
+}
+
 template <int kPass>
 __global__ void __launch_bounds__(256) k_connect(Dev d) {
   const int e = blockIdx.y;
@@ -334,17 +349,18 @@ __global__ void __launch_bounds__(256) k_connect(Dev d) {
       const bool is_barrel = det[ih] < 1184;
       uint32_t mask[4] = {0, 0, 0, 0};
       bool any = false;
+      const float xi = xg[ih], yi = yg[ih], xo = xg[oh], yo = yg[oh];
       for (uint32_t j = 0; j < n; ++j) {
-        const uint32_t o = d.ohc_list[lo + j];
-        const float r1 = d.cell_inner_r[o], z1 = d.cell_inner_z[o];
-        const uint32_t oih = d.cell_inner[o];
+        const float4 rec = d.ohc_rec[lo + j];  // the candidate's inner hit: r, z, x, y
+        const float r1 = rec.x, z1 = rec.y;
         const bool aligned = are_aligned(r1, z1, ri, zi, ro, zo, ptmin_f(), is_barrel ? kThetaBarrel : kThetaForward);
-        const float region = det[oih] < 96 ? kDcaInner : kDcaOuter;
-        const CircleEq eq(xg[oih], yg[oih], xg[ih], yg[ih], xg[oh], yg[oh]);
+        const float region = d.ohc_inner[lo + j] ? kDcaInner : kDcaOuter;
+        const CircleEq eq(rec.z, rec.w, xi, yi, xo, yo);
         bool cut;
         if (eq.c > kHardCurv) cut = false;
         else cut = fabsf(eq.dca0()) < __fmul_rn(region, fabsf(eq.c));
         if (aligned && cut) {
+          const uint32_t o = d.ohc_list[lo + j];
           mask[j >> 5] |= 1u << (j & 31);
           atomicAdd(&d.cn_cnt[o], 1u);
           d.cell_used[o] = 1;
@@ -687,6 +703,7 @@ void launch_ca(const Dev& d, const Launch& L) {
   excl_scan_u32(d.ohc_cnt, d.cap_hits, &d.ev[d.E].n_hits, d.scan_tmp, L.s);
   k_ohc<1><<<g(kTuneHitLists), 256, 0, L.s>>>(d);
   k_sort_hit_lists<0><<<g(kTuneHitLists), 256, 0, L.s>>>(d);
+  k_ohc_records<<<g(kTuneHitLists), 256, 0, L.s>>>(d);
   L.mark("outer_hit_lists");
   // connection and neighbour lists
   k_connect<0><<<g(kTuneConnect), 256, 0, L.s>>>(d);

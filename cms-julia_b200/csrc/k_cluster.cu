@@ -95,68 +95,113 @@ __device__ __forceinline__ void write_module_record(const Dev& d, int e, uint32_
 }
 
 // ------------------------------------------------------------ warp per module
+constexpr int kHistWords = 448;  // >= 420 column bins, 14 per lane
+
+template <int kSlots>
 struct WarpSmem {
-  int32_t lab[kWarpPix];
-  int32_t charge[kWarpPix];
-  uint16_t cid[kWarpPix];   // cluster number (1-based) of each root
-  uint16_t newc[kWarpPix];  // cluster number after the charge cut
+  int32_t lab[32 * kSlots];
+  int32_t charge[32 * kSlots];
+  uint16_t cid[32 * kSlots];   // cluster number (1-based) of each root
+  uint16_t newc[32 * kSlots];  // cluster number after the charge cut
 };
 
-__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_find_clus_warp(Dev d) {
-  __shared__ WarpSmem smem[kWarpsPerBlock];
-  const int e = blockIdx.y;
-  const unsigned lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+// column histogram of one module for the larger warp-clustered modules
+struct WarpHist {
+  uint32_t start[kHistWords];  // first sorted position of each column bin
+  uint32_t cur[kHistWords];
+  uint32_t xy[kWarpPix];       // x | column bin << 16 of each digi
+  uint8_t sorted[kWarpPix];    // digi indices ordered by column bin
+};
+
+// One module of at most 32 * kSlots digis, clustered by one warp with its digis in
+// registers (kSlots per lane).
+template <int kSlots>
+__device__ __forceinline__ void cluster_module_warp(const Dev& d, int e, uint32_t m, const ModRange& r,
+                                                    WarpSmem<kSlots>& S, WarpHist* H) {
+  const unsigned lane = threadIdx.x & 31u;
   const unsigned lt = (1u << lane) - 1u;
-  WarpSmem& S = smem[wib];
-  const EvInfo& E = d.ev[e];
-  const uint32_t nmod = E.n_modules;
-  if (E.word_base + uint64_t(E.n_words) > uint64_t(d.cap_words)) return;
-  for (uint32_t m = blockIdx.x * kWarpsPerBlock + wib; m < nmod; m += gridDim.x * kWarpsPerBlock) {
-    ModRange r;
-    if (!module_range(d, e, m, r)) continue;
-    const int n = r.n;
-    if (n > kWarpPix) {
-      if (lane == 0) {
-        const uint32_t slot = atomicAdd(&d.big_list[0], 1u);
-        if (slot < uint32_t(d.cap_big)) d.big_list[2 + slot] = (uint32_t(e) << 11) | m;
-      }
-      continue;
-    }
-    // load: each lane keeps digis k = lane + 32 j in registers
-    uint32_t xy[kWarpSlots];  // x (16 bits) | column bin << 16; 0xffffffff when not clustered
-    int32_t q[kWarpSlots];
-    uint32_t warn = 0;
-    int crun = n;
+  const int n = r.n;
+  uint32_t xy[kSlots];  // x (16 bits) | column bin << 16; 0xffffffff when not clustered
+  int32_t q[kSlots];
+  uint32_t warn = 0;
+  int crun = n;
 #pragma unroll
-    for (int j = 0; j < kWarpSlots; ++j) {
-      const int k = int(lane) + 32 * j;
-      xy[j] = 0xffffffffu;
-      q[j] = 0;
-      if (k < n) {
-        const uint64_t g = r.g0 + k;
-        const int16_t id = d.mid[g];
-        const int16_t x = d.xx[g], y = d.yy[g];
-        q[j] = d.adc[g];
-        const uint32_t yb = uint32_t(uint16_t(y)) & 511u;
-        // a column past the 418-bin histogram makes the reference's histogram assert
-        // fail; such a digi is flagged and kept out of the clustering
-        const bool in_hist = yb + 2u <= uint32_t(kNBins);
-        if (id != int16_t(kInvId) && !in_hist) warn |= kWarnPixels;
-        const bool valid = id != int16_t(kInvId) && in_hist;
-        if (valid) xy[j] = uint32_t(uint16_t(x)) | (yb << 16);
-        else crun = crun < k ? crun : k;
-        S.lab[k] = valid ? k : -1;
-      }
+  for (int j = 0; j < kSlots; ++j) {
+    const int k = int(lane) + 32 * j;
+    xy[j] = 0xffffffffu;
+    q[j] = 0;
+    if (k < n) {
+      const uint64_t g = r.g0 + k;
+      const int16_t id = d.mid[g];
+      const int16_t x = d.xx[g], y = d.yy[g];
+      q[j] = d.adc[g];
+      const uint32_t yb = uint32_t(uint16_t(y)) & 511u;
+      // a column past the 418-bin histogram makes the reference's histogram assert
+      // fail; such a digi is flagged and kept out of the clustering
+      const bool in_hist = yb + 2u <= uint32_t(kNBins);
+      if (id != int16_t(kInvId) && !in_hist) warn |= kWarnPixels;
+      const bool valid = id != int16_t(kInvId) && in_hist;
+      if (valid) xy[j] = uint32_t(uint16_t(x)) | (yb << 16);
+      else crun = crun < k ? crun : k;
+      S.lab[k] = valid ? k : -1;
     }
-    crun = int(__reduce_min_sync(0xffffffffu, uint32_t(crun)));
-    warn = __reduce_or_sync(0xffffffffu, warn);
+  }
+  crun = int(__reduce_min_sync(0xffffffffu, uint32_t(crun)));
+  warn = __reduce_or_sync(0xffffffffu, warn);
+  __syncwarp();
+  if (H) {
+    // neighbour pairs through a column histogram (count, warp scan, scatter); each digi
+    // then looks at its own and the next column only, as the CTA path does
+    for (int w = int(lane); w < kHistWords; w += 32) H->start[w] = 0;
     __syncwarp();
-    // neighbour pairs (|dx| <= 1, |dcolumn| <= 1), each pair once from its smaller index
-    for (int base = 0; base < n; base += 32) {
-      uint32_t v = 0xffffffffu;
 #pragma unroll
-      for (int j = 0; j < kWarpSlots; ++j)
-        if (j == (base >> 5)) v = xy[j];
+    for (int j = 0; j < kSlots; ++j) {
+      const int k = int(lane) + 32 * j;
+      if (k < n) H->xy[k] = xy[j];
+      if (xy[j] != 0xffffffffu) atomicAdd(&H->start[(xy[j] >> 16) + 1u], 1u);
+    }
+    __syncwarp();
+    constexpr int kPer = kHistWords / 32;
+    uint32_t cnt[kPer], tot = 0;
+#pragma unroll
+    for (int w = 0; w < kPer; ++w) { cnt[w] = H->start[lane * kPer + w]; tot += cnt[w]; }
+    uint32_t run = warp_incl_scan(tot) - tot;
+#pragma unroll
+    for (int w = 0; w < kPer; ++w) {
+      H->start[lane * kPer + w] = run;
+      H->cur[lane * kPer + w] = run;
+      run += cnt[w];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < kSlots; ++j)
+      if (xy[j] != 0xffffffffu) H->sorted[atomicAdd(&H->cur[(xy[j] >> 16) + 1u], 1u)] = uint8_t(lane + 32 * j);
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < kSlots; ++j) {
+      const int k = int(lane) + 32 * j;
+      if (k >= n || xy[j] == 0xffffffffu) continue;
+      const int xk = int(int16_t(xy[j] & 0xffffu));
+      const uint32_t bn = (xy[j] >> 16) + 1u;
+      const uint32_t p1 = H->start[bn + 2u];
+      for (uint32_t pp = H->start[bn]; pp < p1; ++pp) {
+        const int mm = H->sorted[pp];
+        if (mm == k) continue;
+        const uint32_t vm = H->xy[mm];
+        if ((vm >> 16) == (xy[j] >> 16) && mm < k) continue;  // each same-column pair once
+        const int dx = int(int16_t(vm & 0xffffu)) - xk;
+        if (dx > 1 || dx < -1) continue;
+        cc_union(S.lab, k, mm);
+      }
+    }
+  } else {
+    // neighbour pairs (|dx| <= 1, |dcolumn| <= 1) by broadcasting every digi, each pair
+    // once from its smaller index
+#pragma unroll
+    for (int jb = 0; jb < kSlots; ++jb) {
+      const int base = 32 * jb;
+      if (base >= n) break;
+      const uint32_t v = xy[jb];
       const int tmax = n - base < 32 ? n - base : 32;
       for (int t = 0; t < tmax; ++t) {
         const uint32_t vm = __shfl_sync(0xffffffffu, v, t);
@@ -164,9 +209,8 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_find_clus_warp(Dev d) {
         const int mm = base + t;
         const int xm = int(int16_t(vm & 0xffffu)), ym = int(vm >> 16);
 #pragma unroll
-        for (int j = 0; j < kWarpSlots; ++j) {
+        for (int j = 0; j <= jb; ++j) {
           const int k = int(lane) + 32 * j;
-          if (32 * j >= n) break;
           if (k >= mm || xy[j] == 0xffffffffu) continue;
           const int dx = int(int16_t(xy[j] & 0xffffu)) - xm;
           const int dy = int(xy[j] >> 16) - ym;
@@ -174,59 +218,98 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_find_clus_warp(Dev d) {
         }
       }
     }
-    __syncwarp();
+  }
+  __syncwarp();
 #pragma unroll
-    for (int j = 0; j < kWarpSlots; ++j) {
-      const int k = int(lane) + 32 * j;
-      if (k < n && xy[j] != 0xffffffffu) S.lab[k] = cc_find(S.lab, k);
-    }
-    __syncwarp();
-    // number the roots in index order
-    uint32_t nclus = 0;
-    for (int base = 0; base < n; base += 32) {
-      const int k = base + int(lane);
-      const bool root = k < n && S.lab[k] == k;
-      const unsigned b = __ballot_sync(0xffffffffu, root);
-      if (root) S.cid[k] = uint16_t(nclus + __popc(b & lt) + 1);
-      nclus += __popc(b);
-    }
-    for (uint32_t c = lane; c < nclus; c += 32) S.charge[c] = 0;
-    __syncwarp();
-    // cluster_charge_cut: charge sums stop at the first invalid digi
+  for (int j = 0; j < kSlots; ++j) {
+    const int k = int(lane) + 32 * j;
+    if (k < n && xy[j] != 0xffffffffu) S.lab[k] = cc_find(S.lab, k);
+  }
+  __syncwarp();
+  // number the roots in index order
+  uint32_t nclus = 0;
 #pragma unroll
-    for (int j = 0; j < kWarpSlots; ++j) {
-      const int k = int(lane) + 32 * j;
-      if (k < crun) atomicAdd(&S.charge[S.cid[S.lab[k]] - 1], q[j]);
-    }
-    __syncwarp();
-    const int32_t cut = r.this_id < 96 ? 2000 : 4000;
-    uint32_t last_new = 0;
-    for (uint32_t base = 0; base < nclus; base += 32) {
-      const uint32_t c = base + lane;
-      const bool ok = c < nclus && S.charge[c] > cut;
-      const unsigned b = __ballot_sync(0xffffffffu, ok);
-      if (c < nclus) S.newc[c] = ok ? uint16_t(last_new + __popc(b & lt) + 1) : uint16_t(kInvId);
-      last_new += __popc(b);
-    }
-    __syncwarp();
-    const bool changed = d.apply_charge_cut && nclus > 0 && last_new != nclus;
+  for (int j = 0; j < kSlots; ++j) {
+    const int k = int(lane) + 32 * j;
+    if (32 * j >= n) break;
+    const bool root = k < n && S.lab[k] == k;
+    const unsigned b = __ballot_sync(0xffffffffu, root);
+    if (root) S.cid[k] = uint16_t(nclus + __popc(b & lt) + 1);
+    nclus += __popc(b);
+  }
+  for (uint32_t c = lane; c < nclus; c += 32) S.charge[c] = 0;
+  __syncwarp();
+  // cluster_charge_cut: charge sums stop at the first invalid digi
 #pragma unroll
-    for (int j = 0; j < kWarpSlots; ++j) {
-      const int k = int(lane) + 32 * j;
-      if (k >= n) continue;
-      const uint64_t g = r.g0 + k;
-      if (xy[j] == 0xffffffffu) { d.clus[g] = -9999; continue; }
-      const uint32_t cl = S.cid[S.lab[k]];
-      if (changed) {
-        const uint16_t nc = S.newc[cl - 1];
-        d.clus[g] = int32_t(nc);
-        if (nc == kInvId) d.mid[g] = int16_t(kInvId);
-      } else {
-        d.clus[g] = int32_t(cl);
-      }
+  for (int j = 0; j < kSlots; ++j) {
+    const int k = int(lane) + 32 * j;
+    if (k < crun) atomicAdd(&S.charge[S.cid[S.lab[k]] - 1], q[j]);
+  }
+  __syncwarp();
+  const int32_t cut = r.this_id < 96 ? 2000 : 4000;
+  uint32_t last_new = 0;
+  for (uint32_t base = 0; base < nclus; base += 32) {
+    const uint32_t c = base + lane;
+    const bool ok = c < nclus && S.charge[c] > cut;
+    const unsigned b = __ballot_sync(0xffffffffu, ok);
+    if (c < nclus) S.newc[c] = ok ? uint16_t(last_new + __popc(b & lt) + 1) : uint16_t(kInvId);
+    last_new += __popc(b);
+  }
+  __syncwarp();
+  const bool changed = d.apply_charge_cut && nclus > 0 && last_new != nclus;
+#pragma unroll
+  for (int j = 0; j < kSlots; ++j) {
+    const int k = int(lane) + 32 * j;
+    if (k >= n) continue;
+    const uint64_t g = r.g0 + k;
+    if (xy[j] == 0xffffffffu) { d.clus[g] = -9999; continue; }
+    const uint32_t cl = S.cid[S.lab[k]];
+    if (changed) {
+      const uint16_t nc = S.newc[cl - 1];
+      d.clus[g] = int32_t(nc);
+      if (nc == kInvId) d.mid[g] = int16_t(kInvId);
+    } else {
+      d.clus[g] = int32_t(cl);
     }
-    if (lane == 0) write_module_record(d, e, m, r.this_id, changed ? last_new : nclus, warn);
-    __syncwarp();
+  }
+  if (lane == 0) write_module_record(d, e, m, r.this_id, changed ? last_new : nclus, warn);
+  __syncwarp();
+}
+
+// every module position of the batch: modules of <= 32 digis here (one digi per lane),
+// larger ones to the mid-size list (<= kWarpPix) or the CTA list
+__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_find_clus_small(Dev d) {
+  __shared__ WarpSmem<1> smem[kWarpsPerBlock];
+  const int e = blockIdx.y;
+  const unsigned lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+  const EvInfo& E = d.ev[e];
+  const uint32_t nmod = E.n_modules;
+  if (E.word_base + uint64_t(E.n_words) > uint64_t(d.cap_words)) return;
+  for (uint32_t m = blockIdx.x * kWarpsPerBlock + wib; m < nmod; m += gridDim.x * kWarpsPerBlock) {
+    ModRange r;
+    if (!module_range(d, e, m, r)) continue;
+    if (r.n > 32) {
+      if (lane == 0) push_module(d, r.n > kWarpPix ? kListClusBig : kListClusMid, e, m);
+      continue;
+    }
+    cluster_module_warp<1>(d, e, m, r, smem[wib], nullptr);
+  }
+}
+
+// the mid-size modules (33..256 digis), one warp each, eight digis per lane
+constexpr int kMidWarps = 4;  // 7.8 KB of shared memory per warp
+
+__global__ void __launch_bounds__(32 * kMidWarps) k_find_clus_mid(Dev d) {
+  __shared__ WarpSmem<kWarpSlots> smem[kMidWarps];
+  __shared__ WarpHist hist[kMidWarps];
+  const unsigned wib = threadIdx.x >> 5;
+  const uint32_t nl = list_size(d, kListClusMid);
+  for (uint32_t i = blockIdx.x * kMidWarps + wib; i < nl; i += gridDim.x * kMidWarps) {
+    const uint32_t v = list_entry(d, kListClusMid, i);
+    const int e = int(v >> 11);
+    ModRange r;
+    if (!module_range(d, e, v & 2047u, r)) continue;
+    cluster_module_warp<kWarpSlots>(d, e, v & 2047u, r, smem[wib], &hist[wib]);
   }
 }
 
@@ -375,10 +458,9 @@ __device__ void cluster_module_block(const Dev& d, int e, uint32_t m, BlockSmem&
 // the modules the warp path handed over: (event << 11 | module position) entries
 __global__ void __launch_bounds__(256) k_find_clus_block(Dev d) {
   __shared__ BlockSmem S;
-  const uint32_t cnt = d.big_list[0];
-  const uint32_t n = cnt < uint32_t(d.cap_big) ? cnt : uint32_t(d.cap_big);
+  const uint32_t n = list_size(d, kListClusBig);
   for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
-    const uint32_t v = d.big_list[2 + i];
+    const uint32_t v = list_entry(d, kListClusBig, i);
     const int e = int(v >> 11);
     const EvInfo& E = d.ev[e];
     if (E.word_base + uint64_t(E.n_words) > uint64_t(d.cap_words)) continue;
@@ -422,11 +504,13 @@ __global__ void k_hits_module_start(Dev d) {
 }  // namespace
 
 void launch_cluster(const Dev& d, const Launch& L) {
-  cudaMemsetAsync(d.big_list, 0, 2 * sizeof(uint32_t), L.s);
+  cudaMemsetAsync(d.big_list, 0, kListHeader * sizeof(uint32_t), L.s);
   // enough warps that a few events fill the GPU, at least 8 modules per warp otherwise
   const int bx = std::max(4, std::min(250, (148 * 8 * 4) / std::max(1, int(d.E))));
-  k_find_clus_warp<<<dim3(bx, d.E), 32 * kWarpsPerBlock, 0, L.s>>>(d);
-  L.mark("find_clus_warp");
+  k_find_clus_small<<<dim3(bx, d.E), 32 * kWarpsPerBlock, 0, L.s>>>(d);
+  L.mark("find_clus_small");
+  k_find_clus_mid<<<148 * 16, 32 * kMidWarps, 0, L.s>>>(d);
+  L.mark("find_clus_mid");
   k_find_clus_block<<<148 * 2, 256, 0, L.s>>>(d);
   L.mark("find_clus_block");
   k_hits_module_start<<<d.E, 1024, 0, L.s>>>(d);

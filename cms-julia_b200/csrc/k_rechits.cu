@@ -190,10 +190,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_get_hits_warp(Dev d) {
     if (!hit_module(d, e, m, hm)) continue;
     const uint32_t nd = hm.end0 - hm.first0;
     if (nd > uint32_t(kWarpModulePix) || hm.nclus > uint32_t(kWarpClus)) {
-      if (lane == 0) {
-        const uint32_t slot = atomicAdd(&d.big_list[1], 1u);
-        if (slot < uint32_t(d.cap_big)) d.big_list[2 + d.cap_big + slot] = (uint32_t(e) << 11) | m;
-      }
+      if (lane == 0) push_module(d, kListHitsBig, e, m);
       continue;
     }
     const uint32_t nclus = hm.nclus;
@@ -252,10 +249,9 @@ struct BlockHitSmem {
 
 __global__ void __launch_bounds__(256) k_get_hits_block(Dev d) {
   __shared__ BlockHitSmem S;
-  const uint32_t cnt = d.big_list[1];
-  const uint32_t nbig = cnt < uint32_t(d.cap_big) ? cnt : uint32_t(d.cap_big);
+  const uint32_t nbig = list_size(d, kListHitsBig);
   for (uint32_t bi = blockIdx.x; bi < nbig; bi += gridDim.x) {
-    const uint32_t v = d.big_list[2 + d.cap_big + bi];
+    const uint32_t v = list_entry(d, kListHitsBig, bi);
     const int e = int(v >> 11);
     const uint32_t m = v & 2047u;
     const EvInfo& E = d.ev[e];
@@ -371,6 +367,19 @@ __global__ void __launch_bounds__(1024) k_phi_binner(Dev d) {
     }
   }
   for (int b = threadIdx.x; b < kPhiTotBins; b += blockDim.x) poff[b] = s_off[b];
+  __syncthreads();
+  HitRec* rec = d.hit_rec + hb;
+  for (uint32_t p = threadIdx.x; p < ntot; p += blockDim.x) {
+    const uint32_t i = uint32_t(bins[p]) - 1u;
+    HitRec r;
+    r.z = d.zg[hb + i];
+    r.r = d.rg[hb + i];
+    r.iphi = d.iphi[hb + i];
+    r.ysize = d.ysize[hb + i];
+    r.det = d.detind[hb + i];
+    r.id = uint16_t(i);
+    rec[p] = r;
+  }
 }
 
 }  // namespace

@@ -107,8 +107,16 @@ __global__ void k_fast_dup(Dev d) {
 constexpr int kDupMaxTuples = 32768;  // qualities of one event in shared memory
 constexpr int kDupStage = 1024;       // staged track entries per batch of cells
 
+// qualities (0 bad, 1 dup, 2 loose) packed 2 bits per track, 16 per word
+__device__ __forceinline__ uint32_t q_get(const uint32_t* w, uint32_t t) { return (w[t >> 4] >> (2 * (t & 15))) & 3u; }
+__device__ __forceinline__ void q_set_dup(uint32_t* w, uint32_t t) {  // any non-bad quality -> dup
+  const uint32_t sh = 2 * (t & 15);
+  atomicAnd(&w[t >> 4], ~(2u << sh));
+  atomicOr(&w[t >> 4], 1u << sh);
+}
+
 __global__ void __launch_bounds__(32) k_fast_dup_smem(Dev d) {
-  __shared__ uint8_t s_q[kDupMaxTuples];
+  __shared__ uint32_t s_q[kDupMaxTuples / 16];
   __shared__ uint16_t s_t[kDupStage];
   __shared__ uint32_t s_tip[kDupStage];
   __shared__ uint32_t s_off[33];
@@ -121,7 +129,15 @@ __global__ void __launch_bounds__(32) k_fast_dup_smem(Dev d) {
   if (nt > uint32_t(kDupMaxTuples)) return;  // k_fast_dup handles such events
   const uint32_t lo = d.dup_flag[E.cell_base], hi = d.dup_flag[uint64_t(E.cell_base) + E.n_cells_raw];
   if (lo == hi) return;
-  for (uint32_t t = lane; t < nt; t += 32) s_q[t] = d.quality[tb + t];
+  const uint32_t nw = (nt + 15) / 16;
+  for (uint32_t w = lane; w < nw; w += 32) {
+    uint32_t v = 0;
+    for (uint32_t k = 0; k < 16; ++k) {
+      const uint32_t t = 16 * w + k;
+      if (t < nt) v |= uint32_t(d.quality[tb + t] & 3u) << (2 * k);
+    }
+    s_q[w] = v;
+  }
   for (uint32_t q0 = lo; q0 < hi;) {
     // stage up to 32 cells: list start and length (capped at kCellRows)
     const uint32_t q = q0 + lane;
@@ -152,15 +168,17 @@ __global__ void __launch_bounds__(32) k_fast_dup_smem(Dev d) {
     __syncwarp();
     for (uint32_t k = 0; k < ncell; ++k) {
       const uint32_t o = s_off[k], nk = s_off[k + 1] - o;
-      uint32_t key0 = 0xffffffffu, key1 = 0xffffffffu;
+      uint32_t key0 = 0xffffffffu, key1 = 0xffffffffu, q0v = 0, q1v = 0;
       uint16_t t0 = 0, t1 = 0;
       if (lane < nk) {
         t0 = s_t[o + lane];
-        if (s_q[t0] == 2) key0 = s_tip[o + lane];
+        q0v = q_get(s_q, t0);
+        if (q0v == 2) key0 = s_tip[o + lane];
       }
       if (lane + 32 < nk) {
         t1 = s_t[o + lane + 32];
-        if (s_q[t1] == 2) key1 = s_tip[o + lane + 32];
+        q1v = q_get(s_q, t1);
+        if (q1v == 2) key1 = s_tip[o + lane + 32];
       }
       // |tip| < 10000 as the reference's initial best (mc = 10000, strict <)
       const uint32_t lim = __float_as_uint(10000.f);
@@ -172,15 +190,14 @@ __global__ void __launch_bounds__(32) k_fast_dup_smem(Dev d) {
         const uint32_t pos = __reduce_min_sync(0xffffffffu, key0 == kmin ? lane : (key1 == kmin ? lane + 32 : 0xffffffffu));
         im = s_t[o + pos];
       }
-      __syncwarp();
-      if (lane < nk && s_q[t0] != 0 && t0 != im) s_q[t0] = 1;
-      if (lane + 32 < nk && s_q[t1] != 0 && t1 != im) s_q[t1] = 1;
+      if (lane < nk && q0v != 0 && t0 != im) q_set_dup(s_q, t0);
+      if (lane + 32 < nk && q1v != 0 && t1 != im) q_set_dup(s_q, t1);
       __syncwarp();
     }
     q0 += ncell;
   }
   __syncwarp();
-  for (uint32_t t = lane; t < nt; t += 32) d.quality[tb + t] = s_q[t];
+  for (uint32_t t = lane; t < nt; t += 32) d.quality[tb + t] = uint8_t(q_get(s_q, t));
 }
 
 // hit -> loose tuple lists

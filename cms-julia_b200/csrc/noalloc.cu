@@ -37,7 +37,7 @@ struct NoAllocScratch {
   uint32_t chunk_wo[kMaxChunks];
   uint32_t chunk_nmod[kMaxChunks];
   uint32_t clus_module_start[kMaxNumModules + 1];
-  uint32_t big_list[2 + 2 * kMaxNumModules];
+  uint32_t big_list[kListHeader + kNumLists * kMaxNumModules];
   uint32_t status;
 };
 

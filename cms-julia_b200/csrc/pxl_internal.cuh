@@ -91,6 +91,14 @@ struct EvInfo {
   uint32_t n_fit3, n_fit4;          // tuples fitted with 3 and with 4 hits (fit5as4 included)
 };
 
+// The fields the doublet search reads of an outer-hit candidate, packed in phi-bin order
+// so that the search loads one 16-byte record per candidate.
+struct alignas(16) HitRec {
+  float z, r;
+  int16_t iphi, ysize, det;
+  uint16_t id;  // event-local 0-based hit index
+};
+
 // Everything a kernel may need, passed by value.
 struct Dev {
   Conditions c;
@@ -126,6 +134,7 @@ struct Dev {
   uint32_t* hits_layer_start;  // [E][11]
   uint32_t* phi_off;           // [E][1281]
   uint16_t* phi_bins;          // [cap_hits], 1-based hit ids
+  struct HitRec* hit_rec;      // [cap_hits] the binned hits' doublet fields, in bin order
   // doublets: work items and cells
   uint32_t* pair_cum;      // [E][19] cumulative inner-layer sizes over the layer pairs
   uint32_t* item_cnt;      // [cap_items] doublets per inner hit item, then exclusive positions
@@ -139,6 +148,8 @@ struct Dev {
   uint32_t* ohc_cnt;       // [cap_hits + 1] counts -> offsets
   uint32_t* ohc_cur;       // [cap_hits] fill cursors
   uint32_t* ohc_list;      // [cap_cells] global cell indices
+  float4* ohc_rec;         // [cap_cells] per list entry: inner r, z, x, y of the cell (connect's candidate)
+  uint8_t* ohc_inner;      // [cap_cells] per list entry: the cell's inner hit is on an inner-barrel module
   // cell neighbours (CSR over cells)
   uint32_t* cn_mask;       // [cap_cells * 4] pass bits over the first 128 candidates
   uint32_t* cn_cnt;        // [cap_cells + 1]
@@ -176,8 +187,8 @@ struct Dev {
   uint32_t* scan_tmp;      // [scan tile sums]
   uint64_t* scan_tmp64;
   uint32_t* status;        // [1] global status bits (buffer overflow)
-  // modules too large for the warp-per-module kernels: [0] clustering count, [1] rechit
-  // count, then cap_big entries (event << 11 | module position) for each
+  // module work lists (event << 11 | module position): a header of kListHeader counters,
+  // then cap_big entries per list (kListClus*, kListHitsBig)
   uint32_t* big_list;
   int64_t cap_big;
   // launch shape
@@ -230,6 +241,21 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* sh, ui
 }
 
 __device__ __forceinline__ void atomic_or_warn(EvInfo* ev, uint32_t bits) { atomicOr(&ev->warnings, bits); }
+
+// module work lists between the per-module kernels
+enum : int { kListClusBig = 0, kListHitsBig = 1, kListClusMid = 2, kNumLists = 3, kListHeader = 4 };
+
+__device__ __forceinline__ void push_module(const Dev& d, int list, int e, uint32_t m) {
+  const uint32_t slot = atomicAdd(&d.big_list[list], 1u);
+  if (slot < uint32_t(d.cap_big)) d.big_list[kListHeader + size_t(list) * d.cap_big + slot] = (uint32_t(e) << 11) | m;
+}
+__device__ __forceinline__ uint32_t list_size(const Dev& d, int list) {
+  const uint32_t c = d.big_list[list];
+  return c < uint32_t(d.cap_big) ? c : uint32_t(d.cap_big);
+}
+__device__ __forceinline__ uint32_t list_entry(const Dev& d, int list, uint32_t i) {
+  return d.big_list[kListHeader + size_t(list) * d.cap_big + i];
+}
 
 // End of a module's digi range as find_clus and getHits bound it: the 1-based index of the
 // first valid digi with another module id after first1, or n_el if none. The next entry
