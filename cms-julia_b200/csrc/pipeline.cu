@@ -253,11 +253,15 @@ int alloc_batch(PxlCtx* ctx) {
 #undef A
   // input staging
   ctx->raw_cap = size_t(d.cap_words) * 4 + size_t(E) * (4 + 16 * 4 + size_t(d.n_fed_slots + 8) * 24) + 4096;
-  rc = dalloc(ctx, &ctx->d_raw, int64_t(ctx->raw_cap));
-  if (rc) return rc;
-  rc = dalloc(ctx, &ctx->d_ev_off, E + 1);
-  if (rc) return rc;
-  CK(cudaMallocHost(&ctx->h_off, size_t(E + 1) * sizeof(uint64_t)));
+  for (int k = 0; k < PxlCtx::kSlots; ++k) {
+    rc = dalloc(ctx, &ctx->d_raw[k], int64_t(ctx->raw_cap));
+    if (rc) return rc;
+    rc = dalloc(ctx, &ctx->d_ev_off[k], E + 1);
+    if (rc) return rc;
+    CK(cudaMallocHost(&ctx->h_off[k], size_t(E + 1) * sizeof(uint64_t)));
+    CK(cudaEventCreateWithFlags(&ctx->ev_staged[k], cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&ctx->ev_consumed[k], cudaEventDisableTiming));
+  }
   return 0;
 }
 
@@ -269,10 +273,15 @@ int run_chain(PxlCtx* ctx, uint32_t mask, cudaStream_t s) {
   if ((mask & PXL_STAGE_DIGIS) && L.prof) ctx->prof.n = 0;
   // stages run in chain order; a producer boundary may stop after any of them and a
   // later call (pxl_event_continue) resumes from the products already on the device
+  // a direct (non-graph) run over the context's slot-0 input orders itself after that slot's
+  // copy and marks the slot free once the raw data has been unpacked
+  const bool own_slot0 = (mask & PXL_STAGE_DIGIS) && !ctx->capturing && d.raw == ctx->d_raw[0];
+  if (own_slot0) CK(cudaStreamWaitEvent(s, ctx->ev_staged[0], 0));
   if (mask & PXL_STAGE_DIGIS) {
     CK(cudaMemsetAsync(d.err_count, 0, sizeof(uint32_t), s));
     CK(cudaMemsetAsync(d.status, 0, sizeof(uint32_t), s));
     launch_raw(d, L, ctx->fed_slot_of);
+    if (own_slot0) CK(cudaEventRecord(ctx->ev_consumed[0], s));
     launch_cluster(d, L);
     launch_ev_scan(d, s, int(offsetof(EvInfo, n_hits)), int(offsetof(EvInfo, hit_base)));
     launch_ev_clamp(d, s, int(offsetof(EvInfo, n_hits)), int(offsetof(EvInfo, hit_base)), d.cap_hits);
@@ -320,19 +329,32 @@ std::vector<T> dvec(const T* src, int64_t n) {
   return v;
 }
 
+// Host -> device copy of a batch into input slot k on stream s, ordered after the last chain
+// that read the slot; the slot's pinned offsets are reused only once their previous copy ended.
+int stage_slot(PxlCtx* ctx, int k, const uint8_t* blob, const uint64_t* offs, int32_t n, cudaStream_t s) {
+  if (n <= 0 || n > ctx->p.max_events) return PXL_ERR_ARG;
+  uint64_t base = offs[0], nbytes = offs[n] - offs[0];
+  if (offs[n] < offs[0] || nbytes > ctx->raw_cap) return PXL_ERR_CAPACITY;
+  CK(cudaEventSynchronize(ctx->ev_staged[k]));
+  for (int32_t e = 0; e <= n; ++e) ctx->h_off[k][e] = offs[e] - base;
+  CK(cudaStreamWaitEvent(s, ctx->ev_consumed[k], 0));
+  CK(cudaMemcpyAsync(ctx->d_raw[k], blob + base, nbytes, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(ctx->d_ev_off[k], ctx->h_off[k], size_t(n + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+  CK(cudaEventRecord(ctx->ev_staged[k], s));
+  ctx->slot_E[k] = n;
+  return 0;
+}
+
 int stage_input(PxlCtx* ctx, const uint8_t* blob, const uint64_t* offs, int32_t n, bool on_device, cudaStream_t s) {
   if (n <= 0 || n > ctx->p.max_events) return PXL_ERR_ARG;
   if (on_device) {
     ctx->d.raw = blob;
     ctx->d.ev_off = offs;
   } else {
-    uint64_t base = offs[0], nbytes = offs[n] - offs[0];
-    if (nbytes > ctx->raw_cap) return PXL_ERR_CAPACITY;
-    for (int32_t e = 0; e <= n; ++e) ctx->h_off[e] = offs[e] - base;
-    CK(cudaMemcpyAsync(ctx->d_raw, blob + base, nbytes, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(ctx->d_ev_off, ctx->h_off, size_t(n + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
-    ctx->d.raw = ctx->d_raw;
-    ctx->d.ev_off = ctx->d_ev_off;
+    int rc = stage_slot(ctx, 0, blob, offs, n, s);
+    if (rc) return rc;
+    ctx->d.raw = ctx->d_raw[0];
+    ctx->d.ev_off = ctx->d_ev_off[0];
   }
   ctx->d.E = n;
   ctx->last_E = n;
@@ -351,6 +373,32 @@ int choose_shape(PxlCtx* ctx) {
   return 0;
 }
 
+// Captures run_chain(mask) over the current input pointers into slot k's graph.
+int capture_slot(PxlCtx* ctx, int k, uint32_t mask) {
+  if (ctx->graph_exec[k]) { cudaGraphExecDestroy(ctx->graph_exec[k]); ctx->graph_exec[k] = nullptr; }
+  if (ctx->graph[k]) { cudaGraphDestroy(ctx->graph[k]); ctx->graph[k] = nullptr; }
+  CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  ctx->capturing = true;
+  int rc = run_chain(ctx, mask, ctx->stream);
+  ctx->capturing = false;
+  cudaGraph_t g = nullptr;
+  cudaError_t err = cudaStreamEndCapture(ctx->stream, &g);
+  if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+  if (err != cudaSuccess) { std::fprintf(stderr, "pxl: capture failed: %s\n", cudaGetErrorString(err)); return PXL_ERR_CUDA; }
+  ctx->graph[k] = g;
+  CK(cudaGraphInstantiate(&ctx->graph_exec[k], g, 0));
+  return 0;
+}
+
+int launch_slot(PxlCtx* ctx, int k, cudaStream_t s) {
+  CK(cudaStreamWaitEvent(s, ctx->ev_staged[k], 0));
+  CK(cudaGraphLaunch(ctx->graph_exec[k], s));
+  CK(cudaEventRecord(ctx->ev_consumed[k], s));
+  ctx->ev_host_valid = false;
+  ctx->last_E = ctx->graph_E;
+  ctx->last_mask = ctx->graph_mask;
+  return 0;
+}
 }  // namespace
 
 int pxl_fetch_ev(PxlCtx* ctx) { return fetch_ev_impl(ctx); }
@@ -399,11 +447,17 @@ int32_t pxl_ctx_create(const PxlConditions* cond, const PxlParams* params, PxlCt
 int32_t pxl_ctx_destroy(PxlCtx* ctx) {
   if (!ctx) return PXL_ERR_ARG;
   cudaSetDevice(ctx->p.device);
-  if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
-  if (ctx->graph) cudaGraphDestroy(ctx->graph);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (int k = 0; k < PxlCtx::kSlots; ++k) {
+    if (ctx->ev_staged[k]) cudaEventSynchronize(ctx->ev_staged[k]);
+    if (ctx->ev_consumed[k]) cudaEventSynchronize(ctx->ev_consumed[k]);
+    if (ctx->graph_exec[k]) cudaGraphExecDestroy(ctx->graph_exec[k]);
+    if (ctx->graph[k]) cudaGraphDestroy(ctx->graph[k]);
+    if (ctx->h_off[k]) cudaFreeHost(ctx->h_off[k]);
+    if (ctx->ev_staged[k]) cudaEventDestroy(ctx->ev_staged[k]);
+    if (ctx->ev_consumed[k]) cudaEventDestroy(ctx->ev_consumed[k]);
+  }
   for (void* q : ctx->allocs) cudaFree(q);
-  if (ctx->h_off) cudaFreeHost(ctx->h_off);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return 0;
@@ -460,20 +514,28 @@ int32_t pxl_event_continue(PxlCtx* ctx, uint32_t mask, void* stream) {
 int32_t pxl_graph_capture(PxlCtx* ctx, uint32_t mask) {
   if (!ctx || ctx->d.E <= 0) return PXL_ERR_STATE;
   cudaSetDevice(ctx->p.device);
-  if (ctx->graph_exec) { cudaGraphExecDestroy(ctx->graph_exec); ctx->graph_exec = nullptr; }
-  if (ctx->graph) { cudaGraphDestroy(ctx->graph); ctx->graph = nullptr; }
   choose_shape(ctx);
   CK(cudaStreamSynchronize(ctx->stream));
-  CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-  ctx->capturing = true;
-  int rc = run_chain(ctx, mask, ctx->stream);
-  ctx->capturing = false;
-  cudaGraph_t g = nullptr;
-  cudaError_t err = cudaStreamEndCapture(ctx->stream, &g);
-  if (rc) { if (g) cudaGraphDestroy(g); return rc; }
-  if (err != cudaSuccess) { std::fprintf(stderr, "pxl: capture failed: %s\n", cudaGetErrorString(err)); return PXL_ERR_CUDA; }
-  ctx->graph = g;
-  CK(cudaGraphInstantiate(&ctx->graph_exec, g, 0));
+  for (int k = 0; k < PxlCtx::kSlots; ++k) {
+    if (ctx->graph_exec[k]) { cudaGraphExecDestroy(ctx->graph_exec[k]); ctx->graph_exec[k] = nullptr; }
+    if (ctx->graph[k]) { cudaGraphDestroy(ctx->graph[k]); ctx->graph[k] = nullptr; }
+  }
+  // slot 0 replays the current input (the context's own slot-0 buffer or a device batch)
+  int rc = capture_slot(ctx, 0, mask);
+  if (rc) return rc;
+  // the other slots exist when the input is the context's own buffer
+  if (ctx->d.raw == ctx->d_raw[0]) {
+    const uint8_t* raw0 = ctx->d.raw;
+    const uint64_t* off0 = ctx->d.ev_off;
+    for (int k = 1; k < PxlCtx::kSlots && !rc; ++k) {
+      ctx->d.raw = ctx->d_raw[k];
+      ctx->d.ev_off = ctx->d_ev_off[k];
+      rc = capture_slot(ctx, k, mask);
+    }
+    ctx->d.raw = raw0;
+    ctx->d.ev_off = off0;
+    if (rc) return rc;
+  }
   ctx->graph_mask = mask;
   ctx->graph_E = ctx->d.E;
   ctx->last_mask = mask;
@@ -481,14 +543,26 @@ int32_t pxl_graph_capture(PxlCtx* ctx, uint32_t mask) {
 }
 
 int32_t pxl_graph_launch(PxlCtx* ctx, void* stream) {
-  if (!ctx || !ctx->graph_exec) return PXL_ERR_STATE;
+  if (!ctx || !ctx->graph_exec[0]) return PXL_ERR_STATE;
   cudaSetDevice(ctx->p.device);
   cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
-  CK(cudaGraphLaunch(ctx->graph_exec, s));
-  ctx->ev_host_valid = false;
-  ctx->last_E = ctx->graph_E;
-  ctx->last_mask = ctx->graph_mask;
-  return 0;
+  return launch_slot(ctx, 0, s);
+}
+
+int32_t pxl_slot_stage(PxlCtx* ctx, int32_t slot, const uint8_t* blob, const uint64_t* offs, int32_t n,
+                       void* copy_stream) {
+  if (!ctx || !blob || !offs || slot < 0 || slot >= PxlCtx::kSlots) return PXL_ERR_ARG;
+  cudaSetDevice(ctx->p.device);
+  cudaStream_t s = copy_stream ? static_cast<cudaStream_t>(copy_stream) : ctx->stream;
+  return stage_slot(ctx, slot, blob, offs, n, s);
+}
+
+int32_t pxl_slot_launch(PxlCtx* ctx, int32_t slot, void* stream) {
+  if (!ctx || slot < 0 || slot >= PxlCtx::kSlots) return PXL_ERR_ARG;
+  if (!ctx->graph_exec[slot] || ctx->slot_E[slot] != ctx->graph_E) return PXL_ERR_STATE;
+  cudaSetDevice(ctx->p.device);
+  cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+  return launch_slot(ctx, slot, s);
 }
 
 int64_t pxl_results_async(PxlCtx* ctx, uint32_t* host_dst, int64_t max_events, void* stream) {
@@ -504,11 +578,11 @@ int64_t pxl_results_async(PxlCtx* ctx, uint32_t* host_dst, int64_t max_events, v
 }
 
 int32_t pxl_graph_kernel_nodes(PxlCtx* ctx) {
-  if (!ctx || !ctx->graph) return PXL_ERR_STATE;
+  if (!ctx || !ctx->graph[0]) return PXL_ERR_STATE;
   size_t n = 0;
-  CK(cudaGraphGetNodes(ctx->graph, nullptr, &n));
+  CK(cudaGraphGetNodes(ctx->graph[0], nullptr, &n));
   std::vector<cudaGraphNode_t> nodes(n);
-  CK(cudaGraphGetNodes(ctx->graph, nodes.data(), &n));
+  CK(cudaGraphGetNodes(ctx->graph[0], nodes.data(), &n));
   int32_t k = 0;
   for (auto nd : nodes) {
     cudaGraphNodeType t;

@@ -15,9 +15,11 @@ struct PxlCtx {
   int16_t* fed_slot_of = nullptr;
   // host copy of the conditions needed at copy-out
   std::vector<float> avg_geom;
-  // graph
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t graph_exec = nullptr;
+  // input slots: each has its own device raw buffer, offsets and captured graph, so the
+  // copy of one batch overlaps the chain running on the other
+  static constexpr int kSlots = PXL_INPUT_SLOTS;
+  cudaGraph_t graph[kSlots] = {};
+  cudaGraphExec_t graph_exec[kSlots] = {};
   uint32_t graph_mask = 0;
   int graph_E = -1;
   // last run
@@ -26,11 +28,15 @@ struct PxlCtx {
   uint32_t done_mask = 0;
   std::vector<pxl::EvInfo> ev_host;
   bool ev_host_valid = false;
-  // pinned staging for offsets
-  uint64_t* h_off = nullptr;
+  // per slot: pinned staging of the rebased offsets, device input, events staged in it,
+  // an event after its copies and one after the last chain that read it
+  uint64_t* h_off[kSlots] = {};
   size_t raw_cap = 0;
-  uint64_t* d_ev_off = nullptr;
-  uint8_t* d_raw = nullptr;
+  uint64_t* d_ev_off[kSlots] = {};
+  uint8_t* d_raw[kSlots] = {};
+  int32_t slot_E[kSlots] = {};
+  cudaEvent_t ev_staged[kSlots] = {};
+  cudaEvent_t ev_consumed[kSlots] = {};
   // per-kernel timing of non-graph runs
   pxl::Prof prof;
   bool capturing = false;

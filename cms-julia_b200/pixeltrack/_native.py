@@ -13,6 +13,7 @@ PXL_ERR = {-1: "bad argument", -2: "CUDA error", -3: "bad conditions", -4: "capa
 STAGE_DIGIS, STAGE_HITS, STAGE_TUPLES, STAGE_FIT, STAGE_CLASSIFY, STAGE_VERTICES = 1, 2, 4, 8, 16, 32
 STAGE_ALL = 0x3F
 
+INPUT_SLOTS = 2  # PXL_INPUT_SLOTS
 TUNE_STAGES = ("doublets", "hit_lists", "connect", "cell_lists", "fishbone", "ntuplets", "cell_tracks",
                "early_dup", "classify", "hit_to_tuple", "fits")
 
@@ -69,6 +70,9 @@ _SIGS = {
     "pxl_batch_stage": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
                                          ctypes.c_void_p]),
     "pxl_graph_capture": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_uint32]),
+    "pxl_slot_stage": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_int32, ctypes.c_void_p]),
+    "pxl_slot_launch": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]),
     "pxl_graph_launch": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p]),
     "pxl_sync": (ctypes.c_int32, [ctypes.c_void_p]),
     "pxl_autotune": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,

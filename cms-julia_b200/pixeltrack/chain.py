@@ -80,6 +80,7 @@ class PixelChain:
         check(self._lib.pxl_ctx_create(ctypes.byref(c), ctypes.byref(self.params), ctypes.byref(h)), "pxl_ctx_create")
         self._h = h
         self._keep: list = []
+        self._slot_keep: list = [None] * _native.INPUT_SLOTS
 
     def close(self) -> None:
         if getattr(self, "_h", None) and self._h.value:
@@ -138,6 +139,19 @@ class PixelChain:
 
     def launch_graph(self, stream: int | None = None) -> None:
         check(self._lib.pxl_graph_launch(self._h, stream), "pxl_graph_launch")
+
+    def stage_slot(self, slot: int, blob: np.ndarray, offsets: np.ndarray, stream: int | None = None) -> None:
+        """Enqueues the copy of a batch into input slot `slot` on `stream` (pxl_slot_stage).
+        blob should be pinned host memory and must stay unchanged until the copy ends."""
+        blob = np.ascontiguousarray(blob, dtype=np.uint8)
+        offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+        self._slot_keep[slot] = [blob, offsets]
+        check(self._lib.pxl_slot_stage(self._h, slot, blob.ctypes.data, offsets.ctypes.data, len(offsets) - 1,
+                                       stream), "pxl_slot_stage")
+
+    def launch_slot(self, slot: int, stream: int | None = None) -> None:
+        """Replays input slot `slot`'s graph once its copy has ended (pxl_slot_launch)."""
+        check(self._lib.pxl_slot_launch(self._h, slot, stream), "pxl_slot_launch")
 
     def results_async(self, host_ptr: int, max_events: int, stream: int | None = None) -> int:
         return check(self._lib.pxl_results_async(self._h, host_ptr, max_events, stream), "pxl_results_async")

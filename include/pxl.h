@@ -194,10 +194,25 @@ int32_t pxl_batch_run(PxlCtx* ctx, const uint8_t* blob, const uint64_t* event_of
 int32_t pxl_batch_stage(PxlCtx* ctx, const uint8_t* blob, const uint64_t* event_offsets, int32_t n_events,
                         void* stream);
 
-/* Captures the whole chain for the staged batch shape into one CUDA graph
- * (no host synchronisation inside), and replays it. */
+/* Captures the whole chain for the staged batch shape into one CUDA graph per input slot
+ * (no host synchronisation inside), and replays slot 0's graph. Slot 0 is the input that
+ * pxl_batch_stage / pxl_batch_run staged; when that is the context's own buffer, a graph is
+ * also captured for every other slot. */
 int32_t pxl_graph_capture(PxlCtx* ctx, uint32_t stage_mask);
 int32_t pxl_graph_launch(PxlCtx* ctx, void* stream);
+
+/* Double-buffered input for streaming batches. The context holds PXL_INPUT_SLOTS device
+ * input buffers. pxl_slot_stage enqueues on copy_stream the host -> device copy of a batch
+ * into `slot`, after the last chain that read that slot (blob must stay valid until the copy
+ * ends: pinned memory for an asynchronous copy). pxl_slot_launch makes `stream` wait for that
+ * copy and replays the slot's graph (pxl_graph_capture first; the staged event count must be
+ * the captured one, else PXL_ERR_STATE). Staging batch i+1 into one slot while batch i runs
+ * from the other overlaps the input copy with the chain. Products and results are those of
+ * the last launch, as for pxl_graph_launch. */
+#define PXL_INPUT_SLOTS 2
+int32_t pxl_slot_stage(PxlCtx* ctx, int32_t slot, const uint8_t* blob, const uint64_t* event_offsets,
+                       int32_t n_events, void* copy_stream);
+int32_t pxl_slot_launch(PxlCtx* ctx, int32_t slot, void* stream);
 
 /* Enqueues on `stream` the copy of the per-event vertex counts (nvFinal) of the last run into
  * host memory (pinned for an asynchronous copy), one uint32 per event; returns the count. */

@@ -124,3 +124,58 @@ def test_graph_replay_is_deterministic(conditions, events_pu50):
         bc.sync()
         for k, v in first.items():
             assert np.array_equal(v, bc.product(k, n - 1))
+
+
+def test_input_slots_overlap_copy_and_chain(conditions, events_pu50):
+    """Two batches alternate through the two input slots, each copied on a copy stream
+    while the other slot's graph runs: every launch gives the products of a plain run of
+    its own batch."""
+    import torch
+    from pixeltrack import PixelChain, batch_params, gen
+    blob_a, offs_a = events_pu50
+    n = len(offs_a) - 1
+    blob_b, offs_b = gen.events(n, gen.MODE_PU, pu=50, seed=12)
+    batches = [(blob_a, offs_a), (blob_b, offs_b)]
+    want = []
+    with PixelChain(conditions, batch_params(n)) as bc:
+        for blob, offs in batches:
+            bc.run_batch(blob, offs)
+            bc.sync()
+            want.append(([bc.counts(e).n_vertices for e in range(n)], bc.product("xg", n - 1)))
+        pinned = []
+        for blob, _ in batches:
+            t = torch.empty(len(blob), dtype=torch.uint8, pin_memory=True)
+            t.numpy()[:] = blob
+            pinned.append(t.numpy())
+        res = torch.empty(n, dtype=torch.int32, pin_memory=True)
+        stream, copy = torch.cuda.Stream(), torch.cuda.Stream()
+        bc.stage_batch(blob_a, offs_a, stream.cuda_stream)
+        stream.synchronize()
+        bc.capture_graph()
+        bc.stage_slot(0, pinned[0], offs_a, copy.cuda_stream)
+        for i in range(6):
+            k = i % 2
+            bc.launch_slot(k, stream.cuda_stream)
+            bc.results_async(res.data_ptr(), n, stream.cuda_stream)
+            bc.stage_slot(1 - k, pinned[1 - k], batches[1 - k][1], copy.cuda_stream)
+            stream.synchronize()
+            assert res.numpy().tolist() == want[k][0], i
+            assert np.array_equal(bc.product("xg", n - 1), want[k][1]), i
+        copy.synchronize()
+
+
+def test_slot_launch_needs_captured_event_count(conditions, events_pu50):
+    from pixeltrack import PixelChain, batch_params
+    blob, offs = events_pu50
+    n = len(offs) - 1
+    with PixelChain(conditions, batch_params(n)) as bc:
+        with pytest.raises(RuntimeError, match="bad state"):
+            bc.launch_slot(1)
+        bc.stage_batch(blob, offs)
+        bc.capture_graph()
+        bc.stage_slot(1, blob[: int(offs[n - 1])], offs[:n])
+        with pytest.raises(RuntimeError, match="bad state"):
+            bc.launch_slot(1)
+        bc.stage_slot(1, blob, offs)
+        bc.launch_slot(1)
+        bc.sync()
