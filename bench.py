@@ -456,7 +456,9 @@ def main():
     chain.profile(True)
     prof_runs = []
     for _ in range(3):
+        torch.cuda.nvtx.range_push("chain")  # profiler filter: --nvtx --nvtx-include "chain/"
         chain.run_batch(blob, offs, sync=False)
+        torch.cuda.nvtx.range_pop()
         warn = chain.sync()
         prof_runs.append(chain.profile_read())
     chain.profile(False)

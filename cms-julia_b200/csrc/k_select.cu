@@ -121,6 +121,7 @@ __global__ void __launch_bounds__(32) k_fast_dup_smem(Dev d) {
   __shared__ uint32_t s_tip[kDupStage];
   __shared__ uint32_t s_off[33];
   __shared__ uint32_t s_l0[32];
+  __shared__ uint32_t s_seen[kDupMaxTuples / 32];
   const int e = blockIdx.x;
   const unsigned lane = threadIdx.x;
   const EvInfo& E = d.ev[e];
@@ -138,6 +139,8 @@ __global__ void __launch_bounds__(32) k_fast_dup_smem(Dev d) {
     }
     s_q[w] = v;
   }
+  for (uint32_t w = lane; w < uint32_t(kDupMaxTuples / 32); w += 32) s_seen[w] = 0;
+  __syncwarp();
   for (uint32_t q0 = lo; q0 < hi;) {
     // stage up to 32 cells: list start and length (capped at kCellRows)
     const uint32_t q = q0 + lane;
@@ -166,6 +169,36 @@ __global__ void __launch_bounds__(32) k_fast_dup_smem(Dev d) {
       s_tip[x] = __float_as_uint(fabsf(d.t_state[5 * size_t(t) + 1]));
     }
     __syncwarp();
+    // cells that share no track are independent: when no track is listed twice in the
+    // stage, each lane takes one cell (same result as the ordered walk)
+    bool twice = false;
+    for (uint32_t x = lane; x < total; x += 32) {
+      const uint32_t t = s_t[x], bit = 1u << (t & 31);
+      twice |= (atomicOr(&s_seen[t >> 5], bit) & bit) != 0;
+    }
+    __syncwarp();
+    for (uint32_t x = lane; x < total; x += 32) s_seen[s_t[x] >> 5] = 0;
+    __syncwarp();
+    // |tip| < 10000 as the reference's initial best (mc = 10000, strict <)
+    const uint32_t lim = __float_as_uint(10000.f);
+    if (!__any_sync(0xffffffffu, twice)) {
+      if (lane < ncell) {
+        const uint32_t o = s_off[lane], nk = s_off[lane + 1] - o;
+        uint32_t best = lim, im = 0xffffffffu;
+        for (uint32_t j = 0; j < nk; ++j) {
+          const uint32_t t = s_t[o + j];
+          const uint32_t key = s_tip[o + j];
+          if (key < best && q_get(s_q, t) == 2) { best = key; im = t; }
+        }
+        for (uint32_t j = 0; j < nk; ++j) {
+          const uint32_t t = s_t[o + j];
+          if (t != im && q_get(s_q, t) != 0) q_set_dup(s_q, t);
+        }
+      }
+      __syncwarp();
+      q0 += ncell;
+      continue;
+    }
     for (uint32_t k = 0; k < ncell; ++k) {
       const uint32_t o = s_off[k], nk = s_off[k + 1] - o;
       uint32_t key0 = 0xffffffffu, key1 = 0xffffffffu, q0v = 0, q1v = 0;
@@ -180,8 +213,6 @@ __global__ void __launch_bounds__(32) k_fast_dup_smem(Dev d) {
         q1v = q_get(s_q, t1);
         if (q1v == 2) key1 = s_tip[o + lane + 32];
       }
-      // |tip| < 10000 as the reference's initial best (mc = 10000, strict <)
-      const uint32_t lim = __float_as_uint(10000.f);
       if (key0 >= lim) key0 = 0xffffffffu;
       if (key1 >= lim) key1 = 0xffffffffu;
       const uint32_t kmin = __reduce_min_sync(0xffffffffu, key0 < key1 ? key0 : key1);
@@ -285,6 +316,8 @@ __global__ void __launch_bounds__(kVtxThreads) k_vertices(Dev d) {
   __shared__ uint32_t s_off[257];
   __shared__ uint32_t s_cur[256];
   __shared__ uint32_t s_nv, s_nvi, s_warn;
+  __shared__ uint32_t s_vcnt[kMaxVtx], s_voff[kMaxVtx + 1];
+  __shared__ uint16_t s_parent[kMaxVtx];
   for (int v = threadIdx.x; v < kMaxVtx; v += blockDim.x) { zv[v] = 0; wv[v] = 0; vchi2[v] = 0; ptv2[v] = 0; sort_ind[v] = 0; }
   for (uint32_t t = threadIdx.x; t < ntu + kMaxVtx; t += blockDim.x) nn[t] = 0;
   for (uint32_t t = threadIdx.x; t < ntu; t += blockDim.x) d.idv[tb + t] = -1;
@@ -412,12 +445,49 @@ __global__ void __launch_bounds__(kVtxThreads) k_vertices(Dev d) {
     s_nvi = found;
   }
   __syncthreads();
+  // per-vertex track lists in ascending track order (the order of the reference's loops over
+  // all tracks); B (the z histogram) is free again. A vertex made by a split keeps its parent's
+  // list and selects its own tracks by id, as the loops over all tracks do.
+  const uint32_t nv0 = s_nv;
+  for (uint32_t v = threadIdx.x; v < uint32_t(kMaxVtx); v += blockDim.x) { s_vcnt[v] = 0; s_parent[v] = uint16_t(v); }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x)
+    if (iv[i] >= 1 && uint32_t(iv[i]) <= nv0) atomicAdd(&s_vcnt[iv[i] - 1], 1u);
+  __syncthreads();
+  {
+    uint32_t base = 0;
+    for (uint32_t b = 0; b < nv0; b += blockDim.x) {
+      const uint32_t v = b + threadIdx.x;
+      const uint32_t c = v < nv0 ? s_vcnt[v] : 0u;
+      uint32_t tot;
+      const uint32_t ex = block_excl_scan(c, sh, &tot);
+      if (v < nv0) { s_voff[v] = base + ex; s_vcnt[v] = base + ex; }
+      base += tot;
+    }
+    if (threadIdx.x == 0) s_voff[nv0] = base;
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x)
+    if (iv[i] >= 1 && uint32_t(iv[i]) <= nv0) B[atomicAdd(&s_vcnt[iv[i] - 1], 1u)] = i;
+  __syncthreads();
+  for (uint32_t v = threadIdx.x; v < nv0; v += blockDim.x) {
+    const uint32_t lo = s_voff[v], hi = s_voff[v + 1];
+    for (uint32_t p = lo + 1; p < hi; ++p) {
+      const uint32_t x = B[p];
+      uint32_t q = p;
+      while (q > lo && B[q - 1] > x) { B[q] = B[q - 1]; --q; }
+      B[q] = x;
+    }
+  }
+  __syncthreads();
   // fit_vertices, :228-286 (one thread per vertex keeps the track order of the sums)
   auto fit = [&](double chi2max) {
     const uint32_t nvf = s_nvi;
     for (uint32_t v = threadIdx.x; v < nvf; v += blockDim.x) {
+      const uint32_t pv = s_parent[v], lo = s_voff[pv], hi = s_voff[pv + 1];
       float z = 0, w = 0;
-      for (uint32_t i = 0; i < nt; ++i) {
+      for (uint32_t p = lo; p < hi; ++p) {
+        const uint32_t i = B[p];
         if (iv[i] != int32_t(v + 1)) continue;
         const float wi = __fdiv_rn(1.0f, ezt2[i]);
         z = __fadd_rn(z, __fmul_rn(zt[i], wi));
@@ -427,7 +497,8 @@ __global__ void __launch_bounds__(kVtxThreads) k_vertices(Dev d) {
       z = __fdiv_rn(z, w);
       float c2s = 0;
       int32_t cnt = -1;
-      for (uint32_t i = 0; i < nt; ++i) {
+      for (uint32_t p = lo; p < hi; ++p) {
+        const uint32_t i = B[p];
         if (iv[i] != int32_t(v + 1)) continue;
         float c2 = __fsub_rn(z, zt[i]);
         c2 = __fmul_rn(c2, __fdiv_rn(c2, ezt2[i]));
@@ -450,6 +521,7 @@ __global__ void __launch_bounds__(kVtxThreads) k_vertices(Dev d) {
       const uint32_t kv = b + threadIdx.x;
       bool split = false;
       float znew0 = 0, znew1 = 0;
+      const uint32_t lo = kv < nvf ? s_voff[kv] : 0u, hi = kv < nvf ? s_voff[kv + 1] : 0u;
       if (kv < nvf && nn[kv] >= 4 && !(vchi2[kv] < __fmul_rn(9.0f, float(nn[kv])))) {
         if (nn[kv] >= 512) {
           atomicOr(&s_warn, kWarnVertex);
@@ -457,19 +529,21 @@ __global__ void __launch_bounds__(kVtxThreads) k_vertices(Dev d) {
           // 2-means in the vertex's tracks (zz = zt - zv, weights 1/ezt2), at most 20 iterations
           uint32_t nq = 0;
           const float zc = zv[kv];
-          for (uint32_t i = 0; i < nt; ++i) if (iv[i] == int32_t(kv + 1)) ++nq;
+          for (uint32_t p = lo; p < hi; ++p) if (iv[B[p]] == int32_t(kv + 1)) ++nq;
           if (nq != uint32_t(nn[kv] + 1)) atomicOr(&s_warn, kWarnVertex);
-          // new_v assignment kept in the sign of a scratch copy: recompute per iteration
           bool more = true;
           int iter = 20;
-          // first assignment: zz < 0 -> 1 else 2; stored per track in izt's high bit space
-          for (uint32_t i = 0; i < nt; ++i)
+          // first assignment: zz < 0 -> 1 else 2, kept per track in izt
+          for (uint32_t p = lo; p < hi; ++p) {
+            const uint32_t i = B[p];
             if (iv[i] == int32_t(kv + 1)) izt[i] = __fsub_rn(zt[i], zc) < 0 ? 1 : 2;
+          }
           float w0 = 0, w1 = 0;
           while (more) {
             more = false;
             znew0 = znew1 = 0; w0 = w1 = 0;
-            for (uint32_t i = 0; i < nt; ++i) {
+            for (uint32_t p = lo; p < hi; ++p) {
+              const uint32_t i = B[p];
               if (iv[i] != int32_t(kv + 1)) continue;
               const float zz = __fsub_rn(zt[i], zc), ww = __fdiv_rn(1.0f, ezt2[i]);
               if (izt[i] == 1) { znew0 = __fadd_rn(znew0, __fmul_rn(zz, ww)); w0 = __fadd_rn(w0, ww); }
@@ -477,7 +551,8 @@ __global__ void __launch_bounds__(kVtxThreads) k_vertices(Dev d) {
             }
             znew0 = __fdiv_rn(znew0, w0);
             znew1 = __fdiv_rn(znew1, w1);
-            for (uint32_t i = 0; i < nt; ++i) {
+            for (uint32_t p = lo; p < hi; ++p) {
+              const uint32_t i = B[p];
               if (iv[i] != int32_t(kv + 1)) continue;
               const float zz = __fsub_rn(zt[i], zc);
               const float d0 = fabsf(__fsub_rn(znew0, zz)), d1 = fabsf(__fsub_rn(znew1, zz));
@@ -498,9 +573,13 @@ __global__ void __launch_bounds__(kVtxThreads) k_vertices(Dev d) {
       uint32_t tot;
       const uint32_t ex = block_excl_scan(split ? 1u : 0u, sh, &tot);
       if (split) {
-        const int32_t newv = int32_t(s_nvi + ex + 1);
-        for (uint32_t i = 0; i < nt; ++i)
+        const uint32_t slot = s_nvi + ex;  // 0-based id of the new vertex
+        const int32_t newv = int32_t(slot + 1);
+        if (slot < uint32_t(kMaxVtx)) s_parent[slot] = uint16_t(kv);
+        for (uint32_t p = lo; p < hi; ++p) {
+          const uint32_t i = B[p];
           if (iv[i] == int32_t(kv + 1) && izt[i] == 2) iv[i] = newv;
+        }
       }
       __syncthreads();
       if (threadIdx.x == 0) s_nvi += tot;
@@ -515,8 +594,12 @@ __global__ void __launch_bounds__(kVtxThreads) k_vertices(Dev d) {
   if (nvf >= 1) {
     for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) d.idv[tb + itrk[i]] = int16_t(iv[i]);
     for (uint32_t v = threadIdx.x; v < nvf; v += blockDim.x) {
+      const uint32_t pv = s_parent[v], lo = s_voff[pv], hi = s_voff[pv + 1];
       float s = 0;
-      for (uint32_t i = 0; i < nt; ++i) if (iv[i] == int32_t(v + 1)) s = __fadd_rn(s, ptt2[i]);
+      for (uint32_t p = lo; p < hi; ++p) {
+        const uint32_t i = B[p];
+        if (iv[i] == int32_t(v + 1)) s = __fadd_rn(s, ptt2[i]);
+      }
       ptv2[v] = s;
     }
     if (threadIdx.x == 0 && nvf == 1) sort_ind[0] = 1;
