@@ -59,17 +59,29 @@ __global__ void k_items(Dev d, uint32_t* pair_cum) {
   d.ev[e].n_items = d.ev[e].n_hits ? acc : 0u;
 }
 
+// layer pair and event-local 0-based inner hit of work item j
+__device__ __forceinline__ int item_pair(uint32_t j, const uint32_t* cum, const uint32_t* hls, uint32_t* hit) {
+  int pid = 0;
+  while (j >= cum[pid]) ++pid;
+  *hit = ((pid == 0) ? j : j - cum[pid - 1]) + hls[c_layer_pairs[2 * pid]];
+  return pid;
+}
+
+// Doublets of one work item (inner hit x layer pair), candidates in the reference's loop
+// order. kFill false: counts them and keeps the first kLaneSlots outer hits in `stage`
+// (stride kStageStride; event-local hit ids fit 16 bits, hits_per_event <= 65535); true:
+// writes the cells from event-local position cell_pos on.
+constexpr int kLaneSlots = 48;
+constexpr int kStageStride = 256;
 template <bool kFill>
 __device__ __forceinline__ uint32_t doublets_of_item(const Dev& d, int e, uint32_t j, const uint32_t* cum,
                                                      const uint32_t* hls, const HitView& hv, const uint32_t* poff,
                                                      const HitRec* __restrict__ hrec, uint64_t cell_pos, uint64_t cell_lo,
-                                                     uint32_t cap) {
-  int pid = 0;
-  while (j >= cum[pid]) ++pid;
+                                                     uint32_t cap, uint16_t* stage) {
+  uint32_t i;
+  const int pid = item_pair(j, cum, hls, &i);
   const int inner = c_layer_pairs[2 * pid], outer = c_layer_pairs[2 * pid + 1];
   const uint32_t h_off = 128u * uint32_t(outer);
-  uint32_t i = (pid == 0) ? j : j - cum[pid - 1];
-  i += hls[inner];  // event-local 0-based inner hit
   const int16_t mi = hv.detind[i];
   if (mi > 2000) return 0;
   const float me_z = hv.zg[i];
@@ -135,7 +147,9 @@ __device__ __forceinline__ uint32_t doublets_of_item(const Dev& d, int e, uint32
         const float dd = __fsub_rn(ro, me_r);
         if (__dmul_rn(__dmul_rn(dphi_f, dphi_f), __dsub_rn(r2t4, double(rr))) > double(__fmul_rn(dd, dd))) continue;
       }
-      if (kFill) {
+      if (!kFill) {
+        if (cnt < uint32_t(kLaneSlots)) stage[cnt * kStageStride] = uint16_t(oi);
+      } else {
         // cell_pos: the item's first position within the event, cell_lo: the event's region
         const uint64_t local = cell_pos + cnt;
         if (local < cap) {
@@ -145,6 +159,8 @@ __device__ __forceinline__ uint32_t doublets_of_item(const Dev& d, int e, uint32
           d.cell_pair[g] = uint8_t(pid);
           d.cell_id[g] = int32_t(local + 1);
           d.cell_used[g] = 0;
+          d.cn_cur[g] = 0;
+          d.ct_cur[g] = 0;
           d.cell_inner_z[g] = me_z;
           d.cell_inner_r[g] = me_r;
         }
@@ -157,14 +173,80 @@ __device__ __forceinline__ uint32_t doublets_of_item(const Dev& d, int e, uint32
   return cnt;
 }
 
-template <bool kFill>
-__global__ void __launch_bounds__(256) k_doublets(Dev d, const uint32_t* __restrict__ pair_cum) {
+constexpr uint32_t kNoPool = 0xffffffffu;
+
+// Count pass over groups of 32 consecutive items (one warp, one item per lane): each lane
+// counts its item's doublets and stages their outer hits in shared memory; the group then
+// takes one contiguous range of the pool and copies them there in item order, which is the
+// order of the cells. A group with an item above kLaneSlots doublets, or that finds the pool
+// full, records kNoPool and the fill pass searches its candidates again.
+__global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* __restrict__ pair_cum) {
   const int e = blockIdx.y;
   const EvInfo& E = d.ev[e];
   const uint32_t n = E.n_items;
   if (n == 0) return;
   __shared__ uint32_t s_cum[kNPairs];
   __shared__ uint32_t s_hls[11];
+  __shared__ uint16_t s_stage[kLaneSlots * kStageStride];
+  __shared__ uint32_t s_ex[8][33];
+  if (threadIdx.x < kNPairs) s_cum[threadIdx.x] = pair_cum[size_t(e) * kNPairs + threadIdx.x];
+  if (threadIdx.x < 11) s_hls[threadIdx.x] = d.hits_layer_start[size_t(e) * 11 + threadIdx.x];
+  __syncthreads();
+  const uint32_t hb = E.hit_base;
+  HitView hv{d.xg + hb, d.yg + hb, d.zg + hb, d.rg + hb, d.iphi + hb, d.ysize + hb, d.detind + hb};
+  const uint32_t* poff = d.phi_off + size_t(e) * kPhiTotBins;
+  const HitRec* hrec = d.hit_rec + hb;
+  const uint32_t ib = E.item_base;
+  const unsigned lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+  uint16_t* stage = s_stage + threadIdx.x;
+  uint32_t* ex_w = s_ex[w];
+  for (uint32_t j0 = blockIdx.x * blockDim.x + 32u * w; j0 < n; j0 += gridDim.x * blockDim.x) {
+    const uint32_t j = j0 + lane;
+    const bool valid = j < n;
+    const uint32_t cnt = valid ? doublets_of_item<false>(d, e, j, s_cum, s_hls, hv, poff, hrec, 0, 0, 0, stage) : 0u;
+    if (valid) d.item_cnt[ib + j] = cnt;
+    const bool over = __any_sync(0xffffffffu, cnt > uint32_t(kLaneSlots));
+    const uint32_t inc = warp_incl_scan(cnt);
+    const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
+    const uint32_t ex = inc - cnt;
+    uint32_t off = kNoPool;
+    if (!over && total > 0) {
+      uint32_t o = 0;
+      if (lane == 0) o = atomicAdd(d.dbl_pool_ctr, total);
+      o = __shfl_sync(0xffffffffu, o, 0);
+      if (uint64_t(o) + total <= uint64_t(d.cap_cells)) off = o;
+    }
+    if (off != kNoPool) {
+      ex_w[lane] = ex;
+      __syncwarp();
+      for (uint32_t x = lane; x < total; x += 32) {
+        uint32_t a = 0, b = 32;  // last lane whose offset <= x (lanes without doublets share the next one's)
+        while (b - a > 1) {
+          const uint32_t m = (a + b) >> 1;
+          if (ex_w[m] <= x) a = m; else b = m;
+        }
+        d.dbl_pool[off + x] = s_stage[(x - ex_w[a]) * kStageStride + 32u * w + a];
+      }
+    }
+    if (valid) d.item_pool[ib + j] = off == kNoPool ? kNoPool : off + ex;
+    __syncwarp();
+  }
+}
+
+// Fill pass over the same 32-item groups: cells of a group are contiguous, so the warp
+// writes them with consecutive lanes on consecutive cells, outer hits from the pool and the
+// inner hit, pair and inner z / r of each cell's item from shared memory.
+__global__ void __launch_bounds__(256) k_doublets_fill(Dev d, const uint32_t* __restrict__ pair_cum) {
+  const int e = blockIdx.y;
+  const EvInfo& E = d.ev[e];
+  const uint32_t n = E.n_items;
+  if (n == 0) return;
+  __shared__ uint32_t s_cum[kNPairs];
+  __shared__ uint32_t s_hls[11];
+  __shared__ uint32_t s_pos[8][33];
+  __shared__ uint32_t s_hit[8][32];
+  __shared__ float s_z[8][32], s_r[8][32];
+  __shared__ uint8_t s_pid[8][32];
   if (threadIdx.x < kNPairs) s_cum[threadIdx.x] = pair_cum[size_t(e) * kNPairs + threadIdx.x];
   if (threadIdx.x < 11) s_hls[threadIdx.x] = d.hits_layer_start[size_t(e) * 11 + threadIdx.x];
   __syncthreads();
@@ -175,15 +257,55 @@ __global__ void __launch_bounds__(256) k_doublets(Dev d, const uint32_t* __restr
   const uint32_t ib = E.item_base;
   // raw positions of the count scan are made local to the event; the event keeps its
   // first n_cells doublets, stored from cell_base on
-  const uint32_t raw_lo = kFill ? d.item_cnt[ib] : 0u;
+  const uint32_t raw_lo = d.item_cnt[ib];
   const uint64_t cell_lo = E.cell_base;
   const uint32_t keep = E.n_cells;
-  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
-    if (kFill) {
-      doublets_of_item<true>(d, e, j, s_cum, s_hls, hv, poff, hrec, d.item_cnt[ib + j] - raw_lo, cell_lo, keep);
-    } else {
-      d.item_cnt[ib + j] = doublets_of_item<false>(d, e, j, s_cum, s_hls, hv, poff, hrec, 0, 0, 0);
+  const unsigned lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+  for (uint32_t j0 = blockIdx.x * blockDim.x + 32u * w; j0 < n; j0 += gridDim.x * blockDim.x) {
+    const uint32_t j = j0 + lane;
+    const bool valid = j < n;
+    const uint32_t pos = valid ? d.item_cnt[ib + j] - raw_lo : 0u;
+    const uint32_t cnt = valid ? d.item_cnt[ib + j + 1] - d.item_cnt[ib + j] : 0u;
+    const uint32_t pool = valid ? d.item_pool[ib + j] : kNoPool;
+    if (__any_sync(0xffffffffu, cnt > 0 && pool == kNoPool)) {
+      if (cnt > 0) doublets_of_item<true>(d, e, j, s_cum, s_hls, hv, poff, hrec, pos, cell_lo, keep, nullptr);
+      continue;
     }
+    const uint32_t inc = warp_incl_scan(cnt);
+    const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
+    if (total == 0) continue;
+    const uint32_t base = __shfl_sync(0xffffffffu, pos, 0);
+    const uint32_t pool0 = __shfl_sync(0xffffffffu, pool, 0);
+    uint32_t i = 0;
+    const int pid = valid ? item_pair(j, s_cum, s_hls, &i) : 0;
+    s_pos[w][lane] = inc - cnt;
+    if (cnt > 0) {
+      s_hit[w][lane] = i;
+      s_pid[w][lane] = uint8_t(pid);
+      s_z[w][lane] = hv.zg[i];
+      s_r[w][lane] = hv.rg[i];
+    }
+    __syncwarp();
+    for (uint32_t x = lane; x < total; x += 32) {
+      const uint32_t local = base + x;
+      if (local >= keep) break;
+      uint32_t a = 0, b = 32;
+      while (b - a > 1) {
+        const uint32_t m = (a + b) >> 1;
+        if (s_pos[w][m] <= x) a = m; else b = m;
+      }
+      const uint64_t g = cell_lo + local;
+      d.cell_inner[g] = s_hit[w][a];
+      d.cell_outer[g] = d.dbl_pool[pool0 + x];
+      d.cell_pair[g] = s_pid[w][a];
+      d.cell_id[g] = int32_t(local + 1);
+      d.cell_used[g] = 0;
+      d.cn_cur[g] = 0;
+      d.ct_cur[g] = 0;
+      d.cell_inner_z[g] = s_z[w][a];
+      d.cell_inner_r[g] = s_r[w][a];
+    }
+    __syncwarp();
   }
 }
 
@@ -207,24 +329,6 @@ __global__ void k_cell_regions(Dev d) {
   d.ev[e].n_cells_raw = d.ev[e].n_cells;
 }
 
-// zero the per-cell and per-hit counters of the batch (raw cell ranges, gaps included)
-__global__ void k_zero_counters(Dev d) {
-  const int e = blockIdx.y;
-  const EvInfo& E = d.ev[e];
-  const uint64_t cb = E.cell_base;
-  const uint32_t nraw = E.n_cells_raw;
-  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nraw; k += gridDim.x * blockDim.x) {
-    const uint64_t c = cb + k;
-    if (c >= uint64_t(d.cap_cells)) break;
-    d.cn_cnt[c] = 0; d.cn_cur[c] = 0; d.ct_cnt[c] = 0; d.ct_cur[c] = 0; d.tstart_cnt[c] = 0;
-    d.cn_mask[4 * c] = 0; d.cn_mask[4 * c + 1] = 0; d.cn_mask[4 * c + 2] = 0; d.cn_mask[4 * c + 3] = 0;
-  }
-  const uint32_t hb = E.hit_base, nh = E.n_hits;
-  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nh; k += gridDim.x * blockDim.x) {
-    d.ohc_cnt[hb + k] = 0; d.ohc_cur[hb + k] = 0; d.htt_cnt[hb + k] = 0; d.htt_cur[hb + k] = 0;
-  }
-}
-
 // ---------------------------------------------------------------- outer-hit lists
 template <int kPass>
 __global__ void k_ohc(Dev d) {
@@ -236,16 +340,51 @@ __global__ void k_ohc(Dev d) {
     const uint64_t c = cb + k;
     const uint32_t h = hb + d.cell_outer[c];
     if (kPass == 0) {
-      atomicAdd(&d.ohc_cnt[h], 1u);
+      atomicAdd(&d.ohc_cur[h], 1u);
     } else {
-      const uint32_t pos = d.ohc_cnt[h] + atomicAdd(&d.ohc_cur[h], 1u);
-      d.ohc_list[pos] = uint32_t(c);
+      d.ohc_list[atomicAdd(&d.ohc_cnt[h + 1], 1u)] = uint32_t(c);
     }
   }
 }
 
-// sort a short list in place (ascending)
+// bitonic sorting network over N values held in registers (indices are compile-time)
+template <int N>
+__device__ __forceinline__ void bitonic_regs(uint32_t (&v)[N]) {
+#pragma unroll
+  for (int k = 2; k <= N; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+#pragma unroll
+      for (int i = 0; i < N; ++i) {
+        const int l = i ^ j;
+        if (l > i) {
+          const uint32_t lo = min(v[i], v[l]), hi = max(v[i], v[l]);
+          if ((i & k) == 0) { v[i] = lo; v[l] = hi; } else { v[i] = hi; v[l] = lo; }
+        }
+      }
+    }
+  }
+}
+
+template <int N>
+__device__ __forceinline__ void sort_regs(uint32_t* a, uint32_t n) {
+  uint32_t v[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) v[i] = uint32_t(i) < n ? a[i] : 0xffffffffu;  // padding sorts last
+  bitonic_regs<N>(v);
+#pragma unroll
+  for (int i = 0; i < N; ++i)
+    if (uint32_t(i) < n) a[i] = v[i];
+}
+
+// sort a short list in place (ascending; entries are ids below 0xffffffff): one load and
+// one store per entry through a register network up to 32 entries, insertion sort above
 __device__ __forceinline__ void sort_list(uint32_t* a, uint32_t n) {
+  if (n < 2) return;
+  if (n <= 4) { sort_regs<4>(a, n); return; }
+  if (n <= 8) { sort_regs<8>(a, n); return; }
+  if (n <= 16) { sort_regs<16>(a, n); return; }
+  if (n <= 32) { sort_regs<32>(a, n); return; }
   for (uint32_t p = 1; p < n; ++p) {
     const uint32_t v = a[p];
     uint32_t q = p;
@@ -326,8 +465,20 @@ __global__ void __launch_bounds__(256) k_ohc_records(Dev d) {
   }
 }
 
-template <int kPass>
-__global__ void __launch_bounds__(256) k_connect(Dev d) {
+// Connection test of every cell with the cells ending on its inner hit (the outer-hit list,
+// at most kMaxCellsPerHit entries). A warp takes 32 cells and spreads their (cell, candidate)
+// pairs over its lanes, 32 pairs per step; the cheap alignment test runs on every pair, and the
+// pairs that pass it (a few percent) queue in shared memory for the circle / DCA test, which
+// then runs on full warps. Results do not depend on the evaluation order: the pass bits of each
+// cell, a count per neighbour (cn_cur) and the used flags.
+constexpr int kConnWarps = 8;
+constexpr int kConnQueue = 64;
+
+struct ConnCell {
+  float ri, zi, ro, zo, xi, yi, xo, yo;
+};
+
+__global__ void __launch_bounds__(256) k_connect_test(Dev d) {
   const int e = blockIdx.y;
   const EvInfo& E = d.ev[e];
   const uint64_t cb = E.cell_base;
@@ -337,43 +488,111 @@ __global__ void __launch_bounds__(256) k_connect(Dev d) {
   const float* zg = d.zg + hb;
   const float* rg = d.rg + hb;
   const int16_t* det = d.detind + hb;
+  __shared__ ConnCell s_cell[kConnWarps][32];
+  __shared__ uint32_t s_lo[kConnWarps][32];
+  __shared__ uint32_t s_ex[kConnWarps][32];
+  __shared__ uint32_t s_mask[kConnWarps][32][4];
+  __shared__ uint8_t s_barrel[kConnWarps][32];
+  __shared__ uint16_t s_queue[kConnWarps][kConnQueue];  // pair: owner lane << 8 | candidate
+  const unsigned lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  // circle / DCA test of the queued pairs q0 .. q0+31 (lanes past qn idle)
+  auto circle_step = [&](uint32_t q0, uint32_t qn) {
+    if (q0 + lane < qn) {
+      const uint32_t v = s_queue[w][q0 + lane];
+      const uint32_t a = v >> 8, j = v & 0xffu;
+      const uint32_t p = s_lo[w][a] + j;
+      const float4 rec = d.ohc_rec[p];
+      const ConnCell& cc = s_cell[w][a];
+      const float region = d.ohc_inner[p] ? kDcaInner : kDcaOuter;
+      const CircleEq eq(rec.z, rec.w, cc.xi, cc.yi, cc.xo, cc.yo);
+      bool cut;
+      if (eq.c > kHardCurv) cut = false;
+      else cut = fabsf(eq.dca0()) < __fmul_rn(region, fabsf(eq.c));
+      if (cut) {
+        const uint32_t o = d.ohc_list[p];
+        atomicOr(&s_mask[w][a][j >> 5], 1u << (j & 31));
+        atomicAdd(&d.cn_cur[o], 1u);
+        d.cell_used[o] = 1;
+      }
+    }
+  };
+  for (uint32_t k0 = blockIdx.x * blockDim.x + 32u * w; k0 < E.n_cells; k0 += gridDim.x * blockDim.x) {
+    const uint32_t k = k0 + lane;
+    const uint64_t c = cb + k;
+    uint32_t n = 0;
+    if (k < E.n_cells) {
+      const uint32_t ih = d.cell_inner[c], oh = d.cell_outer[c];
+      const uint32_t lo = d.ohc_cnt[hb + ih];
+      n = d.ohc_cnt[hb + ih + 1] - lo;
+      if (n > uint32_t(kMaxCellsPerHit)) n = kMaxCellsPerHit;
+      s_lo[w][lane] = lo;
+      s_cell[w][lane] = ConnCell{d.cell_inner_r[c], d.cell_inner_z[c], rg[oh], zg[oh], xg[ih], yg[ih], xg[oh], yg[oh]};
+      s_barrel[w][lane] = det[ih] < 1184 ? 1 : 0;
+    }
+    s_mask[w][lane][0] = 0; s_mask[w][lane][1] = 0; s_mask[w][lane][2] = 0; s_mask[w][lane][3] = 0;
+    const uint32_t inc = warp_incl_scan(n);
+    const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
+    s_ex[w][lane] = inc - n;
+    __syncwarp();
+    uint32_t qn = 0;
+    for (uint32_t x0 = 0; x0 < total; x0 += 32) {
+      const uint32_t x = x0 + lane;
+      bool al = false;
+      uint32_t a = 0, j = 0;
+      if (x < total) {
+        uint32_t b = 32;  // last lane whose first pair is <= x (lanes without pairs share the next one's)
+        while (b - a > 1) {
+          const uint32_t m = (a + b) >> 1;
+          if (s_ex[w][m] <= x) a = m; else b = m;
+        }
+        j = x - s_ex[w][a];
+        const float4 rec = d.ohc_rec[s_lo[w][a] + j];  // the candidate's inner hit: r, z, x, y
+        const ConnCell& cc = s_cell[w][a];
+        al = are_aligned(rec.x, rec.y, cc.ri, cc.zi, cc.ro, cc.zo, ptmin_f(),
+                         s_barrel[w][a] ? kThetaBarrel : kThetaForward);
+      }
+      const uint32_t bal = __ballot_sync(0xffffffffu, al);
+      if (al) s_queue[w][qn + __popc(bal & lt)] = uint16_t((a << 8) | j);
+      qn += __popc(bal);
+      __syncwarp();
+      if (qn >= 32) {
+        qn -= 32;
+        circle_step(qn, qn + 32);
+        __syncwarp();
+      }
+    }
+    circle_step(0, qn);
+    __syncwarp();
+    if (k < E.n_cells) {
+      const uint4 m = make_uint4(s_mask[w][lane][0], s_mask[w][lane][1], s_mask[w][lane][2], s_mask[w][lane][3]);
+      reinterpret_cast<uint4*>(d.cn_mask)[c] = m;
+      if (m.x | m.y | m.z | m.w) d.cell_used[c] = 1;
+    }
+    __syncwarp();
+  }
+}
+
+// neighbour lists: each passing (candidate o, cell c) pair appends c to o's list
+__global__ void __launch_bounds__(256) k_connect_fill(Dev d) {
+  const int e = blockIdx.y;
+  const EvInfo& E = d.ev[e];
+  const uint64_t cb = E.cell_base;
+  const uint32_t hb = E.hit_base;
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < E.n_cells; k += gridDim.x * blockDim.x) {
     const uint64_t c = cb + k;
-    const uint32_t ih = d.cell_inner[c], oh = d.cell_outer[c];
-    const uint32_t lo = d.ohc_cnt[hb + ih];
-    uint32_t n = d.ohc_cnt[hb + ih + 1] - lo;
-    if (n > uint32_t(kMaxCellsPerHit)) n = kMaxCellsPerHit;
-    if (kPass == 0) {
-      const float ri = d.cell_inner_r[c], zi = d.cell_inner_z[c];
-      const float ro = rg[oh], zo = zg[oh];
-      const bool is_barrel = det[ih] < 1184;
-      uint32_t mask[4] = {0, 0, 0, 0};
-      bool any = false;
-      const float xi = xg[ih], yi = yg[ih], xo = xg[oh], yo = yg[oh];
-      for (uint32_t j = 0; j < n; ++j) {
-        const float4 rec = d.ohc_rec[lo + j];  // the candidate's inner hit: r, z, x, y
-        const float r1 = rec.x, z1 = rec.y;
-        const bool aligned = are_aligned(r1, z1, ri, zi, ro, zo, ptmin_f(), is_barrel ? kThetaBarrel : kThetaForward);
-        const float region = d.ohc_inner[lo + j] ? kDcaInner : kDcaOuter;
-        const CircleEq eq(rec.z, rec.w, xi, yi, xo, yo);
-        bool cut;
-        if (eq.c > kHardCurv) cut = false;
-        else cut = fabsf(eq.dca0()) < __fmul_rn(region, fabsf(eq.c));
-        if (aligned && cut) {
-          const uint32_t o = d.ohc_list[lo + j];
-          mask[j >> 5] |= 1u << (j & 31);
-          atomicAdd(&d.cn_cnt[o], 1u);
-          d.cell_used[o] = 1;
-          any = true;
-        }
-      }
-      if (any) d.cell_used[c] = 1;
-      for (int w = 0; w < 4; ++w) d.cn_mask[4 * c + w] = mask[w];
-    } else {
-      for (uint32_t j = 0; j < n; ++j) {
-        if (!((d.cn_mask[4 * c + (j >> 5)] >> (j & 31)) & 1u)) continue;
+    const uint4 m = reinterpret_cast<const uint4*>(d.cn_mask)[c];
+    if (!(m.x | m.y | m.z | m.w)) continue;
+    const uint32_t lo = d.ohc_cnt[hb + d.cell_inner[c]];
+    const uint32_t words[4] = {m.x, m.y, m.z, m.w};
+#pragma unroll
+    for (int wd = 0; wd < 4; ++wd) {
+      uint32_t bits = words[wd];
+      while (bits) {
+        const uint32_t j = 32u * wd + uint32_t(__ffs(bits) - 1);
+        bits &= bits - 1;
         const uint32_t o = d.ohc_list[lo + j];
-        const uint32_t pos = d.cn_cnt[o] + atomicAdd(&d.cn_cur[o], 1u);
+        const uint32_t pos = atomicAdd(&d.cn_cnt[o + 1], 1u);
         if (pos < uint64_t(d.cap_pairs)) d.cn_list[pos] = uint32_t(c);
         else atomicOr(d.status, kWarnBuffer);
       }
@@ -522,12 +741,14 @@ __device__ void walk(const Dev& d, uint64_t cb, uint64_t start, uint64_t* tuple_
           d.tuple_hits[hp + depth + 1] = oh;
           d.tuple_det[hp + depth + 1] = uint16_t(d.detind[hbase + oh]);
           d.quality[g] = 0;
-          // cell -> track pairs, only for tuples the reference keeps
+          // cell -> track pairs, only for the tuples kept (the event's n_tuples: the
+          // reference's cap, or none when the event is past the batch buffers), so that
+          // the counts equal the entries k_cell_tracks_fill writes
           if (g - tuple_lo < tcap) {
             const uint64_t pp = hp - g;  // sum over earlier tuples of (hits - 1)
             for (int k = 0; k <= depth; ++k) {
               d.tuple_cell[pp + k] = stack_c[k];
-              atomicAdd(&d.ct_cnt[stack_c[k]], 1u);
+              atomicAdd(&d.ct_cur[stack_c[k]], 1u);
             }
           }
         }
@@ -564,7 +785,7 @@ __global__ void __launch_bounds__(128) k_ntuplets(Dev d) {
       if (!is_start(d, c)) continue;
       const uint64_t v = d.tstart_cnt[c];
       uint64_t tp = v >> 32, hp = v & 0xFFFFFFFFull;
-      walk<true>(d, cb, c, &tp, &hp, nullptr, nullptr, d.tstart_cnt[cb] >> 32, d.tuples_per_event, e);
+      walk<true>(d, cb, c, &tp, &hp, nullptr, nullptr, d.tstart_cnt[cb] >> 32, E.n_tuples, e);
     }
   }
 }
@@ -624,8 +845,7 @@ __global__ void k_cell_tracks_fill(Dev d) {
     const uint64_t pp = uint64_t(h0) - g;
     for (uint32_t k = 0; k + 1 < h1 - h0; ++k) {
       const uint32_t c = d.tuple_cell[pp + k];
-      const uint32_t pos = d.ct_cnt[c] + atomicAdd(&d.ct_cur[c], 1u);
-      d.ct_list[pos] = uint32_t(g);
+      d.ct_list[atomicAdd(&d.ct_cnt[c + 1], 1u)] = uint32_t(g);
     }
   }
 }
@@ -684,10 +904,14 @@ void launch_ca(const Dev& d, const Launch& L) {
   auto g = [&](int seg) { return dim3(L.bpe_of(seg), d.E); };
   const int eb = div_up(d.E + 1, 128);
   uint32_t* pair_cum = d.pair_cum;
+  // counters of the cells ending on each hit (the per-cell counters are cleared by the
+  // doublet fill that writes the cells)
+  cudaMemsetAsync(d.ohc_cur, 0, size_t(d.cap_hits) * sizeof(uint32_t), L.s);
   k_items<<<div_up(d.E, 128), 128, 0, L.s>>>(d, pair_cum);
   launch_ev_scan(d, L.s, int(offsetof(EvInfo, n_items)), int(offsetof(EvInfo, item_base)));
   L.mark("doublet_items");
-  k_doublets<false><<<g(kTuneDoublets), 256, 0, L.s>>>(d, pair_cum);
+  cudaMemsetAsync(d.dbl_pool_ctr, 0, sizeof(uint32_t), L.s);
+  k_doublets_count<<<g(kTuneDoublets), 256, 0, L.s>>>(d, pair_cum);
   L.mark("doublets_count");
   excl_scan_u32(d.item_cnt, d.cap_items, &d.ev[d.E].n_items, d.scan_tmp, L.s);
   k_cell_bases<<<eb, 128, 0, L.s>>>(d);
@@ -695,21 +919,20 @@ void launch_ca(const Dev& d, const Launch& L) {
   launch_ev_clamp(d, L.s, int(offsetof(EvInfo, n_cells)), int(offsetof(EvInfo, cell_base)), d.cap_cells);
   k_cell_regions<<<eb, 128, 0, L.s>>>(d);
   L.mark("doublets_scan");
-  k_doublets<true><<<g(kTuneDoublets), 256, 0, L.s>>>(d, pair_cum);
+  k_doublets_fill<<<g(kTuneDoublets), 256, 0, L.s>>>(d, pair_cum);
   L.mark("doublets_fill");
-  k_zero_counters<<<g(kTuneHitLists), 256, 0, L.s>>>(d);
   // cells ending on each hit
   k_ohc<0><<<g(kTuneHitLists), 256, 0, L.s>>>(d);
-  excl_scan_u32(d.ohc_cnt, d.cap_hits, &d.ev[d.E].n_hits, d.scan_tmp, L.s);
+  excl_scan_shift_u32(d.ohc_cur, d.ohc_cnt, d.cap_hits, &d.ev[d.E].n_hits, d.scan_tmp, L.s);
   k_ohc<1><<<g(kTuneHitLists), 256, 0, L.s>>>(d);
   k_sort_hit_lists<0><<<g(kTuneHitLists), 256, 0, L.s>>>(d);
   k_ohc_records<<<g(kTuneHitLists), 256, 0, L.s>>>(d);
   L.mark("outer_hit_lists");
   // connection and neighbour lists
-  k_connect<0><<<g(kTuneConnect), 256, 0, L.s>>>(d);
+  k_connect_test<<<g(kTuneConnect), 256, 0, L.s>>>(d);
   L.mark("connect");
-  excl_scan_u32(d.cn_cnt, d.cap_cells, &d.ev[d.E].n_cells_raw, d.scan_tmp, L.s);
-  k_connect<1><<<g(kTuneCellLists), 256, 0, L.s>>>(d);
+  excl_scan_shift_u32(d.cn_cur, d.cn_cnt, d.cap_cells, &d.ev[d.E].n_cells_raw, d.scan_tmp, L.s);
+  k_connect_fill<<<g(kTuneCellLists), 256, 0, L.s>>>(d);
   k_sort_cell_lists<0><<<g(kTuneCellLists), 256, 0, L.s>>>(d);
   L.mark("neighbour_lists");
   k_fishbone<<<g(kTuneFishbone), 128, 0, L.s>>>(d);
@@ -722,7 +945,7 @@ void launch_ca(const Dev& d, const Launch& L) {
   k_ntuplets<true><<<g(kTuneNtuplets), 128, 0, L.s>>>(d);
   k_tuple_ends<<<div_up(d.E, 128), 128, 0, L.s>>>(d);
   L.mark("ntuplets_fill");
-  excl_scan_u32(d.ct_cnt, d.cap_cells, &d.ev[d.E].n_cells_raw, d.scan_tmp, L.s);
+  excl_scan_shift_u32(d.ct_cur, d.ct_cnt, d.cap_cells, &d.ev[d.E].n_cells_raw, d.scan_tmp, L.s);
   k_cell_tracks_fill<<<g(kTuneCellTracks), 256, 0, L.s>>>(d);
   k_sort_cell_lists<1><<<g(kTuneCellTracks), 256, 0, L.s>>>(d);
   L.mark("cell_tracks");

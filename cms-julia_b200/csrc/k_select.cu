@@ -244,8 +244,8 @@ __global__ void k_hit_to_tuple(Dev d) {
     const uint32_t h0 = d.tuple_off[g], h1 = d.tuple_off[g + 1];
     for (uint32_t p = h0; p < h1; ++p) {
       const uint32_t h = hb + d.tuple_hits[p];
-      if (kPass == 0) atomicAdd(&d.htt_cnt[h], 1u);
-      else d.htt_list[d.htt_cnt[h] + atomicAdd(&d.htt_cur[h], 1u)] = uint32_t(g);
+      if (kPass == 0) atomicAdd(&d.htt_cur[h], 1u);
+      else d.htt_list[atomicAdd(&d.htt_cnt[h + 1], 1u)] = uint32_t(g);
     }
   }
 }
@@ -624,8 +624,9 @@ void launch_classify(const Dev& d, const Launch& L) {
   if (d.tuples_per_event > uint32_t(kDupMaxTuples)) k_fast_dup<<<div_up(d.E, 4), 128, 0, L.s>>>(d);
   else k_fast_dup_smem<<<d.E, 32, 0, L.s>>>(d);
   L.mark("fast_duplicate_remover");
+  cudaMemsetAsync(d.htt_cur, 0, size_t(d.cap_hits) * sizeof(uint32_t), L.s);
   k_hit_to_tuple<0><<<g(kTuneHitToTuple), 256, 0, L.s>>>(d);
-  excl_scan_u32(d.htt_cnt, d.cap_hits, &d.ev[d.E].n_hits, d.scan_tmp, L.s);
+  excl_scan_shift_u32(d.htt_cur, d.htt_cnt, d.cap_hits, &d.ev[d.E].n_hits, d.scan_tmp, L.s);
   k_hit_to_tuple<1><<<g(kTuneHitToTuple), 256, 0, L.s>>>(d);
   L.mark("hit_to_tuple");
   k_triplet_cleaner<<<g(kTuneHitToTuple), 256, 0, L.s>>>(d);

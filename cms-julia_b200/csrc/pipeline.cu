@@ -226,6 +226,7 @@ int alloc_batch(PxlCtx* ctx) {
   A(hits_layer_start, E * 11); A(phi_off, E * kPhiTotBins); A(phi_bins, d.cap_hits); A(hit_rec, d.cap_hits);
   A(pair_cum, E * kNPairs);
   A(item_cnt, d.cap_items + 1);
+  A(item_pool, d.cap_items); A(dbl_pool, d.cap_cells); A(dbl_pool_ctr, 1);
   A(tuple_det, d.cap_tuple_hits);
   A(cell_inner, d.cap_cells); A(cell_outer, d.cap_cells); A(cell_pair, d.cap_cells); A(cell_id, d.cap_cells);
   A(cell_used, d.cap_cells); A(cell_inner_z, d.cap_cells); A(cell_inner_r, d.cap_cells);
@@ -434,7 +435,11 @@ int32_t pxl_ctx_create(const PxlConditions* cond, const PxlParams* params, PxlCt
   PxlCtx* ctx = new PxlCtx();
   if (params) ctx->p = *params;
   else pxl_params_default(&ctx->p);
-  if (ctx->p.max_events <= 0) { delete ctx; return PXL_ERR_ARG; }
+  // event-local hit ids are 16-bit (phi bins, doublet staging)
+  if (ctx->p.max_events <= 0 || ctx->p.hits_per_event <= 0 || ctx->p.hits_per_event > 65535) {
+    delete ctx;
+    return PXL_ERR_ARG;
+  }
   if (cudaSetDevice(ctx->p.device) != cudaSuccess) { delete ctx; return PXL_ERR_CUDA; }
   if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return PXL_ERR_CUDA; }
   int rc = load_conditions(ctx, cond);

@@ -138,6 +138,9 @@ struct Dev {
   // doublets: work items and cells
   uint32_t* pair_cum;      // [E][19] cumulative inner-layer sizes over the layer pairs
   uint32_t* item_cnt;      // [cap_items] doublets per inner hit item, then exclusive positions
+  uint32_t* item_pool;     // [cap_items] first pool entry of the item's outer hits (kNoPool: none)
+  uint32_t* dbl_pool;      // [cap_cells] outer hits found by the count pass, 32-item groups in item order
+  uint32_t* dbl_pool_ctr;  // [1] entries taken from dbl_pool
   uint32_t* cell_inner;    // [cap_cells] event-local 0-based hit index
   uint32_t* cell_outer;
   uint8_t* cell_pair;      // 0-based layer pair
@@ -326,6 +329,10 @@ void launch_vertices(const Dev& d, const Launch& L);  // a18-a20
 // In place exclusive scan of data[0..n), n = min(ncap, *n_dev) (n_dev may be null); data[n] = total.
 void excl_scan_u32(uint32_t* data, int64_t ncap, const uint32_t* n_dev, uint32_t* tmp, cudaStream_t s);
 void excl_scan_u64(uint64_t* data, int64_t ncap, const uint32_t* n_dev, uint64_t* tmp, cudaStream_t s);
+// out[0] = 0, out[i + 1] = exclusive prefix of in[i]: offsets of lists filled by
+// atomicAdd(&out[key + 1], 1) (scan.cu)
+void excl_scan_shift_u32(const uint32_t* in, uint32_t* out, int64_t ncap, const uint32_t* n_dev, uint32_t* tmp,
+                         cudaStream_t s);
 int64_t scan_tmp_elems(int64_t n);
 
 }  // namespace pxl

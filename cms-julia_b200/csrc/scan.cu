@@ -120,6 +120,53 @@ __global__ void k_tile_scan(T* __restrict__ data, int64_t ncap, const uint32_t* 
   if (int64_t(blockIdx.x) == nt - 1 && threadIdx.x == 0) data[n] = sums[nt];
 }
 
+// Shifted form for lists filled by atomic increments: out[0] = 0 and out[i + 1] = the
+// exclusive prefix of in[i]. A fill that takes slot atomicAdd(&out[i + 1], 1) for each of
+// the in[i] entries of key i leaves out[i] = start of key i and out[n] = total: the
+// offsets of the filled lists, with no second counter array to clear.
+template <class T>
+__global__ void k_tile_scan_shift(const T* __restrict__ in, T* __restrict__ out, int64_t ncap, const uint32_t* n_dev,
+                                  const T* __restrict__ sums) {
+  int64_t n = live_n(ncap, n_dev);
+  int64_t nt = (n + kTile - 1) / kTile;
+  int64_t base = int64_t(blockIdx.x) * kTile;
+  if (blockIdx.x == 0 && threadIdx.x == 0) out[0] = 0;
+  if (int64_t(blockIdx.x) >= nt) return;
+  T v[kItems];
+  T tsum = 0;
+  int64_t i0 = base + int64_t(threadIdx.x) * kItems;
+  for (int k = 0; k < kItems; ++k) {
+    int64_t i = i0 + k;
+    v[k] = i < n ? in[i] : T(0);
+    tsum += v[k];
+  }
+  __shared__ T sh[33];
+  const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+  T inc = warp_incl(tsum);
+  if (lane == 31) sh[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    T s = lane < kTpb / 32 ? sh[lane] : T(0);
+    T si = warp_incl(s);
+    if (lane < kTpb / 32) sh[lane] = si - s;
+  }
+  __syncthreads();
+  T run = sums[blockIdx.x] + sh[wid] + inc - tsum;
+  for (int k = 0; k < kItems; ++k) {
+    int64_t i = i0 + k;
+    if (i < n) out[i + 1] = run;
+    run += v[k];
+  }
+}
+
+template <class T>
+void excl_scan_shift(const T* in, T* out, int64_t ncap, const uint32_t* n_dev, T* tmp, cudaStream_t s) {
+  int64_t nt = ncap > 0 ? (ncap + kTile - 1) / kTile : 1;
+  k_tile_sums<T><<<unsigned(nt), kTpb, 0, s>>>(in, ncap, n_dev, tmp);
+  k_scan_sums<T><<<1, 1024, 0, s>>>(tmp, ncap, n_dev);
+  k_tile_scan_shift<T><<<unsigned(nt), kTpb, 0, s>>>(in, out, ncap, n_dev, tmp);
+}
+
 template <class T>
 void excl_scan(T* data, int64_t ncap, const uint32_t* n_dev, T* tmp, cudaStream_t s) {
   int64_t nt = ncap > 0 ? (ncap + kTile - 1) / kTile : 1;
@@ -137,6 +184,10 @@ void excl_scan_u32(uint32_t* data, int64_t ncap, const uint32_t* n_dev, uint32_t
 }
 void excl_scan_u64(uint64_t* data, int64_t ncap, const uint32_t* n_dev, uint64_t* tmp, cudaStream_t s) {
   excl_scan<uint64_t>(data, ncap, n_dev, tmp, s);
+}
+void excl_scan_shift_u32(const uint32_t* in, uint32_t* out, int64_t ncap, const uint32_t* n_dev, uint32_t* tmp,
+                         cudaStream_t s) {
+  excl_scan_shift<uint32_t>(in, out, ncap, n_dev, tmp, s);
 }
 
 }  // namespace pxl

@@ -83,7 +83,7 @@ typedef struct PxlParams {
   int64_t max_hits;                  /* hits per batch */
   int64_t max_doublets;              /* doublets per batch */
   int64_t max_tuples;                /* tuples per batch */
-  int32_t hits_per_event;            /* 49152 (MAX_NUMBER_OF_HITS) */
+  int32_t hits_per_event;            /* 49152 (MAX_NUMBER_OF_HITS); at most 65535 */
   int32_t doublets_per_event;        /* 458752 (maxNumberOfDoublets) */
   int32_t tuples_per_event;          /* 32768 (TrackSOA stride) */
   int32_t fits_per_multiplicity;     /* 24576 (MAX_NUM_OF_CONCURRENT_FITS) */

@@ -29,3 +29,16 @@ def test_context_entry_points_reject_null():
     assert L.pxl_batch_run(None, None, None, 0, 0, 63, None) == -1
     assert L.pxl_autotune(None, None, 0, 1, None) == -1
     assert L.pxl_clusterize_digis_noalloc(1, 1, 1, 1, (1 << 20) + 1, 1, 1, 1, 1, 1, 1, None) == -4
+
+
+def test_context_rejects_hit_cap_beyond_16_bit_ids():
+    """Event-local hit ids are 16-bit on the device, so hits_per_event above 65535 is refused
+    before any device work."""
+    L = _native.lib()
+    h = ctypes.c_void_p()
+    p = _native.PxlParams()
+    assert L.pxl_params_default(ctypes.byref(p)) == 0
+    p.hits_per_event = 65536
+    assert L.pxl_ctx_create(ctypes.byref(_native.PxlConditions()), ctypes.byref(p), ctypes.byref(h)) == -1
+    p.hits_per_event = 0
+    assert L.pxl_ctx_create(ctypes.byref(_native.PxlConditions()), ctypes.byref(p), ctypes.byref(h)) == -1
