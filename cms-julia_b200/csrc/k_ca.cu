@@ -67,119 +67,142 @@ __device__ __forceinline__ int item_pair(uint32_t j, const uint32_t* cum, const 
   return pid;
 }
 
-// Doublets of one work item (inner hit x layer pair), candidates in the reference's loop
-// order. kFill false: counts them and keeps the first kLaneSlots outer hits in `stage`
-// (stride kStageStride; event-local hit ids fit 16 bits, hits_per_event <= 65535); true:
-// writes the cells from event-local position cell_pos on.
-constexpr int kLaneSlots = 48;
-constexpr int kStageStride = 256;
-template <bool kFill>
-__device__ __forceinline__ uint32_t doublets_of_item(const Dev& d, int e, uint32_t j, const uint32_t* cum,
-                                                     const uint32_t* hls, const HitView& hv, const uint32_t* poff,
-                                                     const HitRec* __restrict__ hrec, uint64_t cell_pos, uint64_t cell_lo,
-                                                     uint32_t cap, uint16_t* stage) {
+// Inner-hit part of one work item (inner hit x layer pair): the inner-hit cuts and the
+// outer-layer candidates of the phi window, the bins kl .. kh-1 (wrapping after 128) in the
+// reference's loop order, which are at most two contiguous ranges of the binned hits.
+struct ItemHead {
+  float z, r;
+  int16_t iphi, ysize, cut;
+  uint8_t pid, ok;
+  uint32_t hit;             // event-local 0-based inner hit
+  uint32_t lo0, n0, lo1;    // candidates: [lo0, lo0 + n0) then [lo1, lo1 + n - n0)
+  uint32_t n;
+};
+
+__device__ __forceinline__ ItemHead item_head(uint32_t j, const uint32_t* cum, const uint32_t* hls, const HitView& hv,
+                                              const uint32_t* poff) {
+  ItemHead h{};
   uint32_t i;
   const int pid = item_pair(j, cum, hls, &i);
+  h.pid = uint8_t(pid);
+  h.hit = i;
   const int inner = c_layer_pairs[2 * pid], outer = c_layer_pairs[2 * pid + 1];
-  const uint32_t h_off = 128u * uint32_t(outer);
-  const int16_t mi = hv.detind[i];
-  if (mi > 2000) return 0;
+  if (hv.detind[i] > 2000) return h;
   const float me_z = hv.zg[i];
-  if (double(me_z) < c_min_z[pid] || double(me_z) > c_max_z[pid]) return 0;
+  if (double(me_z) < c_min_z[pid] || double(me_z) > c_max_z[pid]) return h;
   const int32_t me_s = hv.ysize[i];  // idealConditions: every ladder is an outer ladder
-  if ((inner == 0 && outer > 3) && (me_s > 0 && me_s < 36)) return 0;
-  if ((inner == 1 && outer > 3) && (me_s > 0 && me_s < 28)) return 0;
-  const int16_t me_p = hv.iphi[i];
-  const float me_r = hv.rg[i];
-  const int16_t cut = c_phi_cuts[pid];
+  if ((inner == 0 && outer > 3) && (me_s > 0 && me_s < 36)) return h;
+  if ((inner == 1 && outer > 3) && (me_s > 0 && me_s < 28)) return h;
+  h.ok = 1;
+  h.z = me_z;
+  h.r = hv.rg[i];
+  h.iphi = hv.iphi[i];
+  h.ysize = int16_t(me_s);
+  h.cut = c_phi_cuts[pid];
+  const uint32_t h_off = 128u * uint32_t(outer);
+  const uint32_t kl = phi_bin(int16_t(h.iphi - h.cut));
+  uint32_t kh = phi_bin(int16_t(h.iphi + h.cut)) + 1;
+  if (kh == 129) kh = 1;
+  if (kl == kh) return h;
+  if (kl < kh) {
+    h.lo0 = poff[kl + h_off - 1];
+    h.n0 = poff[kh - 1 + h_off] - h.lo0;
+    h.lo1 = 0;
+    h.n = h.n0;
+  } else {
+    h.lo0 = poff[kl + h_off - 1];
+    h.n0 = poff[128 + h_off] - h.lo0;
+    h.lo1 = poff[h_off];
+    h.n = h.n0 + (poff[kh - 1 + h_off] - h.lo1);
+  }
+  return h;
+}
+
+// the outer-hit cuts of one candidate (gpu_pixel_doublets.jl z0 / dphi / size / pt cuts)
+__device__ __forceinline__ bool doublet_pass(const ItemHead& h, const HitRec& hr) {
+  const int pid = h.pid;
+  const int inner = c_layer_pairs[2 * pid], outer = c_layer_pairs[2 * pid + 1];
+  const float me_z = h.z, me_r = h.r;
+  const int16_t me_p = h.iphi, cut = h.cut;
+  const int32_t me_s = h.ysize;
   const float z0_cut = 12.f;
   const float dz_dr_fact = float(8 * 0.0285 / 0.015);
   const double min_radius = 0.5 * 87.78;
   const double r2t4 = 4. * min_radius * min_radius;
-  uint32_t kl = phi_bin(int16_t(me_p - cut));
-  uint32_t kh = phi_bin(int16_t(me_p + cut)) + 1;
-  if (kh == 129) kh = 1;
-  uint32_t cnt = 0;
-  for (uint32_t cb = kl; cb != kh;) {
-    const uint32_t p0 = poff[cb + h_off - 1], p1 = poff[cb + h_off];
-    for (uint32_t p = p0; p < p1; ++p) {
-      const HitRec hr = hrec[p];
-      const uint32_t oi = hr.id;  // event-local 0-based
-      const int16_t mo = hr.det;
-      if (mo > 2000) continue;
-      const float zo = hr.z, ro = hr.r;
-      {  // z0_cut_off
-        const float dr = __fsub_rn(ro, me_r);
-        if (double(dr) > c_max_r[pid] || dr < 0 ||
-            fabsf(__fsub_rn(__fmul_rn(me_z, ro), __fmul_rn(me_r, zo))) > __fmul_rn(z0_cut, dr))
-          continue;
-      }
-      const int16_t mo_p = hr.iphi;
-      const int16_t dphi = int16_t(mo_p - me_p);
-      const int16_t i_dphi = int16_t(dphi < 0 ? -dphi : dphi);
-      if (i_dphi > cut) continue;
-      {  // z_size_cut
-        bool kill;
-        if (outer < 4) {
-          const int16_t so = hr.ysize;
-          const int dy = inner == 0 ? 28 : 20;
-          const int16_t ds = int16_t(so - int16_t(me_s));
-          kill = me_s > 0 && so > 0 && (ds < 0 ? -int(ds) : int(ds)) > dy;
-        } else {
-          kill = false;
-          if (inner < 4 && me_s > 0) {
-            const float t = __fmul_rn(fabsf(__fdiv_rn(__fsub_rn(me_z, zo), __fsub_rn(me_r, ro))), dz_dr_fact);
-            const double tt = __dadd_rn(double(t), 0.5);
-            if (isfinite(tt)) {
-              const long long pred = (long long)trunc(tt);
-              const long long df = (long long)me_s - pred;
-              kill = (df < 0 ? -df : df) > 20;
-            } else {
-              continue;  // the reference raises (InexactError) here
-            }
-          }
-        }
-        if (kill) continue;
-      }
-      {  // pt_cut
-        const double dphi_f = __dmul_rn(double(i_dphi), (2 * 3.141592653589793) / double(1 << 16));
-        const float rr = __fmul_rn(me_r, ro);
-        const float dd = __fsub_rn(ro, me_r);
-        if (__dmul_rn(__dmul_rn(dphi_f, dphi_f), __dsub_rn(r2t4, double(rr))) > double(__fmul_rn(dd, dd))) continue;
-      }
-      if (!kFill) {
-        if (cnt < uint32_t(kLaneSlots)) stage[cnt * kStageStride] = uint16_t(oi);
-      } else {
-        // cell_pos: the item's first position within the event, cell_lo: the event's region
-        const uint64_t local = cell_pos + cnt;
-        if (local < cap) {
-          const uint64_t g = cell_lo + local;
-          d.cell_inner[g] = i;
-          d.cell_outer[g] = oi;
-          d.cell_pair[g] = uint8_t(pid);
-          d.cell_id[g] = int32_t(local + 1);
-          d.cell_used[g] = 0;
-          d.cn_cur[g] = 0;
-          d.ct_cur[g] = 0;
-          d.cell_inner_z[g] = me_z;
-          d.cell_inner_r[g] = me_r;
-        }
-      }
-      ++cnt;
-    }
-    cb = cb + 1;
-    if (cb == 129) cb = 1;
+  if (hr.det > 2000) return false;
+  const float zo = hr.z, ro = hr.r;
+  {  // z0_cut_off
+    const float dr = __fsub_rn(ro, me_r);
+    if (double(dr) > c_max_r[pid] || dr < 0 ||
+        fabsf(__fsub_rn(__fmul_rn(me_z, ro), __fmul_rn(me_r, zo))) > __fmul_rn(z0_cut, dr))
+      return false;
   }
-  return cnt;
+  const int16_t dphi = int16_t(hr.iphi - me_p);
+  const int16_t i_dphi = int16_t(dphi < 0 ? -dphi : dphi);
+  if (i_dphi > cut) return false;
+  {  // z_size_cut
+    if (outer < 4) {
+      const int16_t so = hr.ysize;
+      const int dy = inner == 0 ? 28 : 20;
+      const int16_t ds = int16_t(so - int16_t(me_s));
+      if (me_s > 0 && so > 0 && (ds < 0 ? -int(ds) : int(ds)) > dy) return false;
+    } else if (inner < 4 && me_s > 0) {
+      const float t = __fmul_rn(fabsf(__fdiv_rn(__fsub_rn(me_z, zo), __fsub_rn(me_r, ro))), dz_dr_fact);
+      const double tt = __dadd_rn(double(t), 0.5);
+      if (!isfinite(tt)) return false;  // the reference raises (InexactError) here
+      const long long pred = (long long)trunc(tt);
+      const long long df = (long long)me_s - pred;
+      if ((df < 0 ? -df : df) > 20) return false;
+    }
+  }
+  {  // pt_cut
+    const double dphi_f = __dmul_rn(double(i_dphi), (2 * 3.141592653589793) / double(1 << 16));
+    const float rr = __fmul_rn(me_r, ro);
+    const float dd = __fsub_rn(ro, me_r);
+    if (__dmul_rn(__dmul_rn(dphi_f, dphi_f), __dsub_rn(r2t4, double(rr))) > double(__fmul_rn(dd, dd))) return false;
+  }
+  return true;
+}
+
+__device__ __forceinline__ uint32_t head_candidate(const ItemHead& h, uint32_t k) {
+  return k < h.n0 ? h.lo0 + k : h.lo1 + (k - h.n0);
+}
+
+// All doublets of one item written from event-local position cell_pos on (the fill of
+// groups whose count pass could not keep their outer hits).
+__device__ __forceinline__ void write_item_doublets(const Dev& d, const ItemHead& h, const HitRec* __restrict__ hrec,
+                                                    uint64_t cell_pos, uint64_t cell_lo, uint32_t cap) {
+  if (!h.ok) return;
+  uint32_t cnt = 0;
+  for (uint32_t k = 0; k < h.n; ++k) {
+    const HitRec hr = hrec[head_candidate(h, k)];
+    if (!doublet_pass(h, hr)) continue;
+    const uint64_t local = cell_pos + cnt;
+    if (local < cap) {
+      const uint64_t g = cell_lo + local;
+      d.cell_inner[g] = h.hit;
+      d.cell_outer[g] = hr.id;
+      d.cell_pair[g] = h.pid;
+      d.cell_id[g] = int32_t(local + 1);
+      d.cell_used[g] = 0;
+      d.cn_cur[g] = 0;
+      d.ct_cur[g] = 0;
+      d.cell_inner_z[g] = h.z;
+      d.cell_inner_r[g] = h.r;
+    }
+    ++cnt;
+  }
 }
 
 constexpr uint32_t kNoPool = 0xffffffffu;
+constexpr int kGroupCells = 1024;  // outer hits one 32-item group stages in shared memory
 
-// Count pass over groups of 32 consecutive items (one warp, one item per lane): each lane
-// counts its item's doublets and stages their outer hits in shared memory; the group then
-// takes one contiguous range of the pool and copies them there in item order, which is the
-// order of the cells. A group with an item above kLaneSlots doublets, or that finds the pool
-// full, records kNoPool and the fill pass searches its candidates again.
+// Count pass over groups of 32 consecutive items (one warp). The candidates of the group's
+// items are laid end to end and tested 32 at a time on all lanes; passing candidates keep
+// that order (item, then the reference's candidate order), which is the order of the cells,
+// and stage their outer hit in shared memory. The group then takes one contiguous range of
+// the pool and copies them there. A group with more than kGroupCells doublets, or that finds
+// the pool full, records kNoPool and the fill pass searches its candidates again.
 __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* __restrict__ pair_cum) {
   const int e = blockIdx.y;
   const EvInfo& E = d.ev[e];
@@ -187,8 +210,10 @@ __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* _
   if (n == 0) return;
   __shared__ uint32_t s_cum[kNPairs];
   __shared__ uint32_t s_hls[11];
-  __shared__ uint16_t s_stage[kLaneSlots * kStageStride];
-  __shared__ uint32_t s_ex[8][33];
+  __shared__ ItemHead s_head[8][32];
+  __shared__ uint32_t s_tex[8][32];
+  __shared__ uint32_t s_cnt[8][32];
+  __shared__ uint16_t s_out[8][kGroupCells];
   if (threadIdx.x < kNPairs) s_cum[threadIdx.x] = pair_cum[size_t(e) * kNPairs + threadIdx.x];
   if (threadIdx.x < 11) s_hls[threadIdx.x] = d.hits_layer_start[size_t(e) * 11 + threadIdx.x];
   __syncthreads();
@@ -198,36 +223,58 @@ __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* _
   const HitRec* hrec = d.hit_rec + hb;
   const uint32_t ib = E.item_base;
   const unsigned lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
-  uint16_t* stage = s_stage + threadIdx.x;
-  uint32_t* ex_w = s_ex[w];
+  const unsigned lt = (1u << lane) - 1u;
   for (uint32_t j0 = blockIdx.x * blockDim.x + 32u * w; j0 < n; j0 += gridDim.x * blockDim.x) {
     const uint32_t j = j0 + lane;
     const bool valid = j < n;
-    const uint32_t cnt = valid ? doublets_of_item<false>(d, e, j, s_cum, s_hls, hv, poff, hrec, 0, 0, 0, stage) : 0u;
-    if (valid) d.item_cnt[ib + j] = cnt;
-    const bool over = __any_sync(0xffffffffu, cnt > uint32_t(kLaneSlots));
-    const uint32_t inc = warp_incl_scan(cnt);
-    const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
-    const uint32_t ex = inc - cnt;
-    uint32_t off = kNoPool;
-    if (!over && total > 0) {
-      uint32_t o = 0;
-      if (lane == 0) o = atomicAdd(d.dbl_pool_ctr, total);
-      o = __shfl_sync(0xffffffffu, o, 0);
-      if (uint64_t(o) + total <= uint64_t(d.cap_cells)) off = o;
+    uint32_t nc = 0;
+    if (valid) {
+      const ItemHead h = item_head(j, s_cum, s_hls, hv, poff);
+      if (h.ok) nc = h.n;
+      s_head[w][lane] = h;
     }
-    if (off != kNoPool) {
-      ex_w[lane] = ex;
-      __syncwarp();
-      for (uint32_t x = lane; x < total; x += 32) {
-        uint32_t a = 0, b = 32;  // last lane whose offset <= x (lanes without doublets share the next one's)
+    s_cnt[w][lane] = 0;
+    const uint32_t inc = warp_incl_scan(nc);
+    const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
+    s_tex[w][lane] = inc - nc;
+    __syncwarp();
+    uint32_t nout = 0;
+    for (uint32_t t0 = 0; t0 < total; t0 += 32) {
+      const uint32_t t = t0 + lane;
+      bool pass = false;
+      uint32_t a = 0, oi = 0;
+      if (t < total) {
+        uint32_t b = 32;  // last lane whose first candidate is <= t
         while (b - a > 1) {
           const uint32_t m = (a + b) >> 1;
-          if (ex_w[m] <= x) a = m; else b = m;
+          if (s_tex[w][m] <= t) a = m; else b = m;
         }
-        d.dbl_pool[off + x] = s_stage[(x - ex_w[a]) * kStageStride + 32u * w + a];
+        const ItemHead& h = s_head[w][a];
+        const HitRec hr = hrec[head_candidate(h, t - s_tex[w][a])];
+        pass = doublet_pass(h, hr);
+        oi = hr.id;
       }
+      const uint32_t bal = __ballot_sync(0xffffffffu, pass);
+      if (pass) {
+        atomicAdd(&s_cnt[w][a], 1u);
+        const uint32_t pos = nout + __popc(bal & lt);
+        if (pos < uint32_t(kGroupCells)) s_out[w][pos] = uint16_t(oi);
+      }
+      nout += __popc(bal);
     }
+    __syncwarp();
+    const uint32_t cnt = s_cnt[w][lane];
+    if (valid) d.item_cnt[ib + j] = cnt;
+    uint32_t off = kNoPool;
+    if (nout > 0 && nout <= uint32_t(kGroupCells)) {
+      uint32_t o = 0;
+      if (lane == 0) o = atomicAdd(d.dbl_pool_ctr, nout);
+      o = __shfl_sync(0xffffffffu, o, 0);
+      if (uint64_t(o) + nout <= uint64_t(d.cap_cells)) off = o;
+    }
+    if (off != kNoPool)
+      for (uint32_t x = lane; x < nout; x += 32) d.dbl_pool[off + x] = s_out[w][x];
+    const uint32_t ex = warp_incl_scan(cnt) - cnt;
     if (valid) d.item_pool[ib + j] = off == kNoPool ? kNoPool : off + ex;
     __syncwarp();
   }
@@ -268,7 +315,7 @@ __global__ void __launch_bounds__(256) k_doublets_fill(Dev d, const uint32_t* __
     const uint32_t cnt = valid ? d.item_cnt[ib + j + 1] - d.item_cnt[ib + j] : 0u;
     const uint32_t pool = valid ? d.item_pool[ib + j] : kNoPool;
     if (__any_sync(0xffffffffu, cnt > 0 && pool == kNoPool)) {
-      if (cnt > 0) doublets_of_item<true>(d, e, j, s_cum, s_hls, hv, poff, hrec, pos, cell_lo, keep, nullptr);
+      if (cnt > 0) write_item_doublets(d, item_head(j, s_cum, s_hls, hv, poff), hrec, pos, cell_lo, keep);
       continue;
     }
     const uint32_t inc = warp_incl_scan(cnt);

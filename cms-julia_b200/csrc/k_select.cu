@@ -294,58 +294,36 @@ __global__ void k_triplet_cleaner(Dev d) {
 // ---------------------------------------------------------------- vertices
 constexpr int kVtxThreads = 256;
 constexpr int kMaxVtx = 1024;
+constexpr int kVtxSmemTracks = 2048;  // selected tracks whose vertex arrays fit shared memory
 
-__global__ void __launch_bounds__(kVtxThreads) k_vertices(Dev d) {
-  const int e = blockIdx.x;
-  EvInfo& E = d.ev[e];
+struct VtxShared {
+  uint32_t sh[33];
+  uint32_t off[257];
+  uint32_t cur[256];
+  uint32_t nv, nvi, warn;
+  uint32_t vcnt[kMaxVtx], voff[kMaxVtx + 1];
+  uint16_t parent[kMaxVtx];
+};
+
+// cluster_tracks_by_density, fit_vertices, split_vertices and sort_by_pt2 on the selected
+// tracks of one event (one CTA). TI / TB: types of the per-track vertex ids and neighbour
+// counts and of the histogram / list entries; the arrays are in shared memory for events of
+// up to kVtxSmemTracks selected tracks (16-bit entries) and in global memory above.
+template <typename TI, typename TB>
+__device__ __forceinline__ void vertex_core(Dev& d, EvInfo& E, int e, uint32_t nt, const float* __restrict__ zt,
+                                            const float* __restrict__ ezt2, const float* ptt2, const uint32_t* itrk,
+                                            TI* iv, TI* nn, uint8_t* izt, TB* B, float* zv, float* wv, float* vchi2,
+                                            float* ptv2, uint16_t* sort_ind, VtxShared& S) {
   const uint64_t tb = E.tuple_base;
-  const uint32_t ntu = E.n_tuples;
-  float* zv = d.zv + size_t(e) * kMaxVtx;
-  float* wv = d.wv + size_t(e) * kMaxVtx;
-  float* vchi2 = d.vchi2 + size_t(e) * kMaxVtx;
-  float* ptv2 = d.ptv2 + size_t(e) * kMaxVtx;
-  uint16_t* sort_ind = d.sort_ind + size_t(e) * kMaxVtx;
-  int32_t* nn = d.ndof + tb + size_t(e) * kMaxVtx;  // length n_tuples + 1024
-  float* zt = d.vws_zt + tb;
-  float* ezt2 = d.vws_ezt2 + tb;
-  float* ptt2 = d.vws_ptt2 + tb;
-  int32_t* iv = d.vws_iv + tb;     // 1-based values as the reference stores them
-  uint32_t* itrk = d.vws_itrk + tb;
-  uint8_t* izt = d.vws_izt + tb;
-  __shared__ uint32_t sh[33];
-  __shared__ uint32_t s_off[257];
-  __shared__ uint32_t s_cur[256];
-  __shared__ uint32_t s_nv, s_nvi, s_warn;
-  __shared__ uint32_t s_vcnt[kMaxVtx], s_voff[kMaxVtx + 1];
-  __shared__ uint16_t s_parent[kMaxVtx];
-  for (int v = threadIdx.x; v < kMaxVtx; v += blockDim.x) { zv[v] = 0; wv[v] = 0; vchi2[v] = 0; ptv2[v] = 0; sort_ind[v] = 0; }
-  for (uint32_t t = threadIdx.x; t < ntu + kMaxVtx; t += blockDim.x) nn[t] = 0;
-  for (uint32_t t = threadIdx.x; t < ntu; t += blockDim.x) d.idv[tb + t] = -1;
-  if (threadIdx.x == 0) s_warn = 0;
-  // load_tracks (:51-82): >= 4 hits, loose, pt >= 0.5, in tuple order
-  uint32_t nt = 0;
-  for (uint32_t b = 0; b < ntu; b += blockDim.x) {
-    const uint32_t t = b + threadIdx.x;
-    bool sel = false;
-    if (t < ntu) {
-      const uint64_t g = tb + t;
-      const uint32_t n = d.tuple_off[g + 1] - d.tuple_off[g];
-      sel = n >= 4 && d.quality[g] == 2 && !(d.t_pt[g] < 0.5f);
-    }
-    uint32_t tot;
-    const uint32_t ex = block_excl_scan(sel ? 1u : 0u, sh, &tot);
-    if (sel) {
-      const uint64_t g = tb + t;
-      const uint32_t i = nt + ex;
-      const float pt = d.t_pt[g];
-      itrk[i] = t;
-      zt[i] = d.t_state[5 * g + 4];
-      ezt2[i] = d.t_cov[15 * g + 14];
-      ptt2[i] = __fmul_rn(pt, pt);
-    }
-    nt += tot;
-  }
-  if (threadIdx.x == 0) E.n_vtx_tracks = nt;
+  uint32_t* sh = S.sh;
+  uint32_t* s_off = S.off;
+  uint32_t* s_cur = S.cur;
+  uint32_t& s_nv = S.nv;
+  uint32_t& s_nvi = S.nvi;
+  uint32_t& s_warn = S.warn;
+  uint32_t* s_vcnt = S.vcnt;
+  uint32_t* s_voff = S.voff;
+  uint16_t* s_parent = S.parent;
   // cluster_tracks_by_density (:84-206), HisToContainer{UInt8,256,16000,8,UInt16}
   for (int b = threadIdx.x; b < 257; b += blockDim.x) s_off[b] = 0;
   __syncthreads();
@@ -354,7 +332,7 @@ __global__ void __launch_bounds__(kVtxThreads) k_vertices(Dev d) {
     iz = iz < -128 ? -128 : (iz > 127 ? 127 : iz);
     izt[i] = uint8_t(iz + 128);
     atomicAdd(&s_off[izt[i]], 1u);
-    iv[i] = int32_t(i + 1);
+    iv[i] = TI(i + 1);
   }
   __syncthreads();
   {  // exclusive starts of the 256 bins
@@ -365,19 +343,23 @@ __global__ void __launch_bounds__(kVtxThreads) k_vertices(Dev d) {
     if (threadIdx.x == 0) s_off[256] = tot;
   }
   __syncthreads();
-  uint32_t* B = d.vws_bins + tb;  // histogram contents, 1-based track indices
-  for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
-    const uint32_t pos = atomicAdd(&s_cur[izt[i]], 1u);
-    B[pos] = i + 1;
-  }
-  __syncthreads();
-  for (int b = threadIdx.x; b < 256; b += blockDim.x) {  // decreasing track index within a bin
-    const uint32_t lo = s_off[b], hi = s_off[b + 1];
-    for (uint32_t p = lo + 1; p < hi; ++p) {
-      const uint32_t v = B[p];
-      uint32_t q = p;
-      while (q > lo && B[q - 1] < v) { B[q] = B[q - 1]; --q; }
-      B[q] = v;
+  // histogram contents (1-based track indices), decreasing track index within a bin: one
+  // warp walks the tracks from the last down, 32 at a time, ranking equal bins by lane
+  if (threadIdx.x < 32) {
+    const unsigned lane = threadIdx.x, lt = (1u << lane) - 1u;
+    for (uint32_t b0 = 0; b0 < nt; b0 += 32) {
+      const bool ok = b0 + lane < nt;
+      const uint32_t i = ok ? nt - 1 - (b0 + lane) : 0u;
+      const uint32_t bin = ok ? uint32_t(izt[i]) : 0xffffffffu;
+      const uint32_t peers = __match_any_sync(0xffffffffu, bin);
+      const uint32_t start = ok ? s_cur[bin] : 0u;
+      __syncwarp();
+      if (ok) {
+        const uint32_t rank = __popc(peers & lt);
+        B[start + rank] = TB(i + 1);
+        if (rank == uint32_t(__popc(peers)) - 1u) s_cur[bin] = start + rank + 1;
+      }
+      __syncwarp();
     }
   }
   __syncthreads();
@@ -396,7 +378,7 @@ __global__ void __launch_bounds__(kVtxThreads) k_vertices(Dev d) {
       if (__fmul_rn(dist, dist) > __fmul_rn(chi2_max, __fadd_rn(ezt2[i], ezt2[j]))) continue;
       ++cnt;
     }
-    nn[i] = cnt;
+    nn[i] = TI(cnt);
   }
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
@@ -415,13 +397,13 @@ __global__ void __launch_bounds__(kVtxThreads) k_vertices(Dev d) {
       mdist = dist;
       a = int32_t(j + 1);
     }
-    iv[i] = a;
+    iv[i] = TI(a);
   }
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) {
     int32_t m = iv[i];
-    while (m != iv[m - 1]) m = iv[m - 1];
-    iv[i] = m;
+    while (m != int32_t(iv[m - 1])) m = iv[m - 1];
+    iv[i] = TI(m);
   }
   __syncthreads();
   uint32_t found = 0;
@@ -431,14 +413,14 @@ __global__ void __launch_bounds__(kVtxThreads) k_vertices(Dev d) {
     const bool seed = root && nn[i] >= 2;
     uint32_t tot;
     const uint32_t ex = block_excl_scan(seed ? 1u : 0u, sh, &tot);
-    if (root) iv[i] = seed ? -int32_t(found + ex + 1) : -9998;
+    if (root) iv[i] = TI(seed ? -int32_t(found + ex + 1) : -9998);
     found += tot;
   }
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x)
     if (iv[i] >= 0) iv[i] = iv[iv[i] - 1];
   __syncthreads();
-  for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) iv[i] = -iv[i];
+  for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) iv[i] = TI(-iv[i]);
   if (threadIdx.x == 0) {
     if (found >= uint32_t(kMaxVtx)) { s_warn |= kWarnVertex; found = kMaxVtx - 1; }
     s_nv = found;
@@ -468,7 +450,7 @@ __global__ void __launch_bounds__(kVtxThreads) k_vertices(Dev d) {
   }
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x)
-    if (iv[i] >= 1 && uint32_t(iv[i]) <= nv0) B[atomicAdd(&s_vcnt[iv[i] - 1], 1u)] = i;
+    if (iv[i] >= 1 && uint32_t(iv[i]) <= nv0) B[atomicAdd(&s_vcnt[iv[i] - 1], 1u)] = TB(i);
   __syncthreads();
   for (uint32_t v = threadIdx.x; v < nv0; v += blockDim.x) {
     const uint32_t lo = s_voff[v], hi = s_voff[v + 1];
@@ -476,7 +458,7 @@ __global__ void __launch_bounds__(kVtxThreads) k_vertices(Dev d) {
       const uint32_t x = B[p];
       uint32_t q = p;
       while (q > lo && B[q - 1] > x) { B[q] = B[q - 1]; --q; }
-      B[q] = x;
+      B[q] = TB(x);
     }
   }
   __syncthreads();
@@ -507,7 +489,7 @@ __global__ void __launch_bounds__(kVtxThreads) k_vertices(Dev d) {
         cnt += 1;
       }
       if (cnt > 0) w = __fmul_rn(w, __fdiv_rn(float(cnt), c2s));
-      zv[v] = z; wv[v] = w; vchi2[v] = c2s; nn[v] = cnt;
+      zv[v] = z; wv[v] = w; vchi2[v] = c2s; nn[v] = TI(cnt);
     }
     __syncthreads();
     if (threadIdx.x == 0) s_nv = nvf;
@@ -578,7 +560,7 @@ __global__ void __launch_bounds__(kVtxThreads) k_vertices(Dev d) {
         if (slot < uint32_t(kMaxVtx)) s_parent[slot] = uint16_t(kv);
         for (uint32_t p = lo; p < hi; ++p) {
           const uint32_t i = B[p];
-          if (iv[i] == int32_t(kv + 1) && izt[i] == 2) iv[i] = newv;
+          if (iv[i] == int32_t(kv + 1) && izt[i] == 2) iv[i] = TI(newv);
         }
       }
       __syncthreads();
@@ -608,6 +590,73 @@ __global__ void __launch_bounds__(kVtxThreads) k_vertices(Dev d) {
   if (threadIdx.x == 0) {
     E.n_vtx = nvf;
     if (s_warn) E.warnings |= s_warn;
+  }
+}
+
+__global__ void __launch_bounds__(kVtxThreads) k_vertices(Dev d) {
+  const int e = blockIdx.x;
+  EvInfo& E = d.ev[e];
+  const uint64_t tb = E.tuple_base;
+  const uint32_t ntu = E.n_tuples;
+  float* zv = d.zv + size_t(e) * kMaxVtx;
+  float* wv = d.wv + size_t(e) * kMaxVtx;
+  float* vchi2 = d.vchi2 + size_t(e) * kMaxVtx;
+  float* ptv2 = d.ptv2 + size_t(e) * kMaxVtx;
+  uint16_t* sort_ind = d.sort_ind + size_t(e) * kMaxVtx;
+  int32_t* nn = d.ndof + tb + size_t(e) * kMaxVtx;  // length n_tuples + 1024
+  float* zt = d.vws_zt + tb;
+  float* ezt2 = d.vws_ezt2 + tb;
+  float* ptt2 = d.vws_ptt2 + tb;
+  int32_t* iv = d.vws_iv + tb;     // 1-based values as the reference stores them
+  uint32_t* itrk = d.vws_itrk + tb;
+  uint8_t* izt = d.vws_izt + tb;
+  __shared__ VtxShared S;
+  __shared__ float s_zt[kVtxSmemTracks], s_ezt2[kVtxSmemTracks];
+  __shared__ int16_t s_iv[kVtxSmemTracks], s_nn[kVtxSmemTracks];
+  __shared__ uint16_t s_b[kVtxSmemTracks];
+  __shared__ uint8_t s_izt[kVtxSmemTracks];
+  uint32_t* sh = S.sh;
+  for (int v = threadIdx.x; v < kMaxVtx; v += blockDim.x) { zv[v] = 0; wv[v] = 0; vchi2[v] = 0; ptv2[v] = 0; sort_ind[v] = 0; }
+  for (uint32_t t = threadIdx.x; t < ntu + kMaxVtx; t += blockDim.x) nn[t] = 0;
+  for (uint32_t t = threadIdx.x; t < ntu; t += blockDim.x) d.idv[tb + t] = -1;
+  if (threadIdx.x == 0) S.warn = 0;
+  // load_tracks (:51-82): >= 4 hits, loose, pt >= 0.5, in tuple order
+  uint32_t nt = 0;
+  for (uint32_t b = 0; b < ntu; b += blockDim.x) {
+    const uint32_t t = b + threadIdx.x;
+    bool sel = false;
+    if (t < ntu) {
+      const uint64_t g = tb + t;
+      const uint32_t n = d.tuple_off[g + 1] - d.tuple_off[g];
+      sel = n >= 4 && d.quality[g] == 2 && !(d.t_pt[g] < 0.5f);
+    }
+    uint32_t tot;
+    const uint32_t ex = block_excl_scan(sel ? 1u : 0u, sh, &tot);
+    if (sel) {
+      const uint64_t g = tb + t;
+      const uint32_t i = nt + ex;
+      const float pt = d.t_pt[g];
+      itrk[i] = t;
+      zt[i] = d.t_state[5 * g + 4];
+      ezt2[i] = d.t_cov[15 * g + 14];
+      ptt2[i] = __fmul_rn(pt, pt);
+    }
+    nt += tot;
+  }
+  if (threadIdx.x == 0) E.n_vtx_tracks = nt;
+  __syncthreads();
+  if (nt <= uint32_t(kVtxSmemTracks)) {
+    for (uint32_t i = threadIdx.x; i < nt; i += blockDim.x) { s_zt[i] = zt[i]; s_ezt2[i] = ezt2[i]; }
+    for (uint32_t i = threadIdx.x; i < uint32_t(kVtxSmemTracks); i += blockDim.x) s_nn[i] = 0;
+    __syncthreads();
+    vertex_core<int16_t, uint16_t>(d, E, e, nt, s_zt, s_ezt2, ptt2, itrk, s_iv, s_nn, s_izt, s_b, zv, wv, vchi2, ptv2,
+                                   sort_ind, S);
+    // neighbour counts of the tracks, then ndof of the vertices: the reference's nn array
+    const uint32_t nw = nt > S.nv ? nt : S.nv;
+    for (uint32_t i = threadIdx.x; i < nw; i += blockDim.x) nn[i] = s_nn[i];
+  } else {
+    vertex_core<int32_t, uint32_t>(d, E, e, nt, zt, ezt2, ptt2, itrk, iv, nn, izt, d.vws_bins + tb, zv, wv, vchi2,
+                                   ptv2, sort_ind, S);
   }
 }
 
