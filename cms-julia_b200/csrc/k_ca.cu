@@ -27,7 +27,8 @@ __constant__ double c_min_z[kNPairs] = {-20., 0., -30., -22., 10., -30., -70., -
                                         -30., -70., -70., -20., -22., 0., -30., -70., -70.};
 __constant__ double c_max_z[kNPairs] = {20., 30., 0., 22., 30., -10., 70., 70., 22., 30.,
                                         -15., 70., 70., 20., 22., 30., 0., 70., 70.};
-__constant__ double c_max_r[kNPairs] = {20., 9., 9., 20., 7., 7., 5., 5., 20., 6., 6., 5., 5., 20., 20., 9., 9., 9., 9.};
+__constant__ float c_max_rf[kNPairs] = {20.f, 9.f, 9.f, 20.f, 7.f, 7.f, 5.f, 5.f, 20.f, 6.f, 6.f,
+                                        5.f, 5.f, 20.f, 20.f, 9.f, 9.f, 9.f, 9.f};
 
 // CA parameters (ca_hit_ntuplet_generator.jl:9-30), Float32 as Params stores them
 __device__ __forceinline__ float ptmin_f() { return 0.899999976158f; }
@@ -118,28 +119,29 @@ __device__ __forceinline__ ItemHead item_head(uint32_t j, const uint32_t* cum, c
   return h;
 }
 
-// the outer-hit cuts of one candidate (gpu_pixel_doublets.jl z0 / dphi / size / pt cuts)
-__device__ __forceinline__ bool doublet_pass(const ItemHead& h, const HitRec& hr) {
-  const int pid = h.pid;
+// The outer-hit cuts of one candidate (gpu_pixel_doublets.jl), in the reference's order:
+// doublet_pass_a takes the module, z0 and dphi cuts (about a quarter of the candidates pass),
+// doublet_pass_b the cluster-size and pt cuts. c_max_r holds small integers, so the float
+// comparison with them equals the reference's Float64 one.
+__device__ __forceinline__ bool doublet_pass_a(int pid, float me_z, float me_r, int16_t me_p, int16_t cut,
+                                               const HitRec& hr) {
+  if (hr.det > 2000) return false;
+  const float dr = __fsub_rn(hr.r, me_r);
+  if (dr > c_max_rf[pid] || dr < 0 ||
+      fabsf(__fsub_rn(__fmul_rn(me_z, hr.r), __fmul_rn(me_r, hr.z))) > __fmul_rn(12.f, dr))
+    return false;
+  const int16_t dphi = int16_t(hr.iphi - me_p);
+  const int16_t i_dphi = int16_t(dphi < 0 ? -dphi : dphi);
+  return i_dphi <= cut;
+}
+
+__device__ __forceinline__ bool doublet_pass_b(int pid, float me_z, float me_r, int16_t me_p, int32_t me_s,
+                                               const HitRec& hr) {
   const int inner = c_layer_pairs[2 * pid], outer = c_layer_pairs[2 * pid + 1];
-  const float me_z = h.z, me_r = h.r;
-  const int16_t me_p = h.iphi, cut = h.cut;
-  const int32_t me_s = h.ysize;
-  const float z0_cut = 12.f;
   const float dz_dr_fact = float(8 * 0.0285 / 0.015);
   const double min_radius = 0.5 * 87.78;
   const double r2t4 = 4. * min_radius * min_radius;
-  if (hr.det > 2000) return false;
   const float zo = hr.z, ro = hr.r;
-  {  // z0_cut_off
-    const float dr = __fsub_rn(ro, me_r);
-    if (double(dr) > c_max_r[pid] || dr < 0 ||
-        fabsf(__fsub_rn(__fmul_rn(me_z, ro), __fmul_rn(me_r, zo))) > __fmul_rn(z0_cut, dr))
-      return false;
-  }
-  const int16_t dphi = int16_t(hr.iphi - me_p);
-  const int16_t i_dphi = int16_t(dphi < 0 ? -dphi : dphi);
-  if (i_dphi > cut) return false;
   {  // z_size_cut
     if (outer < 4) {
       const int16_t so = hr.ysize;
@@ -156,12 +158,18 @@ __device__ __forceinline__ bool doublet_pass(const ItemHead& h, const HitRec& hr
     }
   }
   {  // pt_cut
+    const int16_t dphi = int16_t(hr.iphi - me_p);
+    const int16_t i_dphi = int16_t(dphi < 0 ? -dphi : dphi);
     const double dphi_f = __dmul_rn(double(i_dphi), (2 * 3.141592653589793) / double(1 << 16));
     const float rr = __fmul_rn(me_r, ro);
     const float dd = __fsub_rn(ro, me_r);
     if (__dmul_rn(__dmul_rn(dphi_f, dphi_f), __dsub_rn(r2t4, double(rr))) > double(__fmul_rn(dd, dd))) return false;
   }
   return true;
+}
+
+__device__ __forceinline__ bool doublet_pass(const ItemHead& h, const HitRec& hr) {
+  return doublet_pass_a(h.pid, h.z, h.r, h.iphi, h.cut, hr) && doublet_pass_b(h.pid, h.z, h.r, h.iphi, h.ysize, hr);
 }
 
 __device__ __forceinline__ uint32_t head_candidate(const ItemHead& h, uint32_t k) {
@@ -198,11 +206,14 @@ constexpr uint32_t kNoPool = 0xffffffffu;
 constexpr int kGroupCells = 1024;  // outer hits one 32-item group stages in shared memory
 
 // Count pass over groups of 32 consecutive items (one warp). The candidates of the group's
-// items are laid end to end and tested 32 at a time on all lanes; passing candidates keep
-// that order (item, then the reference's candidate order), which is the order of the cells,
-// and stage their outer hit in shared memory. The group then takes one contiguous range of
-// the pool and copies them there. A group with more than kGroupCells doublets, or that finds
-// the pool full, records kNoPool and the fill pass searches its candidates again.
+// items are laid end to end and take the first cuts 32 at a time on all lanes; the survivors
+// (about a quarter) queue in candidate order and take the remaining cuts on full warps, oldest
+// first, so passing candidates come out in the order of the cells (item, then the reference's
+// candidate order). Their outer hits are staged in shared memory; the group then takes one
+// contiguous range of the pool and copies them there. A group with more than kGroupCells
+// doublets, or that finds the pool full, records kNoPool and the fill pass searches again.
+constexpr int kDblQueue = 64;
+
 __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* __restrict__ pair_cum) {
   const int e = blockIdx.y;
   const EvInfo& E = d.ev[e];
@@ -210,9 +221,14 @@ __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* _
   if (n == 0) return;
   __shared__ uint32_t s_cum[kNPairs];
   __shared__ uint32_t s_hls[11];
-  __shared__ ItemHead s_head[8][32];
+  __shared__ float2 s_zr[8][32];
+  __shared__ uint32_t s_pc[8][32];  // inner iphi (low 16 bits) and phi cut (high 16 bits)
+  __shared__ uint32_t s_lo0[8][32], s_n0[8][32], s_lo1[8][32];
+  __shared__ int16_t s_ys[8][32];
+  __shared__ uint8_t s_pid[8][32];
   __shared__ uint32_t s_tex[8][32];
   __shared__ uint32_t s_cnt[8][32];
+  __shared__ uint32_t s_q[8][kDblQueue];  // owner lane << 16 | candidate
   __shared__ uint16_t s_out[8][kGroupCells];
   if (threadIdx.x < kNPairs) s_cum[threadIdx.x] = pair_cum[size_t(e) * kNPairs + threadIdx.x];
   if (threadIdx.x < 11) s_hls[threadIdx.x] = d.hits_layer_start[size_t(e) * 11 + threadIdx.x];
@@ -226,32 +242,32 @@ __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* _
   const unsigned lt = (1u << lane) - 1u;
   for (uint32_t j0 = blockIdx.x * blockDim.x + 32u * w; j0 < n; j0 += gridDim.x * blockDim.x) {
     const uint32_t j = j0 + lane;
-    const bool valid = j < n;
     uint32_t nc = 0;
-    if (valid) {
+    if (j < n) {
       const ItemHead h = item_head(j, s_cum, s_hls, hv, poff);
       if (h.ok) nc = h.n;
-      s_head[w][lane] = h;
+      s_zr[w][lane] = make_float2(h.z, h.r);
+      s_pc[w][lane] = uint32_t(uint16_t(h.iphi)) | (uint32_t(uint16_t(h.cut)) << 16);
+      s_lo0[w][lane] = h.lo0; s_n0[w][lane] = h.n0; s_lo1[w][lane] = h.lo1;
+      s_ys[w][lane] = h.ysize;
+      s_pid[w][lane] = h.pid;
     }
     s_cnt[w][lane] = 0;
     const uint32_t inc = warp_incl_scan(nc);
     const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
     s_tex[w][lane] = inc - nc;
     __syncwarp();
-    uint32_t nout = 0;
-    for (uint32_t t0 = 0; t0 < total; t0 += 32) {
-      const uint32_t t = t0 + lane;
+    uint32_t nout = 0, qhead = 0, qtail = 0;
+    // remaining cuts on queue entries qhead .. qhead + m - 1, one per lane, in queue order
+    auto stage_b = [&](uint32_t m) {
       bool pass = false;
       uint32_t a = 0, oi = 0;
-      if (t < total) {
-        uint32_t b = 32;  // last lane whose first candidate is <= t
-        while (b - a > 1) {
-          const uint32_t m = (a + b) >> 1;
-          if (s_tex[w][m] <= t) a = m; else b = m;
-        }
-        const ItemHead& h = s_head[w][a];
-        const HitRec hr = hrec[head_candidate(h, t - s_tex[w][a])];
-        pass = doublet_pass(h, hr);
+      if (lane < m) {
+        const uint32_t v = s_q[w][(qhead + lane) % kDblQueue];
+        a = v >> 16;
+        const HitRec hr = hrec[v & 0xffffu];
+        const float2 zr = s_zr[w][a];
+        pass = doublet_pass_b(s_pid[w][a], zr.x, zr.y, int16_t(s_pc[w][a] & 0xffffu), s_ys[w][a], hr);
         oi = hr.id;
       }
       const uint32_t bal = __ballot_sync(0xffffffffu, pass);
@@ -261,10 +277,34 @@ __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* _
         if (pos < uint32_t(kGroupCells)) s_out[w][pos] = uint16_t(oi);
       }
       nout += __popc(bal);
+      qhead += m;
+    };
+    uint32_t a = 0;  // owner of this lane's candidate, non-decreasing over the steps
+    for (uint32_t t0 = 0; t0 < total; t0 += 32) {
+      const uint32_t t = t0 + lane;
+      bool pass = false;
+      uint32_t p = 0;
+      if (t < total) {
+        while (a < 31 && s_tex[w][a + 1] <= t) ++a;
+        const uint32_t k = t - s_tex[w][a], n0 = s_n0[w][a];
+        p = k < n0 ? s_lo0[w][a] + k : s_lo1[w][a] + (k - n0);
+        const uint32_t pc = s_pc[w][a];
+        const float2 zr = s_zr[w][a];
+        pass = doublet_pass_a(s_pid[w][a], zr.x, zr.y, int16_t(pc & 0xffffu), int16_t(pc >> 16), hrec[p]);
+      }
+      const uint32_t bal = __ballot_sync(0xffffffffu, pass);
+      if (pass) s_q[w][(qtail + __popc(bal & lt)) % kDblQueue] = (a << 16) | p;
+      qtail += __popc(bal);
+      __syncwarp();
+      if (qtail - qhead >= 32) {
+        stage_b(32);
+        __syncwarp();
+      }
     }
+    stage_b(qtail - qhead);
     __syncwarp();
     const uint32_t cnt = s_cnt[w][lane];
-    if (valid) d.item_cnt[ib + j] = cnt;
+    if (j < n) d.item_cnt[ib + j] = cnt;
     uint32_t off = kNoPool;
     if (nout > 0 && nout <= uint32_t(kGroupCells)) {
       uint32_t o = 0;
@@ -275,7 +315,7 @@ __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* _
     if (off != kNoPool)
       for (uint32_t x = lane; x < nout; x += 32) d.dbl_pool[off + x] = s_out[w][x];
     const uint32_t ex = warp_incl_scan(cnt) - cnt;
-    if (valid) d.item_pool[ib + j] = off == kNoPool ? kNoPool : off + ex;
+    if (j < n) d.item_pool[ib + j] = off == kNoPool ? kNoPool : off + ex;
     __syncwarp();
   }
 }

@@ -114,10 +114,11 @@ struct WarpHist {
 };
 
 // One module of at most 32 * kSlots digis, clustered by one warp with its digis in
-// registers (kSlots per lane).
-template <int kSlots>
+// registers (kSlots per lane; shared-memory store for up to 32 * kStore digis).
+template <int kSlots, int kStore>
 __device__ __forceinline__ void cluster_module_warp(const Dev& d, int e, uint32_t m, const ModRange& r,
-                                                    WarpSmem<kSlots>& S, WarpHist* H) {
+                                                    WarpSmem<kStore>& S, WarpHist* H) {
+  static_assert(kSlots <= kStore, "slots beyond the shared-memory store");
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lt = (1u << lane) - 1u;
   const int n = r.n;

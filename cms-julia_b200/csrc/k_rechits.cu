@@ -175,6 +175,67 @@ struct WarpHitSmem {
   int32_t q[kWarpClus], qfx[kWarpClus], qlx[kWarpClus], qfy[kWarpClus], qly[kWarpClus];
 };
 
+// Per-cluster sums of one module with its digis in registers, kS per lane (the module's
+// digi count rounded up to a power-of-two number of warp slots). The sums go to the hit's
+// record; the CPE of all records then runs one hit per thread in k_cpe.
+template <int kS>
+__device__ __forceinline__ void module_sums(const Dev& d, int e, const HitModule& hm, const uint32_t* cms,
+                                            WarpHitSmem& S) {
+  const unsigned lane = threadIdx.x & 31u;
+  const EvInfo& E = d.ev[e];
+  const uint64_t eb = E.word_base;
+  const uint32_t hb = E.hit_base;
+  const uint32_t nclus = hm.nclus;
+  for (uint32_t k = lane; k < nclus; k += 32) {
+    S.minr[k] = 0xFFFFFFFFu; S.maxr[k] = 0; S.minc[k] = 0xFFFFFFFFu; S.maxc[k] = 0;
+    S.q[k] = 0; S.qfx[k] = 0; S.qlx[k] = 0; S.qfy[k] = 0; S.qly[k] = 0;
+  }
+  __syncwarp();
+  // digis of this module's range that belong to it, kept in registers
+  uint32_t xs[kS], ys[kS];
+  int32_t cls[kS], chs[kS];
+#pragma unroll
+  for (int j = 0; j < kS; ++j) {
+    const uint32_t i = hm.first0 + lane + 32u * j;
+    cls[j] = 0;
+    if (i < hm.end0) {
+      const uint64_t g = eb + i;
+      const int16_t id = d.mid[g];
+      const int32_t cl = d.clus[g];
+      if (id != int16_t(kInvId) && uint32_t(int32_t(id)) == hm.me && cl >= 1 && uint32_t(cl) <= nclus) {
+        cls[j] = cl;
+        xs[j] = uint32_t(int32_t(d.xx[g]));
+        ys[j] = uint32_t(int32_t(d.yy[g]));
+        const int32_t a = d.adc[g];
+        chs[j] = a < 65535 ? a : 65535;
+        atomicMin(&S.minr[cl - 1], xs[j]); atomicMax(&S.maxr[cl - 1], xs[j]);
+        atomicMin(&S.minc[cl - 1], ys[j]); atomicMax(&S.maxc[cl - 1], ys[j]);
+      }
+    }
+  }
+  __syncwarp();
+#pragma unroll
+  for (int j = 0; j < kS; ++j) {
+    if (cls[j] == 0) continue;
+    const int k = cls[j] - 1;
+    atomicAdd(&S.q[k], chs[j]);
+    if (S.minr[k] == xs[j]) atomicAdd(&S.qfx[k], chs[j]);
+    if (S.maxr[k] == xs[j]) atomicAdd(&S.qlx[k], chs[j]);
+    if (S.minc[k] == ys[j]) atomicAdd(&S.qfy[k], chs[j]);
+    if (S.maxc[k] == ys[j]) atomicAdd(&S.qly[k], chs[j]);
+  }
+  __syncwarp();
+  for (uint32_t k = lane; k < nclus; k += 32) {
+    const uint32_t h = cms[hm.me] + k;
+    if (h >= d.hits_per_event) continue;
+    if (uint64_t(hb) + h >= uint64_t(d.cap_hits)) { atomic_or_warn(&d.ev[e], kWarnBuffer); continue; }
+    const size_t o = size_t(hb) + h;
+    d.hit_sum[o] = ClusSumRec{S.minr[k], S.maxr[k], S.minc[k], S.maxc[k], S.q[k], S.qfx[k], S.qlx[k], S.qfy[k], S.qly[k]};
+    d.hit_me[o] = hm.me;
+  }
+  __syncwarp();
+}
+
 __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_get_hits_warp(Dev d) {
   __shared__ WarpHitSmem smem[kWarpsPerBlock];
   const int e = blockIdx.y;
@@ -183,7 +244,6 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_get_hits_warp(Dev d) {
   const EvInfo& E = d.ev[e];
   const uint32_t nmod = E.n_modules;
   if (E.word_base + uint64_t(E.n_words) > uint64_t(d.cap_words)) return;
-  const uint64_t eb = E.word_base;
   const uint32_t* cms = d.clus_module_start + size_t(e) * (kMaxNumModules + 1);
   for (uint32_t m = blockIdx.x * kWarpsPerBlock + wib; m < nmod; m += gridDim.x * kWarpsPerBlock) {
     HitModule hm;
@@ -193,51 +253,24 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_get_hits_warp(Dev d) {
       if (lane == 0) push_module(d, kListHitsBig, e, m);
       continue;
     }
-    const uint32_t nclus = hm.nclus;
-    for (uint32_t k = lane; k < nclus; k += 32) {
-      S.minr[k] = 0xFFFFFFFFu; S.maxr[k] = 0; S.minc[k] = 0xFFFFFFFFu; S.maxc[k] = 0;
-      S.q[k] = 0; S.qfx[k] = 0; S.qlx[k] = 0; S.qfy[k] = 0; S.qly[k] = 0;
-    }
-    __syncwarp();
-    // digis of this module's range that belong to it, kept in registers
-    uint32_t xs[kWarpSlots], ys[kWarpSlots];
-    int32_t cls[kWarpSlots], chs[kWarpSlots];
-#pragma unroll
-    for (int j = 0; j < kWarpSlots; ++j) {
-      const uint32_t i = hm.first0 + lane + 32u * j;
-      cls[j] = 0;
-      if (i < hm.end0) {
-        const uint64_t g = eb + i;
-        const int16_t id = d.mid[g];
-        const int32_t cl = d.clus[g];
-        if (id != int16_t(kInvId) && uint32_t(int32_t(id)) == hm.me && cl >= 1 && uint32_t(cl) <= nclus) {
-          cls[j] = cl;
-          xs[j] = uint32_t(int32_t(d.xx[g]));
-          ys[j] = uint32_t(int32_t(d.yy[g]));
-          const int32_t a = d.adc[g];
-          chs[j] = a < 65535 ? a : 65535;
-          atomicMin(&S.minr[cl - 1], xs[j]); atomicMax(&S.maxr[cl - 1], xs[j]);
-          atomicMin(&S.minc[cl - 1], ys[j]); atomicMax(&S.maxc[cl - 1], ys[j]);
-        }
-      }
-    }
-    __syncwarp();
-#pragma unroll
-    for (int j = 0; j < kWarpSlots; ++j) {
-      if (cls[j] == 0) continue;
-      const int k = cls[j] - 1;
-      atomicAdd(&S.q[k], chs[j]);
-      if (S.minr[k] == xs[j]) atomicAdd(&S.qfx[k], chs[j]);
-      if (S.maxr[k] == xs[j]) atomicAdd(&S.qlx[k], chs[j]);
-      if (S.minc[k] == ys[j]) atomicAdd(&S.qfy[k], chs[j]);
-      if (S.maxc[k] == ys[j]) atomicAdd(&S.qly[k], chs[j]);
-    }
-    __syncwarp();
-    for (uint32_t k = lane; k < nclus; k += 32) {
-      const ClusSum s{S.minr[k], S.maxr[k], S.minc[k], S.maxc[k], S.q[k], S.qfx[k], S.qlx[k], S.qfy[k], S.qly[k]};
-      write_hit(d, e, hm.me, cms[hm.me] + k, s);
-    }
-    __syncwarp();
+    if (nd <= 32) module_sums<1>(d, e, hm, cms, S);
+    else if (nd <= 64) module_sums<2>(d, e, hm, cms, S);
+    else if (nd <= 128) module_sums<4>(d, e, hm, cms, S);
+    else module_sums<kWarpSlots>(d, e, hm, cms, S);
+  }
+}
+
+// CPE of the hits whose cluster sums k_get_hits_warp recorded, one hit per thread
+__global__ void __launch_bounds__(256) k_cpe(Dev d) {
+  const int e = blockIdx.y;
+  const EvInfo& E = d.ev[e];
+  const uint32_t hb = E.hit_base;
+  for (uint32_t h = blockIdx.x * blockDim.x + threadIdx.x; h < E.n_hits; h += gridDim.x * blockDim.x) {
+    const size_t o = size_t(hb) + h;
+    const uint32_t me = d.hit_me[o];
+    if (me == 0xFFFFFFFFu) continue;
+    const ClusSumRec r = d.hit_sum[o];
+    write_hit(d, e, me, h, ClusSum{r.minr, r.maxr, r.minc, r.maxc, r.q, r.qfx, r.qlx, r.qfy, r.qly});
   }
 }
 
@@ -386,8 +419,12 @@ __global__ void __launch_bounds__(1024) k_phi_binner(Dev d) {
 
 void launch_rechits(const Dev& d, const Launch& L) {
   const int bx = std::max(4, std::min(250, (148 * 8 * 4) / std::max(1, int(d.E))));
+  // records of the warp-handled modules' clusters; hits of other modules keep 0xFFFFFFFF
+  cudaMemsetAsync(d.hit_me, 0xFF, size_t(d.cap_hits) * sizeof(uint32_t), L.s);
   k_get_hits_warp<<<dim3(bx, d.E), 32 * kWarpsPerBlock, 0, L.s>>>(d);
   L.mark("get_hits_warp");
+  k_cpe<<<dim3(std::max(1, std::min(64, (148 * 8 * 2) / std::max(1, int(d.E)))), d.E), 256, 0, L.s>>>(d);
+  L.mark("cpe");
   k_get_hits_block<<<148 * 2, 256, 0, L.s>>>(d);
   L.mark("get_hits_block");
   k_phi_binner<<<d.E, 1024, 0, L.s>>>(d);

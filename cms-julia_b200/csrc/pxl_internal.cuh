@@ -93,6 +93,12 @@ struct EvInfo {
 
 // The fields the doublet search reads of an outer-hit candidate, packed in phi-bin order
 // so that the search loads one 16-byte record per candidate.
+// bounding box and charges (total, first / last row and column) of one cluster
+struct ClusSumRec {
+  uint32_t minr, maxr, minc, maxc;
+  int32_t q, qfx, qlx, qfy, qly;
+};
+
 struct alignas(16) HitRec {
   float z, r;
   int16_t iphi, ysize, det;
@@ -135,6 +141,8 @@ struct Dev {
   uint32_t* phi_off;           // [E][1281]
   uint16_t* phi_bins;          // [cap_hits], 1-based hit ids
   struct HitRec* hit_rec;      // [cap_hits] the binned hits' doublet fields, in bin order
+  struct ClusSumRec* hit_sum;  // [cap_hits] per-cluster sums of getHits, input of the CPE
+  uint32_t* hit_me;            // [cap_hits] module of the hit's record, 0xFFFFFFFF when none
   // doublets: work items and cells
   uint32_t* pair_cum;      // [E][19] cumulative inner-layer sizes over the layer pairs
   uint32_t* item_cnt;      // [cap_items] doublets per inner hit item, then exclusive positions
