@@ -150,6 +150,11 @@ __device__ __forceinline__ void cluster_module_warp(const Dev& d, int e, uint32_
   crun = int(__reduce_min_sync(0xffffffffu, uint32_t(crun)));
   warn = __reduce_or_sync(0xffffffffu, warn);
   __syncwarp();
+  // histogram path: neighbour pairs (digi indices < 256) listed in the charge / cluster-number
+  // store, which is free until the labels are final; pairs past its capacity are joined at once
+  uint16_t* pairs = reinterpret_cast<uint16_t*>(S.charge);
+  constexpr uint32_t kPairCap = 32u * kStore * (sizeof(int32_t) + 2 * sizeof(uint16_t)) / sizeof(uint16_t);
+  uint32_t np = 0;
   if (H) {
     // neighbour pairs through a column histogram (count, warp scan, scatter); each digi
     // then looks at its own and the next column only, as the CTA path does
@@ -178,6 +183,9 @@ __device__ __forceinline__ void cluster_module_warp(const Dev& d, int e, uint32_
     for (int j = 0; j < kSlots; ++j)
       if (xy[j] != 0xffffffffu) H->sorted[atomicAdd(&H->cur[(xy[j] >> 16) + 1u], 1u)] = uint8_t(lane + 32 * j);
     __syncwarp();
+    uint32_t& npairs = H->cur[0];  // the scatter cursors are free again
+    if (lane == 0) npairs = 0;
+    __syncwarp();
 #pragma unroll
     for (int j = 0; j < kSlots; ++j) {
       const int k = int(lane) + 32 * j;
@@ -192,9 +200,13 @@ __device__ __forceinline__ void cluster_module_warp(const Dev& d, int e, uint32_
         if ((vm >> 16) == (xy[j] >> 16) && mm < k) continue;  // each same-column pair once
         const int dx = int(int16_t(vm & 0xffffu)) - xk;
         if (dx > 1 || dx < -1) continue;
-        cc_union(S.lab, k, mm);
+        const uint32_t slot = atomicAdd(&npairs, 1u);
+        if (slot < kPairCap) pairs[slot] = uint16_t(k | (mm << 8));
+        else cc_union(S.lab, k, mm);
       }
     }
+    __syncwarp();
+    np = npairs < kPairCap ? npairs : kPairCap;
   } else {
     // neighbour pairs (|dx| <= 1, |dcolumn| <= 1) by broadcasting every digi, each pair
     // once from its smaller index
@@ -220,6 +232,9 @@ __device__ __forceinline__ void cluster_module_warp(const Dev& d, int e, uint32_
       }
     }
   }
+  // the neighbour pairs, joined 32 at a time (any order gives the same components, each
+  // rooted at its smallest digi index)
+  for (uint32_t p = lane; p < np; p += 32) cc_union(S.lab, pairs[p] & 0xff, pairs[p] >> 8);
   __syncwarp();
 #pragma unroll
   for (int j = 0; j < kSlots; ++j) {
