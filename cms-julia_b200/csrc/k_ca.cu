@@ -556,88 +556,99 @@ __global__ void __launch_bounds__(256) k_ohc_records(Dev d) {
 // at most kMaxCellsPerHit entries). A warp takes 32 cells and spreads their (cell, candidate)
 // pairs over its lanes, 32 pairs per step; the cheap alignment test runs on every pair, and the
 // pairs that pass it (a few percent) queue in shared memory for the circle / DCA test, which
-// then runs on full warps. Results do not depend on the evaluation order: the pass bits of each
-// cell, a count per neighbour (cn_cur) and the used flags.
+// then runs on full warps. A passing pair counts one neighbour of the candidate (cn_cur), sets
+// both used flags and goes to the pair list that k_connect_fill turns into neighbour lists; none
+// of these depends on the evaluation order.
 constexpr int kConnWarps = 8;
 constexpr int kConnQueue = 64;
-
-struct ConnCell {
-  float ri, zi, ro, zo, xi, yi, xo, yo;
-};
 
 __global__ void __launch_bounds__(256) k_connect_test(Dev d) {
   const int e = blockIdx.y;
   const EvInfo& E = d.ev[e];
   const uint64_t cb = E.cell_base;
   const uint32_t hb = E.hit_base;
-  const float* xg = d.xg + hb;
-  const float* yg = d.yg + hb;
-  const float* zg = d.zg + hb;
-  const float* rg = d.rg + hb;
-  const int16_t* det = d.detind + hb;
-  __shared__ ConnCell s_cell[kConnWarps][32];
+  const float4* hxyzr = d.hit_xyzr + hb;
+  __shared__ float4 s_rz[kConnWarps][32];  // inner r, z and outer r, z of each cell
+  __shared__ float4 s_xy[kConnWarps][32];  // inner x, y and outer x, y
   __shared__ uint32_t s_lo[kConnWarps][32];
   __shared__ uint32_t s_ex[kConnWarps][32];
-  __shared__ uint32_t s_mask[kConnWarps][32][4];
   __shared__ uint8_t s_barrel[kConnWarps][32];
   __shared__ uint16_t s_queue[kConnWarps][kConnQueue];  // pair: owner lane << 8 | candidate
   const unsigned lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
+  uint64_t c0 = 0;
   // circle / DCA test of the queued pairs q0 .. q0+31 (lanes past qn idle)
   auto circle_step = [&](uint32_t q0, uint32_t qn) {
+    bool cut = false;
+    uint32_t o = 0, c = 0;
     if (q0 + lane < qn) {
       const uint32_t v = s_queue[w][q0 + lane];
       const uint32_t a = v >> 8, j = v & 0xffu;
       const uint32_t p = s_lo[w][a] + j;
       const float4 rec = d.ohc_rec[p];
-      const ConnCell& cc = s_cell[w][a];
+      const float4 xy = s_xy[w][a];
       const float region = d.ohc_inner[p] ? kDcaInner : kDcaOuter;
-      const CircleEq eq(rec.z, rec.w, cc.xi, cc.yi, cc.xo, cc.yo);
-      bool cut;
+      const CircleEq eq(rec.z, rec.w, xy.x, xy.y, xy.z, xy.w);
       if (eq.c > kHardCurv) cut = false;
       else cut = fabsf(eq.dca0()) < __fmul_rn(region, fabsf(eq.c));
       if (cut) {
-        const uint32_t o = d.ohc_list[p];
-        atomicOr(&s_mask[w][a][j >> 5], 1u << (j & 31));
-        atomicAdd(&d.cn_cur[o], 1u);
+        o = d.ohc_list[p];
+        c = uint32_t(c0 + a);
+      }
+    }
+    const uint32_t bal = __ballot_sync(0xffffffffu, cut);
+    if (bal) {
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(d.cn_pair_ctr, uint32_t(__popc(bal)));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (cut) {
+        const uint32_t slot = base + __popc(bal & lt);
         d.cell_used[o] = 1;
+        d.cell_used[c] = 1;
+        if (slot < uint32_t(d.cap_pairs)) {
+          d.cn_pairs[slot] = make_uint2(o, c);
+          atomicAdd(&d.cn_cur[o], 1u);
+        } else {
+          atomicOr(d.status, kWarnBuffer);
+        }
       }
     }
   };
   for (uint32_t k0 = blockIdx.x * blockDim.x + 32u * w; k0 < E.n_cells; k0 += gridDim.x * blockDim.x) {
     const uint32_t k = k0 + lane;
+    c0 = cb + k0;
     const uint64_t c = cb + k;
     uint32_t n = 0;
     if (k < E.n_cells) {
-      const uint32_t ih = d.cell_inner[c], oh = d.cell_outer[c];
+      const uint32_t ih = d.cell_inner[c];
       const uint32_t lo = d.ohc_cnt[hb + ih];
       n = d.ohc_cnt[hb + ih + 1] - lo;
       if (n > uint32_t(kMaxCellsPerHit)) n = kMaxCellsPerHit;
-      s_lo[w][lane] = lo;
-      s_cell[w][lane] = ConnCell{d.cell_inner_r[c], d.cell_inner_z[c], rg[oh], zg[oh], xg[ih], yg[ih], xg[oh], yg[oh]};
-      s_barrel[w][lane] = det[ih] < 1184 ? 1 : 0;
+      if (n > 0) {  // geometry only for cells with candidates
+        const uint32_t oh = d.cell_outer[c];
+        const float4 hi = hxyzr[ih], ho = hxyzr[oh];
+        s_lo[w][lane] = lo;
+        s_rz[w][lane] = make_float4(hi.w, hi.z, ho.w, ho.z);
+        s_xy[w][lane] = make_float4(hi.x, hi.y, ho.x, ho.y);
+        s_barrel[w][lane] = d.detind[hb + ih] < 1184 ? 1 : 0;
+      }
     }
-    s_mask[w][lane][0] = 0; s_mask[w][lane][1] = 0; s_mask[w][lane][2] = 0; s_mask[w][lane][3] = 0;
     const uint32_t inc = warp_incl_scan(n);
     const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
     s_ex[w][lane] = inc - n;
     __syncwarp();
     uint32_t qn = 0;
+    uint32_t a = 0;  // owner of this lane's pair, non-decreasing over the steps
     for (uint32_t x0 = 0; x0 < total; x0 += 32) {
       const uint32_t x = x0 + lane;
       bool al = false;
-      uint32_t a = 0, j = 0;
+      uint32_t j = 0;
       if (x < total) {
-        uint32_t b = 32;  // last lane whose first pair is <= x (lanes without pairs share the next one's)
-        while (b - a > 1) {
-          const uint32_t m = (a + b) >> 1;
-          if (s_ex[w][m] <= x) a = m; else b = m;
-        }
+        while (a < 31 && s_ex[w][a + 1] <= x) ++a;
         j = x - s_ex[w][a];
         const float4 rec = d.ohc_rec[s_lo[w][a] + j];  // the candidate's inner hit: r, z, x, y
-        const ConnCell& cc = s_cell[w][a];
-        al = are_aligned(rec.x, rec.y, cc.ri, cc.zi, cc.ro, cc.zo, ptmin_f(),
-                         s_barrel[w][a] ? kThetaBarrel : kThetaForward);
+        const float4 rz = s_rz[w][a];
+        al = are_aligned(rec.x, rec.y, rz.x, rz.y, rz.z, rz.w, ptmin_f(), s_barrel[w][a] ? kThetaBarrel : kThetaForward);
       }
       const uint32_t bal = __ballot_sync(0xffffffffu, al);
       if (al) s_queue[w][qn + __popc(bal & lt)] = uint16_t((a << 8) | j);
@@ -651,39 +662,16 @@ __global__ void __launch_bounds__(256) k_connect_test(Dev d) {
     }
     circle_step(0, qn);
     __syncwarp();
-    if (k < E.n_cells) {
-      const uint4 m = make_uint4(s_mask[w][lane][0], s_mask[w][lane][1], s_mask[w][lane][2], s_mask[w][lane][3]);
-      reinterpret_cast<uint4*>(d.cn_mask)[c] = m;
-      if (m.x | m.y | m.z | m.w) d.cell_used[c] = 1;
-    }
-    __syncwarp();
   }
 }
 
-// neighbour lists: each passing (candidate o, cell c) pair appends c to o's list
+// neighbour lists from the pair list: each passing (candidate o, cell c) appends c to o's list
 __global__ void __launch_bounds__(256) k_connect_fill(Dev d) {
-  const int e = blockIdx.y;
-  const EvInfo& E = d.ev[e];
-  const uint64_t cb = E.cell_base;
-  const uint32_t hb = E.hit_base;
-  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < E.n_cells; k += gridDim.x * blockDim.x) {
-    const uint64_t c = cb + k;
-    const uint4 m = reinterpret_cast<const uint4*>(d.cn_mask)[c];
-    if (!(m.x | m.y | m.z | m.w)) continue;
-    const uint32_t lo = d.ohc_cnt[hb + d.cell_inner[c]];
-    const uint32_t words[4] = {m.x, m.y, m.z, m.w};
-#pragma unroll
-    for (int wd = 0; wd < 4; ++wd) {
-      uint32_t bits = words[wd];
-      while (bits) {
-        const uint32_t j = 32u * wd + uint32_t(__ffs(bits) - 1);
-        bits &= bits - 1;
-        const uint32_t o = d.ohc_list[lo + j];
-        const uint32_t pos = atomicAdd(&d.cn_cnt[o + 1], 1u);
-        if (pos < uint64_t(d.cap_pairs)) d.cn_list[pos] = uint32_t(c);
-        else atomicOr(d.status, kWarnBuffer);
-      }
-    }
+  uint32_t np = *d.cn_pair_ctr;
+  if (np > uint32_t(d.cap_pairs)) np = uint32_t(d.cap_pairs);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) {
+    const uint2 pc = d.cn_pairs[i];
+    d.cn_list[atomicAdd(&d.cn_cnt[pc.x + 1], 1u)] = pc.y;
   }
 }
 
@@ -1016,10 +1004,11 @@ void launch_ca(const Dev& d, const Launch& L) {
   k_ohc_records<<<g(kTuneHitLists), 256, 0, L.s>>>(d);
   L.mark("outer_hit_lists");
   // connection and neighbour lists
+  cudaMemsetAsync(d.cn_pair_ctr, 0, sizeof(uint32_t), L.s);
   k_connect_test<<<g(kTuneConnect), 256, 0, L.s>>>(d);
   L.mark("connect");
   excl_scan_shift_u32(d.cn_cur, d.cn_cnt, d.cap_cells, &d.ev[d.E].n_cells_raw, d.scan_tmp, L.s);
-  k_connect_fill<<<g(kTuneCellLists), 256, 0, L.s>>>(d);
+  k_connect_fill<<<148 * 8, 256, 0, L.s>>>(d);
   k_sort_cell_lists<0><<<g(kTuneCellLists), 256, 0, L.s>>>(d);
   L.mark("neighbour_lists");
   k_fishbone<<<g(kTuneFishbone), 128, 0, L.s>>>(d);

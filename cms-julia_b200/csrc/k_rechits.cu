@@ -140,7 +140,9 @@ __device__ void write_hit(const Dev& d, int e, uint32_t me, uint32_t h, const Cl
   d.xsize[o] = sxs; d.ysize[o] = sys;
   d.xerr[o] = __fmul_rn(xerr, xerr); d.yerr[o] = __fmul_rn(yerr, yerr);
   d.xg[o] = xg; d.yg[o] = yg; d.zg[o] = zg;
-  d.rg[o] = __fsqrt_rn(__fadd_rn(__fmul_rn(xg, xg), __fmul_rn(yg, yg)));
+  const float rg = __fsqrt_rn(__fadd_rn(__fmul_rn(xg, xg), __fmul_rn(yg, yg)));
+  d.rg[o] = rg;
+  d.hit_xyzr[o] = make_float4(xg, yg, zg, rg);
   d.iphi[o] = atan2s(yg, xg);
 }
 

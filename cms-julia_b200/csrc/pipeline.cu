@@ -223,7 +223,7 @@ int alloc_batch(PxlCtx* ctx) {
   A(xl, d.cap_hits); A(yl, d.cap_hits); A(xerr, d.cap_hits); A(yerr, d.cap_hits);
   A(xg, d.cap_hits); A(yg, d.cap_hits); A(zg, d.cap_hits); A(rg, d.cap_hits);
   A(iphi, d.cap_hits); A(xsize, d.cap_hits); A(ysize, d.cap_hits); A(detind, d.cap_hits); A(charge, d.cap_hits);
-  A(hits_layer_start, E * 11); A(phi_off, E * kPhiTotBins); A(phi_bins, d.cap_hits); A(hit_rec, d.cap_hits); A(hit_sum, d.cap_hits); A(hit_me, d.cap_hits);
+  A(hits_layer_start, E * 11); A(phi_off, E * kPhiTotBins); A(phi_bins, d.cap_hits); A(hit_rec, d.cap_hits); A(hit_sum, d.cap_hits); A(hit_me, d.cap_hits); A(hit_xyzr, d.cap_hits);
   A(pair_cum, E * kNPairs);
   A(item_cnt, d.cap_items + 1);
   A(item_pool, d.cap_items); A(dbl_pool, d.cap_cells); A(dbl_pool_ctr, 1);
@@ -231,7 +231,7 @@ int alloc_batch(PxlCtx* ctx) {
   A(cell_inner, d.cap_cells); A(cell_outer, d.cap_cells); A(cell_pair, d.cap_cells); A(cell_id, d.cap_cells);
   A(cell_used, d.cap_cells); A(cell_inner_z, d.cap_cells); A(cell_inner_r, d.cap_cells);
   A(ohc_cnt, d.cap_hits + 1); A(ohc_cur, d.cap_hits); A(ohc_list, d.cap_cells); A(ohc_rec, d.cap_cells); A(ohc_inner, d.cap_cells);
-  A(cn_mask, 4 * d.cap_cells); A(cn_cnt, d.cap_cells + 1); A(cn_cur, d.cap_cells); A(cn_list, d.cap_pairs);
+  A(cn_pairs, d.cap_pairs); A(cn_pair_ctr, 1); A(cn_cnt, d.cap_cells + 1); A(cn_cur, d.cap_cells); A(cn_list, d.cap_pairs);
   A(tstart_cnt, d.cap_cells + 1);
   A(tuple_off, d.cap_tuples + 1); A(tuple_hits, d.cap_tuple_hits); A(quality, d.cap_tuples);
   A(tuple_cell, d.cap_tuple_hits);

@@ -143,6 +143,7 @@ struct Dev {
   struct HitRec* hit_rec;      // [cap_hits] the binned hits' doublet fields, in bin order
   struct ClusSumRec* hit_sum;  // [cap_hits] per-cluster sums of getHits, input of the CPE
   uint32_t* hit_me;            // [cap_hits] module of the hit's record, 0xFFFFFFFF when none
+  float4* hit_xyzr;            // [cap_hits] global x, y, z, r of each hit
   // doublets: work items and cells
   uint32_t* pair_cum;      // [E][19] cumulative inner-layer sizes over the layer pairs
   uint32_t* item_cnt;      // [cap_items] doublets per inner hit item, then exclusive positions
@@ -162,7 +163,8 @@ struct Dev {
   float4* ohc_rec;         // [cap_cells] per list entry: inner r, z, x, y of the cell (connect's candidate)
   uint8_t* ohc_inner;      // [cap_cells] per list entry: the cell's inner hit is on an inner-barrel module
   // cell neighbours (CSR over cells)
-  uint32_t* cn_mask;       // [cap_cells * 4] pass bits over the first 128 candidates
+  uint2* cn_pairs;         // [cap_pairs] passing (candidate, cell) pairs of the connection test
+  uint32_t* cn_pair_ctr;   // [1] entries of cn_pairs
   uint32_t* cn_cnt;        // [cap_cells + 1]
   uint32_t* cn_cur;        // [cap_cells]
   uint32_t* cn_list;       // [cap_pairs] global cell indices
