@@ -195,8 +195,6 @@ __device__ __forceinline__ void write_item_doublets(const Dev& d, const ItemHead
       d.cell_used[g] = 0;
       d.cn_cur[g] = 0;
       d.ct_cur[g] = 0;
-      d.cell_inner_z[g] = h.z;
-      d.cell_inner_r[g] = h.r;
     }
     ++cnt;
   }
@@ -332,7 +330,6 @@ __global__ void __launch_bounds__(256) k_doublets_fill(Dev d, const uint32_t* __
   __shared__ uint32_t s_hls[11];
   __shared__ uint32_t s_pos[8][33];
   __shared__ uint32_t s_hit[8][32];
-  __shared__ float s_z[8][32], s_r[8][32];
   __shared__ uint8_t s_pid[8][32];
   if (threadIdx.x < kNPairs) s_cum[threadIdx.x] = pair_cum[size_t(e) * kNPairs + threadIdx.x];
   if (threadIdx.x < 11) s_hls[threadIdx.x] = d.hits_layer_start[size_t(e) * 11 + threadIdx.x];
@@ -369,8 +366,6 @@ __global__ void __launch_bounds__(256) k_doublets_fill(Dev d, const uint32_t* __
     if (cnt > 0) {
       s_hit[w][lane] = i;
       s_pid[w][lane] = uint8_t(pid);
-      s_z[w][lane] = hv.zg[i];
-      s_r[w][lane] = hv.rg[i];
     }
     __syncwarp();
     for (uint32_t x = lane; x < total; x += 32) {
@@ -389,8 +384,6 @@ __global__ void __launch_bounds__(256) k_doublets_fill(Dev d, const uint32_t* __
       d.cell_used[g] = 0;
       d.cn_cur[g] = 0;
       d.ct_cur[g] = 0;
-      d.cell_inner_z[g] = s_z[w][a];
-      d.cell_inner_r[g] = s_r[w][a];
     }
     __syncwarp();
   }
@@ -545,9 +538,9 @@ __global__ void __launch_bounds__(256) k_ohc_records(Dev d) {
   const uint32_t hb = E.hit_base;
   const uint32_t lo = d.ohc_cnt[hb], hi = d.ohc_cnt[uint64_t(hb) + E.n_hits];
   for (uint32_t p = lo + blockIdx.x * blockDim.x + threadIdx.x; p < hi; p += gridDim.x * blockDim.x) {
-    const uint32_t o = d.ohc_list[p];
-    const uint32_t oih = d.cell_inner[o];
-    d.ohc_rec[p] = make_float4(d.cell_inner_r[o], d.cell_inner_z[o], d.xg[hb + oih], d.yg[hb + oih]);
+    const uint32_t oih = d.cell_inner[d.ohc_list[p]];
+    const float4 h = d.hit_xyzr[hb + oih];
+    d.ohc_rec[p] = make_float4(h.w, h.z, h.x, h.y);
     d.ohc_inner[p] = d.detind[hb + oih] < 96 ? 1 : 0;
   }
 }
@@ -735,11 +728,12 @@ __global__ void __launch_bounds__(128) k_fishbone(Dev d) {
       const uint32_t c = L[j];
       if (d.cell_used[c] == 0) continue;
       const uint32_t ih = d.cell_inner[c];
+      const float4 hi = d.hit_xyzr[hb + ih];
       idx[curr] = uint8_t(j);
       idet[curr] = uint16_t(det[ih]);
-      dx[curr] = __fsub_rn(xg[ih], xo);
-      dy[curr] = __fsub_rn(yg[ih], yo);
-      dz[curr] = __fsub_rn(d.cell_inner_z[c], zo);
+      dx[curr] = __fsub_rn(hi.x, xo);
+      dy[curr] = __fsub_rn(hi.y, yo);
+      dz[curr] = __fsub_rn(hi.z, zo);
       nrm[curr] = __fadd_rn(__fadd_rn(__fmul_rn(dx[curr], dx[curr]), __fmul_rn(dy[curr], dy[curr])),
                             __fmul_rn(dz[curr], dz[curr]));
       ++curr;

@@ -155,7 +155,6 @@ struct Dev {
   uint8_t* cell_pair;      // 0-based layer pair
   int32_t* cell_id;        // reference doublet id: 1-based, -1 when killed
   uint8_t* cell_used;
-  float* cell_inner_z; float* cell_inner_r;
   // outer-hit-of-cell lists (CSR over hits)
   uint32_t* ohc_cnt;       // [cap_hits + 1] counts -> offsets
   uint32_t* ohc_cur;       // [cap_hits] fill cursors
