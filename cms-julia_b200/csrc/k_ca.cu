@@ -219,14 +219,9 @@ __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* _
   if (n == 0) return;
   __shared__ uint32_t s_cum[kNPairs];
   __shared__ uint32_t s_hls[11];
-  __shared__ float2 s_zr[8][32];
-  __shared__ uint32_t s_pc[8][32];  // inner iphi (low 16 bits) and phi cut (high 16 bits)
-  __shared__ uint32_t s_lo0[8][32], s_n0[8][32], s_lo1[8][32];
-  __shared__ int16_t s_ys[8][32];
-  __shared__ uint8_t s_pid[8][32];
-  __shared__ uint32_t s_tex[8][32];
+  __shared__ uint32_t s_src[8][32];
   __shared__ uint32_t s_cnt[8][32];
-  __shared__ uint32_t s_q[8][kDblQueue];  // owner lane << 16 | candidate
+  __shared__ uint32_t s_q[8][kDblQueue];  // owner << 16 | candidate
   __shared__ uint16_t s_out[8][kGroupCells];
   if (threadIdx.x < kNPairs) s_cum[threadIdx.x] = pair_cum[size_t(e) * kNPairs + threadIdx.x];
   if (threadIdx.x < 11) s_hls[threadIdx.x] = d.hits_layer_start[size_t(e) * 11 + threadIdx.x];
@@ -240,58 +235,71 @@ __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* _
   const unsigned lt = (1u << lane) - 1u;
   for (uint32_t j0 = blockIdx.x * blockDim.x + 32u * w; j0 < n; j0 += gridDim.x * blockDim.x) {
     const uint32_t j = j0 + lane;
-    uint32_t nc = 0;
-    if (j < n) {
-      const ItemHead h = item_head(j, s_cum, s_hls, hv, poff);
-      if (h.ok) nc = h.n;
-      s_zr[w][lane] = make_float2(h.z, h.r);
-      s_pc[w][lane] = uint32_t(uint16_t(h.iphi)) | (uint32_t(uint16_t(h.cut)) << 16);
-      s_lo0[w][lane] = h.lo0; s_n0[w][lane] = h.n0; s_lo1[w][lane] = h.lo1;
-      s_ys[w][lane] = h.ysize;
-      s_pid[w][lane] = h.pid;
-    }
+    ItemHead h{};
+    if (j < n) h = item_head(j, s_cum, s_hls, hv, poff);
+    const uint32_t nc = h.ok ? h.n : 0u;
+    // items with candidates, compacted: compact index c holds the item of lane s_src[c], and
+    // its head is fetched from lane c by shuffles
+    const uint32_t busy = __ballot_sync(0xffffffffu, nc > 0);
+    const uint32_t m = __popc(busy);
+    if (nc > 0) s_src[w][__popc(busy & lt)] = lane;
     s_cnt[w][lane] = 0;
-    const uint32_t inc = warp_incl_scan(nc);
-    const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
-    s_tex[w][lane] = inc - nc;
     __syncwarp();
+    const uint32_t src = lane < m ? s_src[w][lane] : lane;
+    const float cz = __shfl_sync(0xffffffffu, h.z, src), cr = __shfl_sync(0xffffffffu, h.r, src);
+    const uint32_t cpc = __shfl_sync(0xffffffffu, uint32_t(uint16_t(h.iphi)) | (uint32_t(uint16_t(h.cut)) << 16), src);
+    const uint32_t cpy = __shfl_sync(0xffffffffu, uint32_t(h.pid) | (uint32_t(uint16_t(h.ysize)) << 16), src);
+    const uint32_t clo0 = __shfl_sync(0xffffffffu, h.lo0, src), clo1 = __shfl_sync(0xffffffffu, h.lo1, src);
+    const uint32_t cn0 = __shfl_sync(0xffffffffu, h.n0, src);
+    const uint32_t cn_src = __shfl_sync(0xffffffffu, nc, src);
+    const uint32_t cn = lane < m ? cn_src : 0u;
+    const uint32_t cinc = warp_incl_scan(cn);
+    const uint32_t total = __shfl_sync(0xffffffffu, cinc, 31);
+    const uint32_t ctex = cinc - cn;  // first candidate of compact item `lane`
     uint32_t nout = 0, qhead = 0, qtail = 0;
-    // remaining cuts on queue entries qhead .. qhead + m - 1, one per lane, in queue order
-    auto stage_b = [&](uint32_t m) {
+    // remaining cuts on queue entries qhead .. qhead + mm - 1, one per lane, in queue order
+    auto stage_b = [&](uint32_t mm) {
+      const uint32_t v = lane < mm ? s_q[w][(qhead + lane) % kDblQueue] : 0u;
+      const uint32_t o = v >> 16;
+      const float z = __shfl_sync(0xffffffffu, cz, o), r = __shfl_sync(0xffffffffu, cr, o);
+      const uint32_t pc = __shfl_sync(0xffffffffu, cpc, o), py = __shfl_sync(0xffffffffu, cpy, o);
       bool pass = false;
-      uint32_t a = 0, oi = 0;
-      if (lane < m) {
-        const uint32_t v = s_q[w][(qhead + lane) % kDblQueue];
-        a = v >> 16;
+      uint32_t oi = 0;
+      if (lane < mm) {
         const HitRec hr = hrec[v & 0xffffu];
-        const float2 zr = s_zr[w][a];
-        pass = doublet_pass_b(s_pid[w][a], zr.x, zr.y, int16_t(s_pc[w][a] & 0xffffu), s_ys[w][a], hr);
+        pass = doublet_pass_b(int(py & 0xffu), z, r, int16_t(pc & 0xffffu), int16_t(py >> 16), hr);
         oi = hr.id;
       }
       const uint32_t bal = __ballot_sync(0xffffffffu, pass);
       if (pass) {
-        atomicAdd(&s_cnt[w][a], 1u);
+        atomicAdd(&s_cnt[w][o], 1u);
         const uint32_t pos = nout + __popc(bal & lt);
         if (pos < uint32_t(kGroupCells)) s_out[w][pos] = uint16_t(oi);
       }
       nout += __popc(bal);
-      qhead += m;
+      qhead += mm;
     };
-    uint32_t a = 0;  // owner of this lane's candidate, non-decreasing over the steps
+    int cur = -1;  // compact item owning the candidate before the step
     for (uint32_t t0 = 0; t0 < total; t0 += 32) {
+      const uint32_t starts = __reduce_or_sync(
+          0xffffffffu, (lane < m && ctex >= t0 && ctex < t0 + 32u && cn > 0) ? (1u << (ctex - t0)) : 0u);
       const uint32_t t = t0 + lane;
+      const uint32_t o = uint32_t(cur + int(__popc(starts & ((2u << lane) - 1u))));
+      cur += int(__popc(starts));
+      const uint32_t oc = o < 32u ? o : 0u;
+      const float z = __shfl_sync(0xffffffffu, cz, oc), r = __shfl_sync(0xffffffffu, cr, oc);
+      const uint32_t pc = __shfl_sync(0xffffffffu, cpc, oc), py = __shfl_sync(0xffffffffu, cpy, oc);
+      const uint32_t lo0 = __shfl_sync(0xffffffffu, clo0, oc), lo1 = __shfl_sync(0xffffffffu, clo1, oc);
+      const uint32_t n0 = __shfl_sync(0xffffffffu, cn0, oc), tx = __shfl_sync(0xffffffffu, ctex, oc);
       bool pass = false;
       uint32_t p = 0;
       if (t < total) {
-        while (a < 31 && s_tex[w][a + 1] <= t) ++a;
-        const uint32_t k = t - s_tex[w][a], n0 = s_n0[w][a];
-        p = k < n0 ? s_lo0[w][a] + k : s_lo1[w][a] + (k - n0);
-        const uint32_t pc = s_pc[w][a];
-        const float2 zr = s_zr[w][a];
-        pass = doublet_pass_a(s_pid[w][a], zr.x, zr.y, int16_t(pc & 0xffffu), int16_t(pc >> 16), hrec[p]);
+        const uint32_t k = t - tx;
+        p = k < n0 ? lo0 + k : lo1 + (k - n0);
+        pass = doublet_pass_a(int(py & 0xffu), z, r, int16_t(pc & 0xffffu), int16_t(pc >> 16), hrec[p]);
       }
       const uint32_t bal = __ballot_sync(0xffffffffu, pass);
-      if (pass) s_q[w][(qtail + __popc(bal & lt)) % kDblQueue] = (a << 16) | p;
+      if (pass) s_q[w][(qtail + __popc(bal & lt)) % kDblQueue] = (oc << 16) | p;
       qtail += __popc(bal);
       __syncwarp();
       if (qtail - qhead >= 32) {
@@ -301,7 +309,7 @@ __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* _
     }
     stage_b(qtail - qhead);
     __syncwarp();
-    const uint32_t cnt = s_cnt[w][lane];
+    const uint32_t cnt = nc > 0 ? s_cnt[w][__popc(busy & lt)] : 0u;
     if (j < n) d.item_cnt[ib + j] = cnt;
     uint32_t off = kNoPool;
     if (nout > 0 && nout <= uint32_t(kGroupCells)) {
