@@ -219,10 +219,12 @@ __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* _
   if (n == 0) return;
   __shared__ uint32_t s_cum[kNPairs];
   __shared__ uint32_t s_hls[11];
-  __shared__ uint32_t s_src[8][32];
-  __shared__ uint32_t s_cnt[8][32];
+  __shared__ uint4 s_rng[8][32];   // per compacted item: lo0, n0, lo1, first candidate
+  __shared__ uint4 s_geo[8][32];   // per compacted item: z, r (float bits), iphi | cut << 16, pid | ysize << 16
+  __shared__ uint32_t s_beg[8][32], s_end[8][32], s_over[8][32];
   __shared__ uint32_t s_q[8][kDblQueue];  // owner << 16 | candidate
   __shared__ uint16_t s_out[8][kGroupCells];
+  __shared__ uint8_t s_own[8][kGroupCells];
   if (threadIdx.x < kNPairs) s_cum[threadIdx.x] = pair_cum[size_t(e) * kNPairs + threadIdx.x];
   if (threadIdx.x < 11) s_hls[threadIdx.x] = d.hits_layer_start[size_t(e) * 11 + threadIdx.x];
   __syncthreads();
@@ -238,68 +240,61 @@ __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* _
     ItemHead h{};
     if (j < n) h = item_head(j, s_cum, s_hls, hv, poff);
     const uint32_t nc = h.ok ? h.n : 0u;
-    // items with candidates, compacted: compact index c holds the item of lane s_src[c], and
-    // its head is fetched from lane c by shuffles
+    // items with candidates, compacted (compact index = rank among them); the candidates
+    // of compacted item c start at position ctex
     const uint32_t busy = __ballot_sync(0xffffffffu, nc > 0);
-    const uint32_t m = __popc(busy);
-    if (nc > 0) s_src[w][__popc(busy & lt)] = lane;
-    s_cnt[w][lane] = 0;
+    const uint32_t ci = __popc(busy & lt);
+    const uint32_t ctex = warp_incl_scan(nc) - nc;
+    const uint32_t total = __shfl_sync(0xffffffffu, ctex + nc, 31);
+    if (nc > 0) {
+      s_rng[w][ci] = make_uint4(h.lo0, h.n0, h.lo1, ctex);
+      s_geo[w][ci] = make_uint4(__float_as_uint(h.z), __float_as_uint(h.r),
+                                uint32_t(uint16_t(h.iphi)) | (uint32_t(uint16_t(h.cut)) << 16),
+                                uint32_t(h.pid) | (uint32_t(uint16_t(h.ysize)) << 16));
+    }
+    s_beg[w][lane] = 0; s_end[w][lane] = 0; s_over[w][lane] = 0;
     __syncwarp();
-    const uint32_t src = lane < m ? s_src[w][lane] : lane;
-    const float cz = __shfl_sync(0xffffffffu, h.z, src), cr = __shfl_sync(0xffffffffu, h.r, src);
-    const uint32_t cpc = __shfl_sync(0xffffffffu, uint32_t(uint16_t(h.iphi)) | (uint32_t(uint16_t(h.cut)) << 16), src);
-    const uint32_t cpy = __shfl_sync(0xffffffffu, uint32_t(h.pid) | (uint32_t(uint16_t(h.ysize)) << 16), src);
-    const uint32_t clo0 = __shfl_sync(0xffffffffu, h.lo0, src), clo1 = __shfl_sync(0xffffffffu, h.lo1, src);
-    const uint32_t cn0 = __shfl_sync(0xffffffffu, h.n0, src);
-    const uint32_t cn_src = __shfl_sync(0xffffffffu, nc, src);
-    const uint32_t cn = lane < m ? cn_src : 0u;
-    const uint32_t cinc = warp_incl_scan(cn);
-    const uint32_t total = __shfl_sync(0xffffffffu, cinc, 31);
-    const uint32_t ctex = cinc - cn;  // first candidate of compact item `lane`
     uint32_t nout = 0, qhead = 0, qtail = 0;
     // remaining cuts on queue entries qhead .. qhead + mm - 1, one per lane, in queue order
     auto stage_b = [&](uint32_t mm) {
-      const uint32_t v = lane < mm ? s_q[w][(qhead + lane) % kDblQueue] : 0u;
-      const uint32_t o = v >> 16;
-      const float z = __shfl_sync(0xffffffffu, cz, o), r = __shfl_sync(0xffffffffu, cr, o);
-      const uint32_t pc = __shfl_sync(0xffffffffu, cpc, o), py = __shfl_sync(0xffffffffu, cpy, o);
       bool pass = false;
-      uint32_t oi = 0;
+      uint32_t o = 0, oi = 0;
       if (lane < mm) {
+        const uint32_t v = s_q[w][(qhead + lane) % kDblQueue];
+        o = v >> 16;
+        const uint4 g = s_geo[w][o];
         const HitRec hr = hrec[v & 0xffffu];
-        pass = doublet_pass_b(int(py & 0xffu), z, r, int16_t(pc & 0xffffu), int16_t(py >> 16), hr);
+        pass = doublet_pass_b(int(g.w & 0xffu), __uint_as_float(g.x), __uint_as_float(g.y), int16_t(g.z & 0xffffu),
+                              int16_t(g.w >> 16), hr);
         oi = hr.id;
       }
       const uint32_t bal = __ballot_sync(0xffffffffu, pass);
       if (pass) {
-        atomicAdd(&s_cnt[w][o], 1u);
         const uint32_t pos = nout + __popc(bal & lt);
-        if (pos < uint32_t(kGroupCells)) s_out[w][pos] = uint16_t(oi);
+        if (pos < uint32_t(kGroupCells)) { s_out[w][pos] = uint16_t(oi); s_own[w][pos] = uint8_t(o); }
+        else atomicAdd(&s_over[w][o], 1u);
       }
       nout += __popc(bal);
       qhead += mm;
     };
-    int cur = -1;  // compact item owning the candidate before the step
+    int cur = -1;  // compacted item owning the candidate before the step
     for (uint32_t t0 = 0; t0 < total; t0 += 32) {
-      const uint32_t starts = __reduce_or_sync(
-          0xffffffffu, (lane < m && ctex >= t0 && ctex < t0 + 32u && cn > 0) ? (1u << (ctex - t0)) : 0u);
+      const uint32_t starts = __reduce_or_sync(0xffffffffu, (nc > 0 && ctex >= t0 && ctex < t0 + 32u) ? (1u << (ctex - t0)) : 0u);
       const uint32_t t = t0 + lane;
       const uint32_t o = uint32_t(cur + int(__popc(starts & ((2u << lane) - 1u))));
       cur += int(__popc(starts));
-      const uint32_t oc = o < 32u ? o : 0u;
-      const float z = __shfl_sync(0xffffffffu, cz, oc), r = __shfl_sync(0xffffffffu, cr, oc);
-      const uint32_t pc = __shfl_sync(0xffffffffu, cpc, oc), py = __shfl_sync(0xffffffffu, cpy, oc);
-      const uint32_t lo0 = __shfl_sync(0xffffffffu, clo0, oc), lo1 = __shfl_sync(0xffffffffu, clo1, oc);
-      const uint32_t n0 = __shfl_sync(0xffffffffu, cn0, oc), tx = __shfl_sync(0xffffffffu, ctex, oc);
       bool pass = false;
       uint32_t p = 0;
       if (t < total) {
-        const uint32_t k = t - tx;
-        p = k < n0 ? lo0 + k : lo1 + (k - n0);
-        pass = doublet_pass_a(int(py & 0xffu), z, r, int16_t(pc & 0xffffu), int16_t(pc >> 16), hrec[p]);
+        const uint4 rg = s_rng[w][o];
+        const uint4 g = s_geo[w][o];
+        const uint32_t k = t - rg.w;
+        p = k < rg.y ? rg.x + k : rg.z + (k - rg.y);
+        pass = doublet_pass_a(int(g.w & 0xffu), __uint_as_float(g.x), __uint_as_float(g.y), int16_t(g.z & 0xffffu),
+                              int16_t(g.z >> 16), hrec[p]);
       }
       const uint32_t bal = __ballot_sync(0xffffffffu, pass);
-      if (pass) s_q[w][(qtail + __popc(bal & lt)) % kDblQueue] = (oc << 16) | p;
+      if (pass) s_q[w][(qtail + __popc(bal & lt)) % kDblQueue] = (o << 16) | p;
       qtail += __popc(bal);
       __syncwarp();
       if (qtail - qhead >= 32) {
@@ -309,7 +304,15 @@ __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* _
     }
     stage_b(qtail - qhead);
     __syncwarp();
-    const uint32_t cnt = nc > 0 ? s_cnt[w][__popc(busy & lt)] : 0u;
+    // doublets per item: the staged outputs are in item order, so each item's are one run
+    const uint32_t nst = nout < uint32_t(kGroupCells) ? nout : uint32_t(kGroupCells);
+    for (uint32_t x = lane; x < nst; x += 32) {
+      const uint32_t o = s_own[w][x];
+      if (x == 0 || s_own[w][x - 1] != o) s_beg[w][o] = x;
+      if (x + 1 == nst || s_own[w][x + 1] != o) s_end[w][o] = x + 1;
+    }
+    __syncwarp();
+    const uint32_t cnt = nc > 0 ? s_end[w][ci] - s_beg[w][ci] + s_over[w][ci] : 0u;
     if (j < n) d.item_cnt[ib + j] = cnt;
     uint32_t off = kNoPool;
     if (nout > 0 && nout <= uint32_t(kGroupCells)) {
