@@ -125,13 +125,14 @@ def segment_bytes(name: str, c: dict) -> float | None:
         "module_starts": 4 * D,                    # moduleInd read by the count and fill passes
         "find_clus_small": 14 * D,                 # moduleInd,x,y,adc in; clus (and moduleInd) out (modules <= 32 digis;
                                                    # the larger ones only read their range bounds here)
-        "get_hits_warp": 14 * D + 44 * H,          # digis in; 44 B hit SoA out
+        "get_hits_warp": 14 * D + 40 * H,          # digis in; per-cluster sums out
+        "cpe": 40 * H + 60 * H,                    # sums in; hit SoA and packed coordinates out
         "phi_binner": 4 * H,                       # iphi in; bins out
-        "doublets_count": 14 * I + 4 * I,          # inner hit fields in; count out
-        "doublets_fill": 14 * I + 4 * I + 22 * C,  # + cell SoA out
-        "connect": 28 * C + 16 * C,                # cell fields in; neighbour masks out
-        "outer_hit_lists": 37 * C,                 # cell outer/inner/r/z in; lists and candidate records out
-        "neighbour_lists": 16 * C,                 # masks and list entries
+        "doublets_count": 26 * I + 16 * H + 4 * C, # item fields in, binned hit records (once), counts / pool out
+        "doublets_fill": 8 * I + 4 * C + 22 * C,   # counts and pool in, cell SoA out
+        "connect": 24 * C + 22 * H,                # cell hits and outer-hit records in, hit coordinates (once)
+        "outer_hit_lists": 41 * C + 8 * H,         # outer hits in, lists sorted, candidate records out
+        "neighbour_lists": 16 * C,                 # pair list in, lists filled and sorted
         "ntuplets_fill": 5 * T + 6 * TH,           # tuple offsets, hits, detector indices out
         "fast_duplicate_remover": 12 * T,          # qualities in and out, cell track lists in
         "broken_line_fit_4": 22 * TH + 4 * TH + 8 * T + 93 * T,
@@ -143,9 +144,8 @@ def segment_bytes(name: str, c: dict) -> float | None:
 # dram__bytes_read.sum + dram__bytes_write.sum per unit of work, from ncu captures of the
 # 300-event case (profiles/), scaled to a launch by the units it processes
 TRAFFIC_PER_UNIT = {
-    "get_hits_warp": ("words", (182.15e6 + 103.86e6) / 12_349_460),
-    "doublets_fill": ("cells", (374.91e6 + 786.06e6) / 25_257_080),
-    "vertices": ("tuples", (79.25e6 + 18.84e6) / 2_062_854),
+    "doublets_count": ("hits", (77.28e6 + 114.70e6) / 3_215_253),
+    "connect": ("cells", (619.12e6 + 77.25e6) / 25_257_080),
 }
 
 FIT_B = 0.0114256972711507  # 1/(pT R) at 3.8 T, GeV^-1 cm^-1
@@ -475,7 +475,12 @@ def main():
         totals["tuples"] += c.n_tuples
         totals["tuple_hits"] += c.n_tuple_hits
         totals["vertices"] += c.n_vertices
-    totals["items"] = int(totals["hits"] * 3.2)
+        # doublet work items: inner hits over the 19 layer pairs (layer 0 is the inner layer
+        # of 6 pairs, layer 1 of 4, layer 2 of 3, layers 4 and 7 of 2, layers 5 and 8 of 1)
+        if c.n_hits:
+            hls = chain.product("hits_layer_start", e).astype(np.int64)
+            nl = np.diff(hls[:11])
+            totals["items"] += int(6 * nl[0] + 4 * nl[1] + 3 * nl[2] + 2 * nl[4] + nl[5] + 2 * nl[7] + nl[8])
     if args.profile_only:
         print(json.dumps({"segments_ms": seg_ms, "totals": totals, "warnings": warn}), flush=True)
         return
