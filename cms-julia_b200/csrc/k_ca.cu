@@ -702,6 +702,8 @@ __global__ void k_sort_cell_lists(Dev d) {
       sort_list(list + lo, hi - lo);
       if (hi - lo > uint32_t(kCellRows)) atomic_or_warn(&d.ev[e], kWarnLists);
     }
+    // cells with two or more tracks, for the duplicate remover
+    if (kKind == 1 && cnt[c + 1] - cnt[c] >= 2) atomicOr(&d.dup_bits[c >> 5], 1u << (c & 31));
   }
   if (cols) atomicAdd(&s_cols, cols);
   __syncthreads();
@@ -1028,6 +1030,7 @@ void launch_ca(const Dev& d, const Launch& L) {
   L.mark("ntuplets_fill");
   excl_scan_shift_u32(d.ct_cur, d.ct_cnt, d.cap_cells, &d.ev[d.E].n_cells_raw, d.scan_tmp, L.s);
   k_cell_tracks_fill<<<g(kTuneCellTracks), 256, 0, L.s>>>(d);
+  cudaMemsetAsync(d.dup_bits, 0, size_t(d.cap_cells / 32 + 2) * sizeof(uint32_t), L.s);
   k_sort_cell_lists<1><<<g(kTuneCellTracks), 256, 0, L.s>>>(d);
   L.mark("cell_tracks");
   k_early_dup<<<g(kTuneEarlyDup), 256, 0, L.s>>>(d);

@@ -44,21 +44,13 @@ __global__ void k_classify(Dev d) {
   }
 }
 
-// cells with two or more tracks, compacted in cell order
-template <int kPass>
-__global__ void k_dup_cells(Dev d) {
-  const int e = blockIdx.y;
-  const EvInfo& E = d.ev[e];
-  const uint64_t cb = E.cell_base;
-  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < E.n_cells_raw; k += gridDim.x * blockDim.x) {
-    const uint64_t c = cb + k;
-    if (c >= uint64_t(d.cap_cells)) break;
-    if (kPass == 0) {
-      d.dup_flag[c] = (k < E.n_cells && d.ct_cnt[c + 1] - d.ct_cnt[c] >= 2) ? 1u : 0u;
-    } else if (k < E.n_cells && d.ct_cnt[c + 1] - d.ct_cnt[c] >= 2) {
-      d.dup_cells[d.dup_flag[c]] = uint32_t(c);
-    }
-  }
+// Bits of the event's cells [c_lo, c_hi) in word wi of the two-or-more-tracks bitmap
+// (set by k_sort_cell_lists<1>): walking the words in order walks those cells in order.
+__device__ __forceinline__ uint32_t dup_word(const Dev& d, uint64_t wi, uint64_t c_lo, uint64_t c_hi) {
+  uint32_t m = d.dup_bits[wi];
+  if (wi == (c_lo >> 5)) m &= ~0u << (c_lo & 31);
+  if (wi == ((c_hi - 1) >> 5) && (c_hi & 31)) m &= (1u << (c_hi & 31)) - 1u;
+  return m;
 }
 
 // kernel_fast_duplicate_remover: one warp per event, cells in order
@@ -67,9 +59,13 @@ __global__ void k_fast_dup(Dev d) {
   if (e >= d.E) return;
   const unsigned lane = threadIdx.x & 31u;
   const EvInfo& E = d.ev[e];
-  const uint32_t lo = d.dup_flag[E.cell_base], hi = d.dup_flag[uint64_t(E.cell_base) + E.n_cells_raw];
-  for (uint32_t q = lo; q < hi; ++q) {
-    const uint32_t c = d.dup_cells[q];
+  if (E.n_cells == 0) return;
+  const uint64_t c_lo = E.cell_base, c_hi = c_lo + E.n_cells;
+  for (uint64_t wi = c_lo >> 5; wi <= (c_hi - 1) >> 5; ++wi) {
+   uint32_t bits = dup_word(d, wi, c_lo, c_hi);
+   while (bits) {
+    const uint32_t c = uint32_t(32 * wi) + uint32_t(__ffs(bits) - 1);
+    bits &= bits - 1;
     const uint32_t l0 = d.ct_cnt[c];
     uint32_t n = d.ct_cnt[c + 1] - l0;
     if (n > uint32_t(kCellRows)) n = kCellRows;
@@ -96,6 +92,7 @@ __global__ void k_fast_dup(Dev d) {
       if (d.quality[t] != 0 && t != im) d.quality[t] = 1;
     }
     __syncwarp();
+   }
   }
 }
 
@@ -122,14 +119,15 @@ __global__ void __launch_bounds__(32) k_fast_dup_smem(Dev d) {
   __shared__ uint32_t s_off[33];
   __shared__ uint32_t s_l0[32];
   __shared__ uint32_t s_seen[kDupMaxTuples / 32];
+  __shared__ uint32_t s_clist[32 * 32];  // the cells of 32 bitmap words, in order
   const int e = blockIdx.x;
   const unsigned lane = threadIdx.x;
   const EvInfo& E = d.ev[e];
   const uint64_t tb = E.tuple_base;
   const uint32_t nt = E.n_tuples;
   if (nt > uint32_t(kDupMaxTuples)) return;  // k_fast_dup handles such events
-  const uint32_t lo = d.dup_flag[E.cell_base], hi = d.dup_flag[uint64_t(E.cell_base) + E.n_cells_raw];
-  if (lo == hi) return;
+  if (E.n_cells == 0) return;
+  const uint64_t c_lo = E.cell_base, c_hi = c_lo + E.n_cells;
   const uint32_t nw = (nt + 15) / 16;
   for (uint32_t w = lane; w < nw; w += 32) {
     uint32_t v = 0;
@@ -141,12 +139,21 @@ __global__ void __launch_bounds__(32) k_fast_dup_smem(Dev d) {
   }
   for (uint32_t w = lane; w < uint32_t(kDupMaxTuples / 32); w += 32) s_seen[w] = 0;
   __syncwarp();
-  for (uint32_t q0 = lo; q0 < hi;) {
+  for (uint64_t w0 = c_lo >> 5; w0 <= (c_hi - 1) >> 5; w0 += 32) {
+   // the next 32 bitmap words' cells, in order
+   const uint64_t wi = w0 + lane;
+   uint32_t bits = wi <= (c_hi - 1) >> 5 ? dup_word(d, wi, c_lo, c_hi) : 0u;
+   const uint32_t nb = __popc(bits);
+   const uint32_t winc = warp_incl_scan(nb);
+   const uint32_t hi = __shfl_sync(0xffffffffu, winc, 31);
+   for (uint32_t pos = winc - nb; bits; bits &= bits - 1) s_clist[pos++] = uint32_t(32 * wi) + uint32_t(__ffs(bits) - 1);
+   __syncwarp();
+   for (uint32_t q0 = 0; q0 < hi;) {
     // stage up to 32 cells: list start and length (capped at kCellRows)
     const uint32_t q = q0 + lane;
     uint32_t n = 0, l0 = 0;
     if (q < hi) {
-      const uint32_t c = d.dup_cells[q];
+      const uint32_t c = s_clist[q];
       l0 = d.ct_cnt[c];
       n = d.ct_cnt[c + 1] - l0;
       if (n > uint32_t(kCellRows)) n = kCellRows;
@@ -226,6 +233,8 @@ __global__ void __launch_bounds__(32) k_fast_dup_smem(Dev d) {
       __syncwarp();
     }
     q0 += ncell;
+  }
+   __syncwarp();
   }
   __syncwarp();
   for (uint32_t t = lane; t < nt; t += 32) d.quality[tb + t] = uint8_t(q_get(s_q, t));
@@ -666,10 +675,6 @@ void launch_classify(const Dev& d, const Launch& L) {
   auto g = [&](int seg) { return dim3(L.bpe_of(seg), d.E); };
   k_classify<<<g(kTuneClassify), 256, 0, L.s>>>(d);
   L.mark("classify");
-  k_dup_cells<0><<<g(kTuneClassify), 256, 0, L.s>>>(d);
-  excl_scan_u32(d.dup_flag, d.cap_cells, &d.ev[d.E].n_cells_raw, d.scan_tmp, L.s);
-  k_dup_cells<1><<<g(kTuneClassify), 256, 0, L.s>>>(d);
-  L.mark("dup_cell_list");
   if (d.tuples_per_event > uint32_t(kDupMaxTuples)) k_fast_dup<<<div_up(d.E, 4), 128, 0, L.s>>>(d);
   else k_fast_dup_smem<<<d.E, 32, 0, L.s>>>(d);
   L.mark("fast_duplicate_remover");

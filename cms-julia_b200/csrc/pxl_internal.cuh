@@ -186,8 +186,7 @@ struct Dev {
   uint32_t* htt_cur;
   uint32_t* htt_list;      // [cap_tuple_hits]
   // cells with >= 2 tracks, compacted per event
-  uint32_t* dup_cells;     // [cap_cells]
-  uint32_t* dup_flag;      // [cap_cells + 1]
+  uint32_t* dup_bits;      // [cap_cells / 32 + 2] cells with two or more tracks, one bit each
   // vertices, per event
   int16_t* idv;            // [cap_tuples] per tuple (global tuple index), -1 when unused
   float* vws_zt; float* vws_ezt2; float* vws_ptt2;  // [cap_tuples] vertex-finder workspace per selected track
