@@ -128,7 +128,8 @@ def segment_bytes(name: str, c: dict) -> float | None:
         "get_hits_warp": 14 * D + 40 * H,          # digis in; per-cluster sums out
         "cpe": 40 * H + 60 * H,                    # sums in; hit SoA and packed coordinates out
         "phi_binner": 4 * H,                       # iphi in; bins out
-        "doublets_count": 26 * I + 16 * H + 4 * C, # item fields in, binned hit records (once), counts / pool out
+        "doublets_count": 30 * H + 8 * I + 4 * C,  # inner-hit fields and binned hit records (once per hit) in,
+                                                   # per-item counts and pool offsets, pooled outer hits out
         "doublets_fill": 8 * I + 4 * C + 22 * C,   # counts and pool in, cell SoA out
         "connect": 24 * C + 22 * H,                # cell hits and outer-hit records in, hit coordinates (once)
         "outer_hit_lists": 41 * C + 8 * H,         # outer hits in, lists sorted, candidate records out
