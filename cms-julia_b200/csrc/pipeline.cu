@@ -629,7 +629,7 @@ int32_t pxl_autotune(PxlCtx* ctx, const int32_t* candidates, int32_t n_candidate
       {"doublets_count", kTuneDoublets}, {"doublets_fill", kTuneDoublets}, {"outer_hit_lists", kTuneHitLists},
       {"connect", kTuneConnect}, {"neighbour_lists", kTuneCellLists}, {"fishbone", kTuneFishbone},
       {"ntuplets_count", kTuneNtuplets}, {"ntuplets_fill", kTuneNtuplets}, {"cell_tracks", kTuneCellTracks},
-      {"dup_multiplicity", kTuneEarlyDup}, {"classify", kTuneClassify}, {"dup_cell_list", kTuneClassify},
+      {"dup_multiplicity", kTuneEarlyDup}, {"classify", kTuneClassify},
       {"hit_to_tuple", kTuneHitToTuple}, {"triplet_cleaner", kTuneHitToTuple},
       {"broken_line_fit_3", kTuneFitTuples}, {"broken_line_fit_4", kTuneFitTuples}};
   cudaSetDevice(ctx->p.device);
