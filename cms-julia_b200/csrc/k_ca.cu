@@ -468,6 +468,17 @@ __device__ __forceinline__ void sort_regs(uint32_t* a, uint32_t n) {
     if (uint32_t(i) < n) a[i] = v[i];
 }
 
+// Sorts a list of at most kMax entries in place with a register network and returns true;
+// longer lists are left to k_sort_long (a list kernel keeps the few registers of its largest
+// network, which sets its occupancy).
+template <int kMax>
+__device__ __forceinline__ bool sort_short(uint32_t* a, uint32_t n) {
+  if (n < 2) return true;
+  if (n <= 4) { sort_regs<4>(a, n); return true; }
+  if (n <= 8) { sort_regs<8>(a, n); return true; }
+  return false;
+}
+
 // sort a short list in place (ascending; entries are ids below 0xffffffff): one load and
 // one store per entry through a register network up to 32 entries, insertion sort above
 __device__ __forceinline__ void sort_list(uint32_t* a, uint32_t n) {
@@ -485,6 +496,23 @@ __device__ __forceinline__ void sort_list(uint32_t* a, uint32_t n) {
 }
 
 // per-hit lists (kind 0: cells ending on the hit; 2: tuples through the hit, descending)
+// lists above the short-sort limit, sorted afterwards by k_sort_long (a list of n entries
+// needs n > 8, so the buffer of cap_long = entries / 9 entries cannot overflow)
+__device__ __forceinline__ void push_long_list(const Dev& d, uint32_t lo, uint32_t n) {
+  const uint32_t slot = atomicAdd(d.long_ctr, 1u);
+  if (slot < uint32_t(d.cap_long)) d.long_lists[slot] = make_uint2(lo, n);
+  else atomicOr(d.status, kWarnBuffer);
+}
+
+__global__ void __launch_bounds__(256) k_sort_long(Dev d, uint32_t* list) {
+  uint32_t nl = *d.long_ctr;
+  if (nl > uint32_t(d.cap_long)) nl = uint32_t(d.cap_long);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nl; i += gridDim.x * blockDim.x) {
+    const uint2 l = d.long_lists[i];
+    sort_list(list + l.x, l.y);
+  }
+}
+
 template <int kKind>
 __global__ void k_sort_hit_lists(Dev d) {
   const int e = blockIdx.y;
@@ -699,7 +727,7 @@ __global__ void k_sort_cell_lists(Dev d) {
     if (uint64_t(hi) > lcap) hi = uint32_t(lcap);
     if (hi > lo) {
       ++cols;
-      sort_list(list + lo, hi - lo);
+      if (!sort_short<8>(list + lo, hi - lo)) push_long_list(d, lo, hi - lo);
       if (hi - lo > uint32_t(kCellRows)) atomic_or_warn(&d.ev[e], kWarnLists);
     }
     // cells with two or more tracks, for the duplicate remover
@@ -982,6 +1010,14 @@ __global__ void k_multiplicity(Dev d) {
 
 }  // namespace
 
+// a list-sorting kernel followed by the sort of the lists it left long
+template <class F>
+void launch_sorted(const Dev& d, const Launch& L, uint32_t* list, F&& sort_kernel) {
+  cudaMemsetAsync(d.long_ctr, 0, sizeof(uint32_t), L.s);
+  sort_kernel(L.s);
+  k_sort_long<<<148 * 4, 256, 0, L.s>>>(d, list);
+}
+
 void launch_ca(const Dev& d, const Launch& L) {
   auto g = [&](int seg) { return dim3(L.bpe_of(seg), d.E); };
   const int eb = div_up(d.E + 1, 128);
@@ -1016,7 +1052,7 @@ void launch_ca(const Dev& d, const Launch& L) {
   L.mark("connect");
   excl_scan_shift_u32(d.cn_cur, d.cn_cnt, d.cap_cells, &d.ev[d.E].n_cells_raw, d.scan_tmp, L.s);
   k_connect_fill<<<148 * 8, 256, 0, L.s>>>(d);
-  k_sort_cell_lists<0><<<g(kTuneCellLists), 256, 0, L.s>>>(d);
+  launch_sorted(d, L, d.cn_list, [&](cudaStream_t s) { k_sort_cell_lists<0><<<g(kTuneCellLists), 256, 0, s>>>(d); });
   L.mark("neighbour_lists");
   k_fishbone<<<g(kTuneFishbone), 128, 0, L.s>>>(d);
   L.mark("fishbone");
@@ -1031,7 +1067,7 @@ void launch_ca(const Dev& d, const Launch& L) {
   excl_scan_shift_u32(d.ct_cur, d.ct_cnt, d.cap_cells, &d.ev[d.E].n_cells_raw, d.scan_tmp, L.s);
   k_cell_tracks_fill<<<g(kTuneCellTracks), 256, 0, L.s>>>(d);
   cudaMemsetAsync(d.dup_bits, 0, size_t(d.cap_cells / 32 + 2) * sizeof(uint32_t), L.s);
-  k_sort_cell_lists<1><<<g(kTuneCellTracks), 256, 0, L.s>>>(d);
+  launch_sorted(d, L, d.ct_list, [&](cudaStream_t s) { k_sort_cell_lists<1><<<g(kTuneCellTracks), 256, 0, s>>>(d); });
   L.mark("cell_tracks");
   k_early_dup<<<g(kTuneEarlyDup), 256, 0, L.s>>>(d);
   k_multiplicity<<<d.E, 256, 0, L.s>>>(d);

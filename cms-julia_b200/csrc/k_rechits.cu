@@ -238,7 +238,7 @@ __device__ __forceinline__ void module_sums(const Dev& d, int e, const HitModule
   __syncwarp();
 }
 
-__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_get_hits_warp(Dev d) {
+__global__ void __launch_bounds__(32 * kWarpsPerBlock, 4) k_get_hits_warp(Dev d) {
   __shared__ WarpHitSmem smem[kWarpsPerBlock];
   const int e = blockIdx.y;
   const unsigned lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;

@@ -111,7 +111,7 @@ struct Dev {
   int32_t E;
   int32_t n_fed_slots;
   // limits
-  int64_t cap_words, cap_hits, cap_cells, cap_tuples, cap_tuple_hits, cap_items, cap_pairs;
+  int64_t cap_words, cap_hits, cap_cells, cap_tuples, cap_tuple_hits, cap_items, cap_pairs, cap_long;
   uint32_t hits_per_event, doublets_per_event, tuples_per_event, fits_per_mult;
   int32_t include_errors, use_quality;
   int32_t apply_charge_cut;  // 1 in the chain; 0 only for the stand-alone clustering entry
@@ -167,6 +167,8 @@ struct Dev {
   uint32_t* cn_cnt;        // [cap_cells + 1]
   uint32_t* cn_cur;        // [cap_cells]
   uint32_t* cn_list;       // [cap_pairs] global cell indices
+  uint2* long_lists;       // [cap_long] (first entry, length) of the lists left to k_sort_long
+  uint32_t* long_ctr;      // [1]
   // tuples
   uint64_t* tstart_cnt;    // [cap_cells + 1] (tuples << 32 | hits) per start cell -> exclusive positions
   uint32_t* tuple_off;     // [cap_tuples + 1] global hit offsets (0-based, packed)
