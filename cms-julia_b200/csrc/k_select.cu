@@ -112,22 +112,76 @@ __device__ __forceinline__ void q_set_dup(uint32_t* w, uint32_t t) {  // any non
   atomicOr(&w[t >> 4], 1u << sh);
 }
 
+// The inputs of the ordered walk, gathered with a whole CTA per event: the cells with two
+// or more tracks in cell order (from the bitmap), and for each its track entries (at most
+// kCellRows) as (event-local tuple id, |tip| bits), laid end to end with offsets.
+__global__ void __launch_bounds__(256) k_dup_prep(Dev d) {
+  const int e = blockIdx.x;
+  EvInfo& E = d.ev[e];
+  __shared__ uint32_t sh[33];
+  if (E.n_cells == 0 || E.n_tuples > uint32_t(kDupMaxTuples)) {
+    if (threadIdx.x == 0) E.n_dup_cells = 0;
+    return;
+  }
+  const uint64_t tb = E.tuple_base;
+  const uint64_t c_lo = E.cell_base, c_hi = c_lo + E.n_cells;
+  uint32_t* list = d.dup_list + c_lo;
+  // cells, in order
+  uint32_t ndup = 0;
+  for (uint64_t w0 = c_lo >> 5; w0 <= (c_hi - 1) >> 5; w0 += blockDim.x) {
+    const uint64_t wi = w0 + threadIdx.x;
+    uint32_t bits = wi <= (c_hi - 1) >> 5 ? dup_word(d, wi, c_lo, c_hi) : 0u;
+    uint32_t tot;
+    uint32_t pos = ndup + block_excl_scan(__popc(bits), sh, &tot);
+    for (; bits; bits &= bits - 1) list[pos++] = uint32_t(32 * wi) + uint32_t(__ffs(bits) - 1);
+    ndup += tot;
+  }
+  __syncthreads();
+  // entries
+  uint32_t* eoff = d.dup_eoff + c_lo + e;
+  uint16_t* et = d.dup_et + E.tuple_hit_base;
+  uint32_t* ek = d.dup_ek + E.tuple_hit_base;
+  uint32_t base = 0;
+  for (uint32_t q0 = 0; q0 < ndup; q0 += blockDim.x) {
+    const uint32_t q = q0 + threadIdx.x;
+    uint32_t n = 0, l0 = 0;
+    if (q < ndup) {
+      const uint32_t c = list[q];
+      l0 = d.ct_cnt[c];
+      n = d.ct_cnt[c + 1] - l0;
+      if (n > uint32_t(kCellRows)) n = kCellRows;
+    }
+    uint32_t tot;
+    const uint32_t o = base + block_excl_scan(n, sh, &tot);
+    if (q < ndup) {
+      eoff[q] = o;
+      for (uint32_t j = 0; j < n; ++j) {
+        const uint32_t t = d.ct_list[l0 + j];
+        et[o + j] = uint16_t(t - tb);
+        ek[o + j] = __float_as_uint(fabsf(d.t_state[5 * size_t(t) + 1]));
+      }
+    }
+    base += tot;
+  }
+  if (threadIdx.x == 0) {
+    eoff[ndup] = base;
+    E.n_dup_cells = ndup;
+  }
+}
+
 __global__ void __launch_bounds__(32) k_fast_dup_smem(Dev d) {
   __shared__ uint32_t s_q[kDupMaxTuples / 16];
   __shared__ uint16_t s_t[kDupStage];
   __shared__ uint32_t s_tip[kDupStage];
   __shared__ uint32_t s_off[33];
-  __shared__ uint32_t s_l0[32];
   __shared__ uint32_t s_seen[kDupMaxTuples / 32];
-  __shared__ uint32_t s_clist[32 * 32];  // the cells of 32 bitmap words, in order
   const int e = blockIdx.x;
   const unsigned lane = threadIdx.x;
   const EvInfo& E = d.ev[e];
   const uint64_t tb = E.tuple_base;
   const uint32_t nt = E.n_tuples;
   if (nt > uint32_t(kDupMaxTuples)) return;  // k_fast_dup handles such events
-  if (E.n_cells == 0) return;
-  const uint64_t c_lo = E.cell_base, c_hi = c_lo + E.n_cells;
+  if (E.n_dup_cells == 0) return;
   const uint32_t nw = (nt + 15) / 16;
   for (uint32_t w = lane; w < nw; w += 32) {
     uint32_t v = 0;
@@ -139,41 +193,28 @@ __global__ void __launch_bounds__(32) k_fast_dup_smem(Dev d) {
   }
   for (uint32_t w = lane; w < uint32_t(kDupMaxTuples / 32); w += 32) s_seen[w] = 0;
   __syncwarp();
-  for (uint64_t w0 = c_lo >> 5; w0 <= (c_hi - 1) >> 5; w0 += 32) {
-   // the next 32 bitmap words' cells, in order
-   const uint64_t wi = w0 + lane;
-   uint32_t bits = wi <= (c_hi - 1) >> 5 ? dup_word(d, wi, c_lo, c_hi) : 0u;
-   const uint32_t nb = __popc(bits);
-   const uint32_t winc = warp_incl_scan(nb);
-   const uint32_t hi = __shfl_sync(0xffffffffu, winc, 31);
-   for (uint32_t pos = winc - nb; bits; bits &= bits - 1) s_clist[pos++] = uint32_t(32 * wi) + uint32_t(__ffs(bits) - 1);
-   __syncwarp();
-   for (uint32_t q0 = 0; q0 < hi;) {
-    // stage up to 32 cells: list start and length (capped at kCellRows)
+  // the event's cells with two or more tracks, in order, and their track entries as
+  // k_dup_prep laid them out: offsets (ndup + 1) and (tuple, |tip| bits) per entry
+  const uint32_t ndup = E.n_dup_cells;
+  const uint32_t* eoff = d.dup_eoff + E.cell_base + e;
+  const uint16_t* et = d.dup_et + E.tuple_hit_base;
+  const uint32_t* ek = d.dup_ek + E.tuple_hit_base;
+  for (uint32_t q0 = 0; q0 < ndup;) {
+    // stage up to 32 cells whose entries fit kDupStage
     const uint32_t q = q0 + lane;
-    uint32_t n = 0, l0 = 0;
-    if (q < hi) {
-      const uint32_t c = s_clist[q];
-      l0 = d.ct_cnt[c];
-      n = d.ct_cnt[c + 1] - l0;
-      if (n > uint32_t(kCellRows)) n = kCellRows;
-    }
-    const uint32_t inc = warp_incl_scan(n);
-    const bool fits = q < hi && inc <= uint32_t(kDupStage);
+    const uint32_t o_lo = eoff[q0];
+    const uint32_t o = q <= ndup ? eoff[q] : 0xffffffffu;
+    const uint32_t o_next = __shfl_down_sync(0xffffffffu, o, 1);
+    const uint32_t o_last = q0 + 32 <= ndup ? eoff[q0 + 32] : 0xffffffffu;
+    const uint32_t end = lane == 31 ? o_last : o_next;  // end of cell q's entries
+    const bool fits = q < ndup && end - o_lo <= uint32_t(kDupStage);
     const uint32_t ncell = __popc(__ballot_sync(0xffffffffu, fits));
-    if (fits) { s_off[lane] = inc - n; s_l0[lane] = l0; }
-    const uint32_t total = __shfl_sync(0xffffffffu, inc, ncell - 1);
+    const uint32_t total = __shfl_sync(0xffffffffu, end, ncell - 1) - o_lo;
+    if (lane < ncell) s_off[lane] = o - o_lo;
     if (lane == 0) s_off[ncell] = total;
-    __syncwarp();
     for (uint32_t x = lane; x < total; x += 32) {
-      uint32_t a = 0, b = ncell;  // last cell whose offset <= x
-      while (b - a > 1) {
-        const uint32_t m = (a + b) >> 1;
-        if (s_off[m] <= x) a = m; else b = m;
-      }
-      const uint32_t t = d.ct_list[s_l0[a] + (x - s_off[a])];
-      s_t[x] = uint16_t(t - tb);
-      s_tip[x] = __float_as_uint(fabsf(d.t_state[5 * size_t(t) + 1]));
+      s_t[x] = et[o_lo + x];
+      s_tip[x] = ek[o_lo + x];
     }
     __syncwarp();
     // cells that share no track are independent: when no track is listed twice in the
@@ -233,8 +274,6 @@ __global__ void __launch_bounds__(32) k_fast_dup_smem(Dev d) {
       __syncwarp();
     }
     q0 += ncell;
-  }
-   __syncwarp();
   }
   __syncwarp();
   for (uint32_t t = lane; t < nt; t += 32) d.quality[tb + t] = uint8_t(q_get(s_q, t));
@@ -676,7 +715,10 @@ void launch_classify(const Dev& d, const Launch& L) {
   k_classify<<<g(kTuneClassify), 256, 0, L.s>>>(d);
   L.mark("classify");
   if (d.tuples_per_event > uint32_t(kDupMaxTuples)) k_fast_dup<<<div_up(d.E, 4), 128, 0, L.s>>>(d);
-  else k_fast_dup_smem<<<d.E, 32, 0, L.s>>>(d);
+  else {
+    k_dup_prep<<<d.E, 256, 0, L.s>>>(d);
+    k_fast_dup_smem<<<d.E, 32, 0, L.s>>>(d);
+  }
   L.mark("fast_duplicate_remover");
   cudaMemsetAsync(d.htt_cur, 0, size_t(d.cap_hits) * sizeof(uint32_t), L.s);
   k_hit_to_tuple<0><<<g(kTuneHitToTuple), 256, 0, L.s>>>(d);

@@ -242,7 +242,8 @@ int alloc_batch(PxlCtx* ctx) {
   A(t_chi2, d.cap_tuples); A(t_fitted, d.cap_tuples);
   A(fit_list, d.cap_tuples);
   A(htt_cnt, d.cap_hits + 1); A(htt_cur, d.cap_hits); A(htt_list, d.cap_tuple_hits);
-  A(dup_bits, d.cap_cells / 32 + 2);
+  A(dup_bits, d.cap_cells / 32 + 2); A(dup_list, d.cap_cells); A(dup_eoff, d.cap_cells + E + 1);
+  A(dup_et, d.cap_tuple_hits); A(dup_ek, d.cap_tuple_hits);
   A(vws_zt, d.cap_tuples); A(vws_ezt2, d.cap_tuples); A(vws_ptt2, d.cap_tuples); A(vws_iv, d.cap_tuples);
   A(vws_itrk, d.cap_tuples); A(vws_izt, d.cap_tuples); A(vws_bins, d.cap_tuples);
   A(idv, d.cap_tuples); A(zv, E * 1024); A(wv, E * 1024); A(vchi2, E * 1024); A(ptv2, E * 1024);

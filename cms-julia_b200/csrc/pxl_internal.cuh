@@ -189,6 +189,10 @@ struct Dev {
   uint32_t* htt_list;      // [cap_tuple_hits]
   // cells with >= 2 tracks, compacted per event
   uint32_t* dup_bits;      // [cap_cells / 32 + 2] cells with two or more tracks, one bit each
+  uint32_t* dup_list;      // [cap_cells] those cells in order, at the event's cell base
+  uint32_t* dup_eoff;      // [cap_cells + E + 1] their entry offsets, at cell base + event index
+  uint16_t* dup_et;        // [cap_tuple_hits] entries: event-local tuple id, at the tuple-hit base
+  uint32_t* dup_ek;        // [cap_tuple_hits] entries: |tip| bits
   // vertices, per event
   int16_t* idv;            // [cap_tuples] per tuple (global tuple index), -1 when unused
   float* vws_zt; float* vws_ezt2; float* vws_ptt2;  // [cap_tuples] vertex-finder workspace per selected track
