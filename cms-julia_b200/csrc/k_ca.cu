@@ -179,7 +179,7 @@ __device__ __forceinline__ uint32_t head_candidate(const ItemHead& h, uint32_t k
 // All doublets of one item written from event-local position cell_pos on (the fill of
 // groups whose count pass could not keep their outer hits).
 __device__ __forceinline__ void write_item_doublets(const Dev& d, const ItemHead& h, const HitRec* __restrict__ hrec,
-                                                    uint64_t cell_pos, uint64_t cell_lo, uint32_t cap) {
+                                                    uint64_t cell_pos, uint64_t cell_lo, uint32_t cap, uint32_t hb) {
   if (!h.ok) return;
   uint32_t cnt = 0;
   for (uint32_t k = 0; k < h.n; ++k) {
@@ -190,6 +190,7 @@ __device__ __forceinline__ void write_item_doublets(const Dev& d, const ItemHead
       const uint64_t g = cell_lo + local;
       d.cell_inner[g] = h.hit;
       d.cell_outer[g] = hr.id;
+      atomicAdd(&d.ohc_cur[hb + hr.id], 1u);
       d.cell_pair[g] = h.pid;
       d.cell_id[g] = int32_t(local + 1);
       d.cell_used[g] = 0;
@@ -363,7 +364,7 @@ __global__ void __launch_bounds__(256) k_doublets_fill(Dev d, const uint32_t* __
     const uint32_t cnt = valid ? d.item_cnt[ib + j + 1] - d.item_cnt[ib + j] : 0u;
     const uint32_t pool = valid ? d.item_pool[ib + j] : kNoPool;
     if (__any_sync(0xffffffffu, cnt > 0 && pool == kNoPool)) {
-      if (cnt > 0) write_item_doublets(d, item_head(j, s_cum, s_hls, hv, poff), hrec, pos, cell_lo, keep);
+      if (cnt > 0) write_item_doublets(d, item_head(j, s_cum, s_hls, hv, poff), hrec, pos, cell_lo, keep, hb);
       continue;
     }
     const uint32_t inc = warp_incl_scan(cnt);
@@ -389,7 +390,9 @@ __global__ void __launch_bounds__(256) k_doublets_fill(Dev d, const uint32_t* __
       }
       const uint64_t g = cell_lo + local;
       d.cell_inner[g] = s_hit[w][a];
-      d.cell_outer[g] = d.dbl_pool[pool0 + x];
+      const uint32_t oh = d.dbl_pool[pool0 + x];
+      d.cell_outer[g] = oh;
+      atomicAdd(&d.ohc_cur[hb + oh], 1u);  // cells ending on each hit
       d.cell_pair[g] = s_pid[w][a];
       d.cell_id[g] = int32_t(local + 1);
       d.cell_used[g] = 0;
@@ -421,20 +424,15 @@ __global__ void k_cell_regions(Dev d) {
 }
 
 // ---------------------------------------------------------------- outer-hit lists
-template <int kPass>
-__global__ void k_ohc(Dev d) {
+// cells ending on each hit: slots from the shifted scan of the counts the doublet fill took
+__global__ void k_ohc_fill(Dev d) {
   const int e = blockIdx.y;
   const EvInfo& E = d.ev[e];
   const uint64_t cb = E.cell_base;
   const uint32_t hb = E.hit_base;
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < E.n_cells; k += gridDim.x * blockDim.x) {
     const uint64_t c = cb + k;
-    const uint32_t h = hb + d.cell_outer[c];
-    if (kPass == 0) {
-      atomicAdd(&d.ohc_cur[h], 1u);
-    } else {
-      d.ohc_list[atomicAdd(&d.ohc_cnt[h + 1], 1u)] = uint32_t(c);
-    }
+    d.ohc_list[atomicAdd(&d.ohc_cnt[hb + d.cell_outer[c] + 1], 1u)] = uint32_t(c);
   }
 }
 
@@ -579,8 +577,7 @@ __global__ void __launch_bounds__(256) k_ohc_records(Dev d) {
   for (uint32_t p = lo + blockIdx.x * blockDim.x + threadIdx.x; p < hi; p += gridDim.x * blockDim.x) {
     const uint32_t oih = d.cell_inner[d.ohc_list[p]];
     const float4 h = d.hit_xyzr[hb + oih];
-    d.ohc_rec[p] = make_float4(h.w, h.z, h.x, h.y);
-    d.ohc_inner[p] = d.detind[hb + oih] < 96 ? 1 : 0;
+    d.ohc_rec[p] = make_float2(d.detind[hb + oih] < 96 ? -h.w : h.w, h.z);
   }
 }
 
@@ -617,10 +614,10 @@ __global__ void __launch_bounds__(256) k_connect_test(Dev d) {
       const uint32_t v = s_queue[w][q0 + lane];
       const uint32_t a = v >> 8, j = v & 0xffu;
       const uint32_t p = s_lo[w][a] + j;
-      const float4 rec = d.ohc_rec[p];
       const float4 xy = s_xy[w][a];
-      const float region = d.ohc_inner[p] ? kDcaInner : kDcaOuter;
-      const CircleEq eq(rec.z, rec.w, xy.x, xy.y, xy.z, xy.w);
+      const float region = signbit(d.ohc_rec[p].x) ? kDcaInner : kDcaOuter;
+      const float4 h1 = hxyzr[d.cell_inner[d.ohc_list[p]]];  // the candidate's inner hit
+      const CircleEq eq(h1.x, h1.y, xy.x, xy.y, xy.z, xy.w);
       if (eq.c > kHardCurv) cut = false;
       else cut = fabsf(eq.dca0()) < __fmul_rn(region, fabsf(eq.c));
       if (cut) {
@@ -678,9 +675,9 @@ __global__ void __launch_bounds__(256) k_connect_test(Dev d) {
       if (x < total) {
         while (a < 31 && s_ex[w][a + 1] <= x) ++a;
         j = x - s_ex[w][a];
-        const float4 rec = d.ohc_rec[s_lo[w][a] + j];  // the candidate's inner hit: r, z, x, y
+        const float2 rec = d.ohc_rec[s_lo[w][a] + j];  // the candidate's inner hit: r (sign: inner barrel), z
         const float4 rz = s_rz[w][a];
-        al = are_aligned(rec.x, rec.y, rz.x, rz.y, rz.z, rz.w, ptmin_f(), s_barrel[w][a] ? kThetaBarrel : kThetaForward);
+        al = are_aligned(fabsf(rec.x), rec.y, rz.x, rz.y, rz.z, rz.w, ptmin_f(), s_barrel[w][a] ? kThetaBarrel : kThetaForward);
       }
       const uint32_t bal = __ballot_sync(0xffffffffu, al);
       if (al) s_queue[w][qn + __popc(bal & lt)] = uint16_t((a << 8) | j);
@@ -1039,10 +1036,9 @@ void launch_ca(const Dev& d, const Launch& L) {
   L.mark("doublets_scan");
   k_doublets_fill<<<g(kTuneDoublets), 256, 0, L.s>>>(d, pair_cum);
   L.mark("doublets_fill");
-  // cells ending on each hit
-  k_ohc<0><<<g(kTuneHitLists), 256, 0, L.s>>>(d);
+  // cells ending on each hit (counted by the doublet fill)
   excl_scan_shift_u32(d.ohc_cur, d.ohc_cnt, d.cap_hits, &d.ev[d.E].n_hits, d.scan_tmp, L.s);
-  k_ohc<1><<<g(kTuneHitLists), 256, 0, L.s>>>(d);
+  k_ohc_fill<<<g(kTuneHitLists), 256, 0, L.s>>>(d);
   k_sort_hit_lists<0><<<g(kTuneHitLists), 256, 0, L.s>>>(d);
   k_ohc_records<<<g(kTuneHitLists), 256, 0, L.s>>>(d);
   L.mark("outer_hit_lists");

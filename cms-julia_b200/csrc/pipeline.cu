@@ -230,7 +230,7 @@ int alloc_batch(PxlCtx* ctx) {
   A(tuple_det, d.cap_tuple_hits);
   A(cell_inner, d.cap_cells); A(cell_outer, d.cap_cells); A(cell_pair, d.cap_cells); A(cell_id, d.cap_cells);
   A(cell_used, d.cap_cells);
-  A(ohc_cnt, d.cap_hits + 1); A(ohc_cur, d.cap_hits); A(ohc_list, d.cap_cells); A(ohc_rec, d.cap_cells); A(ohc_inner, d.cap_cells);
+  A(ohc_cnt, d.cap_hits + 1); A(ohc_cur, d.cap_hits); A(ohc_list, d.cap_cells); A(ohc_rec, d.cap_cells);
   A(cn_pairs, d.cap_pairs); A(cn_pair_ctr, 1); d.cap_long = std::max({d.cap_cells, d.cap_pairs, d.cap_tuple_hits}) / 9 + 1;
   A(long_lists, d.cap_long); A(long_ctr, 1); A(cn_cnt, d.cap_cells + 1); A(cn_cur, d.cap_cells); A(cn_list, d.cap_pairs);
   A(tstart_cnt, d.cap_cells + 1);

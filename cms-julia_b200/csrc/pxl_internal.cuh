@@ -159,8 +159,8 @@ struct Dev {
   uint32_t* ohc_cnt;       // [cap_hits + 1] counts -> offsets
   uint32_t* ohc_cur;       // [cap_hits] fill cursors
   uint32_t* ohc_list;      // [cap_cells] global cell indices
-  float4* ohc_rec;         // [cap_cells] per list entry: inner r, z, x, y of the cell (connect's candidate)
-  uint8_t* ohc_inner;      // [cap_cells] per list entry: the cell's inner hit is on an inner-barrel module
+  float2* ohc_rec;         // [cap_cells] per list entry: r, z of the cell's inner hit (connect's candidate);
+                           // r negative when that hit is on an inner-barrel module
   // cell neighbours (CSR over cells)
   uint2* cn_pairs;         // [cap_pairs] passing (candidate, cell) pairs of the connection test
   uint32_t* cn_pair_ctr;   // [1] entries of cn_pairs
