@@ -123,7 +123,7 @@ def segment_bytes(name: str, c: dict) -> float | None:
     table = {
         "unpack_calib": 4 * D + 22 * D,            # words in; xx,yy,adc,moduleInd,clus,pdigi,rawId out
         "module_starts": 4 * D,                    # moduleInd read by the count and fill passes
-        "find_clus_small": 14 * D,                 # moduleInd,x,y,adc in; clus (and moduleInd) out (modules <= 32 digis;
+        "find_clus_tiny": 14 * D,                  # moduleInd,x,y,adc in; clus (and moduleInd) out (modules <= 16 digis;
                                                    # the larger ones only read their range bounds here)
         "get_hits_warp": 14 * D + 40 * H,          # digis in; per-cluster sums out
         "cpe": 40 * H + 60 * H,                    # sums in; hit SoA and packed coordinates out

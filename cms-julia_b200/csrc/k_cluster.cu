@@ -294,21 +294,137 @@ __device__ __forceinline__ void cluster_module_warp(const Dev& d, int e, uint32_
 
 // every module position of the batch: modules of <= 32 digis here (one digi per lane),
 // larger ones to the mid-size list (<= kWarpPix) or the CTA list
-__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_find_clus_small(Dev d) {
-  __shared__ WarpSmem<1> smem[kWarpsPerBlock];
+// ------------------------------------------------------------ thread per module
+constexpr int kThreadPix = 16;  // modules of at most this many digis: one thread each
+
+// One module of at most kThreadPix digis clustered by one thread, all in registers:
+// neighbour sets as bitmasks, each component grown from the smallest digi not yet taken,
+// so components come out in the order of their smallest index, which numbers them as the
+// reference's min-propagation does; the charge cut keeps that order.
+__device__ __forceinline__ void cluster_module_thread(const Dev& d, int e, uint32_t m, const ModRange& r) {
+  const int n = r.n;
+  uint32_t xy[kThreadPix];  // x (16 bits) | column bin << 16
+  int32_t q[kThreadPix];
+  uint32_t valid = 0, warn = 0;
+  int crun = n;
+#pragma unroll
+  for (int k = 0; k < kThreadPix; ++k) {
+    xy[k] = 0;
+    q[k] = 0;
+    if (k < n) {
+      const uint64_t g = r.g0 + k;
+      const int16_t id = d.mid[g];
+      q[k] = d.adc[g];
+      const uint32_t yb = uint32_t(uint16_t(d.yy[g])) & 511u;
+      // a column past the 418-bin histogram makes the reference's histogram assert fail;
+      // such a digi is flagged and kept out of the clustering
+      const bool in_hist = yb + 2u <= uint32_t(kNBins);
+      if (id != int16_t(kInvId) && !in_hist) warn |= kWarnPixels;
+      if (id != int16_t(kInvId) && in_hist) {
+        xy[k] = uint32_t(uint16_t(d.xx[g])) | (yb << 16);
+        valid |= 1u << k;
+      } else if (k < crun) {
+        crun = k;
+      }
+    }
+  }
+  // 8-connected neighbours (|dx| <= 1, |dcolumn| <= 1)
+  uint32_t adj[kThreadPix];
+#pragma unroll
+  for (int a = 0; a < kThreadPix; ++a) adj[a] = 0;
+#pragma unroll
+  for (int a = 0; a < kThreadPix; ++a) {
+#pragma unroll
+    for (int b = a + 1; b < kThreadPix; ++b) {
+      const int dx = int(int16_t(xy[a] & 0xffffu)) - int(int16_t(xy[b] & 0xffffu));
+      const int dy = int(xy[a] >> 16) - int(xy[b] >> 16);
+      if (((valid >> a) & (valid >> b) & 1u) && dx <= 1 && dx >= -1 && dy <= 1 && dy >= -1) {
+        adj[a] |= 1u << b;
+        adj[b] |= 1u << a;
+      }
+    }
+  }
+  // components in the order of their smallest digi: cluster number (4 bits per digi, 0-based),
+  // charge (digis before the first invalid one) and the number after the charge cut
+  const int32_t cut = r.this_id < 96 ? 2000 : 4000;
+  uint64_t cl_of = 0, new_of = 0;  // 4 bits per digi
+  uint32_t removed = 0;            // digis of clusters the cut removes
+  uint32_t nclus = 0, kept = 0;
+  for (uint32_t rest = valid; rest;) {
+    uint32_t comp = rest & (0u - rest);  // the smallest digi left
+    for (;;) {
+      uint32_t grown = comp;
+#pragma unroll
+      for (int k = 0; k < kThreadPix; ++k)
+        if ((comp >> k) & 1u) grown |= adj[k];
+      if (grown == comp) break;
+      comp = grown;
+    }
+    rest &= ~comp;
+    int32_t charge = 0;
+#pragma unroll
+    for (int k = 0; k < kThreadPix; ++k)
+      if (((comp >> k) & 1u) && k < crun) charge += q[k];
+    const bool ok = charge > cut;
+#pragma unroll
+    for (int k = 0; k < kThreadPix; ++k)
+      if ((comp >> k) & 1u) {
+        cl_of |= uint64_t(nclus) << (4 * k);
+        new_of |= uint64_t(ok ? kept : 0u) << (4 * k);
+      }
+    if (!ok) removed |= comp;
+    ++nclus;
+    if (ok) ++kept;
+  }
+  const bool changed = d.apply_charge_cut && nclus > 0 && kept != nclus;
+#pragma unroll
+  for (int k = 0; k < kThreadPix; ++k) {
+    if (k >= n) continue;
+    const uint64_t g = r.g0 + k;
+    if (!((valid >> k) & 1u)) { d.clus[g] = -9999; continue; }
+    if (changed) {
+      if ((removed >> k) & 1u) {
+        d.clus[g] = int32_t(kInvId);
+        d.mid[g] = int16_t(kInvId);
+      } else {
+        d.clus[g] = int32_t((new_of >> (4 * k)) & 15u) + 1;
+      }
+    } else {
+      d.clus[g] = int32_t((cl_of >> (4 * k)) & 15u) + 1;
+    }
+  }
+  write_module_record(d, e, m, r.this_id, changed ? kept : nclus, warn);
+}
+
+// every module position of the batch: modules of <= kThreadPix digis here, one thread
+// each; larger ones to the work lists of the warp (<= 32, <= kWarpPix digis) and CTA paths
+__global__ void __launch_bounds__(128, 6) k_find_clus_tiny(Dev d) {
   const int e = blockIdx.y;
-  const unsigned lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
   const EvInfo& E = d.ev[e];
   const uint32_t nmod = E.n_modules;
   if (E.word_base + uint64_t(E.n_words) > uint64_t(d.cap_words)) return;
-  for (uint32_t m = blockIdx.x * kWarpsPerBlock + wib; m < nmod; m += gridDim.x * kWarpsPerBlock) {
+  for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < nmod; m += gridDim.x * blockDim.x) {
     ModRange r;
     if (!module_range(d, e, m, r)) continue;
-    if (r.n > 32) {
-      if (lane == 0) push_module(d, r.n > kWarpPix ? kListClusBig : kListClusMid, e, m);
+    if (r.n > kThreadPix) {
+      push_module(d, r.n > kWarpPix ? kListClusBig : (r.n > 32 ? kListClusMid : kListClusSmall), e, m);
       continue;
     }
-    cluster_module_warp<1>(d, e, m, r, smem[wib], nullptr);
+    cluster_module_thread(d, e, m, r);
+  }
+}
+
+// modules of kThreadPix+1 .. 32 digis (work list), one warp each, one digi per lane
+__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_find_clus_small(Dev d) {
+  __shared__ WarpSmem<1> smem[kWarpsPerBlock];
+  const unsigned wib = threadIdx.x >> 5;
+  const uint32_t nl = list_size(d, kListClusSmall);
+  for (uint32_t i = blockIdx.x * kWarpsPerBlock + wib; i < nl; i += gridDim.x * kWarpsPerBlock) {
+    const uint32_t v = list_entry(d, kListClusSmall, i);
+    const int e = int(v >> 11);
+    ModRange r;
+    if (!module_range(d, e, v & 2047u, r)) continue;
+    cluster_module_warp<1>(d, e, v & 2047u, r, smem[wib], nullptr);
   }
 }
 
@@ -522,8 +638,10 @@ __global__ void k_hits_module_start(Dev d) {
 void launch_cluster(const Dev& d, const Launch& L) {
   cudaMemsetAsync(d.big_list, 0, kListHeader * sizeof(uint32_t), L.s);
   // enough warps that a few events fill the GPU, at least 8 modules per warp otherwise
-  const int bx = std::max(4, std::min(250, (148 * 8 * 4) / std::max(1, int(d.E))));
-  k_find_clus_small<<<dim3(bx, d.E), 32 * kWarpsPerBlock, 0, L.s>>>(d);
+  // one thread per module position (at most 2000 per event)
+  k_find_clus_tiny<<<dim3(div_up(kMaxNumModules, 128), d.E), 128, 0, L.s>>>(d);
+  L.mark("find_clus_tiny");
+  k_find_clus_small<<<148 * 64, 32 * kWarpsPerBlock, 0, L.s>>>(d);
   L.mark("find_clus_small");
   k_find_clus_mid<<<148 * 16, 32 * kMidWarps, 0, L.s>>>(d);
   L.mark("find_clus_mid");

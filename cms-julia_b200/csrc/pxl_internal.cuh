@@ -260,7 +260,7 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* sh, ui
 __device__ __forceinline__ void atomic_or_warn(EvInfo* ev, uint32_t bits) { atomicOr(&ev->warnings, bits); }
 
 // module work lists between the per-module kernels
-enum : int { kListClusBig = 0, kListHitsBig = 1, kListClusMid = 2, kNumLists = 3, kListHeader = 4 };
+enum : int { kListClusBig = 0, kListHitsBig = 1, kListClusMid = 2, kListClusSmall = 3, kNumLists = 4, kListHeader = 4 };
 
 __device__ __forceinline__ void push_module(const Dev& d, int list, int e, uint32_t m) {
   const uint32_t slot = atomicAdd(&d.big_list[list], 1u);

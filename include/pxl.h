@@ -261,7 +261,7 @@ int32_t pxl_clusterize_digis(PxlCtx* ctx, const uint16_t* id, const int16_t* x, 
  * or a path that must not block on cudaMalloc/cudaFree). It allocates nothing: inputs
  * (id, x, y, adc; n digis) and outputs (module_start[2001], clus_in_module[2000],
  * module_id[2000], clus[n], id_out[n]) are the caller's device buffers, and the scratch
- * is a fixed file-scope device array of the library (about 80 KB on every GPU that loads
+ * is a fixed file-scope device array of the library (about 90 KB on every GPU that loads
  * it, held until exit). At most 1,048,576 digis per call; larger n returns
  * PXL_ERR_CAPACITY. The first call on a device looks the array up on that device, so make
  * it before any stream capture. Calls share the array: calls that overlap on the GPU race.
