@@ -961,22 +961,26 @@ __global__ void k_cell_tracks_fill(Dev d) {
 __global__ void k_early_dup(Dev d) {
   const int e = blockIdx.y;
   const EvInfo& E = d.ev[e];
-  const uint64_t cb = E.cell_base;
-  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < E.n_cells; k += gridDim.x * blockDim.x) {
-    const uint64_t c = cb + k;
-    const uint32_t lo = d.ct_cnt[c];
-    uint32_t n = d.ct_cnt[c + 1] - lo;
-    if (n > uint32_t(kCellRows)) n = kCellRows;
-    if (n < 2) continue;
-    uint32_t maxn = 0;
-    for (uint32_t j = 0; j < n; ++j) {
-      const uint32_t t = d.ct_list[lo + j];
-      const uint32_t s = d.tuple_off[t + 1] - d.tuple_off[t];
-      maxn = s > maxn ? s : maxn;
-    }
-    for (uint32_t j = 0; j < n; ++j) {
-      const uint32_t t = d.ct_list[lo + j];
-      if (d.tuple_off[t + 1] - d.tuple_off[t] != maxn) d.quality[t] = 1;
+  if (E.n_cells == 0) return;
+  // only cells with two or more tracks act: walk their bitmap
+  const uint64_t c_lo = E.cell_base, c_hi = c_lo + E.n_cells;
+  for (uint64_t wi = (c_lo >> 5) + blockIdx.x * blockDim.x + threadIdx.x; wi <= (c_hi - 1) >> 5;
+       wi += uint64_t(gridDim.x) * blockDim.x) {
+    for (uint32_t bits = dup_word(d, wi, c_lo, c_hi); bits; bits &= bits - 1) {
+      const uint64_t c = 32 * wi + uint32_t(__ffs(bits) - 1);
+      const uint32_t lo = d.ct_cnt[c];
+      uint32_t n = d.ct_cnt[c + 1] - lo;
+      if (n > uint32_t(kCellRows)) n = kCellRows;
+      uint32_t maxn = 0;
+      for (uint32_t j = 0; j < n; ++j) {
+        const uint32_t t = d.ct_list[lo + j];
+        const uint32_t s = d.tuple_off[t + 1] - d.tuple_off[t];
+        maxn = s > maxn ? s : maxn;
+      }
+      for (uint32_t j = 0; j < n; ++j) {
+        const uint32_t t = d.ct_list[lo + j];
+        if (d.tuple_off[t + 1] - d.tuple_off[t] != maxn) d.quality[t] = 1;
+      }
     }
   }
 }

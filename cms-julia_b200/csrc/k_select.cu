@@ -44,14 +44,6 @@ __global__ void k_classify(Dev d) {
   }
 }
 
-// Bits of the event's cells [c_lo, c_hi) in word wi of the two-or-more-tracks bitmap
-// (set by k_sort_cell_lists<1>): walking the words in order walks those cells in order.
-__device__ __forceinline__ uint32_t dup_word(const Dev& d, uint64_t wi, uint64_t c_lo, uint64_t c_hi) {
-  uint32_t m = d.dup_bits[wi];
-  if (wi == (c_lo >> 5)) m &= ~0u << (c_lo & 31);
-  if (wi == ((c_hi - 1) >> 5) && (c_hi & 31)) m &= (1u << (c_hi & 31)) - 1u;
-  return m;
-}
 
 // kernel_fast_duplicate_remover: one warp per event, cells in order
 __global__ void k_fast_dup(Dev d) {

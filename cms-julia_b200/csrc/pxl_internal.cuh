@@ -290,6 +290,15 @@ __device__ __forceinline__ uint32_t module_end1(const int16_t* mid, uint64_t eb,
   return n_el;
 }
 
+// Bits of the event's cells [c_lo, c_hi) in word wi of the two-or-more-tracks bitmap
+// (set by k_sort_cell_lists<1> in k_ca.cu): walking the words in order walks those cells in order.
+__device__ __forceinline__ uint32_t dup_word(const Dev& d, uint64_t wi, uint64_t c_lo, uint64_t c_hi) {
+  uint32_t m = d.dup_bits[wi];
+  if (wi == (c_lo >> 5)) m &= ~0u << (c_lo & 31);
+  if (wi == ((c_hi - 1) >> 5) && (c_hi & 31)) m &= (1u << (c_hi & 31)) - 1u;
+  return m;
+}
+
 inline int div_up(int64_t a, int64_t b) { return int((a + b - 1) / b); }
 
 // ---------------------------------------------------------------- launchers (per stage file)
