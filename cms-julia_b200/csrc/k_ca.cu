@@ -4,13 +4,15 @@
 // gpu_ca_cell.jl:130-270, gpu_fishbone.jl:4-63, circle_eq.jl:18-93 and
 // ca_hit_ntuplet_generator_kernels_impl.jl:45-211.
 //
-// Output order equals the serial reference's: doublets are counted per inner
-// hit, scanned and written in the reference's loop order (so doublet ids are
-// the reference's ids); per-key lists (cells ending on a hit, neighbours of a
-// cell, tracks of a cell) are filled with atomics and then sorted, which
-// restores the reference's push order (ascending producer index); tuples are
-// counted per start cell, scanned, and written in the reference's depth-first
-// order, so tuple ids match too.
+// Output order equals the serial reference's: doublets are counted per work item
+// (inner hit x layer pair), scanned and written in the reference's loop order (so
+// doublet ids are the reference's ids); per-key lists (cells ending on a hit,
+// neighbours of a cell, tracks of a cell) are filled with atomics at the offsets of a
+// shifted scan and then sorted, which restores the reference's push order (ascending
+// producer index); tuples are counted per start cell, scanned, and written in the
+// reference's depth-first order, so tuple ids match too. The doublet and connection
+// tests lay their (item, candidate) and (cell, candidate) pairs end to end over the
+// lanes of a warp, so that lanes stay busy whatever the candidate counts.
 #include <cstddef>
 
 #include "pxl_internal.cuh"

@@ -5,9 +5,9 @@
 // hist_to_container.jl:217-270 (fill_many_from_vector).
 // One warp per module (a CTA for the few modules above 256 digis or 128
 // clusters, handed over through a device work list); per-cluster reductions
-// use shared-memory integer atomics (order independent), then one thread per
-// cluster evaluates the CPE in FP32 with round-to-nearest and no contraction,
-// as the reference does.
+// use shared-memory integer atomics (order independent) and are recorded per hit;
+// k_cpe then evaluates the CPE one hit per thread in FP32 with round-to-nearest and
+// no contraction, as the reference does.
 #include <algorithm>
 
 #include "pxl_internal.cuh"

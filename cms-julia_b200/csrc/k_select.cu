@@ -5,10 +5,10 @@
 // and plugin-PixelVertexFinding/gpu_vertex_finder.jl:51-436.
 //
 // kernel_fast_duplicate_remover is order dependent (a cell sees the marks of the
-// cells before it), so it runs cell by cell within an event, one warp per event,
-// the lanes sharing the work of each cell. The triplet cleaner only ever writes
-// "dup" and tests "!= bad", so its hits run in parallel. Vertex sums keep the
-// reference's track order (one thread per vertex walks the tracks in order).
+// cells before it), so it walks the cells in order within an event, one warp per
+// event, taking 32 cells at once when they share no track. The triplet cleaner only
+// ever writes "dup" and tests "!= bad", so its hits run in parallel. Vertex sums keep
+// the reference's track order (one thread per vertex walks its tracks in order).
 #include <cstddef>
 
 #include "pxl_internal.cuh"
