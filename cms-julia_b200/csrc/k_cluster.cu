@@ -10,14 +10,16 @@
 // (so the final root is again the smallest index), and roots are numbered by a
 // scan in index order: the same cluster ids as the reference.
 //
-// Two paths share that scheme:
-//  * one warp per module for modules of at most kWarpPix digis (nearly all of
-//    them: a PU50 module holds about 22). The warp keeps its digis in
-//    registers, finds neighbour pairs by broadcasting every digi of the module
-//    through shuffles, and scans with ballots; it never waits on a CTA barrier.
-//  * one CTA per module for larger modules, which the warp path appends to a
-//    device work list: pixels are binned by column in shared memory and only
-//    the same and the next column are searched.
+// Three paths share the numbering:
+//  * one thread per module for modules of at most 16 digis (about three quarters
+//    of them at PU50): neighbour sets as bitmasks, components grown from the
+//    smallest digi left, all in registers;
+//  * one warp per module for modules of at most kWarpPix digis, from work lists.
+//    The warp keeps its digis in registers, finds neighbour pairs by broadcasting
+//    every digi (up to 32 digis) or through a column histogram (up to kWarpPix),
+//    joins them with the union-find, and scans with ballots;
+//  * one CTA per module for larger modules: pixels are binned by column in shared
+//    memory and only the same and the next column are searched.
 #include <algorithm>
 
 #include "pxl_internal.cuh"
