@@ -42,3 +42,9 @@ def test_context_rejects_hit_cap_beyond_16_bit_ids():
     assert L.pxl_ctx_create(ctypes.byref(_native.PxlConditions()), ctypes.byref(p), ctypes.byref(h)) == -1
     p.hits_per_event = 0
     assert L.pxl_ctx_create(ctypes.byref(_native.PxlConditions()), ctypes.byref(p), ctypes.byref(h)) == -1
+
+
+def test_input_slot_entry_points_reject_bad_arguments():
+    L = _native.lib()
+    assert L.pxl_slot_stage(None, 0, 1, 1, 1, None) == -1
+    assert L.pxl_slot_launch(None, 0, None) == -1
