@@ -145,8 +145,8 @@ def segment_bytes(name: str, c: dict) -> float | None:
 # dram__bytes_read.sum + dram__bytes_write.sum per unit of work, from ncu captures of the
 # 300-event case (profiles/), scaled to a launch by the units it processes
 TRAFFIC_PER_UNIT = {
-    "doublets_count": ("hits", (77.28e6 + 114.70e6) / 3_215_253),
-    "connect": ("cells", (619.12e6 + 77.25e6) / 25_257_080),
+    "doublets_count": ("hits", (77.30e6 + 113.63e6) / 3_215_253),
+    "connect": ("cells", (483.81e6 + 75.11e6) / 25_257_080),
 }
 
 FIT_B = 0.0114256972711507  # 1/(pT R) at 3.8 T, GeV^-1 cm^-1
