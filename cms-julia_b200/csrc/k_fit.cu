@@ -49,7 +49,11 @@ __device__ void fit_tuple(const Dev& d, uint64_t g, uint32_t hb, const uint32_t*
 // per multiplicity (the bin is read in decreasing id, so the largest ids win).
 // One block per event: the fitted tuples go to the event's region of fit_list
 // (3-hit from the front, 4-hit from the back) so that every warp of the fit
-// kernel runs one hit count; the others get zero outputs here.
+// kernel runs one hit count; the others get zero outputs here. The first pass
+// sets t_fitted for every tuple (the fit kernel writes it again) and takes list
+// slots one atomic per warp; the second zeroes the state and covariance words of
+// the tuples left out, walking the packed arrays word by word so that the stores
+// coalesce.
 __global__ void __launch_bounds__(256) k_fit_list(Dev d) {
   const int e = blockIdx.x;
   EvInfo& E = d.ev[e];
@@ -58,37 +62,59 @@ __global__ void __launch_bounds__(256) k_fit_list(Dev d) {
   __syncthreads();
   const uint64_t tb = E.tuple_base;
   const uint32_t nt = E.n_tuples;
-  for (uint32_t t = threadIdx.x; t < nt; t += blockDim.x) {
+  const unsigned lane = threadIdx.x & 31u;
+  const uint32_t nt_pad = (nt + 31u) & ~31u;
+  for (uint32_t t = threadIdx.x; t < nt_pad; t += blockDim.x) {
     const uint64_t g = tb + t;
-    const uint32_t n = d.tuple_off[g + 1] - d.tuple_off[g];
-    bool fit = n >= 3 && n <= 5 && d.quality[g] != 1;
-    if (fit) {
-      const uint32_t cnt = E.tm_off[n] - E.tm_off[n - 1];
-      if (cnt > d.fits_per_mult) {
-        uint32_t larger = 0;
-        for (uint32_t u = t + 1; u < nt; ++u) {
-          const uint64_t gu = tb + u;
-          if (d.tuple_off[gu + 1] - d.tuple_off[gu] == n && d.quality[gu] != 1) ++larger;
+    bool fit = false;
+    uint32_t n = 0;
+    if (t < nt) {
+      n = d.tuple_off[g + 1] - d.tuple_off[g];
+      fit = n >= 3 && n <= 5 && d.quality[g] != 1;
+      if (fit) {
+        const uint32_t cnt = E.tm_off[n] - E.tm_off[n - 1];
+        if (cnt > d.fits_per_mult) {
+          uint32_t larger = 0;
+          for (uint32_t u = t + 1; u < nt; ++u) {
+            const uint64_t gu = tb + u;
+            if (d.tuple_off[gu + 1] - d.tuple_off[gu] == n && d.quality[gu] != 1) ++larger;
+          }
+          fit = larger < d.fits_per_mult;
         }
-        fit = larger < d.fits_per_mult;
       }
     }
+    const unsigned m3 = __ballot_sync(0xffffffffu, fit && n == 3);
+    const unsigned m4 = __ballot_sync(0xffffffffu, fit && n != 3);
+    uint32_t b3 = 0, b4 = 0;
+    if (lane == 0) {
+      if (m3) b3 = atomicAdd(&s_n3, uint32_t(__popc(m3)));
+      if (m4) b4 = atomicAdd(&s_n4, uint32_t(__popc(m4)));
+    }
+    b3 = __shfl_sync(0xffffffffu, b3, 0);
+    b4 = __shfl_sync(0xffffffffu, b4, 0);
+    const unsigned below = (1u << lane) - 1u;
+    if (t >= nt) continue;
+    d.t_fitted[g] = fit ? 1 : 0;
     if (fit) {
-      if (n == 3) d.fit_list[tb + atomicAdd(&s_n3, 1u)] = t;
-      else d.fit_list[tb + nt - 1 - atomicAdd(&s_n4, 1u)] = t;
+      if (n == 3) d.fit_list[tb + b3 + __popc(m3 & below)] = t;
+      else d.fit_list[tb + nt - 1 - (b4 + __popc(m4 & below))] = t;
       continue;
     }
-    for (int k = 0; k < 5; ++k) d.t_state[5 * g + k] = 0.f;
-    for (int k = 0; k < 15; ++k) d.t_cov[15 * g + k] = 0.f;
-    d.t_pt[g] = 0.f; d.t_eta[g] = 0.f; d.t_chi2[g] = 0.f; d.t_fitted[g] = 0;
+    d.t_pt[g] = 0.f; d.t_eta[g] = 0.f; d.t_chi2[g] = 0.f;
   }
   __syncthreads();
+  for (uint32_t w = threadIdx.x; w < 5 * nt; w += blockDim.x)
+    if (!d.t_fitted[tb + w / 5]) d.t_state[5 * tb + w] = 0.f;
+  for (uint32_t w = threadIdx.x; w < 15 * nt; w += blockDim.x)
+    if (!d.t_fitted[tb + w / 15]) d.t_cov[15 * tb + w] = 0.f;
   if (threadIdx.x == 0) { E.n_fit3 = s_n3; E.n_fit4 = s_n4; }
 }
 
-// one hit count per launch, so that each instantiation keeps only its own registers
+// one hit count per launch, so that each instantiation keeps only its own registers.
+// Capped at 128 registers (four blocks per SM): the 4-hit fit spills a few hundred
+// bytes to L1 but runs twice the warps, which hides more of its FP64 latency.
 template <int N>
-__global__ void __launch_bounds__(128) k_fit_tuples(Dev d) {
+__global__ void __launch_bounds__(128, 4) k_fit_tuples(Dev d) {
   const int e = blockIdx.y;
   const EvInfo& E = d.ev[e];
   const uint64_t tb = E.tuple_base;
@@ -164,7 +190,7 @@ __global__ void k_fit_plan_fill(const int32_t* __restrict__ offs, int32_t n, Fit
 namespace {
 
 template <int N, class T>
-__global__ void __launch_bounds__(128) k_fit_bucket(const double* __restrict__ hits, const float* __restrict__ ge,
+__global__ void __launch_bounds__(128, 4) k_fit_bucket(const double* __restrict__ hits, const float* __restrict__ ge,
                                                     const int32_t* __restrict__ offs, const FitPlan* __restrict__ plan,
                                                     double B, float* state, float* cov, float* chi2, float* pt,
                                                     float* eta, int32_t* status) {
