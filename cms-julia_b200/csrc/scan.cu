@@ -1,6 +1,10 @@
 // Device-wide exclusive scans over packed arrays (three passes: tile sums,
 // scan of the tile sums in one block, tile scan with the tile's offset).
 // In place: data[0..n) becomes the exclusive prefix and data[n] the total.
+// The tile passes move every element with coalesced global loads and stores and
+// hand each thread its kItems consecutive elements through shared memory padded
+// by one word per 128 bytes, which keeps both access patterns free of bank
+// conflicts for 32- and 64-bit elements.
 #include "pxl_internal.cuh"
 
 namespace pxl {
@@ -10,6 +14,32 @@ namespace {
 constexpr int kTpb = 256;
 constexpr int kItems = 8;
 constexpr int kTile = kTpb * kItems;
+constexpr int kSumItems = 4;  // tile sums per thread in the single-block pass
+
+// shared-memory slot of tile element j: one padding element per 128 bytes
+template <class T>
+__device__ __forceinline__ int pad_idx(int j) {
+  return j + j / (128 / int(sizeof(T)));
+}
+template <class T>
+__host__ __device__ constexpr int tile_smem_elems() {
+  return kTile + kTile / (128 / int(sizeof(T)));
+}
+
+// Loads tile elements base .. base + kTile (zero at and past n) with coalesced
+// reads and returns this thread's kItems consecutive ones in v.
+template <class T>
+__device__ __forceinline__ void load_tile(const T* __restrict__ src, int64_t base, int64_t n, T* s,
+                                          T (&v)[kItems]) {
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    const int j = k * kTpb + int(threadIdx.x);
+    s[pad_idx<T>(j)] = base + j < n ? src[base + j] : T(0);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) v[k] = s[pad_idx<T>(int(threadIdx.x) * kItems + k)];
+}
 
 // n_dev (optional) holds the live element count; tiles past it do nothing, so a
 // launch sized for the buffer capacity costs only the live part.
@@ -49,7 +79,8 @@ __device__ T warp_incl(T v) {
   return v;
 }
 
-// exclusive scan of the tile sums in one block of 1024 threads
+// exclusive scan of the tile sums in one block of 1024 threads, kSumItems
+// consecutive sums per thread
 template <class T>
 __global__ void k_scan_sums(T* __restrict__ sums, int64_t ncap, const uint32_t* n_dev) {
   int64_t n = live_n(ncap, n_dev);
@@ -59,10 +90,16 @@ __global__ void k_scan_sums(T* __restrict__ sums, int64_t ncap, const uint32_t* 
   if (threadIdx.x == 0) carry = 0;
   __syncthreads();
   const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
-  for (int64_t b = 0; b < nt; b += blockDim.x) {
-    int64_t i = b + threadIdx.x;
-    T v = i < nt ? sums[i] : T(0);
-    T inc = warp_incl(v);
+  for (int64_t b = 0; b < nt; b += int64_t(blockDim.x) * kSumItems) {
+    const int64_t i0 = b + int64_t(threadIdx.x) * kSumItems;
+    T v[kSumItems];
+    T tsum = 0;
+#pragma unroll
+    for (int k = 0; k < kSumItems; ++k) {
+      v[k] = i0 + k < nt ? sums[i0 + k] : T(0);
+      tsum += v[k];
+    }
+    T inc = warp_incl(tsum);
     if (lane == 31) sh[wid] = inc;
     __syncthreads();
     if (wid == 0) {
@@ -72,8 +109,12 @@ __global__ void k_scan_sums(T* __restrict__ sums, int64_t ncap, const uint32_t* 
       if (lane == 31) sh[32] = si;
     }
     __syncthreads();
-    T r = carry + sh[wid] + inc - v;
-    if (i < nt) sums[i] = r;
+    T r = carry + sh[wid] + inc - tsum;
+#pragma unroll
+    for (int k = 0; k < kSumItems; ++k) {
+      if (i0 + k < nt) sums[i0 + k] = r;
+      r += v[k];
+    }
     __syncthreads();
     if (threadIdx.x == 0) carry += sh[32];
     __syncthreads();
@@ -91,15 +132,13 @@ __global__ void k_tile_scan(T* __restrict__ data, int64_t ncap, const uint32_t* 
     return;
   }
   if (int64_t(blockIdx.x) >= nt) return;
+  __shared__ T s_tile[tile_smem_elems<T>()];
   // each thread owns kItems consecutive elements
   T v[kItems];
+  load_tile<T>(data, base, n, s_tile, v);
   T tsum = 0;
-  int64_t i0 = base + int64_t(threadIdx.x) * kItems;
-  for (int k = 0; k < kItems; ++k) {
-    int64_t i = i0 + k;
-    v[k] = i < n ? data[i] : T(0);
-    tsum += v[k];
-  }
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) tsum += v[k];
   __shared__ T sh[33];
   const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
   T inc = warp_incl(tsum);
@@ -111,11 +150,18 @@ __global__ void k_tile_scan(T* __restrict__ data, int64_t ncap, const uint32_t* 
     if (lane < kTpb / 32) sh[lane] = si - s;
   }
   __syncthreads();
+  // a thread rewrites only the slots it read, so no barrier is needed before
   T run = sums[blockIdx.x] + sh[wid] + inc - tsum;
+#pragma unroll
   for (int k = 0; k < kItems; ++k) {
-    int64_t i = i0 + k;
-    if (i < n) data[i] = run;
+    s_tile[pad_idx<T>(int(threadIdx.x) * kItems + k)] = run;
     run += v[k];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    const int j = k * kTpb + int(threadIdx.x);
+    if (base + j < n) data[base + j] = s_tile[pad_idx<T>(j)];
   }
   if (int64_t(blockIdx.x) == nt - 1 && threadIdx.x == 0) data[n] = sums[nt];
 }
@@ -132,14 +178,12 @@ __global__ void k_tile_scan_shift(const T* __restrict__ in, T* __restrict__ out,
   int64_t base = int64_t(blockIdx.x) * kTile;
   if (blockIdx.x == 0 && threadIdx.x == 0) out[0] = 0;
   if (int64_t(blockIdx.x) >= nt) return;
+  __shared__ T s_tile[tile_smem_elems<T>()];
   T v[kItems];
+  load_tile<T>(in, base, n, s_tile, v);
   T tsum = 0;
-  int64_t i0 = base + int64_t(threadIdx.x) * kItems;
-  for (int k = 0; k < kItems; ++k) {
-    int64_t i = i0 + k;
-    v[k] = i < n ? in[i] : T(0);
-    tsum += v[k];
-  }
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) tsum += v[k];
   __shared__ T sh[33];
   const unsigned lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
   T inc = warp_incl(tsum);
@@ -152,10 +196,16 @@ __global__ void k_tile_scan_shift(const T* __restrict__ in, T* __restrict__ out,
   }
   __syncthreads();
   T run = sums[blockIdx.x] + sh[wid] + inc - tsum;
+#pragma unroll
   for (int k = 0; k < kItems; ++k) {
-    int64_t i = i0 + k;
-    if (i < n) out[i + 1] = run;
+    s_tile[pad_idx<T>(int(threadIdx.x) * kItems + k)] = run;
     run += v[k];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    const int j = k * kTpb + int(threadIdx.x);
+    if (base + j < n) out[base + j + 1] = s_tile[pad_idx<T>(j)];
   }
 }
 
