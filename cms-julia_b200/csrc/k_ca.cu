@@ -879,24 +879,62 @@ __device__ __forceinline__ bool is_start(const Dev& d, uint64_t c) {
   return p < 8 || p > 12;  // minHitsPerNtuplet = 3 (…_impl.jl:125)
 }
 
+// Thread per walk: a warp looks at 32 cells at a time and queues in shared memory the
+// ones that start a walk (count pass: start cells with at least one neighbour; fill pass:
+// start cells the count pass gave tuples), then walks 32 queued cells at once, so that
+// every lane of a walking warp has a tree to walk. The count pass writes zero for the
+// cells it does not walk; the fill takes each walk's positions from the scanned counts,
+// so the order of the walks does not matter.
+constexpr int kNtupWarps = 4;
+constexpr int kNtupQueue = 64;
+
 template <bool kFill>
-__global__ void __launch_bounds__(128) k_ntuplets(Dev d) {
+__global__ void __launch_bounds__(32 * kNtupWarps) k_ntuplets(Dev d) {
   const int e = blockIdx.y;
   const EvInfo& E = d.ev[e];
   const uint64_t cb = E.cell_base;
-  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < E.n_cells; k += gridDim.x * blockDim.x) {
-    const uint64_t c = cb + k;
+  __shared__ uint32_t s_queue[kNtupWarps][kNtupQueue];
+  const unsigned lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  const uint32_t ncell = E.n_cells;
+  const uint64_t tuple_lo = kFill && ncell > 0 ? d.tstart_cnt[cb] >> 32 : 0;
+  // walks the queued cells q0 .. qn (at most 32; lanes past qn idle)
+  auto walk_queued = [&](uint32_t q0, uint32_t qn) {
+    if (q0 + lane >= qn) return;
+    const uint64_t c = cb + s_queue[w][q0 + lane];
     if (!kFill) {
       uint32_t nt = 0, nh = 0;
-      if (is_start(d, c)) walk<false>(d, cb, c, nullptr, nullptr, &nt, &nh, 0, 0, e);
+      walk<false>(d, cb, c, nullptr, nullptr, &nt, &nh, 0, 0, e);
       d.tstart_cnt[c] = (uint64_t(nt) << 32) | nh;
     } else {
-      if (!is_start(d, c)) continue;
       const uint64_t v = d.tstart_cnt[c];
       uint64_t tp = v >> 32, hp = v & 0xFFFFFFFFull;
-      walk<true>(d, cb, c, &tp, &hp, nullptr, nullptr, d.tstart_cnt[cb] >> 32, E.n_tuples, e);
+      walk<true>(d, cb, c, &tp, &hp, nullptr, nullptr, tuple_lo, E.n_tuples, e);
+    }
+  };
+  uint32_t qn = 0;
+  for (uint32_t k0 = blockIdx.x * blockDim.x + 32u * w; k0 < ncell; k0 += gridDim.x * blockDim.x) {
+    const uint32_t k = k0 + lane;
+    bool walker = false;
+    if (k < ncell) {
+      const uint64_t c = cb + k;
+      if (is_start(d, c)) {
+        if (!kFill) walker = d.cn_cnt[c + 1] > d.cn_cnt[c];
+        else walker = (d.tstart_cnt[c + 1] >> 32) != (d.tstart_cnt[c] >> 32);
+      }
+      if (!kFill && !walker) d.tstart_cnt[c] = 0;
+    }
+    const unsigned b = __ballot_sync(0xffffffffu, walker);
+    if (walker) s_queue[w][qn + __popc(b & lt)] = k;
+    qn += __popc(b);
+    __syncwarp();
+    if (qn >= 32) {
+      qn -= 32;
+      walk_queued(qn, qn + 32);
+      __syncwarp();
     }
   }
+  walk_queued(0, qn);
 }
 
 __global__ void k_tuple_bases(Dev d) {
@@ -1059,11 +1097,11 @@ void launch_ca(const Dev& d, const Launch& L) {
   k_fishbone<<<g(kTuneFishbone), 128, 0, L.s>>>(d);
   L.mark("fishbone");
   // ntuplets
-  k_ntuplets<false><<<g(kTuneNtuplets), 128, 0, L.s>>>(d);
+  k_ntuplets<false><<<g(kTuneNtuplets), 32 * kNtupWarps, 0, L.s>>>(d);
   L.mark("ntuplets_count");
   excl_scan_u64(d.tstart_cnt, d.cap_cells, &d.ev[d.E].n_cells_raw, d.scan_tmp64, L.s);
   k_tuple_bases<<<eb, 128, 0, L.s>>>(d);
-  k_ntuplets<true><<<g(kTuneNtuplets), 128, 0, L.s>>>(d);
+  k_ntuplets<true><<<g(kTuneNtuplets), 32 * kNtupWarps, 0, L.s>>>(d);
   k_tuple_ends<<<div_up(d.E, 128), 128, 0, L.s>>>(d);
   L.mark("ntuplets_fill");
   excl_scan_shift_u32(d.ct_cur, d.ct_cnt, d.cap_cells, &d.ev[d.E].n_cells_raw, d.scan_tmp, L.s);

@@ -82,7 +82,7 @@ __device__ T warp_incl(T v) {
 // exclusive scan of the tile sums in one block of 1024 threads, kSumItems
 // consecutive sums per thread
 template <class T>
-__global__ void k_scan_sums(T* __restrict__ sums, int64_t ncap, const uint32_t* n_dev) {
+__global__ void __launch_bounds__(1024) k_scan_sums(T* __restrict__ sums, int64_t ncap, const uint32_t* n_dev) {
   int64_t n = live_n(ncap, n_dev);
   int64_t nt = (n + kTile - 1) / kTile;
   __shared__ T sh[33];
