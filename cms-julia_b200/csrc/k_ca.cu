@@ -763,20 +763,32 @@ __global__ void __launch_bounds__(128) k_fishbone(Dev d) {
     float dx[kMaxCellsPerHit], dy[kMaxCellsPerHit], dz[kMaxCellsPerHit], nrm[kMaxCellsPerHit];
     uint16_t idet[kMaxCellsPerHit];
     uint8_t idx[kMaxCellsPerHit];
+    // gathered kFishBatch entries at a time: each stage's loads are independent of one
+    // another, so a batch waits for four load latencies rather than four per entry
+    constexpr int kFishBatch = 8;
     uint32_t curr = 0;
-    for (uint32_t j = 0; j < n; ++j) {
-      const uint32_t c = L[j];
-      if (d.cell_used[c] == 0) continue;
-      const uint32_t ih = d.cell_inner[c];
-      const float4 hi = d.hit_xyzr[hb + ih];
-      idx[curr] = uint8_t(j);
-      idet[curr] = uint16_t(det[ih]);
-      dx[curr] = __fsub_rn(hi.x, xo);
-      dy[curr] = __fsub_rn(hi.y, yo);
-      dz[curr] = __fsub_rn(hi.z, zo);
-      nrm[curr] = __fadd_rn(__fadd_rn(__fmul_rn(dx[curr], dx[curr]), __fmul_rn(dy[curr], dy[curr])),
-                            __fmul_rn(dz[curr], dz[curr]));
-      ++curr;
+    for (uint32_t j0 = 0; j0 < n; j0 += kFishBatch) {
+      uint32_t cb8[kFishBatch], ih8[kFishBatch];
+      bool used[kFishBatch];
+#pragma unroll
+      for (int i = 0; i < kFishBatch; ++i) cb8[i] = j0 + i < n ? L[j0 + i] : 0u;
+#pragma unroll
+      for (int i = 0; i < kFishBatch; ++i) used[i] = j0 + i < n && d.cell_used[cb8[i]] != 0;
+#pragma unroll
+      for (int i = 0; i < kFishBatch; ++i) ih8[i] = used[i] ? d.cell_inner[cb8[i]] : 0u;
+#pragma unroll
+      for (int i = 0; i < kFishBatch; ++i) {
+        if (!used[i]) continue;
+        const float4 hi = d.hit_xyzr[hb + ih8[i]];
+        idx[curr] = uint8_t(j0 + i);
+        idet[curr] = uint16_t(det[ih8[i]]);
+        dx[curr] = __fsub_rn(hi.x, xo);
+        dy[curr] = __fsub_rn(hi.y, yo);
+        dz[curr] = __fsub_rn(hi.z, zo);
+        nrm[curr] = __fadd_rn(__fadd_rn(__fmul_rn(dx[curr], dx[curr]), __fmul_rn(dy[curr], dy[curr])),
+                              __fmul_rn(dz[curr], dz[curr]));
+        ++curr;
+      }
     }
     if (curr < 2) continue;
     for (uint32_t ic = 0; ic + 1 < curr; ++ic) {
