@@ -12,7 +12,8 @@
 // producer index); tuples are counted per start cell, scanned, and written in the
 // reference's depth-first order, so tuple ids match too. The doublet and connection
 // tests lay their (item, candidate) and (cell, candidate) pairs end to end over the
-// lanes of a warp, so that lanes stay busy whatever the candidate counts.
+// lanes of a warp, so that lanes stay busy whatever the candidate counts; the tuple
+// walks run from per-warp queues of the start cells that walk, one tree per lane.
 #include <cstddef>
 
 #include "pxl_internal.cuh"
