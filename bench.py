@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--fit-tracks", type=int, default=1 << 20)
     ap.add_argument("--fit-oracle-sample", type=int, default=4000)
     ap.add_argument("--no-fits", action="store_true")
+    ap.add_argument("--fits-only", action="store_true", help="only the stand-alone fit and adjoint measurements")
     ap.add_argument("--uneven-events", type=int, default=4096)
     ap.add_argument("--uneven-steps", type=int, default=3)
     ap.add_argument("--no-uneven", action="store_true")
@@ -395,7 +396,8 @@ def run_reference(args, rank: int, world: int) -> None:
     from oracle import oracle
     from pixeltrack import gen
     conds = gen.conditions()
-    n = max(8, min(args.cpu_sample, args.events))
+    # the same events as our arm's step (rank 0's batch)
+    n = args.events
     blob, offs = gen.events(n, gen.MODE_PU, pu=args.pu, seed=args.seed)
     orc = oracle.Oracle(conds)
     threads = os.cpu_count() or 1
@@ -435,6 +437,12 @@ def main():
     if pdist.init("nccl"):
         import torch.distributed as dist
     from pixeltrack import PixelChain, batch_params, default_params, gen
+    if args.fits_only:
+        fits = bench_fits(args, local, rank, world)
+        adjoint = bench_adjoint(args, local, rank, world)
+        if rank == 0:
+            print(json.dumps({"fits": fits, "adjoint": adjoint}), flush=True)
+        return
     conds = gen.conditions()
     E = args.events
     blob, offs = gen.events(E, gen.MODE_PU, pu=args.pu, seed=pdist.rank_seed(args.seed, rank))

@@ -16,6 +16,10 @@
 // All calls share it and it keeps the last call's contents: the scratch that
 // must start at zero is cleared by each call, and calls that overlap on the GPU
 // (different streams, or host threads without ordering) race on it.
+//
+// Capacity warnings of the chain (more than 2000 module runs, more than 4000 pixels or
+// 1024 clusters in a module) stay in the shared scratch and are not returned: a
+// module_start[0] of 2000 means that the module list overflowed.
 #include <cstdio>
 #include <mutex>
 
@@ -99,6 +103,13 @@ extern "C" int32_t pxl_clusterize_digis_noalloc(const uint16_t* id, const int16_
     s = g_addr[dev];
   }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // the scratch address is the current device's: a stream of another device would run the
+  // kernels there with this device's address
+  if (st) {
+    int sdev = -1;
+    if (cudaStreamGetDevice(st, &sdev) != cudaSuccess) return PXL_ERR_CUDA;
+    if (sdev != dev) return PXL_ERR_ARG;
+  }
   const int32_t nchunks = int32_t((uint32_t(n) + kChunk - 1) / kChunk);
   if (n > 0 && cudaMemcpyAsync(id_out, id, size_t(n) * sizeof(uint16_t), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
     return PXL_ERR_CUDA;

@@ -265,7 +265,9 @@ int32_t pxl_clusterize_digis(PxlCtx* ctx, const uint16_t* id, const int16_t* x, 
  * it, held until exit). At most 1,048,576 digis per call; larger n returns
  * PXL_ERR_CAPACITY. The first call on a device looks the array up on that device, so make
  * it before any stream capture. Calls share the array: calls that overlap on the GPU race.
- * Enqueued on `stream` (a cudaStream_t or NULL); the caller synchronises.
+ * Enqueued on `stream` (a cudaStream_t of the current device, or NULL; a stream of another
+ * device returns PXL_ERR_ARG); the caller synchronises. Capacity warnings are not returned
+ * (the status is 0 or an error): module_start[0] == 2000 means the module list overflowed.
  * No counterpart in the reference: it adds an allocation-free form of the clustering. */
 int32_t pxl_clusterize_digis_noalloc(const uint16_t* id, const int16_t* x, const int16_t* y, const int32_t* adc,
                                      int32_t n, int32_t apply_charge_cut, uint32_t* module_start,

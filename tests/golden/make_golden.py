@@ -14,7 +14,7 @@ brokenline_fixtures.json
     (line 81), read from that file, plus the CPU oracle's FP64 fit of each. The reference
     test prints and asserts nothing, so the fit values are oracle-generated goldens.
 
-Usage: python tests/golden/make_golden.py [--reference /root/reference]
+Usage: python tests/golden/make_golden.py --reference <root of a CMS-Julia checkout>
 """
 from __future__ import annotations
 
@@ -123,7 +123,7 @@ def parse_brokenline(ref: Path):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="root of a CMS-Julia checkout (holds src/julia-serial)")
     args = ap.parse_args()
     for kn in range(5):
         i, x, y, a, ncl = generate_clusters(kn)

@@ -42,13 +42,14 @@ def _noalloc(z, cut):
             "id": ido.cpu().numpy().view(np.uint16)}
 
 
-def test_noalloc_matches_context_entry_on_two_calls(conditions):
+@pytest.mark.parametrize("cut", [True, False])
+def test_noalloc_matches_context_entry_on_two_calls(conditions, cut):
     from pixeltrack import PixelChain, default_params
     with PixelChain(conditions, default_params()) as chain:
         for kn in (3, 0):  # two calls in a row: the second one reuses the first one's scratch
             z = np.load(GOLDEN / f"clustering_kn{kn}.npz")
-            ref = chain.clusterize_digis(z["id"], z["x"], z["y"], z["adc"], charge_cut=True)
-            got = _noalloc(z, True)
+            ref = chain.clusterize_digis(z["id"], z["x"], z["y"], z["adc"], charge_cut=cut)
+            got = _noalloc(z, cut)
             nm = int(ref["module_start"][0])
             assert int(got["module_start"][0]) == nm
             assert np.array_equal(got["module_start"][:nm + 1], ref["module_start"][:nm + 1])
@@ -56,6 +57,23 @@ def test_noalloc_matches_context_entry_on_two_calls(conditions):
             assert np.array_equal(got["clus_in_module"], ref["clus_in_module"])
             assert np.array_equal(got["clus"], ref["clus"])
             assert np.array_equal(got["id"], ref["id"])
+
+
+def test_noalloc_empty_input():
+    """n = 0 with null digi pointers: one empty chunk, no module."""
+    import torch
+
+    from pixeltrack import _native
+    dev = torch.device("cuda:0")
+    ms = torch.full((2001,), 7, dtype=torch.int32, device=dev)
+    cim = torch.zeros(2000, dtype=torch.int32, device=dev)
+    mid = torch.zeros(2000, dtype=torch.int32, device=dev)
+    s = torch.cuda.current_stream(dev)
+    rc = _native.lib().pxl_clusterize_digis_noalloc(None, None, None, None, 0, 1, ms.data_ptr(), cim.data_ptr(),
+                                                    mid.data_ptr(), None, None, s.cuda_stream)
+    assert rc == 0
+    s.synchronize()
+    assert int(ms[0]) == 0
 
 
 def test_noalloc_rejects_oversize():
