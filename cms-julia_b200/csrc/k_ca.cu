@@ -128,7 +128,7 @@ __device__ __forceinline__ ItemHead item_head(uint32_t j, const uint32_t* cum, c
 // comparison with them equals the reference's Float64 one.
 __device__ __forceinline__ bool doublet_pass_a(int pid, float me_z, float me_r, int16_t me_p, int16_t cut,
                                                const HitRec& hr) {
-  if (hr.det > 2000) return false;
+  if (hr.det() > 2000) return false;
   const float dr = __fsub_rn(hr.r, me_r);
   if (dr > c_max_rf[pid] || dr < 0 ||
       fabsf(__fsub_rn(__fmul_rn(me_z, hr.r), __fmul_rn(me_r, hr.z))) > __fmul_rn(12.f, dr))
@@ -192,8 +192,8 @@ __device__ __forceinline__ void write_item_doublets(const Dev& d, const ItemHead
     if (local < cap) {
       const uint64_t g = cell_lo + local;
       d.cell_inner[g] = h.hit;
-      d.cell_outer[g] = hr.id;
-      atomicAdd(&d.ohc_cur[hb + hr.id], 1u);
+      d.cell_outer[g] = hr.id();
+      atomicAdd(&d.ohc_cur[hb + hr.id()], 1u);
       d.cell_pair[g] = h.pid;
       d.cell_id[g] = int32_t(local + 1);
       d.cell_used[g] = 0;
@@ -205,7 +205,7 @@ __device__ __forceinline__ void write_item_doublets(const Dev& d, const ItemHead
 }
 
 constexpr uint32_t kNoPool = 0xffffffffu;
-constexpr int kGroupCells = 1024;  // outer hits one 32-item group stages in shared memory
+constexpr int kGroupCells = 768;  // outer hits one 32-item group stages in shared memory
 
 // Count pass over groups of 32 consecutive items (one warp). The candidates of the group's
 // items are laid end to end and take the first cuts 32 at a time on all lanes; the survivors
@@ -226,8 +226,8 @@ __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* _
   __shared__ uint4 s_rng[8][32];   // per compacted item: lo0, n0, lo1, first candidate
   __shared__ uint4 s_geo[8][32];   // per compacted item: z, r (float bits), iphi | cut << 16, pid | ysize << 16
   __shared__ uint32_t s_beg[8][32], s_end[8][32], s_over[8][32];
-  __shared__ uint32_t s_q[8][kDblQueue];  // owner << 16 | candidate
-  __shared__ uint16_t s_out[8][kGroupCells];
+  __shared__ uint32_t s_q[8][kDblQueue];  // owner << kHitIdBits | candidate
+  __shared__ uint32_t s_out[8][kGroupCells];
   __shared__ uint8_t s_own[8][kGroupCells];
   if (threadIdx.x < kNPairs) s_cum[threadIdx.x] = pair_cum[size_t(e) * kNPairs + threadIdx.x];
   if (threadIdx.x < 11) s_hls[threadIdx.x] = d.hits_layer_start[size_t(e) * 11 + threadIdx.x];
@@ -265,17 +265,17 @@ __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* _
       uint32_t o = 0, oi = 0;
       if (lane < mm) {
         const uint32_t v = s_q[w][(qhead + lane) % kDblQueue];
-        o = v >> 16;
+        o = v >> kHitIdBits;
         const uint4 g = s_geo[w][o];
-        const HitRec hr = hrec[v & 0xffffu];
+        const HitRec hr = hrec[v & (kMaxHitsPerEvent - 1u)];
         pass = doublet_pass_b(int(g.w & 0xffu), __uint_as_float(g.x), __uint_as_float(g.y), int16_t(g.z & 0xffffu),
                               int16_t(g.w >> 16), hr);
-        oi = hr.id;
+        oi = hr.id();
       }
       const uint32_t bal = __ballot_sync(0xffffffffu, pass);
       if (pass) {
         const uint32_t pos = nout + __popc(bal & lt);
-        if (pos < uint32_t(kGroupCells)) { s_out[w][pos] = uint16_t(oi); s_own[w][pos] = uint8_t(o); }
+        if (pos < uint32_t(kGroupCells)) { s_out[w][pos] = oi; s_own[w][pos] = uint8_t(o); }
         else atomicAdd(&s_over[w][o], 1u);
       }
       nout += __popc(bal);
@@ -298,7 +298,7 @@ __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* _
                               int16_t(g.z >> 16), hrec[p]);
       }
       const uint32_t bal = __ballot_sync(0xffffffffu, pass);
-      if (pass) s_q[w][(qtail + __popc(bal & lt)) % kDblQueue] = (o << 16) | p;
+      if (pass) s_q[w][(qtail + __popc(bal & lt)) % kDblQueue] = (o << kHitIdBits) | p;
       qtail += __popc(bal);
       __syncwarp();
       if (qtail - qhead >= 32) {
@@ -739,7 +739,7 @@ __global__ void k_sort_cell_lists(Dev d) {
     // columns of the fixed column store: one per cell with a non-empty list plus the reserved one
     uint32_t* counter = kKind == 0 ? &d.ev[e].n_cols_nb : &d.ev[e].n_cols_tr;
     const uint32_t before = atomicAdd(counter, s_cols);
-    if (before + s_cols + 1 > uint32_t(kMaxActiveColumns)) atomic_or_warn(&d.ev[e], kWarnColumns);
+    if (before + s_cols + 1 > d.columns_per_event) atomic_or_warn(&d.ev[e], kWarnColumns);
   }
 }
 
@@ -981,16 +981,26 @@ __global__ void k_tuple_bases(Dev d) {
   E.dup_cell_base = 0;
 }
 
-// tuple hit offsets end markers and the live sizes for the per-tuple loops
+// Tuple hit offsets end markers and the live sizes for the per-tuple loops. An event with more
+// tuples than it keeps ends as the reference's bulk_finalize_fill leaves an overflowing
+// container (hist_to_container.jl:150-161): the offset after the last kept tuple is set to that
+// tuple's start, so the last kept tuple shows no hits (its doublets still list it).
 __global__ void k_tuple_ends(Dev d) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= d.E) return;
   EvInfo& E = d.ev[e];
   E.n_tuple_hits = 0;
-  if (uint64_t(E.tuple_base) + E.n_tuples_raw <= uint64_t(d.cap_tuples)) {
-    d.tuple_off[uint64_t(E.tuple_base) + E.n_tuples_raw] = E.tuple_hit_base + E.n_tuple_hits_raw;
+  E.last_tuple_end = 0;
+  const uint64_t tb = E.tuple_base;
+  if (tb + E.n_tuples_raw <= uint64_t(d.cap_tuples)) {
+    d.tuple_off[tb + E.n_tuples_raw] = E.tuple_hit_base + E.n_tuple_hits_raw;
+    const uint32_t nt = E.n_tuples;
+    if (nt > 0 && nt < E.n_tuples_raw) {
+      E.last_tuple_end = d.tuple_off[tb + nt];
+      d.tuple_off[tb + nt] = d.tuple_off[tb + nt - 1];
+    }
     // hits of the tuples kept (the first n_tuples)
-    E.n_tuple_hits = d.tuple_off[uint64_t(E.tuple_base) + E.n_tuples] - E.tuple_hit_base;
+    E.n_tuple_hits = d.tuple_off[tb + nt] - E.tuple_hit_base;
   }
 }
 
@@ -1001,7 +1011,9 @@ __global__ void k_cell_tracks_fill(Dev d) {
   const uint64_t tb = E.tuple_base;
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < E.n_tuples; t += gridDim.x * blockDim.x) {
     const uint64_t g = tb + t;
-    const uint32_t h0 = d.tuple_off[g], h1 = d.tuple_off[g + 1];
+    // the walk registered every doublet of the last kept tuple, also when its visible size is 0
+    const uint32_t h0 = d.tuple_off[g];
+    const uint32_t h1 = (t + 1 == E.n_tuples && E.last_tuple_end) ? E.last_tuple_end : d.tuple_off[g + 1];
     const uint64_t pp = uint64_t(h0) - g;
     for (uint32_t k = 0; k + 1 < h1 - h0; ++k) {
       const uint32_t c = d.tuple_cell[pp + k];

@@ -385,17 +385,17 @@ __global__ void __launch_bounds__(1024) k_phi_binner(Dev d) {
     }
   }
   __syncthreads();
-  uint16_t* bins = d.phi_bins + hb;
+  uint32_t* bins = d.phi_bins + hb;
   for (uint32_t i = threadIdx.x; i < ntot; i += blockDim.x) {
     uint32_t w = atomicSub(&s_off[bin_of(i) - 1], 1u);
-    bins[w - 1] = uint16_t(i + 1);
+    bins[w - 1] = i + 1;
   }
   __syncthreads();
   // order each bin by decreasing hit id
   for (int b = threadIdx.x; b < kPhiTotBins - 1; b += blockDim.x) {
     const uint32_t lo = s_off[b], hi = s_off[b + 1];
     for (uint32_t p = lo + 1; p < hi; ++p) {
-      uint16_t v = bins[p];
+      const uint32_t v = bins[p];
       uint32_t q = p;
       while (q > lo && bins[q - 1] < v) { bins[q] = bins[q - 1]; --q; }
       bins[q] = v;
@@ -405,14 +405,14 @@ __global__ void __launch_bounds__(1024) k_phi_binner(Dev d) {
   __syncthreads();
   HitRec* rec = d.hit_rec + hb;
   for (uint32_t p = threadIdx.x; p < ntot; p += blockDim.x) {
-    const uint32_t i = uint32_t(bins[p]) - 1u;
+    const uint32_t i = bins[p] - 1u;
     HitRec r;
     r.z = d.zg[hb + i];
     r.r = d.rg[hb + i];
     r.iphi = d.iphi[hb + i];
     r.ysize = d.ysize[hb + i];
-    r.det = d.detind[hb + i];
-    r.id = uint16_t(i);
+    // hits sit on modules below 2000, so the detector index fits the record's 11 bits
+    r.det_id = (uint32_t(d.detind[hb + i]) << kHitIdBits) | i;
     rec[p] = r;
   }
 }

@@ -45,13 +45,14 @@ __global__ void k_classify(Dev d) {
 }
 
 
-// kernel_fast_duplicate_remover: one warp per event, cells in order
-__global__ void k_fast_dup(Dev d) {
+// kernel_fast_duplicate_remover: one warp per event, cells in order, qualities in global
+// memory; for the events above min_tuples tuples, which the shared-memory form cannot hold
+__global__ void k_fast_dup(Dev d, uint32_t min_tuples) {
   const int e = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
   if (e >= d.E) return;
   const unsigned lane = threadIdx.x & 31u;
   const EvInfo& E = d.ev[e];
-  if (E.n_cells == 0) return;
+  if (E.n_cells == 0 || E.n_tuples <= min_tuples) return;
   const uint64_t c_lo = E.cell_base, c_hi = c_lo + E.n_cells;
   for (uint64_t wi = c_lo >> 5; wi <= (c_hi - 1) >> 5; ++wi) {
    uint32_t bits = dup_word(d, wi, c_lo, c_hi);
@@ -93,8 +94,12 @@ __global__ void k_fast_dup(Dev d) {
 // shared memory, then walks the cells in order with shared-memory reads only. The
 // argmin takes the smallest |tip| bit pattern (|tip| >= 0 orders as its bits) and,
 // among equal ones, the first position: the reference's strict < in list order.
-constexpr int kDupMaxTuples = 32768;  // qualities of one event in shared memory
-constexpr int kDupStage = 1024;       // staged track entries per batch of cells
+constexpr int kDupMaxTuples = 32768;        // qualities of one event in shared memory (the reference's cap)
+constexpr int kDupLargeTuples = 256 * 1024;  // the same for extended-capacity events, 104 KB of shared memory
+constexpr int kDupStage = 1024;             // staged track entries per batch of cells
+
+template <int kMaxT>
+constexpr size_t dup_smem_bytes() { return 4 * (size_t(kMaxT) / 16 + size_t(kMaxT) / 32 + 2 * kDupStage + 33); }
 
 // qualities (0 bad, 1 dup, 2 loose) packed 2 bits per track, 16 per word
 __device__ __forceinline__ uint32_t q_get(const uint32_t* w, uint32_t t) { return (w[t >> 4] >> (2 * (t & 15))) & 3u; }
@@ -111,7 +116,7 @@ __global__ void __launch_bounds__(256) k_dup_prep(Dev d) {
   const int e = blockIdx.x;
   EvInfo& E = d.ev[e];
   __shared__ uint32_t sh[33];
-  if (E.n_cells == 0 || E.n_tuples > uint32_t(kDupMaxTuples)) {
+  if (E.n_cells == 0 || E.n_tuples > uint32_t(kDupLargeTuples)) {
     if (threadIdx.x == 0) E.n_dup_cells = 0;
     return;
   }
@@ -131,7 +136,7 @@ __global__ void __launch_bounds__(256) k_dup_prep(Dev d) {
   __syncthreads();
   // entries
   uint32_t* eoff = d.dup_eoff + c_lo + e;
-  uint16_t* et = d.dup_et + E.tuple_hit_base;
+  uint32_t* et = d.dup_et + E.tuple_hit_base;
   uint32_t* ek = d.dup_ek + E.tuple_hit_base;
   uint32_t base = 0;
   for (uint32_t q0 = 0; q0 < ndup; q0 += blockDim.x) {
@@ -149,7 +154,7 @@ __global__ void __launch_bounds__(256) k_dup_prep(Dev d) {
       eoff[q] = o;
       for (uint32_t j = 0; j < n; ++j) {
         const uint32_t t = d.ct_list[l0 + j];
-        et[o + j] = uint16_t(t - tb);
+        et[o + j] = uint32_t(t - tb);
         ek[o + j] = __float_as_uint(fabsf(d.t_state[5 * size_t(t) + 1]));
       }
     }
@@ -161,18 +166,21 @@ __global__ void __launch_bounds__(256) k_dup_prep(Dev d) {
   }
 }
 
+// Events of kMinT < n_tuples <= kMaxT tuples (dynamic shared memory of dup_smem_bytes<kMaxT>()).
+template <int kMaxT, int kMinT>
 __global__ void __launch_bounds__(32) k_fast_dup_smem(Dev d) {
-  __shared__ uint32_t s_q[kDupMaxTuples / 16];
-  __shared__ uint16_t s_t[kDupStage];
-  __shared__ uint32_t s_tip[kDupStage];
-  __shared__ uint32_t s_off[33];
-  __shared__ uint32_t s_seen[kDupMaxTuples / 32];
+  extern __shared__ uint32_t s_dup[];
+  uint32_t* s_q = s_dup;                          // [kMaxT / 16]
+  uint32_t* s_seen = s_q + kMaxT / 16;            // [kMaxT / 32]
+  uint32_t* s_t = s_seen + kMaxT / 32;            // [kDupStage]
+  uint32_t* s_tip = s_t + kDupStage;              // [kDupStage]
+  uint32_t* s_off = s_tip + kDupStage;            // [33]
   const int e = blockIdx.x;
   const unsigned lane = threadIdx.x;
   const EvInfo& E = d.ev[e];
   const uint64_t tb = E.tuple_base;
   const uint32_t nt = E.n_tuples;
-  if (nt > uint32_t(kDupMaxTuples)) return;  // k_fast_dup handles such events
+  if (nt > uint32_t(kMaxT) || nt <= uint32_t(kMinT)) return;  // another form handles such events
   if (E.n_dup_cells == 0) return;
   const uint32_t nw = (nt + 15) / 16;
   for (uint32_t w = lane; w < nw; w += 32) {
@@ -183,13 +191,13 @@ __global__ void __launch_bounds__(32) k_fast_dup_smem(Dev d) {
     }
     s_q[w] = v;
   }
-  for (uint32_t w = lane; w < uint32_t(kDupMaxTuples / 32); w += 32) s_seen[w] = 0;
+  for (uint32_t w = lane; w < uint32_t(kMaxT / 32); w += 32) s_seen[w] = 0;
   __syncwarp();
   // the event's cells with two or more tracks, in order, and their track entries as
   // k_dup_prep laid them out: offsets (ndup + 1) and (tuple, |tip| bits) per entry
   const uint32_t ndup = E.n_dup_cells;
   const uint32_t* eoff = d.dup_eoff + E.cell_base + e;
-  const uint16_t* et = d.dup_et + E.tuple_hit_base;
+  const uint32_t* et = d.dup_et + E.tuple_hit_base;
   const uint32_t* ek = d.dup_ek + E.tuple_hit_base;
   for (uint32_t q0 = 0; q0 < ndup;) {
     // stage up to 32 cells whose entries fit kDupStage
@@ -242,7 +250,7 @@ __global__ void __launch_bounds__(32) k_fast_dup_smem(Dev d) {
     for (uint32_t k = 0; k < ncell; ++k) {
       const uint32_t o = s_off[k], nk = s_off[k + 1] - o;
       uint32_t key0 = 0xffffffffu, key1 = 0xffffffffu, q0v = 0, q1v = 0;
-      uint16_t t0 = 0, t1 = 0;
+      uint32_t t0 = 0, t1 = 0;
       if (lane < nk) {
         t0 = s_t[o + lane];
         q0v = q_get(s_q, t0);
@@ -706,11 +714,14 @@ void launch_classify(const Dev& d, const Launch& L) {
   auto g = [&](int seg) { return dim3(L.bpe_of(seg), d.E); };
   k_classify<<<g(kTuneClassify), 256, 0, L.s>>>(d);
   L.mark("classify");
-  if (d.tuples_per_event > uint32_t(kDupMaxTuples)) k_fast_dup<<<div_up(d.E, 4), 128, 0, L.s>>>(d);
-  else {
-    k_dup_prep<<<d.E, 256, 0, L.s>>>(d);
-    k_fast_dup_smem<<<d.E, 32, 0, L.s>>>(d);
+  // events by tuple count: shared-memory qualities up to 32K tuples (every event at the
+  // reference's capacities), a 104 KB form up to 256K, global memory above
+  k_dup_prep<<<d.E, 256, 0, L.s>>>(d);
+  k_fast_dup_smem<kDupMaxTuples, 0><<<d.E, 32, dup_smem_bytes<kDupMaxTuples>(), L.s>>>(d);
+  if (d.tuples_per_event > uint32_t(kDupMaxTuples)) {
+    k_fast_dup_smem<kDupLargeTuples, kDupMaxTuples><<<d.E, 32, dup_smem_bytes<kDupLargeTuples>(), L.s>>>(d);
   }
+  if (d.tuples_per_event > uint32_t(kDupLargeTuples)) k_fast_dup<<<div_up(d.E, 4), 128, 0, L.s>>>(d, kDupLargeTuples);
   L.mark("fast_duplicate_remover");
   cudaMemsetAsync(d.htt_cur, 0, size_t(d.cap_hits) * sizeof(uint32_t), L.s);
   k_hit_to_tuple<0><<<g(kTuneHitToTuple), 256, 0, L.s>>>(d);
@@ -719,6 +730,13 @@ void launch_classify(const Dev& d, const Launch& L) {
   L.mark("hit_to_tuple");
   k_triplet_cleaner<<<g(kTuneHitToTuple), 256, 0, L.s>>>(d);
   L.mark("triplet_cleaner");
+}
+
+int prepare_select_kernels() {
+  const cudaError_t err = cudaFuncSetAttribute(k_fast_dup_smem<kDupLargeTuples, kDupMaxTuples>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               int(dup_smem_bytes<kDupLargeTuples>()));
+  return err == cudaSuccess ? 0 : -1;
 }
 
 void launch_vertices(const Dev& d, const Launch& L) {

@@ -207,6 +207,7 @@ int alloc_batch(PxlCtx* ctx) {
   d.doublets_per_event = uint32_t(p.doublets_per_event);
   d.tuples_per_event = uint32_t(p.tuples_per_event);
   d.fits_per_mult = uint32_t(p.fits_per_multiplicity);
+  d.columns_per_event = uint32_t(p.columns_per_event);
   d.include_errors = p.include_errors;
   d.use_quality = p.use_quality;
   d.apply_charge_cut = 1;
@@ -299,21 +300,49 @@ int run_chain(PxlCtx* ctx, uint32_t mask, cudaStream_t s) {
   return 0;
 }
 
+// Records that the context's last work went to stream s.
+int note_done(PxlCtx* ctx, cudaStream_t s) {
+  CK(cudaEventRecord(ctx->last_done, s));
+  if (s != ctx->stream) CK(cudaStreamWaitEvent(ctx->stream, ctx->last_done, 0));
+  return 0;
+}
+
 int fetch_ev_impl(PxlCtx* ctx) {
   if (ctx->ev_host_valid) return 0;
-  CK(cudaStreamSynchronize(ctx->stream));
   ctx->ev_host.resize(size_t(ctx->last_E) + 1);
-  CK(cudaMemcpy(ctx->ev_host.data(), ctx->d.ev, ctx->ev_host.size() * sizeof(EvInfo), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpyAsync(ctx->ev_host.data(), ctx->d.ev, ctx->ev_host.size() * sizeof(EvInfo), cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
   ctx->ev_host_valid = true;
   return 0;
 }
 
+// Device -> host copy on the context's stream (ordered after its work, waiting for nothing else).
 template <class T>
-int64_t copy_dev(const T* src, int64_t n, void* dst, int64_t max_bytes) {
+int64_t copy_dev(cudaStream_t s, const T* src, int64_t n, void* dst, int64_t max_bytes) {
   if (n < 0) return -1;
   if (dst && max_bytes > 0 && n > 0) {
     size_t nb = size_t(std::min<int64_t>(n * int64_t(sizeof(T)), max_bytes));
-    if (cudaMemcpy(dst, src, nb, cudaMemcpyDeviceToHost) != cudaSuccess) return PXL_ERR_CUDA;
+    if (cudaMemcpyAsync(dst, src, nb, cudaMemcpyDeviceToHost, s) != cudaSuccess) return PXL_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return PXL_ERR_CUDA;
+  }
+  return n;
+}
+
+// 32-bit hit ids as the reference's 16-bit hindex_type; PXL_ERR_CAPACITY when an id does not fit
+// (an extended-capacity event above 65535 hits)
+int64_t copy_dev_u16(cudaStream_t s, const uint32_t* src, int64_t n, uint32_t add, void* dst, int64_t max_bytes) {
+  if (n < 0) return -1;
+  if (dst && max_bytes > 0 && n > 0) {
+    std::vector<uint32_t> v(static_cast<size_t>(n));
+    if (copy_dev(s, src, n, v.data(), n * 4) < 0) return PXL_ERR_CUDA;
+    std::vector<uint16_t> w(static_cast<size_t>(n));
+    for (int64_t k = 0; k < n; ++k) {
+      const uint32_t x = v[size_t(k)] + add;
+      if (x > 0xFFFFu) return PXL_ERR_CAPACITY;
+      w[size_t(k)] = uint16_t(x);
+    }
+    std::memcpy(dst, w.data(), size_t(std::min<int64_t>(2 * n, max_bytes)));
   }
   return n;
 }
@@ -326,9 +355,9 @@ int64_t copy_host(const std::vector<T>& v, void* dst, int64_t max_bytes) {
 }
 
 template <class T>
-std::vector<T> dvec(const T* src, int64_t n) {
+std::vector<T> dvec(cudaStream_t s, const T* src, int64_t n) {
   std::vector<T> v(size_t(std::max<int64_t>(n, 0)));
-  if (n > 0) cudaMemcpy(v.data(), src, size_t(n) * sizeof(T), cudaMemcpyDeviceToHost);
+  if (n > 0) copy_dev(s, src, n, v.data(), n * int64_t(sizeof(T)));
   return v;
 }
 
@@ -397,6 +426,7 @@ int launch_slot(PxlCtx* ctx, int k, cudaStream_t s) {
   CK(cudaStreamWaitEvent(s, ctx->ev_staged[k], 0));
   CK(cudaGraphLaunch(ctx->graph_exec[k], s));
   CK(cudaEventRecord(ctx->ev_consumed[k], s));
+  if (int rc = note_done(ctx, s)) return rc;
   ctx->ev_host_valid = false;
   ctx->last_E = ctx->graph_E;
   ctx->last_mask = ctx->graph_mask;
@@ -428,6 +458,18 @@ int32_t pxl_params_default(PxlParams* p) {
   p->use_quality = 1;
   p->blocks_per_event = 0;
   p->threads_per_block = 0;
+  p->columns_per_event = kMaxActiveColumns;
+  return 0;
+}
+
+int32_t pxl_params_extended(PxlParams* p) {
+  const int32_t rc = pxl_params_default(p);
+  if (rc) return rc;
+  p->hits_per_event = 256 * 1024;
+  p->doublets_per_event = 4 * 1024 * 1024;
+  p->tuples_per_event = 256 * 1024;
+  p->fits_per_multiplicity = 256 * 1024;
+  p->columns_per_event = 4 * 1024 * 1024;
   return 0;
 }
 
@@ -437,14 +479,22 @@ int32_t pxl_ctx_create(const PxlConditions* cond, const PxlParams* params, PxlCt
   PxlCtx* ctx = new PxlCtx();
   if (params) ctx->p = *params;
   else pxl_params_default(&ctx->p);
-  // event-local hit ids are 16-bit (phi bins, doublet staging)
-  if (ctx->p.max_events <= 0 || ctx->p.hits_per_event <= 0 || ctx->p.hits_per_event > 65535) {
+  // event-local hit ids take kHitIdBits bits in the doublet search's hit records
+  const PxlParams& q = ctx->p;
+  if (q.max_events <= 0 || q.hits_per_event <= 0 || uint32_t(q.hits_per_event) > kMaxHitsPerEvent ||
+      q.doublets_per_event <= 0 || q.tuples_per_event <= 0 || q.fits_per_multiplicity <= 0 ||
+      q.columns_per_event <= 0) {
     delete ctx;
     return PXL_ERR_ARG;
   }
   if (cudaSetDevice(ctx->p.device) != cudaSuccess) { delete ctx; return PXL_ERR_CUDA; }
   if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return PXL_ERR_CUDA; }
-  int rc = load_conditions(ctx, cond);
+  if (cudaEventCreateWithFlags(&ctx->last_done, cudaEventDisableTiming) != cudaSuccess) {
+    pxl_ctx_destroy(ctx);
+    return PXL_ERR_CUDA;
+  }
+  int rc = prepare_select_kernels() ? PXL_ERR_CUDA : 0;
+  if (!rc) rc = load_conditions(ctx, cond);
   if (!rc) rc = alloc_batch(ctx);
   if (rc) { pxl_ctx_destroy(ctx); return rc; }
   *out = ctx;
@@ -464,6 +514,7 @@ int32_t pxl_ctx_destroy(PxlCtx* ctx) {
     if (ctx->ev_staged[k]) cudaEventDestroy(ctx->ev_staged[k]);
     if (ctx->ev_consumed[k]) cudaEventDestroy(ctx->ev_consumed[k]);
   }
+  if (ctx->last_done) { cudaEventSynchronize(ctx->last_done); cudaEventDestroy(ctx->last_done); }
   for (void* q : ctx->allocs) cudaFree(q);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -488,14 +539,7 @@ int32_t pxl_batch_run(PxlCtx* ctx, const uint8_t* blob, const uint64_t* offs, in
   ctx->last_mask = mask;
   rc = run_chain(ctx, mask, s);
   if (rc) return rc;
-  if (s != ctx->stream) {
-    cudaEvent_t ev;
-    CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-    CK(cudaEventRecord(ev, s));
-    CK(cudaStreamWaitEvent(ctx->stream, ev, 0));
-    cudaEventDestroy(ev);
-  }
-  return 0;
+  return note_done(ctx, s);
 }
 
 int32_t pxl_event_run(PxlCtx* ctx, const uint8_t* raw_event, size_t nbytes, uint32_t mask, void* stream) {
@@ -515,7 +559,8 @@ int32_t pxl_event_continue(PxlCtx* ctx, uint32_t mask, void* stream) {
   ctx->ev_host_valid = false;
   int rc = run_chain(ctx, mask, s);
   ctx->last_mask |= mask;
-  return rc;
+  if (rc) return rc;
+  return note_done(ctx, s);
 }
 
 int32_t pxl_graph_capture(PxlCtx* ctx, uint32_t mask) {
@@ -579,6 +624,7 @@ int64_t pxl_results_async(PxlCtx* ctx, uint32_t* host_dst, int64_t max_events, v
   const int64_t n = std::min<int64_t>(max_events, ctx->last_E);
   if (n <= 0) return 0;
   // one uint32 (n_vtx) per event, gathered from the per-event records
+  CK(cudaStreamWaitEvent(s, ctx->last_done, 0));
   CK(cudaMemcpy2DAsync(host_dst, sizeof(uint32_t), &ctx->d.ev[0].n_vtx, sizeof(EvInfo), sizeof(uint32_t), size_t(n),
                        cudaMemcpyDeviceToHost, s));
   return n;
@@ -675,7 +721,8 @@ int32_t pxl_autotune(PxlCtx* ctx, const int32_t* candidates, int32_t n_candidate
 int32_t pxl_sync(PxlCtx* ctx) {
   if (!ctx) return PXL_ERR_ARG;
   cudaSetDevice(ctx->p.device);
-  CK(cudaDeviceSynchronize());
+  // waits for this context's work only (its stream is ordered after the last work it enqueued)
+  CK(cudaStreamSynchronize(ctx->stream));
   CK(cudaGetLastError());
   ctx->ev_host_valid = false;
   int rc = fetch_ev(ctx);
@@ -683,7 +730,7 @@ int32_t pxl_sync(PxlCtx* ctx) {
   uint32_t w = 0;
   for (int e = 0; e < ctx->last_E; ++e) w |= ctx->ev_host[e].warnings;
   uint32_t st = 0;
-  CK(cudaMemcpy(&st, ctx->d.status, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+  if (copy_dev(ctx->stream, ctx->d.status, 1, &st, 4) < 0) return PXL_ERR_CUDA;
   return int32_t(w | st);
 }
 
@@ -712,44 +759,46 @@ int64_t pxl_copy_product(PxlCtx* ctx, int32_t e, int32_t product, void* dst, int
   cudaSetDevice(ctx->p.device);
   if (fetch_ev(ctx)) return PXL_ERR_CUDA;
   const Dev& d = ctx->d;
+  const cudaStream_t s = ctx->stream;
   const EvInfo& E = ctx->ev_host[e];
   const uint64_t wb = E.word_base, hb = E.hit_base;
   const int64_t nw = E.n_words, nh = E.n_hits;
   const size_t M1 = kMaxNumModules + 1;
   switch (product) {
-    case PXL_P_XX: return copy_dev(d.xx + wb, nw, dst, max_bytes);
-    case PXL_P_YY: return copy_dev(d.yy + wb, nw, dst, max_bytes);
-    case PXL_P_ADC: return copy_dev(d.adc + wb, nw, dst, max_bytes);
-    case PXL_P_MODULE_IND: return copy_dev(d.mid + wb, nw, dst, max_bytes);
-    case PXL_P_CLUS: return copy_dev(d.clus + wb, nw, dst, max_bytes);
-    case PXL_P_PDIGI: return copy_dev(d.pdigi + wb, nw, dst, max_bytes);
-    case PXL_P_RAW_ID: return copy_dev(d.rawid + wb, nw, dst, max_bytes);
-    case PXL_P_MODULE_START: return copy_dev(d.module_start + size_t(e) * M1, int64_t(M1), dst, max_bytes);
-    case PXL_P_CLUS_IN_MODULE: return copy_dev(d.clus_in_module + size_t(e) * kMaxNumModules, kMaxNumModules, dst, max_bytes);
-    case PXL_P_MODULE_ID: return copy_dev(d.module_id + size_t(e) * kMaxNumModules, kMaxNumModules, dst, max_bytes);
-    case PXL_P_CLUS_MODULE_START: return copy_dev(d.clus_module_start + size_t(e) * M1, int64_t(M1), dst, max_bytes);
-    case PXL_P_XL: return copy_dev(d.xl + hb, nh, dst, max_bytes);
-    case PXL_P_YL: return copy_dev(d.yl + hb, nh, dst, max_bytes);
-    case PXL_P_XERR: return copy_dev(d.xerr + hb, nh, dst, max_bytes);
-    case PXL_P_YERR: return copy_dev(d.yerr + hb, nh, dst, max_bytes);
-    case PXL_P_XG: return copy_dev(d.xg + hb, nh, dst, max_bytes);
-    case PXL_P_YG: return copy_dev(d.yg + hb, nh, dst, max_bytes);
-    case PXL_P_ZG: return copy_dev(d.zg + hb, nh, dst, max_bytes);
-    case PXL_P_RG: return copy_dev(d.rg + hb, nh, dst, max_bytes);
-    case PXL_P_IPHI: return copy_dev(d.iphi + hb, nh, dst, max_bytes);
-    case PXL_P_CHARGE: return copy_dev(d.charge + hb, nh, dst, max_bytes);
-    case PXL_P_XSIZE: return copy_dev(d.xsize + hb, nh, dst, max_bytes);
-    case PXL_P_YSIZE: return copy_dev(d.ysize + hb, nh, dst, max_bytes);
-    case PXL_P_DET_IND: return copy_dev(d.detind + hb, nh, dst, max_bytes);
-    case PXL_P_HITS_LAYER_START: return copy_dev(d.hits_layer_start + size_t(e) * 11, 11, dst, max_bytes);
-    case PXL_P_PHI_OFF: return copy_dev(d.phi_off + size_t(e) * kPhiTotBins, kPhiTotBins, dst, max_bytes);
-    case PXL_P_PHI_BINS: return copy_dev(d.phi_bins + hb, nh, dst, max_bytes);
+    case PXL_P_XX: return copy_dev(s, d.xx + wb, nw, dst, max_bytes);
+    case PXL_P_YY: return copy_dev(s, d.yy + wb, nw, dst, max_bytes);
+    case PXL_P_ADC: return copy_dev(s, d.adc + wb, nw, dst, max_bytes);
+    case PXL_P_MODULE_IND: return copy_dev(s, d.mid + wb, nw, dst, max_bytes);
+    case PXL_P_CLUS: return copy_dev(s, d.clus + wb, nw, dst, max_bytes);
+    case PXL_P_PDIGI: return copy_dev(s, d.pdigi + wb, nw, dst, max_bytes);
+    case PXL_P_RAW_ID: return copy_dev(s, d.rawid + wb, nw, dst, max_bytes);
+    case PXL_P_MODULE_START: return copy_dev(s, d.module_start + size_t(e) * M1, int64_t(M1), dst, max_bytes);
+    case PXL_P_CLUS_IN_MODULE: return copy_dev(s, d.clus_in_module + size_t(e) * kMaxNumModules, kMaxNumModules, dst, max_bytes);
+    case PXL_P_MODULE_ID: return copy_dev(s, d.module_id + size_t(e) * kMaxNumModules, kMaxNumModules, dst, max_bytes);
+    case PXL_P_CLUS_MODULE_START: return copy_dev(s, d.clus_module_start + size_t(e) * M1, int64_t(M1), dst, max_bytes);
+    case PXL_P_XL: return copy_dev(s, d.xl + hb, nh, dst, max_bytes);
+    case PXL_P_YL: return copy_dev(s, d.yl + hb, nh, dst, max_bytes);
+    case PXL_P_XERR: return copy_dev(s, d.xerr + hb, nh, dst, max_bytes);
+    case PXL_P_YERR: return copy_dev(s, d.yerr + hb, nh, dst, max_bytes);
+    case PXL_P_XG: return copy_dev(s, d.xg + hb, nh, dst, max_bytes);
+    case PXL_P_YG: return copy_dev(s, d.yg + hb, nh, dst, max_bytes);
+    case PXL_P_ZG: return copy_dev(s, d.zg + hb, nh, dst, max_bytes);
+    case PXL_P_RG: return copy_dev(s, d.rg + hb, nh, dst, max_bytes);
+    case PXL_P_IPHI: return copy_dev(s, d.iphi + hb, nh, dst, max_bytes);
+    case PXL_P_CHARGE: return copy_dev(s, d.charge + hb, nh, dst, max_bytes);
+    case PXL_P_XSIZE: return copy_dev(s, d.xsize + hb, nh, dst, max_bytes);
+    case PXL_P_YSIZE: return copy_dev(s, d.ysize + hb, nh, dst, max_bytes);
+    case PXL_P_DET_IND: return copy_dev(s, d.detind + hb, nh, dst, max_bytes);
+    case PXL_P_HITS_LAYER_START: return copy_dev(s, d.hits_layer_start + size_t(e) * 11, 11, dst, max_bytes);
+    case PXL_P_PHI_OFF: return copy_dev(s, d.phi_off + size_t(e) * kPhiTotBins, kPhiTotBins, dst, max_bytes);
+    case PXL_P_PHI_BINS: return copy_dev_u16(s, d.phi_bins + hb, nh, 0, dst, max_bytes);
+    case PXL_P_PHI_BINS32: return copy_dev(s, d.phi_bins + hb, nh, dst, max_bytes);
     case PXL_P_AVERAGE_GEOMETRY: return copy_host(ctx->avg_geom, dst, max_bytes);
     case PXL_P_ERRORS: {
       uint32_t total = 0;
-      cudaMemcpy(&total, d.err_count, sizeof(uint32_t), cudaMemcpyDeviceToHost);
+      if (copy_dev(s, d.err_count, 1, &total, 4) < 0) return PXL_ERR_CUDA;
       total = std::min<uint32_t>(total, uint32_t(d.cap_words));
-      std::vector<uint32_t> all = dvec(d.err, int64_t(total) * 5);
+      std::vector<uint32_t> all = dvec(s, d.err, int64_t(total) * 5);
       std::vector<std::pair<uint32_t, std::array<uint32_t, 4>>> mine;
       for (uint32_t k = 0; k < total; ++k)
         if (all[5 * k] == uint32_t(e))
@@ -793,12 +842,14 @@ int32_t pxl_clusterize_digis(PxlCtx* ctx, const uint16_t* id, const int16_t* x, 
   launch_modstart(d, L);
   launch_cluster(d, L);
   CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(module_start, d.module_start, (kMaxNumModules + 1) * 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(clus_in_module, d.clus_in_module, kMaxNumModules * 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(module_id, d.module_id, kMaxNumModules * 4, cudaMemcpyDeviceToHost, s));
+  if (n > 0) {
+    CK(cudaMemcpyAsync(clus, d.clus, size_t(n) * 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(id_out, d.mid, size_t(n) * 2, cudaMemcpyDeviceToHost, s));
+  }
   CK(cudaStreamSynchronize(s));
-  CK(cudaMemcpy(module_start, d.module_start, (kMaxNumModules + 1) * 4, cudaMemcpyDeviceToHost));
-  CK(cudaMemcpy(clus_in_module, d.clus_in_module, kMaxNumModules * 4, cudaMemcpyDeviceToHost));
-  CK(cudaMemcpy(module_id, d.module_id, kMaxNumModules * 4, cudaMemcpyDeviceToHost));
-  CK(cudaMemcpy(clus, d.clus, size_t(n) * 4, cudaMemcpyDeviceToHost));
-  CK(cudaMemcpy(id_out, d.mid, size_t(n) * 2, cudaMemcpyDeviceToHost));
   ctx->ev_host_valid = false;
   ctx->last_E = 0;
   return 0;

@@ -10,6 +10,9 @@ struct PxlCtx {
   PxlParams p{};
   int device = 0;
   cudaStream_t stream = nullptr;
+  // recorded after the last work this context enqueued, on whichever stream it went: the
+  // context's reads (sync, counts, copy-out) order themselves after it and wait for nothing else
+  cudaEvent_t last_done = nullptr;
   pxl::Dev d{};
   std::vector<void*> allocs;
   int16_t* fed_slot_of = nullptr;

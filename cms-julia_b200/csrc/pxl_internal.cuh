@@ -28,7 +28,9 @@ constexpr int kNPairs = 19;
 constexpr int kTupleStride = 32 * 1024;
 constexpr int kMaxCellsPerHit = 128;
 constexpr int kCellRows = 64;
-constexpr int kMaxActiveColumns = 512 * 1024 / 8;
+constexpr int kMaxActiveColumns = 512 * 1024 / 8;  // MAX_NUM_OF_ACTIVE_DOUBLETS, the default column cap
+constexpr uint32_t kHitIdBits = 21;                // event-local hit ids are below 2^21
+constexpr uint32_t kMaxHitsPerEvent = 1u << kHitIdBits;
 constexpr int kMaxFedSlots = 160;
 constexpr int kWarpModulePix = 256;  // modules up to this many digis are clustered by one warp
 
@@ -89,6 +91,10 @@ struct EvInfo {
   uint32_t n_dup_cells, dup_cell_base;
   uint32_t n_cols_nb, n_cols_tr;    // non-empty neighbour / track lists (column store use)
   uint32_t n_fit3, n_fit4;          // tuples fitted with 3 and with 4 hits (fit5as4 included)
+  // when the event found more tuples than it keeps: the hit offset where the last kept tuple's
+  // hits really end (its visible size is 0, as the reference's overflowing bulk_finalize_fill
+  // leaves it); 0 otherwise
+  uint32_t last_tuple_end;
 };
 
 // The fields the doublet search reads of an outer-hit candidate, packed in phi-bin order
@@ -101,8 +107,10 @@ struct ClusSumRec {
 
 struct alignas(16) HitRec {
   float z, r;
-  int16_t iphi, ysize, det;
-  uint16_t id;  // event-local 0-based hit index
+  int16_t iphi, ysize;
+  uint32_t det_id;  // detector index (below 2048) << kHitIdBits | event-local 0-based hit index
+  __host__ __device__ int det() const { return int(det_id >> kHitIdBits); }
+  __host__ __device__ uint32_t id() const { return det_id & (kMaxHitsPerEvent - 1u); }
 };
 
 // Everything a kernel may need, passed by value.
@@ -112,7 +120,7 @@ struct Dev {
   int32_t n_fed_slots;
   // limits
   int64_t cap_words, cap_hits, cap_cells, cap_tuples, cap_tuple_hits, cap_items, cap_pairs, cap_long;
-  uint32_t hits_per_event, doublets_per_event, tuples_per_event, fits_per_mult;
+  uint32_t hits_per_event, doublets_per_event, tuples_per_event, fits_per_mult, columns_per_event;
   int32_t include_errors, use_quality;
   int32_t apply_charge_cut;  // 1 in the chain; 0 only for the stand-alone clustering entry
   // inputs
@@ -139,7 +147,7 @@ struct Dev {
   int16_t* iphi; int16_t* xsize; int16_t* ysize; int16_t* detind; uint32_t* charge;
   uint32_t* hits_layer_start;  // [E][11]
   uint32_t* phi_off;           // [E][1281]
-  uint16_t* phi_bins;          // [cap_hits], 1-based hit ids
+  uint32_t* phi_bins;          // [cap_hits], 1-based hit ids
   struct HitRec* hit_rec;      // [cap_hits] the binned hits' doublet fields, in bin order
   struct ClusSumRec* hit_sum;  // [cap_hits] per-cluster sums of getHits, input of the CPE
   uint32_t* hit_me;            // [cap_hits] module of the hit's record, 0xFFFFFFFF when none
@@ -191,7 +199,7 @@ struct Dev {
   uint32_t* dup_bits;      // [cap_cells / 32 + 2] cells with two or more tracks, one bit each
   uint32_t* dup_list;      // [cap_cells] those cells in order, at the event's cell base
   uint32_t* dup_eoff;      // [cap_cells + E + 1] their entry offsets, at cell base + event index
-  uint16_t* dup_et;        // [cap_tuple_hits] entries: event-local tuple id, at the tuple-hit base
+  uint32_t* dup_et;        // [cap_tuple_hits] entries: event-local tuple id, at the tuple-hit base
   uint32_t* dup_ek;        // [cap_tuple_hits] entries: |tip| bits
   // vertices, per event
   int16_t* idv;            // [cap_tuples] per tuple (global tuple index), -1 when unused
@@ -346,6 +354,7 @@ void launch_rechits(const Dev& d, const Launch& L);   // a8-a9
 void launch_ca(const Dev& d, const Launch& L);        // a10-a14
 void launch_fit(const Dev& d, const Launch& L);       // a15-a16
 void launch_classify(const Dev& d, const Launch& L);  // a17
+int prepare_select_kernels();  // kernel attributes (dynamic shared memory) on the current device
 void launch_vertices(const Dev& d, const Launch& L);  // a18-a20
 
 // global scans over packed arrays (scan.cu)

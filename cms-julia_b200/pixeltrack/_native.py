@@ -43,6 +43,7 @@ class PxlParams(ctypes.Structure):
         ("tuples_per_event", ctypes.c_int32), ("fits_per_multiplicity", ctypes.c_int32),
         ("include_errors", ctypes.c_int32), ("use_quality", ctypes.c_int32),
         ("blocks_per_event", ctypes.c_int32), ("threads_per_block", ctypes.c_int32),
+        ("columns_per_event", ctypes.c_int32),
     ]
 
 
@@ -59,6 +60,7 @@ _gen = None
 _SIGS = {
     "pxl_version": (ctypes.c_int32, []),
     "pxl_params_default": (ctypes.c_int32, [ctypes.POINTER(PxlParams)]),
+    "pxl_params_extended": (ctypes.c_int32, [ctypes.POINTER(PxlParams)]),
     "pxl_ctx_create": (ctypes.c_int32, [ctypes.POINTER(PxlConditions), ctypes.POINTER(PxlParams),
                                         ctypes.POINTER(ctypes.c_void_p)]),
     "pxl_ctx_destroy": (ctypes.c_int32, [ctypes.c_void_p]),

@@ -22,10 +22,11 @@ PRODUCTS: dict[str, tuple[int, type]] = {
     "xg": (24, np.float32), "yg": (25, np.float32), "zg": (26, np.float32), "rg": (27, np.float32),
     "iphi": (28, np.int16), "charge": (29, np.uint32), "xsize": (30, np.int16), "ysize": (31, np.int16),
     "det_ind": (32, np.int16), "hits_layer_start": (33, np.uint32), "phi_off": (34, np.uint32),
-    "phi_bins": (35, np.uint16), "agc": (36, np.float32),
+    "phi_bins": (37, np.uint32), "phi_bins16": (35, np.uint16), "agc": (36, np.float32),
     "cells": (40, np.int32), "cell_neighbors": (41, np.uint32), "cell_tracks": (42, np.uint32),
     "outer_hit_of_cell": (43, np.uint32), "tuple_multiplicity": (44, np.uint32),
-    "tuple_off": (50, np.uint32), "tuple_hits": (51, np.uint16), "det_hits": (52, np.uint16),
+    "tuple_off": (50, np.uint32), "tuple_hits": (67, np.uint32), "tuple_hits16": (51, np.uint16),
+    "det_hits": (52, np.uint16),
     "quality": (53, np.uint8), "chi2": (54, np.float32), "eta": (55, np.float32), "pt": (56, np.float32),
     "state": (57, np.float32), "cov": (58, np.float32), "fitted": (59, np.uint8),
     "idv": (60, np.int16), "zv": (61, np.float32), "wv": (62, np.float32), "vchi2": (63, np.float32),
@@ -56,13 +57,24 @@ def default_params(**kw) -> PxlParams:
     return p
 
 
+def extended_params(**kw) -> PxlParams:
+    """The reference's parameters with the extended per-event capacities (pxl_params_extended)."""
+    p = PxlParams()
+    check(_native.lib().pxl_params_extended(ctypes.byref(p)), "pxl_params_extended")
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
 def batch_params(n_events: int, words_per_event: int = 64_000, hits_per_event_avg: int = 16_000,
-                 doublets_per_event_avg: int = 160_000, tuples_per_event_avg: int = 12_000, **kw) -> PxlParams:
+                 doublets_per_event_avg: int = 160_000, tuples_per_event_avg: int = 12_000, extended: bool = False,
+                 **kw) -> PxlParams:
     """Buffer sizes for a batch of n_events with the given per-event averages; the per-event
-    semantic capacities stay at the reference's values unless overridden."""
-    return default_params(max_events=n_events, max_words=n_events * words_per_event,
-                          max_hits=n_events * hits_per_event_avg, max_doublets=n_events * doublets_per_event_avg,
-                          max_tuples=n_events * tuples_per_event_avg, **kw)
+    semantic capacities stay at the reference's values, or take the extended ones."""
+    make = extended_params if extended else default_params
+    return make(max_events=n_events, max_words=n_events * words_per_event,
+                max_hits=n_events * hits_per_event_avg, max_doublets=n_events * doublets_per_event_avg,
+                max_tuples=n_events * tuples_per_event_avg, **kw)
 
 
 class PixelChain:

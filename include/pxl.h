@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define PXL_ABI_VERSION 1
+#define PXL_ABI_VERSION 2
 
 /* fatal status codes */
 #define PXL_ERR_ARG (-1)
@@ -83,7 +83,7 @@ typedef struct PxlParams {
   int64_t max_hits;                  /* hits per batch */
   int64_t max_doublets;              /* doublets per batch */
   int64_t max_tuples;                /* tuples per batch */
-  int32_t hits_per_event;            /* 49152 (MAX_NUMBER_OF_HITS); at most 65535 */
+  int32_t hits_per_event;            /* 49152 (MAX_NUMBER_OF_HITS); at most 2097152 (2^21) */
   int32_t doublets_per_event;        /* 458752 (maxNumberOfDoublets) */
   int32_t tuples_per_event;          /* 32768 (TrackSOA stride) */
   int32_t fits_per_multiplicity;     /* 24576 (MAX_NUM_OF_CONCURRENT_FITS) */
@@ -91,6 +91,8 @@ typedef struct PxlParams {
   int32_t use_quality;               /* 1 */
   int32_t blocks_per_event;          /* launch shape; 0 = chosen by the autotuner */
   int32_t threads_per_block;         /* launch shape; 0 = chosen by the autotuner */
+  int32_t columns_per_event;         /* 65536 (MAX_NUM_OF_ACTIVE_DOUBLETS): cells with a neighbour or
+                                        track list; a warning (PXL_WARN_COLUMNS) above it */
 } PxlParams;
 
 typedef struct PxlEventCounts {
@@ -131,17 +133,21 @@ enum PxlProduct {
   PXL_P_XSIZE = 30, PXL_P_YSIZE = 31, PXL_P_DET_IND = 32, /* int16 */
   PXL_P_HITS_LAYER_START = 33, /* uint32[11] */
   PXL_P_PHI_OFF = 34,          /* uint32[1281] */
-  PXL_P_PHI_BINS = 35,         /* uint16[n_hits], 1-based hit ids */
+  PXL_P_PHI_BINS = 35,         /* uint16[n_hits], 1-based hit ids (PXL_ERR_CAPACITY above 65535 hits) */
   PXL_P_AVERAGE_GEOMETRY = 36, /* float[6*148+2], beam-spot shifted */
+  PXL_P_PHI_BINS32 = 37,       /* uint32[n_hits], 1-based hit ids (any hit count) */
   /* CA internals, for parity tests */
   PXL_P_CELLS = 40,            /* int32[5*n_doublets]: inner, outer (1-based), layer pair (1-based), doublet id, used */
   PXL_P_CELL_NEIGHBORS = 41,   /* uint32 CSR: n_doublets+1 offsets, then 1-based cell ids */
   PXL_P_CELL_TRACKS = 42,      /* uint32 CSR: n_doublets+1 offsets, then tuple ids */
   PXL_P_OUTER_HIT_OF_CELL = 43,/* uint32 CSR: n_hits+1 offsets, then 1-based cell ids */
   PXL_P_TUPLE_MULTIPLICITY = 44, /* uint32[9] offsets then uint32 tuple ids (bin order) */
-  /* TrackSOA (CUDADataFormats/PixelTrackHeterogeneous.jl:10-62), stride 32768 */
+  /* TrackSOA (CUDADataFormats/PixelTrackHeterogeneous.jl:10-62), stride 32768, or the context's
+   * tuples_per_event when larger (extended capacity); the same stride for the ZVertexSoA's
+   * per-track arrays (idv, ndof) */
   PXL_P_HIT_INDICES_OFF = 50,  /* uint32[32769], 1-based starts as bulk_fill stores them */
-  PXL_P_HIT_INDICES = 51,      /* uint16[n_tuple_hits], 1-based hit ids */
+  PXL_P_HIT_INDICES = 51,      /* uint16[n_tuple_hits], 1-based hit ids (PXL_ERR_CAPACITY above 65535 hits) */
+  PXL_P_HIT_INDICES32 = 67,    /* uint32[n_tuple_hits], 1-based hit ids (any hit count) */
   PXL_P_DET_INDICES = 52,      /* uint16[n_tuple_hits] */
   PXL_P_QUALITY = 53,          /* uint8[32768]: 0 bad, 1 dup, 2 loose */
   PXL_P_CHI2 = 54, PXL_P_ETA = 55, PXL_P_PT = 56, /* float[32768] */
@@ -161,6 +167,14 @@ int32_t pxl_version(void);
 
 /* Fills the reference's parameters and default batch sizes. */
 int32_t pxl_params_default(PxlParams* params);
+
+/* The defaults with the extended per-event capacities: 262144 hits, 4194304 doublets,
+ * 262144 tuples and fits per multiplicity, 4194304 list columns. High-pileup events
+ * (pileup 200 gives about 31K hits, 0.8M doublets and 70K tuples) then run whole where the
+ * reference's capacities (ca_hit_ntuplet_generator.jl:40, PixelTrackHeterogeneous.jl:55,
+ * gpu_clustering_constants.jl:14) truncate them. Hit ids are 32-bit throughout. Batch sizes
+ * (max_*) stay the caller's to set. No counterpart in the reference. */
+int32_t pxl_params_extended(PxlParams* params);
 
 /* Uploads the conditions and allocates every device buffer of a batch.
  * Replaces the ES producers' produce() and the producers' constructors. */

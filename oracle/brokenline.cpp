@@ -382,15 +382,16 @@ int bl_fit_track(const double* hits, const float* ge, int n, double B, double* s
 // launchBrokenLineKernelsOnCPU, broken_line_fit_on_gpu.jl:166-203
 void fit_tuples(const Conditions& cond, EventOut& ev) {
   const double B = double(float(0.0114256972711507));
-  ev.pt.assign(kTupleBins, 0.f); ev.eta.assign(kTupleBins, 0.f); ev.chi2.assign(kTupleBins, 0.f);
-  ev.state.assign(size_t(kTupleBins) * 5, 0.f); ev.cov.assign(size_t(kTupleBins) * 15, 0.f);
-  ev.fitted.assign(kTupleBins, 0);
+  const uint32_t nb = ev.caps.tuples;
+  ev.pt.assign(nb, 0.f); ev.eta.assign(nb, 0.f); ev.chi2.assign(nb, 0.f);
+  ev.state.assign(size_t(nb) * 5, 0.f); ev.cov.assign(size_t(nb) * 15, 0.f);
+  ev.fitted.assign(nb, 0);
   const int passes[3][2] = {{3, 3}, {4, 4}, {4, 5}};  // (hits in fit, multiplicity bin); fit5as4
   for (auto& ps : passes) {
     int N = ps[0], nb = ps[1];
     uint32_t b0 = ev.tm_off[nb - 1], b1 = ev.tm_off[nb];
     uint32_t cnt = b1 - b0;
-    if (cnt > uint32_t(kMaxFitsPerMultiplicity)) { ev.flags |= kFlagFitsCapped; cnt = kMaxFitsPerMultiplicity; }
+    if (cnt > ev.caps.fits_per_mult) { ev.flags |= kFlagFitsCapped; cnt = ev.caps.fits_per_mult; }
     for (uint32_t t = 0; t < cnt; ++t) {
       uint32_t tk = ev.tm_bins[b0 + t];
       uint32_t hs = ev.tuple_off[tk - 1];  // 1-based start

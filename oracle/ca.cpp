@@ -29,7 +29,6 @@ const float kThetaForward = float(0.00300000002608);
 const float kHardCurv = float(0.0328407224959);
 const float kDcaInner = float(0.15000000596);
 const float kDcaOuter = float(0.25);
-const uint32_t kMaxDoublets = 458752;
 
 // CircleEq{Float32}, circle_eq.jl:18-47 and dca0 :287-291
 struct CircleEq {
@@ -77,21 +76,22 @@ inline uint32_t phi_bin(int16_t t) { return (uint32_t(int32_t(t >> 9)) & 127u) +
 
 void ca_tuples(const Conditions&, EventOut& ev) {
   const uint32_t nh = ev.n_hits;
+  const Caps& caps = ev.caps;
   // reset (resetCAHitNTupletGeneratorKernels, init_doublets)
-  ev.cell_neighbors.init(kCellNeighborsRows, kMaxActiveDoublets);
-  ev.cell_tracks.init(kCellTracksRows, kMaxActiveDoublets);
+  ev.cell_neighbors.init_lazy(kCellNeighborsRows, int(caps.columns));
+  ev.cell_tracks.init_lazy(kCellTracksRows, int(caps.columns));
   ev.cell_neighbors.extend();
   ev.cell_tracks.extend();
   ev.outer_hit_of_cell.init(kMaxCellsPerHit, std::max<uint32_t>(nh, 1));
   ev.cells.clear();
   ev.n_cells = 0;
-  ev.tuple_off.assign(kTupleBins + 1, 0);
-  ev.tuple_hits.assign(kTupleHitCap, 0);
-  ev.quality.assign(kTupleBins, 0);
+  ev.tuple_off.assign(caps.tuples + 1, 0);
+  ev.tuple_hits.assign(caps.tuple_hits, 0);
+  ev.quality.assign(caps.tuples, 0);
   ev.n_tuples = 0;
   ev.n_tuple_hits = 0;
   std::fill(ev.tm_off, ev.tm_off + 9, 0u);
-  ev.tm_bins.assign(48 * 1024, 0);
+  ev.tm_bins.assign(caps.multiplicity, 0);
 
   if (nh != 0) {
     // ---- doublets_from_histo, gpu_pixel_doublets.jl:121-360
@@ -173,10 +173,10 @@ void ca_tuples(const Conditions&, EventOut& ev) {
             if (dphi_f * dphi_f * (min_radius_2t4 - double(rr)) > double(dd * dd)) continue;
           }
           ev.n_cells += 1;
-          if (ev.n_cells > kMaxDoublets) { ev.n_cells -= 1; ev.flags |= kFlagDoubletsCapped; capped = true; break; }
+          if (ev.n_cells > caps.doublets) { ev.n_cells -= 1; ev.flags |= kFlagDoubletsCapped; capped = true; break; }
           Cell c;
           c.outer_neighbors = 1; c.tracks = 1; c.doublet_id = int32_t(ev.n_cells); c.layer_pair_id = int16_t(pid + 1);
-          c.used = 0; c.inner_z = ev.zg[i - 1]; c.inner_r = ev.rg[i - 1]; c.inner_hit = uint16_t(i); c.outer_hit = uint16_t(oi);
+          c.used = 0; c.inner_z = ev.zg[i - 1]; c.inner_r = ev.rg[i - 1]; c.inner_hit = i; c.outer_hit = oi;
           ev.cells.push_back(c);
           ev.outer_hit_of_cell.push(oi, ev.n_cells);
         }
@@ -213,7 +213,7 @@ void ca_tuples(const Conditions&, EventOut& ev) {
           Cell& oo = cells[oc - 1];
           if (oo.outer_neighbors == 1) {
             uint32_t col = ev.cell_neighbors.extend();
-            if (col == uint32_t(kMaxActiveDoublets)) ev.flags |= kFlagColumnsFull;
+            if (col == caps.columns) ev.flags |= kFlagColumnsFull;
             if (col > 1) oo.outer_neighbors = col;
           }
           if (oo.outer_neighbors > 1) {
@@ -266,7 +266,7 @@ void ca_tuples(const Conditions&, EventOut& ev) {
     uint32_t tmp[8];
     int depth = 0;
     auto emit = [&](const Cell& self) {
-      uint16_t hits[6];
+      uint32_t hits[6];
       int len = depth;
       for (int k = 0; k < len; ++k) hits[k] = cells[tmp[k] - 1].inner_hit;
       hits[len] = self.outer_hit;
@@ -274,8 +274,8 @@ void ca_tuples(const Conditions&, EventOut& ev) {
       uint32_t c0 = ev.n_tuples, c1 = ev.n_tuple_hits;
       ev.n_tuples += 1;
       ev.n_tuple_hits += n;
-      if (ev.n_tuples > uint32_t(kTupleBins)) { ev.flags |= kFlagTuplesOverflow; return; }
-      if (c1 + n > uint32_t(kTupleHitCap)) { ev.flags |= kFlagTuplesOverflow; return; }
+      if (ev.n_tuples > caps.tuples) { ev.flags |= kFlagTuplesOverflow; return; }
+      if (c1 + n > caps.tuple_hits) { ev.flags |= kFlagTuplesOverflow; return; }
       uint32_t it = ev.n_tuples;
       ev.tuple_off[it - 1] = c1 + 1;
       for (uint32_t k = 0; k < n; ++k) ev.tuple_hits[c1 + k] = hits[k];
@@ -284,7 +284,7 @@ void ca_tuples(const Conditions&, EventOut& ev) {
         Cell& c = cells[tmp[k] - 1];
         if (c.tracks == 1) {
           uint32_t col = ev.cell_tracks.extend();
-          if (col == uint32_t(kMaxActiveDoublets)) ev.flags |= kFlagColumnsFull;
+          if (col == caps.columns) ev.flags |= kFlagColumnsFull;
           if (col > 1) c.tracks = col;
         }
         if (c.tracks > 1) ev.cell_tracks.push(c.tracks, it);
@@ -318,8 +318,8 @@ void ca_tuples(const Conditions&, EventOut& ev) {
   // bulk_finalize_fill, hist_to_container.jl:246-257
   {
     uint32_t m = ev.n_tuples, n = ev.n_tuple_hits;
-    if (m > uint32_t(kTupleBins)) ev.tuple_off[kTupleBins] = ev.tuple_off[kTupleBins - 1];
-    else for (uint32_t i = m + 1; i <= uint32_t(kTupleBins) + 1; ++i) ev.tuple_off[i - 1] = n + 1;
+    if (m > caps.tuples) ev.tuple_off[caps.tuples] = ev.tuple_off[caps.tuples - 1];
+    else for (uint32_t i = m + 1; i <= caps.tuples + 1; ++i) ev.tuple_off[i - 1] = n + 1;
   }
   auto tsize = [&](uint32_t it) { return ev.tuple_off[it] - ev.tuple_off[it - 1]; };  // it 1-based
   // kernel_early_duplicate_remover, …_impl.jl:143-166
@@ -335,7 +335,7 @@ void ca_tuples(const Conditions&, EventOut& ev) {
     }
   }
   // kernel_countMultiplicity / finalize! / kernel_fillMultiplicity, :174-211
-  uint32_t ntb = std::min<uint32_t>(ev.n_tuples, kTupleBins);
+  uint32_t ntb = std::min<uint32_t>(ev.n_tuples, caps.tuples);
   for (uint32_t it = 1; it <= ntb; ++it) {
     uint32_t n = tsize(it);
     if (n < 3 || ev.quality[it - 1] == 1) continue;
@@ -348,16 +348,18 @@ void ca_tuples(const Conditions&, EventOut& ev) {
     if (n >= 9) continue;
     uint32_t w = ev.tm_off[n - 1];
     ev.tm_off[n - 1] -= 1;
-    ev.tm_bins[w - 1] = uint16_t(it);
+    if (w >= 1 && w <= caps.multiplicity) ev.tm_bins[w - 1] = it;
   }
   // kernel_fill_hit_indices, :25-38
-  ev.det_hits.assign(kTupleHitCap, 0);
-  uint32_t sz = std::min<uint32_t>(ev.tuple_off[kTupleBins] - 1, kTupleHitCap);
+  ev.det_hits.assign(caps.tuple_hits, 0);
+  uint32_t sz = std::min<uint32_t>(ev.tuple_off[caps.tuples] - 1, caps.tuple_hits);
   for (uint32_t k = 0; k < sz; ++k) ev.det_hits[k] = uint16_t(ev.det_ind[ev.tuple_hits[k] - 1]);
 }
 
 // classify_tuples, ca_hit_ntuplet_generator_kernels.jl:319-328
 void classify_tuples(const Conditions&, EventOut& ev) {
+  const Caps& caps = ev.caps;
+  const uint32_t kNone = 0xFFFFFFFFu;  // no tuple (the reference's sentinel 60000 is above its 32K tuple ids)
   const float chi2_coeff[4] = {0.68177776f, 0.74609577f, -0.08035491f, 0.00315399f};
   const float chi2_max_pt = 10.0f, chi2_scale = 30.0f;
   const float trip_tip = 0.3f, trip_pt = 0.5f, trip_zip = 12.0f;
@@ -366,7 +368,7 @@ void classify_tuples(const Conditions&, EventOut& ev) {
   auto tip = [&](uint32_t it) { return ev.state[size_t(it - 1) * 5 + 1]; };
   auto zip = [&](uint32_t it) { return ev.state[size_t(it - 1) * 5 + 4]; };
   // kernel_classify_tracks, …_impl.jl:213-247
-  for (uint32_t it = 1; it <= uint32_t(kTupleBins); ++it) {
+  for (uint32_t it = 1; it <= caps.tuples; ++it) {
     uint32_t n = tsize(it);
     if (n == 0) break;
     if (ev.quality[it - 1] == 1) continue;
@@ -388,7 +390,7 @@ void classify_tuples(const Conditions&, EventOut& ev) {
     uint32_t nt = ev.cell_tracks.length(col);
     if (nt < 2) continue;
     float mc = 10000.f;
-    uint32_t im = 60000;
+    uint32_t im = kNone;
     for (uint32_t k = 0; k < nt; ++k) {
       uint32_t it = ev.cell_tracks.at(col, k);
       if (ev.quality[it - 1] == 2 && std::fabs(tip(it)) < mc) { mc = std::fabs(tip(it)); im = it; }
@@ -399,23 +401,23 @@ void classify_tuples(const Conditions&, EventOut& ev) {
     }
   }
   // kernel_count_hit_in_tracks / finalize! / kernel_fill_hit_in_tracks, :281-311
-  const uint32_t nbins = kMaxNumClusters;  // HitToTuple bins, one per hit id
+  const uint32_t nbins = caps.hits;  // HitToTuple bins, one per hit id
   ev.hit_to_tuple_off.assign(nbins + 1, 0);
-  ev.hit_to_tuple_bins.assign(4 * 48 * 1024, 0);
-  for (uint32_t it = 1; it <= uint32_t(kTupleBins); ++it) {
+  ev.hit_to_tuple_bins.assign(caps.hit_to_tuple, 0);
+  for (uint32_t it = 1; it <= caps.tuples; ++it) {
     if (tsize(it) == 0) break;
     if (ev.quality[it - 1] != 2) continue;
     for (uint32_t h = ev.tuple_off[it - 1]; h <= ev.tuple_off[it] - 1; ++h) ev.hit_to_tuple_off[ev.tuple_hits[h - 1] - 1] += 1;
   }
   for (uint32_t b = 1; b <= nbins; ++b) ev.hit_to_tuple_off[b] += ev.hit_to_tuple_off[b - 1];
-  for (uint32_t it = 1; it <= uint32_t(kTupleBins); ++it) {
+  for (uint32_t it = 1; it <= caps.tuples; ++it) {
     if (tsize(it) == 0) break;
     if (ev.quality[it - 1] != 2) continue;
     for (uint32_t h = ev.tuple_off[it - 1]; h <= ev.tuple_off[it] - 1; ++h) {
       uint32_t b = ev.tuple_hits[h - 1];
       uint32_t w = ev.hit_to_tuple_off[b - 1];
       ev.hit_to_tuple_off[b - 1] -= 1;
-      ev.hit_to_tuple_bins[w - 1] = uint16_t(it);
+      if (w >= 1 && w <= caps.hit_to_tuple) ev.hit_to_tuple_bins[w - 1] = it;
     }
   }
   // kernel_triplet_cleaner, :313-362
@@ -423,7 +425,7 @@ void classify_tuples(const Conditions&, EventOut& ev) {
     uint32_t b0 = ev.hit_to_tuple_off[idx - 1], b1 = ev.hit_to_tuple_off[idx];
     if (b1 - b0 < 2) continue;
     float mc = 10000.f;
-    uint32_t im = 60000, maxnh = 0;
+    uint32_t im = kNone, maxnh = 0;
     for (uint32_t p = b0; p < b1; ++p) maxnh = std::max(maxnh, tsize(ev.hit_to_tuple_bins[p]));
     for (uint32_t p = b0; p < b1; ++p) {
       uint32_t it = ev.hit_to_tuple_bins[p];

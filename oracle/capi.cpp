@@ -1,5 +1,6 @@
 // Test infrastructure (CPU oracle): C-ABI used by tests/, smoke() and the
 // cpu_baseline leg of bench.py to drive the oracle and read its products.
+#include <algorithm>
 #include <chrono>
 #include <cstring>
 #include <string>
@@ -30,8 +31,19 @@ int64_t put_arr(const T* v, size_t n, void* dst, int64_t max_bytes) {
   return int64_t(n);
 }
 
+// The per-event counts: the tuples are those the container keeps (at most the capacity, the
+// last one of an overflowing container holding no hits), not the raw counter.
+void event_counts(const EventOut& e, uint32_t* v) {
+  const uint32_t nt = std::min(e.n_tuples, e.caps.tuples);
+  const uint32_t nth = e.tuple_off.empty() ? 0u : e.tuple_off[nt] - 1;
+  const uint32_t c[11] = {e.word_counter, e.n_modules, e.n_clusters, e.n_hits, e.n_cells, nt, nth,
+                          e.nv_final, e.n_vtx_tracks, e.flags, uint32_t(e.errors.size())};
+  std::memcpy(v, c, sizeof(c));
+}
+
 void run_event(const Conditions& c, const Options& o, const uint8_t* raw, size_t n, EventOut& ev) {
   ev.flags = 0;
+  ev.caps = o.caps;
   raw_to_clusters(c, raw, n, o, ev);
   if (o.stage_mask & 2) make_hits(c, ev);
   if (o.stage_mask & 4) ca_tuples(c, ev);
@@ -53,6 +65,23 @@ OrcCtx* orc_ctx_create(const uint8_t* cab, size_t ncab, const uint8_t* fed, size
 
 void orc_ctx_destroy(OrcCtx* c) { delete c; }
 
+// Per-event capacities (0 keeps a value): the reference's by default, larger ones for the
+// extended mode. The tuple-hit, multiplicity and hit-to-tuple capacities follow the tuples.
+void orc_set_caps(OrcCtx* c, uint32_t hits, uint32_t doublets, uint32_t tuples, uint32_t fits_per_mult,
+                  uint32_t columns) {
+  Caps& k = c->opt.caps;
+  if (hits) k.hits = hits;
+  if (doublets) k.doublets = doublets;
+  if (tuples) {
+    k.tuples = tuples;
+    k.tuple_hits = 5 * tuples;
+    k.multiplicity = std::max<uint32_t>(tuples, 48 * 1024);
+    k.hit_to_tuple = 4 * k.multiplicity;
+  }
+  if (fits_per_mult) k.fits_per_mult = fits_per_mult;
+  if (columns) k.columns = columns;
+}
+
 int32_t orc_run_event(OrcCtx* c, const uint8_t* raw, size_t nbytes, int32_t stage_mask) {
   c->opt.stage_mask = stage_mask;
   run_event(c->cond, c->opt, raw, nbytes, c->ev);
@@ -62,10 +91,7 @@ int32_t orc_run_event(OrcCtx* c, const uint8_t* raw, size_t nbytes, int32_t stag
 // counts: word_counter, n_modules, n_clusters, n_hits, n_cells, n_tuples, n_tuple_hits,
 // nv_final, n_vtx_tracks, flags, n_errors
 int32_t orc_counts(OrcCtx* c, uint32_t* out) {
-  const EventOut& e = c->ev;
-  uint32_t v[11] = {e.word_counter, e.n_modules, e.n_clusters, e.n_hits, e.n_cells, e.n_tuples, e.n_tuple_hits,
-                    e.nv_final, e.n_vtx_tracks, e.flags, uint32_t(e.errors.size())};
-  std::memcpy(out, v, sizeof(v));
+  event_counts(c->ev, out);
   return 11;
 }
 
@@ -213,11 +239,7 @@ double orc_run_batch(OrcCtx* c, const uint8_t* blob, const uint64_t* offsets, in
       EventOut ev;
       for (int e = t; e < n_events; e += nt) {
         run_event(c->cond, o, blob + offsets[e], size_t(offsets[e + 1] - offsets[e]), ev);
-        if (counts) {
-          uint32_t v[11] = {ev.word_counter, ev.n_modules, ev.n_clusters, ev.n_hits, ev.n_cells, ev.n_tuples,
-                            ev.n_tuple_hits, ev.nv_final, ev.n_vtx_tracks, ev.flags, uint32_t(ev.errors.size())};
-          std::memcpy(counts + size_t(e) * 11, v, sizeof(v));
-        }
+        if (counts) event_counts(ev, counts + size_t(e) * 11);
       }
     });
   }

@@ -96,20 +96,51 @@ struct Cell {
   int16_t layer_pair_id;     // 1-based pair index
   uint16_t used;
   float inner_z, inner_r;
-  uint16_t inner_hit, outer_hit;  // 1-based hit ids
+  // 1-based hit ids: the reference's UInt16 (hindex_type, ca_constants.jl:19) never wraps at
+  // its 48K hit capacity, so 32 bits give the same values there and room for the extended mode
+  uint32_t inner_hit, outer_hit;
 };
 
-// Fixed-row column store (PreAllocMatrix, CUDACore/simple_matrix.jl:1-58).
+// Per-event capacities. The defaults are the reference's; the extended mode raises them so
+// that high-pileup events are not truncated (hit ids, tuple ids and list entries are 32-bit).
+struct Caps {
+  uint32_t hits = kMaxNumClusters;              // MAX_NUMBER_OF_HITS clamp of clusModuleStart
+  uint32_t doublets = 458752;                   // maxNumberOfDoublets
+  uint32_t tuples = kTupleBins;                 // TrackSOA stride
+  uint32_t tuple_hits = kTupleHitCap;           // 5 hits per tuple slot
+  uint32_t fits_per_mult = kMaxFitsPerMultiplicity;
+  uint32_t columns = kMaxActiveDoublets;        // PreAllocMatrix columns (neighbours, tracks)
+  uint32_t multiplicity = 48 * 1024;            // TupleMultiplicity entries (MAX_TUPLES)
+  uint32_t hit_to_tuple = 4 * 48 * 1024;        // HitToTuple entries (4 * MAX_TUPLES)
+  bool extended() const { return hits != kMaxNumClusters || doublets != 458752u || tuples != uint32_t(kTupleBins); }
+};
+
+// Fixed-row column store (PreAllocMatrix, CUDACore/simple_matrix.jl:1-58). init() makes every
+// column addressable (columns indexed directly, as outer_hit_of_cell is by hit id);
+// init_lazy() leaves the columns to extend(), which hands them out in order and backs only
+// the ones handed out (the reference preallocates them all; the contents are the same).
 struct ColumnStore {
   int rows = 0, cols = 0;
   uint32_t ncol = 0;
   std::vector<uint32_t> data, len;
   void init(int r, int c) {
-    if (rows != r || cols != c) { rows = r; cols = c; data.assign(size_t(r) * c, 0); len.assign(c, 0); }
+    if (rows != r || cols != c || len.size() != size_t(c)) { rows = r; cols = c; data.assign(size_t(r) * c, 0); len.assign(c, 0); }
     ncol = 0;
     std::fill(len.begin(), len.end(), 0u);
   }
-  uint32_t extend() { if (ncol == uint32_t(cols)) return uint32_t(cols); return ++ncol; }
+  void init_lazy(int r, int c) {
+    rows = r; cols = c; ncol = 0;
+    len.clear();
+  }
+  uint32_t extend() {
+    if (ncol == uint32_t(cols)) return uint32_t(cols);
+    ++ncol;
+    if (len.size() < ncol) {
+      len.resize(ncol, 0);
+      if (data.size() < size_t(ncol) * rows) data.resize(std::max(size_t(ncol) * rows, 2 * data.size()));
+    }
+    return ncol;
+  }
   void push(uint32_t col, uint32_t v) {  // 1-based column
     uint32_t& l = len[col - 1];
     if (l == uint32_t(rows)) return;
@@ -144,7 +175,7 @@ struct EventOut {
   std::vector<uint32_t> charge;
   uint32_t hits_layer_start[11];
   uint32_t phi_off[kPhiTotBins];
-  std::vector<uint16_t> phi_bins;
+  std::vector<uint32_t> phi_bins;     // 1-based hit ids
   float agc_ladder[6][kLadders], agc_endcap_z[2];
   // a10-a14
   uint32_t n_cells = 0;
@@ -152,18 +183,18 @@ struct EventOut {
   ColumnStore cell_neighbors, cell_tracks, outer_hit_of_cell;
   uint32_t n_tuples = 0, n_tuple_hits = 0;
   std::vector<uint32_t> tuple_off;   // kTupleBins + 1, 1-based starts as the reference stores them
-  std::vector<uint16_t> tuple_hits;  // 1-based hit ids
+  std::vector<uint32_t> tuple_hits;  // 1-based hit ids
   std::vector<uint16_t> det_hits;    // det_indices bins
   std::vector<uint8_t> quality;      // 0 bad, 1 dup, 2 loose
   uint32_t tm_off[9];                // TupleMultiplicity offsets
-  std::vector<uint16_t> tm_bins;
+  std::vector<uint32_t> tm_bins;     // tuple ids
   // a15-a16
   std::vector<float> pt, eta, chi2;  // kTupleBins
   std::vector<float> state, cov;     // kTupleBins x 5, kTupleBins x 15 (row per tuple)
   std::vector<uint8_t> fitted;       // 1 if the tuple went through the broken-line fit
   // a17
   std::vector<uint32_t> hit_to_tuple_off;
-  std::vector<uint16_t> hit_to_tuple_bins;
+  std::vector<uint32_t> hit_to_tuple_bins;
   // a18-a20
   uint32_t nv_final = 0, n_vtx_tracks = 0;
   std::vector<int16_t> idv;
@@ -172,6 +203,7 @@ struct EventOut {
   std::vector<uint16_t> sort_ind;
   // flags for conditions where the reference would raise (assertion or domain error)
   uint32_t flags = 0;
+  Caps caps;  // capacities of the last run (from Options)
 };
 
 enum Flags : uint32_t {
@@ -191,6 +223,7 @@ enum Flags : uint32_t {
 struct Options {
   bool include_errors = true, use_quality = true, is_run2 = true;
   int stage_mask = 0x3F;  // 1 raw2digi+clusters, 2 rechits, 4 CA, 8 fit, 16 classify, 32 vertices
+  Caps caps;
 };
 
 void raw_to_clusters(const Conditions& c, const uint8_t* raw_event, size_t nbytes, const Options& o, EventOut& ev);

@@ -21,16 +21,22 @@ DTYPES = {
     "module_id": np.uint32, "clus_module_start": np.uint32, "xl": np.float32, "yl": np.float32,
     "xerr": np.float32, "yerr": np.float32, "xg": np.float32, "yg": np.float32, "zg": np.float32, "rg": np.float32,
     "iphi": np.int16, "charge": np.uint32, "xsize": np.int16, "ysize": np.int16, "det_ind": np.int16,
-    "hits_layer_start": np.uint32, "phi_off": np.uint32, "phi_bins": np.uint16, "agc": np.float32,
+    "hits_layer_start": np.uint32, "phi_off": np.uint32, "phi_bins": np.uint32, "agc": np.float32,
     "cells": np.int32, "cell_neighbors": np.uint32, "cell_tracks": np.uint32, "outer_hit_of_cell": np.uint32,
-    "tuple_off": np.uint32, "tuple_hits": np.uint16, "det_hits": np.uint16, "quality": np.uint8,
-    "tm_off": np.uint32, "tm_bins": np.uint16, "pt": np.float32, "eta": np.float32, "chi2": np.float32,
+    "tuple_off": np.uint32, "tuple_hits": np.uint32, "det_hits": np.uint16, "quality": np.uint8,
+    "tm_off": np.uint32, "tm_bins": np.uint32, "pt": np.float32, "eta": np.float32, "chi2": np.float32,
     "state": np.float32, "cov": np.float32, "fitted": np.uint8, "hit_to_tuple_off": np.uint32,
-    "hit_to_tuple_bins": np.uint16, "idv": np.int16, "zv": np.float32, "wv": np.float32, "vchi2": np.float32,
+    "hit_to_tuple_bins": np.uint32, "idv": np.int16, "zv": np.float32, "wv": np.float32, "vchi2": np.float32,
     "ptv2": np.float32, "ndof": np.int32, "sort_ind": np.uint16, "errors": np.uint32,
 }
 COUNT_NAMES = ("n_words", "n_modules", "n_clusters", "n_hits", "n_cells", "n_tuples", "n_tuple_hits", "nv_final",
                "n_vtx_tracks", "flags", "n_errors")
+
+# Per-event capacities of the extended mode (hits, doublets, tuples, fits per multiplicity,
+# list columns): no pileup-200 event of the synthetic generator reaches them. The reference's
+# own values (48K hits, 458,752 doublets, 32K tuples, 24K fits, 64K columns) are the default.
+EXTENDED_CAPS = {"hits": 256 * 1024, "doublets": 4 * 1024 * 1024, "tuples": 256 * 1024,
+                 "fits_per_mult": 256 * 1024, "columns": 4 * 1024 * 1024}
 
 _lib = None
 
@@ -51,6 +57,7 @@ def lib() -> ctypes.CDLL:
         _lib.orc_ctx_create.restype = V
         _lib.orc_ctx_create.argtypes = [V, ctypes.c_size_t] * 5
         _lib.orc_ctx_destroy.argtypes = [V]
+        _lib.orc_set_caps.argtypes = [V] + [ctypes.c_uint32] * 5
         _lib.orc_run_event.restype = ctypes.c_int32
         _lib.orc_run_event.argtypes = [V, V, ctypes.c_size_t, ctypes.c_int32]
         _lib.orc_counts.argtypes = [V, V]
@@ -71,7 +78,9 @@ def lib() -> ctypes.CDLL:
 
 
 class Oracle:
-    def __init__(self, conds: dict[str, bytes]):
+    """caps: per-event capacities (keys of EXTENDED_CAPS), the reference's when None."""
+
+    def __init__(self, conds: dict[str, bytes], caps: dict[str, int] | None = None):
         self._l = lib()
         names = ("cablingMap.bin", "fedIds.bin", "gain.bin", "cpefast.bin", "beamspot.bin")
         self._bufs = [conds[n] for n in names]
@@ -81,6 +90,9 @@ class Oracle:
         self._h = self._l.orc_ctx_create(*args)
         if not self._h:
             raise RuntimeError("oracle: bad conditions")
+        if caps:
+            self._l.orc_set_caps(self._h, *(int(caps.get(k, 0)) for k in ("hits", "doublets", "tuples",
+                                                                            "fits_per_mult", "columns")))
 
     def close(self):
         if self._h:

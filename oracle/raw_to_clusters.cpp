@@ -301,7 +301,7 @@ void raw_to_clusters(const Conditions& c, const uint8_t* raw, size_t nbytes, con
   for (int i = 0; i < kMaxNumModules; ++i) ms[i + 1] = std::min(kMaxHitsInModule, ev.clus_in_module[i]);
   for (int i = 2; i <= kMaxNumModules; ++i) ms[i] += ms[i - 1];
   for (int i = 0; i <= kMaxNumModules; ++i)
-    if (ms[i] > kMaxNumClusters) { ms[i] = kMaxNumClusters; ev.flags |= kFlagHitsClamped; }
+    if (ms[i] > ev.caps.hits) { ms[i] = ev.caps.hits; ev.flags |= kFlagHitsClamped; }
   ev.n_clusters = ms[kMaxNumModules - 1];  // setNClusters!(…, clus_module_start_d[MAX_NUM_MODULES]) (1-based)
 }
 

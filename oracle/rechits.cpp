@@ -191,7 +191,7 @@ void make_hits(const Conditions& cond, EventOut& ev) {
         uint32_t hfirst = ev.clus_module_start[me] + start;  // 1-based
         for (uint32_t ic = 0; ic < nin; ++ic) {
           uint32_t h = hfirst - 1 + ic + 1;  // 1-based hit index
-          if (h > kMaxNumClusters) break;
+          if (h > ev.caps.hits) break;
           Clus& k = cl[ic];
           position_corr(cp, d, k);
           error_from_db(d, k);
@@ -244,7 +244,7 @@ void make_hits(const Conditions& cond, EventOut& ev) {
     uint32_t b = binof(ev.iphi[i]) + 128u * uint32_t(ih);
     uint32_t w = ev.phi_off[b - 1];
     ev.phi_off[b - 1] -= 1;
-    if (w >= 1 && w <= nh) ev.phi_bins[w - 1] = uint16_t(i + 1);
+    if (w >= 1 && w <= nh) ev.phi_bins[w - 1] = i + 1;
   }
 }
 

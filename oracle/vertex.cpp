@@ -12,24 +12,25 @@ void make_vertices(const Conditions&, EventOut& ev) {
   const int32_t min_T = 2;
   const float eps = 0.07f, err_max = 0.01f, chi2_max = 9.0f;
   const float pt_min = 0.5f;
-  ev.idv.assign(kMaxVtxTracks, -1);
+  const uint32_t ntb = ev.caps.tuples;  // ZVertexSoA track stride (the TrackSOA's)
+  ev.idv.assign(ntb, -1);
   ev.zv.assign(kMaxVtx, 0.f); ev.wv.assign(kMaxVtx, 0.f); ev.vchi2.assign(kMaxVtx, 0.f); ev.ptv2.assign(kMaxVtx, 0.f);
-  ev.ndof.assign(kMaxVtxTracks, 0);
+  ev.ndof.assign(ntb, 0);
   ev.sort_ind.assign(kMaxVtx, 0);
   ev.nv_final = 0;
   // WorkSpace
-  std::vector<uint16_t> itrk;
+  std::vector<uint32_t> itrk;
   std::vector<float> zt, ezt2, ptt2;
   // load_tracks, :51-82
   auto tsize = [&](uint32_t it) { return ev.tuple_off[it] - ev.tuple_off[it - 1]; };
-  for (uint32_t idx = 1; idx <= uint32_t(kTupleBins); ++idx) {
+  for (uint32_t idx = 1; idx <= ntb; ++idx) {
     uint32_t nh = tsize(idx);
     if (nh == 0) break;
     if (nh < 4) continue;
     if (ev.quality[idx - 1] != 2) continue;
     float pt = ev.pt[idx - 1];
     if (pt < pt_min) continue;
-    itrk.push_back(uint16_t(idx));
+    itrk.push_back(idx);
     zt.push_back(ev.state[size_t(idx - 1) * 5 + 4]);
     ezt2.push_back(ev.cov[size_t(idx - 1) * 15 + 14]);
     ptt2.push_back(pt * pt);
@@ -42,7 +43,7 @@ void make_vertices(const Conditions&, EventOut& ev) {
   // cluster_tracks_by_density, :84-206 with HisToContainer{UInt8,256,16000,8,UInt16}
   const float err2_max = err_max * err_max;
   uint32_t off[257] = {};
-  std::vector<uint16_t> bins(std::max<uint32_t>(nt, 1));
+  std::vector<uint32_t> bins(std::max<uint32_t>(nt, 1));
   for (uint32_t i = 0; i < nt; ++i) {
     double zz = double(zt[i]) * 10.;
     int32_t iz = int32_t(std::trunc(zz));
@@ -55,7 +56,7 @@ void make_vertices(const Conditions&, EventOut& ev) {
   for (uint32_t i = 0; i < nt; ++i) {
     uint32_t w = off[izt[i]];
     off[izt[i]] -= 1;
-    bins[w - 1] = uint16_t(i + 1);
+    bins[w - 1] = i + 1;
   }
   // for_each_in_bins(hist, izt[i], 1, f): bins max(1,b-1)..min(256,b+1) (1-based bins)
   auto for_each = [&](uint8_t v, auto&& f) {

@@ -31,7 +31,7 @@ def test_bindings_cover_the_header():
 
 def test_version_without_gpu():
     from pixeltrack import _native
-    assert _native.lib().pxl_version() == 1
+    assert _native.lib().pxl_version() == 2
 
 
 def test_params_default_are_the_reference_capacities():
@@ -41,7 +41,18 @@ def test_params_default_are_the_reference_capacities():
     assert p.doublets_per_event == 458752
     assert p.tuples_per_event == 32 * 1024
     assert p.fits_per_multiplicity == 24 * 1024
+    assert p.columns_per_event == 64 * 1024
     assert p.max_words == 150 * 2000
+
+
+def test_params_extended_raise_only_the_per_event_capacities():
+    from pixeltrack.chain import default_params, extended_params
+    d, x = default_params(), extended_params()
+    assert x.hits_per_event == 256 * 1024 and x.doublets_per_event == 4 * 1024 * 1024
+    assert x.tuples_per_event == 256 * 1024 and x.fits_per_multiplicity == 256 * 1024
+    assert x.columns_per_event == 4 * 1024 * 1024
+    for f in ("max_events", "max_words", "max_hits", "max_doublets", "max_tuples", "include_errors", "use_quality"):
+        assert getattr(x, f) == getattr(d, f)
 
 
 def test_missing_library_fails_loudly(monkeypatch, tmp_path):

@@ -31,17 +31,17 @@ def test_context_entry_points_reject_null():
     assert L.pxl_clusterize_digis_noalloc(1, 1, 1, 1, (1 << 20) + 1, 1, 1, 1, 1, 1, 1, None) == -4
 
 
-def test_context_rejects_hit_cap_beyond_16_bit_ids():
-    """Event-local hit ids are 16-bit on the device, so hits_per_event above 65535 is refused
-    before any device work."""
+def test_context_rejects_capacities_out_of_range():
+    """Event-local hit ids take 21 bits in the device's hit records, so hits_per_event above
+    2^21 is refused before any device work, as are non-positive per-event capacities."""
     L = _native.lib()
     h = ctypes.c_void_p()
-    p = _native.PxlParams()
-    assert L.pxl_params_default(ctypes.byref(p)) == 0
-    p.hits_per_event = 65536
-    assert L.pxl_ctx_create(ctypes.byref(_native.PxlConditions()), ctypes.byref(p), ctypes.byref(h)) == -1
-    p.hits_per_event = 0
-    assert L.pxl_ctx_create(ctypes.byref(_native.PxlConditions()), ctypes.byref(p), ctypes.byref(h)) == -1
+    for field, bad in (("hits_per_event", (1 << 21) + 1), ("hits_per_event", 0), ("doublets_per_event", 0),
+                       ("tuples_per_event", -1), ("fits_per_multiplicity", 0), ("columns_per_event", 0)):
+        p = _native.PxlParams()
+        assert L.pxl_params_extended(ctypes.byref(p)) == 0
+        setattr(p, field, bad)
+        assert L.pxl_ctx_create(ctypes.byref(_native.PxlConditions()), ctypes.byref(p), ctypes.byref(h)) == -1, field
 
 
 def test_input_slot_entry_points_reject_bad_arguments():

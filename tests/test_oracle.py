@@ -126,3 +126,36 @@ def test_forward_mode_gradient_matches_central_differences():
                 hm[i, k] -= 1e-6
                 fd[i, k] = (chi(hp, ge) - chi(hm, ge)) / 2e-6
         assert np.abs(g - fd).max() <= 1e-6 * np.abs(fd).max()
+
+
+def test_extended_capacities_keep_whole_events(conditions):
+    """Pileup-200 events pass the reference's per-event doublet and tuple capacities
+    (ca_hit_ntuplet_generator.jl:40, PixelTrackHeterogeneous.jl:55), which truncate them; the
+    extended mode keeps them whole and agrees with the reference mode wherever no capacity is
+    reached (a PU50 event is identical in both)."""
+    from pixeltrack import gen
+    blob, offs = gen.events(2, gen.MODE_PU, pu=200, seed=77)
+    ref, ext = oracle.Oracle(conditions), oracle.Oracle(conditions, oracle.EXTENDED_CAPS)
+    for e in range(2):
+        ev = blob[offs[e]:offs[e + 1]]
+        ref.run_event(ev)
+        ext.run_event(ev)
+        cr, cx = ref.counts(), ext.counts()
+        assert cr["n_cells"] == 458752 and cr["flags"] & 0x10  # doublets capped
+        assert cr["n_tuples"] == 32768 and cr["flags"] & 0x40   # tuples capped at the TrackSOA stride
+        assert cx["flags"] == 0 and cx["n_cells"] > 458752 and cx["n_tuples"] > cr["n_tuples"]
+        assert cx["n_hits"] == cr["n_hits"]
+        # the kept doublets are the first ones (inner, outer hit and layer pair; the used flag
+        # and the fishbone's kills depend on the doublets past the cap)
+        n = cr["n_cells"]
+        assert np.array_equal(ext.get("cells").reshape(-1, 5)[:n, :3], ref.get("cells").reshape(-1, 5)[:, :3])
+    blob, offs = gen.events(1, gen.MODE_PU, pu=50, seed=11)
+    ref.run_event(blob[offs[0]:offs[1]])
+    ext.run_event(blob[offs[0]:offs[1]])
+    assert ref.counts() == ext.counts()
+    nt = ref.counts()["n_tuples"]
+    for name in ("cells", "phi_bins", "tuple_hits", "cell_neighbors", "cell_tracks"):
+        assert np.array_equal(ref.get(name), ext.get(name)[:len(ref.get(name))]), name
+    for name in ("quality", "pt", "chi2"):
+        assert np.array_equal(ref.get(name)[:nt], ext.get(name)[:nt]), name
+    assert ref.get("zv").tolist() == ext.get("zv").tolist()
