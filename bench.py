@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--uneven-events", type=int, default=4096)
     ap.add_argument("--uneven-steps", type=int, default=3)
     ap.add_argument("--no-uneven", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="skip the per-event comparison with the oracle")
     ap.add_argument("--adjoint-sample", type=int, default=500)
     ap.add_argument("--bpe", type=int, default=0, help="blocks per event for the per-event kernels (0: automatic)")
     return ap.parse_args()
@@ -155,57 +156,97 @@ FIT_B = 0.0114256972711507  # 1/(pT R) at 3.8 T, GeV^-1 cm^-1
 
 def bench_uneven(args, local: int, rank: int, world: int, plain_value: float) -> dict:
     """Batched uneven events: 4096 events with pileup drawn uniformly from [0, 200] (about
-    1k-130k digis each), packed by prefix offsets into one batch, launch shapes from the
-    autotuner, one captured CUDA graph per step. Events above PU ~140 reach the reference's
-    per-event doublet and tuple capacities, which truncate them as the reference does."""
+    12k-130k digis each), in the extended-capacity mode (no event truncated), run as two
+    resident 2048-event halves, each one captured CUDA graph over prefix-offset packed input,
+    launch shapes from the autotuner. The parity check (outside the timed region) compares
+    every event's counts with the oracle run with the same capacities, and every product of
+    the ten largest events."""
     import torch
     from pixeltrack import dist as pdist
     from pixeltrack import PixelChain, batch_params, gen
     E = args.uneven_events
+    H = E // 2
     conds = gen.conditions()
     blob, offs = gen.events(E, gen.MODE_UNIFORM, pu=200.0, seed=args.seed + 31 + 7919 * rank)
     words = int(np.diff(offs).sum() // 4)
-    params = batch_params(E, words_per_event=int(words / E * 1.2) + 4096, hits_per_event_avg=20_000,
-                          doublets_per_event_avg=280_000, tuples_per_event_avg=24_000, device=local)
+    params = batch_params(H, words_per_event=int(words / E * 1.4) + 4096, hits_per_event_avg=24_000,
+                          doublets_per_event_avg=360_000, tuples_per_event_avg=36_000, device=local,
+                          extended=True)
     chain = PixelChain(conds, params)
     stream = torch.cuda.Stream(device=local)
     sh = stream.cuda_stream
-    chain.stage_batch(blob, offs, sh)
+    halves = [(blob[int(offs[k * H]):int(offs[(k + 1) * H])], offs[k * H:(k + 1) * H + 1] - offs[k * H])
+              for k in range(2)]
+    chain.stage_batch(*halves[0], sh)
     stream.synchronize()
     tuned = chain.autotune()
-    chain.stage_batch(blob, offs, sh)
+    # both halves resident in the context's two input slots, one graph per slot
+    chain.stage_batch(*halves[0], sh)
     stream.synchronize()
     chain.capture_graph()
+    chain.stage_slot(1, *halves[1], sh)
+    stream.synchronize()
     for _ in range(args.warmup):
-        chain.launch_graph(sh)
+        chain.launch_slot(0, sh)
+        chain.launch_slot(1, sh)
     warn = chain.sync()
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t0.record(stream)
     for _ in range(args.uneven_steps):
-        chain.launch_graph(sh)
+        chain.launch_slot(0, sh)
+        chain.launch_slot(1, sh)
     t1.record(stream)
     t1.synchronize()
     ms = pdist.max_over_ranks(t0.elapsed_time(t1), device=torch.device("cuda", local)) / args.uneven_steps
+    # per-event counts of each half, and the full products of the largest events
+    counts = []
+    big = set(np.argsort(np.diff(offs))[-10:].tolist())
+    parity = {"events": E, "caps": "extended"}
+    prod_err = {}
+    orc = None
+    if not args.no_parity:
+        from oracle import oracle
+        from oracle.compare import compare_event
+        orc = oracle.Oracle(conds, oracle.EXTENDED_CAPS)
+    for k in range(2):
+        chain.launch_slot(k, sh)
+        warn |= chain.sync()
+        for e in range(H):
+            counts.append(chain.counts(e))
+            if orc is not None and k * H + e in big:
+                g = k * H + e
+                orc.run_event(blob[int(offs[g]):int(offs[g + 1])], 63)
+                errs = compare_event(chain, orc, e)
+                if errs:
+                    prod_err[g] = errs[:3]
+    chain.close()
+    if orc is not None:
+        from oracle.compare import compare_counts
+        _, ocnt = orc.run_batch(blob, offs, os.cpu_count() or 1, counts=True)
+        bad = compare_counts(counts, ocnt)
+        parity.update({"count_mismatch_events": len(bad), "first_mismatch": bad[:5],
+                       "product_sample": sorted(big), "product_mismatch_events": len(prod_err),
+                       "product_errors": prod_err})
     tot = {"digis_min": 10 ** 9, "digis_max": 0, "hits": 0, "cells": 0, "tuples": 0, "vertices": 0,
            "capped_events": 0, "buffer_overflow_events": 0}
     from pixeltrack._native import WARN_BITS
-    for e in range(E):
-        c = chain.counts(e)
+    for c in counts:
         tot["digis_min"] = min(tot["digis_min"], c.n_words)
         tot["digis_max"] = max(tot["digis_max"], c.n_words)
         tot["hits"] += c.n_hits
         tot["cells"] += c.n_doublets
         tot["tuples"] += c.n_tuples
         tot["vertices"] += c.n_vertices
-        tot["capped_events"] += int(bool(c.warnings & 0x50))
+        tot["capped_events"] += int(bool(c.warnings & 0x5D))
         tot["buffer_overflow_events"] += int(bool(c.warnings & 0x800))
-    chain.close()
     value = world * E / (ms / 1e3)
-    return {"workload": f"{E} synthetic events, pileup uniform in [0, 200], batched by prefix offsets, autotuned "
-                        "launch shapes, one CUDA graph per step", "events_per_step": E, "value": value,
+    return {"workload": f"{E} synthetic events, pileup uniform in [0, 200], extended per-event capacities, two "
+                        f"resident {H}-event halves per step, each one CUDA graph over prefix-offset packed input, "
+                        "autotuned launch shapes", "events_per_step": E, "value": value,
             "unit": "events/s", "ms_per_step": ms, "steps": args.uneven_steps, "raw_bytes_per_step": int(offs[-1]),
             "over_plain_per_event_pu50": value / world / plain_value if plain_value else None,
-            "blocks_per_event": tuned, "totals": tot, "warnings": [n for b, n in WARN_BITS.items() if warn & b]}
+            "blocks_per_event": tuned, "totals": tot, "warnings": [n for b, n in WARN_BITS.items() if warn & b],
+            "parity": parity}
 
 
 def bench_fits(args, local: int, rank: int, world: int) -> dict:
@@ -376,6 +417,25 @@ def bench_adjoint(args, local: int, rank: int, world: int) -> dict:
             "dtype": "f64 arithmetic, f32 outputs, f64 alignment accumulation"}
 
 
+def pu50_parity(chain, conds, blob, offs, E: int) -> dict:
+    """Every event's counts against the oracle (all host threads), and every product of a few
+    events (first, middle, last and the three largest), on the chain's last run."""
+    from oracle import oracle
+    from oracle.compare import compare_counts, compare_event
+    orc = oracle.Oracle(conds)
+    _, ocnt = orc.run_batch(blob, offs, os.cpu_count() or 1, counts=True)
+    bad = compare_counts([chain.counts(e) for e in range(E)], ocnt)
+    sample = sorted({0, E // 2, E - 1, *np.argsort(np.diff(offs))[-3:].tolist()})
+    prod_err = {}
+    for e in sample:
+        orc.run_event(blob[int(offs[e]):int(offs[e + 1])], 63)
+        errs = compare_event(chain, orc, e)
+        if errs:
+            prod_err[e] = errs[:3]
+    return {"events": E, "caps": "reference", "count_mismatch_events": len(bad), "first_mismatch": bad[:5],
+            "product_sample": sample, "product_mismatch_events": len(prod_err), "product_errors": prod_err}
+
+
 def oracle_fit_sample(w: dict, m: int):
     from oracle import oracle
     return oracle.bl_fit_batch(w["hits"][: w["offsets"][m]], w["ge"][: w["offsets"][m]], w["offsets"][: m + 1], FIT_B, 1)
@@ -493,6 +553,8 @@ def main():
     if args.profile_only:
         print(json.dumps({"segments_ms": seg_ms, "totals": totals, "warnings": warn}), flush=True)
         return
+    # parity of the batch with the oracle (outside every timed region)
+    parity = None if args.no_parity else pu50_parity(chain, conds, blob, offs, E)
 
     # batched graph: input in HBM, one replay per step
     chain.stage_batch(blob, offs, sh)
@@ -612,7 +674,7 @@ def main():
             "batched_over_plain": value / world / plain_value,
             "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": kernels_per_step * args.steps,
             "clocks": clk.summary(), "segments_ms": seg_ms, "totals": totals, "warnings": warn, "fits": fits,
-            "adjoint": adjoint, "uneven_pu0_200": uneven,
+            "adjoint": adjoint, "uneven_pu0_200": uneven, "parity": parity,
             "vertices_per_event": nv_check / E,
         }
         print(json.dumps(line), flush=True)

@@ -31,6 +31,7 @@ CUDA_SOURCES = [
     "k_riemann.cu",
     "k_select.cu",
     "k_products.cu",
+    "k_export.cu",
     "noalloc.cu",
     "pipeline.cu",
 ]

@@ -515,6 +515,10 @@ int32_t pxl_ctx_destroy(PxlCtx* ctx) {
     if (ctx->ev_consumed[k]) cudaEventDestroy(ctx->ev_consumed[k]);
   }
   if (ctx->last_done) { cudaEventSynchronize(ctx->last_done); cudaEventDestroy(ctx->last_done); }
+  for (auto& x : ctx->exp) {
+    if (x.copied) { cudaEventSynchronize(x.copied); cudaEventDestroy(x.copied); }
+    if (x.ready) cudaEventDestroy(x.ready);
+  }
   for (void* q : ctx->allocs) cudaFree(q);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;

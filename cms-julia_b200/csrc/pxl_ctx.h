@@ -45,6 +45,9 @@ struct PxlCtx {
   bool capturing = false;
   // blocks per event of the tunable stages (0 = the default shape), set by pxl_autotune
   int tune[pxl::kTuneCount] = {};
+  // pxl_export_async: two alternating device export sets (allocated by the first call)
+  pxl::ExportSet exp[2];
+  int exp_next = 0;
 };
 
 // reads the events' counters back (synchronises the context stream)

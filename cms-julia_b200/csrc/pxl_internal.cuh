@@ -220,6 +220,17 @@ struct Dev {
   int32_t bpe;             // blocks per event for per-event kernels
 };
 
+// One set of device export buffers of pxl_export_async: the batch's loose tracks and vertices
+// packed event after event (index rows: first track, tracks, first vertex, vertices).
+struct ExportSet {
+  uint32_t* index = nullptr;
+  float* state = nullptr; float* cov = nullptr; float* pt = nullptr; float* eta = nullptr; float* chi2 = nullptr;
+  uint8_t* n_hits = nullptr; int16_t* vertex = nullptr; uint32_t* tuple = nullptr;
+  float* zv = nullptr; float* wv = nullptr; float* vchi2 = nullptr; float* ptv2 = nullptr; int32_t* ndof = nullptr;
+  uint32_t cap_tracks = 0, cap_vertices = 0;
+  cudaEvent_t ready = nullptr, copied = nullptr;  // kernels done (compute stream), copies done (copy stream)
+};
+
 // Track lists by hit count for the stand-alone fits (workspace layout).
 constexpr int kFitMaxN = 8;
 struct FitPlan {

@@ -7,9 +7,9 @@ reference's producer interface. Import fails loudly if the library is missing.
 from . import _native
 from ._native import (STAGE_ALL, STAGE_CLASSIFY, STAGE_DIGIS, STAGE_FIT, STAGE_HITS, STAGE_TUPLES,
                       STAGE_VERTICES)
-from .chain import PRODUCTS, PixelChain, batch_params, default_params, extended_params
+from .chain import PRODUCTS, PixelChain, TrackExport, batch_params, default_params, extended_params
 
-__all__ = ["PixelChain", "default_params", "extended_params", "batch_params", "PRODUCTS", "STAGE_ALL", "STAGE_DIGIS", "STAGE_HITS",
+__all__ = ["PixelChain", "TrackExport", "default_params", "extended_params", "batch_params", "PRODUCTS", "STAGE_ALL", "STAGE_DIGIS", "STAGE_HITS",
            "STAGE_TUPLES", "STAGE_FIT", "STAGE_CLASSIFY", "STAGE_VERTICES", "native_library"]
 
 

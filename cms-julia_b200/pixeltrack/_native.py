@@ -53,6 +53,12 @@ class PxlEventCounts(ctypes.Structure):
         "n_vertices", "n_vertex_tracks", "warnings", "n_errors")]
 
 
+class PxlExport(ctypes.Structure):
+    _fields_ = [("max_tracks", ctypes.c_int64), ("max_vertices", ctypes.c_int64)] + [
+        (n, ctypes.c_void_p) for n in ("index", "state", "cov", "pt", "eta", "chi2", "n_hits", "vertex", "tuple",
+                                       "zv", "wv", "vchi2", "ptv2", "ndof")]
+
+
 _lib = None
 _gen = None
 
@@ -80,6 +86,9 @@ _SIGS = {
     "pxl_autotune": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
                                       ctypes.c_void_p]),
     "pxl_graph_kernel_nodes": (ctypes.c_int32, [ctypes.c_void_p]),
+    "pxl_export_async": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(PxlExport), ctypes.c_void_p,
+                                          ctypes.c_void_p]),
+    "pxl_export_bytes": (ctypes.c_int64, [ctypes.POINTER(PxlExport), ctypes.c_int32]),
     "pxl_results_async": (ctypes.c_int64, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]),
     "pxl_profile_enable": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_int32]),
     "pxl_profile_read": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float),

@@ -168,6 +168,11 @@ class PixelChain:
     def results_async(self, host_ptr: int, max_events: int, stream: int | None = None) -> int:
         return check(self._lib.pxl_results_async(self._h, host_ptr, max_events, stream), "pxl_results_async")
 
+    def export_async(self, out: "TrackExport", stream: int | None = None, copy_stream: int | None = None) -> None:
+        """Compacted loose tracks and vertices of the last run into `out`'s pinned host arrays,
+        one copy per array (pxl_export_async); read `out` after copy_stream reaches the copies."""
+        check(self._lib.pxl_export_async(self._h, ctypes.byref(out.desc), stream, copy_stream), "pxl_export_async")
+
     def sync(self) -> int:
         return check(self._lib.pxl_sync(self._h), "pxl_sync")
 
@@ -224,3 +229,50 @@ class PixelChain:
                                              n, int(charge_cut), ms.ctypes.data, cim.ctypes.data, mid.ctypes.data,
                                              clus.ctypes.data, ido.ctypes.data), "pxl_clusterize_digis")
         return {"module_start": ms, "clus_in_module": cim, "module_id": mid, "clus": clus, "id": ido}
+
+
+class TrackExport:
+    """Pinned host arrays for pxl_export_async: per track state (5), pt, eta, chi2, hit count,
+    vertex and tuple slot (and the 15 covariance terms with cov=True), per vertex zv, wv, chi2,
+    ptv2 and ndof, and the per-event index (first track, tracks, first vertex, vertices)."""
+
+    def __init__(self, n_events: int, max_tracks: int, max_vertices: int, cov: bool = False):
+        import torch
+        pin = lambda n, dt: torch.empty(int(n), dtype=dt, pin_memory=True)
+        self.n_events = n_events
+        self.arrays = {"index": pin(4 * (n_events + 1), torch.int32), "state": pin(5 * max_tracks, torch.float32),
+                       "pt": pin(max_tracks, torch.float32), "eta": pin(max_tracks, torch.float32),
+                       "chi2": pin(max_tracks, torch.float32), "n_hits": pin(max_tracks, torch.uint8),
+                       "vertex": pin(max_tracks, torch.int16), "tuple": pin(max_tracks, torch.int32),
+                       "zv": pin(max_vertices, torch.float32), "wv": pin(max_vertices, torch.float32),
+                       "vchi2": pin(max_vertices, torch.float32), "ptv2": pin(max_vertices, torch.float32),
+                       "ndof": pin(max_vertices, torch.int32)}
+        if cov:
+            self.arrays["cov"] = pin(15 * max_tracks, torch.float32)
+        self.desc = _native.PxlExport(max_tracks=max_tracks, max_vertices=max_vertices)
+        for k, t in self.arrays.items():
+            setattr(self.desc, k, t.data_ptr())
+
+    def bytes(self) -> int:
+        return int(_native.lib().pxl_export_bytes(ctypes.byref(self.desc), self.n_events))
+
+    def index(self) -> np.ndarray:
+        """(n_events + 1, 4) uint32: first track, tracks, first vertex, vertices; last row the totals."""
+        return self.arrays["index"].numpy().view(np.uint32).reshape(-1, 4)
+
+    def event(self, e: int) -> dict[str, np.ndarray]:
+        """The tracks and vertices of event e (after the copies completed)."""
+        ft, nt, fv, nv = (int(v) for v in self.index()[e])
+        out = {}
+        for k, t in self.arrays.items():
+            if k == "index":
+                continue
+            a = t.numpy()
+            if k in ("state", "cov"):
+                w = 5 if k == "state" else 15
+                out[k] = a[w * ft:w * (ft + nt)].reshape(nt, w)
+            elif k in ("zv", "wv", "vchi2", "ptv2", "ndof"):
+                out[k] = a[fv:fv + nv]
+            else:
+                out[k] = a[ft:ft + nt]
+        return out

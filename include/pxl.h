@@ -232,6 +232,41 @@ int32_t pxl_slot_launch(PxlCtx* ctx, int32_t slot, void* stream);
  * host memory (pinned for an asynchronous copy), one uint32 per event; returns the count. */
 int64_t pxl_results_async(PxlCtx* ctx, uint32_t* host_dst, int64_t max_events, void* stream);
 
+/* Compacted track and vertex collections of the last run, for a consumer of a whole batch:
+ * the tracks of quality loose (TrackSOA, CUDADataFormats/PixelTrackHeterogeneous.jl:10-62,
+ * the ones the vertex finder takes) and the vertices (ZVertexSoA, z_vertex_soa.jl:4-26) of all
+ * events, packed event after event (tracks in tuple order), each array copied to host memory
+ * in ONE device->host copy. The compaction kernels go on `stream` (ordered after the context's
+ * last run), the copies on `copy_stream` (NULL: the same stream); nothing synchronises the
+ * host. Two device export sets alternate, so the copies of one batch overlap the next chain;
+ * the host arrays must stay untouched until copy_stream reaches the copies (pinned memory for
+ * a truly asynchronous copy). The first call allocates the export sets (about 100 bytes per
+ * tuple of the batch capacity, twice). Every pointer may be NULL (not copied). A batch with
+ * more tracks (vertices) than max_tracks (max_vertices) copies only the first ones; index row
+ * n_events holds the totals, so the caller can tell. No counterpart in the reference, which
+ * hands one event at a time to its consumers. */
+typedef struct PxlExport {
+  int64_t max_tracks;    /* capacity of the per-track host arrays */
+  int64_t max_vertices;  /* capacity of the per-vertex host arrays */
+  uint32_t* index;       /* [n_events + 1][4]: first track, tracks, first vertex, vertices; last row: totals */
+  float* state;          /* [max_tracks][5]: phi, tip, q/pT, cot(theta), zip (TrackSOA stateAtBS) */
+  float* cov;            /* [max_tracks][15] */
+  float* pt;             /* [max_tracks] */
+  float* eta;            /* [max_tracks] */
+  float* chi2;           /* [max_tracks] */
+  uint8_t* n_hits;       /* [max_tracks] hits of the track's tuple */
+  int16_t* vertex;       /* [max_tracks] the track's vertex as ZVertexSoA's idv holds it (-1: none) */
+  uint32_t* tuple;       /* [max_tracks] the track's 1-based tuple slot in its event's TrackSOA */
+  float* zv;             /* [max_vertices] */
+  float* wv;             /* [max_vertices] */
+  float* vchi2;          /* [max_vertices] */
+  float* ptv2;           /* [max_vertices] */
+  int32_t* ndof;         /* [max_vertices] */
+} PxlExport;
+int32_t pxl_export_async(PxlCtx* ctx, const PxlExport* out, void* stream, void* copy_stream);
+/* Bytes that pxl_export_async copies for `out` and a batch of n_events. */
+int64_t pxl_export_bytes(const PxlExport* out, int32_t n_events);
+
 /* Number of kernel nodes in the captured graph (the kernels one replay launches). */
 int32_t pxl_graph_kernel_nodes(PxlCtx* ctx);
 
