@@ -4,8 +4,8 @@ One step = the whole chain (raw FED words -> digis -> clusters -> rechits -> CA
 ntuplets -> broken-line fits -> classification -> vertices) over one batch of
 synthetic PU50 events (1000 by default), replayed as one CUDA graph with the input
 already in HBM. Also measured: the same metric end to end through the public API
-(host->device copy of the raw events from pinned memory and device->host read of the
-per-event vertex counts inside the timed region), the plain per-event launch sequence,
+(host->device copy of the raw events from pinned memory and device->host copy of the
+batch's track and vertex collections inside the timed region), the plain per-event launch sequence,
 per-kernel times (live CUDA events) for the roofline of the dominant kernel, and the
 CPU baseline (the serial restatement of the reference on the host cores).
 
@@ -578,38 +578,54 @@ def main():
     ms_per_step = ms / args.steps
     value = world * E * args.steps / (ms / 1e3)
 
-    # end to end through the public API: pinned host raw events in, per-event results out.
-    # Batch i+1 is copied into the other input slot on a copy stream while batch i runs.
+    # end to end through the public API: pinned host raw events in; the batch's track and vertex
+    # collections out (pxl_export_async: the loose tracks' parameters, hit counts and vertex
+    # ids, the vertices, and the per-event index, one copy per array). Batch i+1 is copied into
+    # the other input slot on a copy stream while batch i runs, and batch i's collections go
+    # to host memory on a third stream while batch i+1 runs.
+    from pixeltrack import TrackExport
     pinned = torch.empty(len(blob), dtype=torch.uint8, pin_memory=True)
     pinned.numpy()[:] = blob
     pinned_np = pinned.numpy()
-    res = [torch.empty(E, dtype=torch.int32, pin_memory=True) for _ in range(2)]
+    probe = TrackExport(E, max_tracks=0, max_vertices=0)  # totals of this batch, to size the host arrays
+    chain.export_async(probe)
+    chain.sync()
+    torch.cuda.synchronize()
+    n_loose, n_vtx = int(probe.index()[E, 1]), int(probe.index()[E, 3])
+    outs = [TrackExport(E, max_tracks=n_loose + n_loose // 8 + 1024, max_vertices=n_vtx + n_vtx // 8 + 64)
+            for _ in range(2)]
     h2d = int(offs[-1] - offs[0]) + 8 * (E + 1)
-    d2h = 4 * E
+    d2h = outs[0].bytes()
     copy = torch.cuda.Stream(device=local)
+    d2h_stream = torch.cuda.Stream(device=local)
 
     def e2e_steps(n):
         chain.stage_slot(0, pinned_np, offs, copy.cuda_stream)
         for i in range(n):
             chain.launch_slot(i % 2, sh)
-            chain.results_async(res[i % 2].data_ptr(), E, sh)
+            chain.export_async(outs[i % 2], sh, d2h_stream.cuda_stream)
             if i + 1 < n:
                 chain.stage_slot((i + 1) % 2, pinned_np, offs, copy.cuda_stream)
 
     e2e_steps(args.warmup)
     stream.synchronize()
+    d2h_stream.synchronize()
     if dist:
         dist.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     e0.record(stream)
     copy.wait_event(e0)
+    d2h_stream.wait_event(e0)
     e2e_steps(args.steps)
+    stream.wait_stream(d2h_stream)
     e1.record(stream)
     e1.synchronize()
     ems = pdist.max_over_ranks(e0.elapsed_time(e1), device="cuda")
     e2e_value = world * E * args.steps / (ems / 1e3)
-    nv_check = int(res[(args.steps - 1) % 2].numpy().sum())
+    last = outs[(args.steps - 1) % 2].index()
+    nv_check = int(last[E, 3])
+    assert int(last[E, 1]) == n_loose and nv_check == n_vtx, "exported collections differ between steps"
 
     # plain per-event launch sequence (one event per launch sequence, input already in HBM)
     plain = PixelChain(conds, default_params(device=local))

@@ -87,12 +87,14 @@ __device__ __forceinline__ bool module_range(const Dev& d, int e, uint32_t m, Mo
 // Module positions are clustered in parallel; a module id seen in several runs of one
 // event (only malformed data does that) keeps the count of its last run, as the serial
 // loop leaves it: the count is stored with its position as the key of an atomicMax
-// ((position + 1) << 11 | count, count <= 1024) and k_hits_module_start strips the key.
+// ((position + 1) << kCountBits | count, count <= 4000) and k_hits_module_start strips the key.
+constexpr uint32_t kCountBits = 13;
+constexpr uint32_t kCountMask = (1u << kCountBits) - 1u;
 __device__ __forceinline__ void write_module_record(const Dev& d, int e, uint32_t m, int16_t this_id, uint32_t nclus,
                                                     uint32_t warn) {
   d.module_id[size_t(e) * kMaxNumModules + m] = uint32_t(uint16_t(this_id));
   if (uint16_t(this_id) < uint16_t(kMaxNumModules))
-    atomicMax(&d.clus_in_module[size_t(e) * kMaxNumModules + uint16_t(this_id)], ((m + 1u) << 11) | nclus);
+    atomicMax(&d.clus_in_module[size_t(e) * kMaxNumModules + uint16_t(this_id)], ((m + 1u) << kCountBits) | nclus);
   if (warn) atomic_or_warn(&d.ev[e], warn);
 }
 
@@ -274,7 +276,7 @@ __device__ __forceinline__ void cluster_module_warp(const Dev& d, int e, uint32_
     last_new += __popc(b);
   }
   __syncwarp();
-  const bool changed = d.apply_charge_cut && nclus > 0 && last_new != nclus;
+  const bool changed = d.apply_charge_cut && !d.ev[e].repeated_ids && nclus > 0 && last_new != nclus;
 #pragma unroll
   for (int j = 0; j < kSlots; ++j) {
     const int k = int(lane) + 32 * j;
@@ -378,7 +380,7 @@ __device__ __forceinline__ void cluster_module_thread(const Dev& d, int e, uint3
     ++nclus;
     if (ok) ++kept;
   }
-  const bool changed = d.apply_charge_cut && nclus > 0 && kept != nclus;
+  const bool changed = d.apply_charge_cut && !d.ev[e].repeated_ids && nclus > 0 && kept != nclus;
 #pragma unroll
   for (int k = 0; k < kThreadPix; ++k) {
     if (k >= n) continue;
@@ -566,12 +568,13 @@ __device__ void cluster_module_block(const Dev& d, int e, uint32_t m, BlockSmem&
     last_new = c2;
   }
   __syncthreads();
-  const bool changed = d.apply_charge_cut && nclus_eff > 0 && last_new != nclus_eff;
+  const bool cut_here = d.apply_charge_cut && !d.ev[e].repeated_ids;
+  const bool changed = cut_here && nclus_eff > 0 && last_new != nclus_eff;
   for (int k = threadIdx.x; k < n; k += blockDim.x) {
     const uint64_t g = g0 + k;
     if (S.lab[k] < 0) { d.clus[g] = -9999; continue; }
     uint32_t cl = S.sorted[S.lab[k]];
-    if (d.apply_charge_cut && nclus > uint32_t(kMaxClustersPerModule) && k < crun && cl > uint32_t(kMaxClustersPerModule)) {
+    if (cut_here && nclus > uint32_t(kMaxClustersPerModule) && k < crun && cl > uint32_t(kMaxClustersPerModule)) {
       d.clus[g] = int32_t(kInvId);
       d.mid[g] = int16_t(kInvId);
       continue;
@@ -602,12 +605,115 @@ __global__ void __launch_bounds__(256) k_find_clus_block(Dev d) {
   }
 }
 
+// cluster_charge_cut (gpu_cluster_charge_cut.jl:14-104) in the reference's serial order, for the
+// events where a module id starts more than one run: there a run's cut reads the count the id's
+// LAST run left (find_clus writes every count first), as changed by the cuts of its earlier
+// runs, and the renumbering of cluster ids beyond that count reads the new numbers of the
+// module cut before it (the per-event newclusId buffer is never cleared). One warp per event
+// walks the runs in order, 32 digis at a time; the fused kernels left these events uncut.
+// A cluster id past 1024 in the sums or the renumbering (the reference indexes out of bounds and
+// raises) sets the clusters warning and is skipped.
+__global__ void __launch_bounds__(32) k_charge_cut_serial(Dev d) {
+  const int e = blockIdx.x;
+  const EvInfo& E = d.ev[e];
+  if (!d.apply_charge_cut || !E.repeated_ids) return;
+  if (E.word_base + uint64_t(E.n_words) > uint64_t(d.cap_words)) return;
+  __shared__ int32_t s_charge[kMaxClustersPerModule];
+  __shared__ uint16_t s_new[kMaxClustersPerModule];
+  __shared__ uint8_t s_ok[kMaxClustersPerModule];
+  const unsigned lane = threadIdx.x;
+  const unsigned lt = (1u << lane) - 1u;
+  for (int c = lane; c < kMaxClustersPerModule; c += 32) s_new[c] = 0;  // one buffer per event
+  uint32_t* cim = d.clus_in_module + size_t(e) * kMaxNumModules;
+  const uint32_t* ms = d.module_start + size_t(e) * (kMaxNumModules + 1);
+  const uint64_t eb = E.word_base;
+  const uint32_t n_el = E.n_words, nmod = E.n_modules;
+  uint32_t warn = 0;
+  __syncwarp();
+  // first index >= i0 (0-based) whose digi ends the run: any id but this_id (invalid
+  // included, the sums' skip test is always false) or, with skip_inv, a valid other id
+  for (uint32_t m = 0; m < nmod; ++m) {
+    const uint32_t first = ms[m + 1] - 1u;  // 0-based
+    if (first >= n_el) continue;
+    const int16_t this_id = d.mid[eb + first];
+    if (uint16_t(this_id) >= uint16_t(kMaxNumModules)) continue;
+    uint32_t nclus = cim[uint16_t(this_id)] & kCountMask;
+    if (nclus == 0) continue;
+    if (nclus > uint32_t(kMaxClustersPerModule)) {
+      for (uint32_t i0 = first; i0 < n_el; i0 += 32) {
+        const uint32_t i = i0 + lane;
+        const bool stop = i >= n_el || d.mid[eb + i] != this_id;
+        const uint32_t sb = __ballot_sync(0xffffffffu, stop);
+        const uint32_t end = sb ? uint32_t(__ffs(sb) - 1) : 32u;
+        if (lane < end && d.clus[eb + i] > kMaxClustersPerModule) {
+          d.mid[eb + i] = int16_t(kInvId);
+          d.clus[eb + i] = int32_t(kInvId);
+        }
+        __syncwarp();
+        if (sb) break;
+      }
+      nclus = kMaxClustersPerModule;
+    }
+    for (int c = lane; c < kMaxClustersPerModule; c += 32) s_charge[c] = 0;
+    __syncwarp();
+    for (uint32_t i0 = first; i0 < n_el; i0 += 32) {
+      const uint32_t i = i0 + lane;
+      const bool stop = i >= n_el || d.mid[eb + i] != this_id;
+      const uint32_t sb = __ballot_sync(0xffffffffu, stop);
+      const uint32_t end = sb ? uint32_t(__ffs(sb) - 1) : 32u;
+      if (lane < end) {
+        const int32_t cl = d.clus[eb + i];
+        if (cl >= 1 && cl <= kMaxClustersPerModule) atomicAdd(&s_charge[cl - 1], d.adc[eb + i]);
+        else warn |= kWarnClusters;
+      }
+      if (sb) break;
+    }
+    __syncwarp();
+    const int32_t cut = this_id < 96 ? 2000 : 4000;
+    uint32_t carry = 0;
+    for (uint32_t c0 = 0; c0 < nclus; c0 += 32) {
+      const uint32_t c = c0 + lane;
+      const bool ok = c < nclus && s_charge[c] > cut;
+      const uint32_t b = __ballot_sync(0xffffffffu, ok);
+      if (c < nclus) { s_ok[c] = ok; s_new[c] = uint16_t(carry + __popc(b & ((lt << 1) | 1u))); }
+      carry += __popc(b);
+    }
+    __syncwarp();
+    if (carry == nclus) continue;  // nClus == newclusId[nClus]
+    if (lane == 0) cim[uint16_t(this_id)] = carry;
+    for (uint32_t c = lane; c < nclus; c += 32)
+      if (!s_ok[c]) s_new[c] = kInvId;
+    __syncwarp();
+    for (uint32_t i0 = first; i0 < n_el; i0 += 32) {
+      const uint32_t i = i0 + lane;
+      const int16_t id = i < n_el ? d.mid[eb + i] : int16_t(0);
+      const bool stop = i >= n_el || (id != int16_t(kInvId) && id != this_id);
+      const uint32_t sb = __ballot_sync(0xffffffffu, stop);
+      const uint32_t end = sb ? uint32_t(__ffs(sb) - 1) : 32u;
+      if (lane < end && id != int16_t(kInvId)) {
+        const int32_t cl = d.clus[eb + i];
+        if (cl >= 1 && cl <= kMaxClustersPerModule) {
+          const uint16_t nc = s_new[cl - 1];
+          d.clus[eb + i] = int32_t(nc);
+          if (nc == kInvId) d.mid[eb + i] = int16_t(kInvId);
+        } else {
+          warn |= kWarnClusters;
+        }
+      }
+      if (sb) break;
+    }
+    __syncwarp();
+  }
+  warn = __reduce_or_sync(0xffffffffu, warn);
+  if (lane == 0 && warn) atomic_or_warn(&d.ev[e], warn);
+}
+
 // fill_hits_module_start + nClusters, one block per event
 __global__ void k_hits_module_start(Dev d) {
   const int e = blockIdx.x;
   __shared__ uint32_t sh[33];
   uint32_t* cim = d.clus_in_module + size_t(e) * kMaxNumModules;
-  for (int i = threadIdx.x; i < kMaxNumModules; i += blockDim.x) cim[i] &= 0x7FFu;  // strip the position key
+  for (int i = threadIdx.x; i < kMaxNumModules; i += blockDim.x) cim[i] &= kCountMask;  // strip the position key
   __syncthreads();
   uint32_t* cms = d.clus_module_start + size_t(e) * (kMaxNumModules + 1);
   const uint32_t cap = d.hits_per_event;
@@ -649,6 +755,7 @@ void launch_cluster(const Dev& d, const Launch& L) {
   L.mark("find_clus_mid");
   k_find_clus_block<<<148 * 2, 256, 0, L.s>>>(d);
   L.mark("find_clus_block");
+  k_charge_cut_serial<<<d.E, 32, 0, L.s>>>(d);
   k_hits_module_start<<<d.E, 1024, 0, L.s>>>(d);
   L.mark("hits_module_start");
 }

@@ -43,15 +43,18 @@ __device__ __forceinline__ int32_t ld_i32(const uint8_t* p) {
 
 // One block per event: FedRawDataCollection directory (bin/ReadRAW.jl:23-31), then the
 // payload word counts in fedIds order (SiPixelRawToClusterCUDA.jl:75-131: skip FED 40,
-// skip empty FEDs, payload = bytes [8, size-8)).
+// skip empty FEDs, payload = bytes [8, size-8)). The directory is a chain of records whose
+// positions depend on every earlier size, so one thread follows it; the FED header and
+// trailer checks then run one FED per thread.
 __global__ void k_fed_table(Dev d, const int16_t* __restrict__ fed_slot_of) {
   const int e = blockIdx.x;
   const int NF = d.n_fed_slots;
   __shared__ uint64_t s_src[kMaxFedSlots];
   __shared__ uint32_t s_nw[kMaxFedSlots];
+  __shared__ int32_t s_len[kMaxFedSlots];
   __shared__ uint32_t sh[33];
   __shared__ uint32_t s_warn;
-  for (int f = threadIdx.x; f < NF; f += blockDim.x) { s_nw[f] = 0; s_src[f] = 0; }
+  for (int f = threadIdx.x; f < NF; f += blockDim.x) { s_nw[f] = 0; s_src[f] = 0; s_len[f] = 0; }
   if (threadIdx.x == 0) s_warn = 0;
   __syncthreads();
   const uint64_t off0 = d.ev_off[e], off1 = d.ev_off[e + 1];
@@ -72,6 +75,7 @@ __global__ void k_fed_table(Dev d, const int16_t* __restrict__ fed_slot_of) {
             uint32_t nw32 = nw64 == 0 ? 0u : (size >= 16 ? uint32_t(size - 16) / 4 : 0u);
             s_nw[slot] = nw32;
             s_src[slot] = off0 + p + 8 + 8;
+            s_len[slot] = size;
           }
         }
         p += 8 + uint64_t(size);
@@ -79,6 +83,26 @@ __global__ void k_fed_table(Dev d, const int16_t* __restrict__ fed_slot_of) {
     }
   }
   __syncthreads();
+  // Header and trailer checks (SiPixelRawToClusterCUDA.jl:90-128, ErrorChecker.jl:82-137). The
+  // reference's checker stores no error record (_includeErrors = false, ErrorChecker.jl:30-35):
+  // a header failing check() ends its loop silently and a foreign source id only prints. A header
+  // announcing more headers, a trailer failing check() or announcing more trailers, a
+  // fragment_length other than the FED's 64-bit word count, or a size that is not a whole
+  // number of 64-bit words make the reference raise; they set PXL_WARN_FED_FORMAT here and the
+  // payload [8, size - 8) is unpacked as on the valid path.
+  for (int f = threadIdx.x; f < NF; f += blockDim.x) {
+    const int32_t len = s_len[f];
+    if (len < 8) continue;  // empty FEDs are skipped (n_words == 0)
+    const uint8_t* fd = d.raw + s_src[f] - 8;  // the FED's data: header, payload, trailer
+    const uint32_t h0 = uint32_t(ld_i32(fd)), h1 = uint32_t(ld_i32(fd + 4));
+    const uint32_t t0 = uint32_t(ld_i32(fd + len - 8)), t1 = uint32_t(ld_i32(fd + len - 4));
+    bool raise = (len & 7) != 0 || len < 16;
+    if ((h1 >> 28) == 0x5u && ((h0 >> 3) & 1u)) raise = true;   // more_headers (fed_header.jl:177)
+    if ((t1 >> 28) != 0xAu) raise = true;                         // trailer check() (fed_trailer.jl:214)
+    else if ((t1 & 0xFFFFFFu) != uint32_t(len) / 8u) raise = true;  // fragment_length (fed_trailer.jl:193)
+    else if ((t0 >> 3) & 1u) raise = true;                        // more_trailers (fed_trailer.jl:201)
+    if (raise) atomicOr(&s_warn, kWarnFedFormat);
+  }
   uint32_t carry = 0;
   for (int b = 0; b < NF; b += blockDim.x) {
     int f = b + threadIdx.x;
@@ -101,7 +125,137 @@ __global__ void k_fed_table(Dev d, const int16_t* __restrict__ fed_slot_of) {
   }
 }
 
-// raw_to_digi_kernal + calib_digis for the words of one FED (blockIdx.x = FED slot).
+// raw_to_digi_kernal + calib_digis of one FED word ww: event-local word index local, global
+// digi index g, FED id fed + 1200.
+__device__ __forceinline__ void unpack_word(const Dev& d, int e, uint32_t local, uint64_t g, uint8_t fed, uint32_t ww) {
+  const Conditions& c = d.c;
+  int16_t xx = 0, yy = 0, mid = int16_t(kInvId);
+  int32_t adc = 0;
+  uint32_t pdigi = 0, rawid = 0;
+  d.clus[g] = int32_t(local + 1);  // count_modules: clus[i] = i
+  if (ww != 0) {
+    const uint32_t link = (ww >> 26) & 0x3Fu, roc = (ww >> 21) & 0x1Fu;
+    const uint32_t index = uint32_t(fed) * kMaxLink * kMaxRoc + (link - 1u) * kMaxRoc + roc + 1u;  // 1-based
+    // check_roc: only code 25 survives the reference's comparisons (SiPixelRawToClusterGPUKernel.jl:394-468)
+    const uint8_t etype = (roc == 25u) ? 25 : 0;
+    const bool skip_roc = roc < 8u ? false : (etype != 0);
+    bool keep = true;
+    if (d.include_errors && skip_roc) {
+      uint32_t pos = atomicAdd(&d.ev[e].n_errors, 1u);
+      uint32_t gp = atomicAdd(d.err_count, 1u);
+      if (gp < uint32_t(d.cap_words)) {
+        d.err[5 * size_t(gp) + 0] = uint32_t(e);
+        d.err[5 * size_t(gp) + 1] = local;
+        d.err[5 * size_t(gp) + 2] = 0xffffffffu;
+        d.err[5 * size_t(gp) + 3] = ww;
+        d.err[5 * size_t(gp) + 4] = 25u | (uint32_t(fed) << 8);
+      }
+      (void)pos;
+      keep = false;
+    }
+    uint64_t cab = 0;
+    if (keep) {
+      if (index < 1u || index > kCablingSize) { atomic_or_warn(&d.ev[e], kWarnModules); keep = false; }
+      else cab = c.cab[index - 1];
+    }
+    if (keep && d.use_quality && ((cab >> 56) & 1u)) keep = false;
+    if (keep) {
+      const uint32_t raw_id = uint32_t(cab);
+      const bool barrel = ((raw_id >> 25) & 0x7u) == 1u;
+      const uint32_t layer = barrel ? ((raw_id >> 20) & 0xFu) : 0u;
+      const uint32_t the_module = barrel ? ((raw_id >> 2) & 0x3FFu) : 0u;
+      const uint32_t panel = barrel ? 0u : ((raw_id >> 10) & 0x3u);
+      const int side = barrel ? ((the_module < 5u) ? -1 : 1) : ((panel == 1u) ? -1 : 1);
+      const uint32_t roc_in_det = uint32_t((cab >> 48) & 0xFFu);
+      int32_t row, col;
+      bool conv_err = false;
+      if (layer == 1u) {
+        col = int32_t((ww >> 15) & 0x3Fu);
+        row = int32_t((ww >> 8) & 0x7Fu);
+        if (d.include_errors && !(row < 80 && col < 52)) conv_err = true;
+      } else {
+        const int32_t dcol = int32_t((ww >> 16) & 0x1Fu), pxid = int32_t((ww >> 8) & 0xFFu);
+        row = 80 - pxid / 2;
+        col = dcol * 2 + pxid % 2;
+        if (row < 0) { atomic_or_warn(&d.ev[e], kWarnModules); keep = false; }
+        else if (d.include_errors && !((dcol < 26) & (2 <= pxid) & (pxid < 162))) conv_err = true;
+      }
+      if (keep && conv_err) {
+        atomicAdd(&d.ev[e].n_errors, 1u);
+        uint32_t gp = atomicAdd(d.err_count, 1u);
+        if (gp < uint32_t(d.cap_words)) {
+          d.err[5 * size_t(gp) + 0] = uint32_t(e);
+          d.err[5 * size_t(gp) + 1] = local;
+          d.err[5 * size_t(gp) + 2] = raw_id;
+          d.err[5 * size_t(gp) + 3] = ww;
+          d.err[5 * size_t(gp) + 4] = 37u | (uint32_t(fed) << 8);
+        }
+        keep = false;
+      }
+      if (keep) {
+        // frame_conversion, SiPixelRawToClusterGPUKernel.jl:271-350
+        int32_t sr, sc, ro, co;
+        const bool flip = barrel ? (side == -1 && layer != 1u) : true;
+        if (flip) {
+          if (roc_in_det < 8u) { sr = 1; sc = -1; ro = 0; co = (8 - int32_t(roc_in_det)) * 52 - 1; }
+          else { sr = -1; sc = 1; ro = 159; co = (int32_t(roc_in_det) - 8) * 52; }
+        } else {
+          if (roc_in_det < 8u) { sr = -1; sc = 1; ro = 159; co = int32_t(roc_in_det) * 52; }
+          else { sr = 1; sc = -1; ro = 0; co = (16 - int32_t(roc_in_det)) * 52 - 1; }
+        }
+        const int32_t grow = sr * row + ro, gcol = sc * col + co;
+        if (grow < 0 || gcol < 0) {
+          atomic_or_warn(&d.ev[e], kWarnModules);
+        } else {
+          xx = int16_t(grow);
+          yy = int16_t(gcol);
+          adc = int32_t(ww & 0xFFu);
+          const uint32_t a = uint32_t(adc) < 1023u ? uint32_t(adc) : 1023u;
+          pdigi = uint32_t(grow) | (uint32_t(gcol) << 11) | (a << 22);
+          mid = int16_t(uint32_t(cab >> 32) & 0xFFFFu);
+          rawid = raw_id;
+          // calib_digis, gpu_calib_pixel.jl:41-70, with get_ped_and_gain
+          if (mid != int16_t(kInvId) && (mid < 0 || mid >= kMaxNumModules)) {
+            atomic_or_warn(&d.ev[e], kWarnModules);  // the reference indexes its 2000-entry gain table out of range
+            mid = int16_t(kInvId);
+          }
+          if (mid != int16_t(kInvId)) {
+            const float cf = mid < 96 ? 50.f : 47.f;
+            const float off = mid < 96 ? -670.f : -60.f;
+            const int m = mid;
+            const uint32_t offset = c.gain_first[m] + uint32_t(int32_t(yy)) * c.gain_lcd[m] +
+                                    2u * (uint32_t(int32_t(xx)) / c.rows_avg);
+            const uint32_t kk = offset / 2;
+            if (kk >= c.n_gain_pairs) {
+              atomic_or_warn(&d.ev[e], kWarnModules);
+            } else {
+              const uint16_t pr = c.gain_pairs[kk];
+              const uint32_t sg = pr & 0xFFu, sp = pr >> 8;
+              const bool bad = sp == c.dead_flag || sp == c.noisy_flag;
+              const float ped = __fadd_rn(__fmul_rn(float(sp), c.ped_prec), c.min_ped);
+              const float gain = __fadd_rn(__fmul_rn(float(sg), c.gain_prec), c.min_gain);
+              if (bad) {
+                mid = int16_t(kInvId);
+                adc = 0;
+              } else {
+                const float vcal = __fsub_rn(__fmul_rn(float(adc), gain), __fmul_rn(ped, gain));
+                const float v = __fadd_rn(__fmul_rn(vcal, cf), off);
+                const int32_t t = int32_t(truncf(v));
+                adc = t > 100 ? t : 100;
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+  d.xx[g] = xx; d.yy[g] = yy; d.adc[g] = adc; d.mid[g] = mid; d.pdigi[g] = pdigi; d.rawid[g] = rawid;
+}
+
+// raw_to_digi_kernal + calib_digis for the words of one FED (blockIdx.x = FED slot). The payload
+// is read with 128-bit loads where it sits on 4-byte boundaries (always, for FED sizes in whole
+// 64-bit words): the words before the first 16-byte boundary and after the last one are read
+// singly, the rest four per thread.
 __global__ void k_unpack(Dev d) {
   const int f = blockIdx.x, e = blockIdx.y;
   const int NF = d.n_fed_slots;
@@ -117,133 +271,41 @@ __global__ void k_unpack(Dev d) {
   }
   const uint8_t* src = d.raw + d.fed_src[fs];
   const uint8_t fed = uint8_t(d.c.fed_ids[f] - 1200u);
-  const Conditions& c = d.c;
-  for (uint32_t k = threadIdx.x; k < nw; k += blockDim.x) {
-    const uint64_t g = gbase + k;
-    const uint32_t local = wo + k;
-    uint32_t ww;
-    memcpy(&ww, src + 4ull * k, 4);
-    int16_t xx = 0, yy = 0, mid = int16_t(kInvId);
-    int32_t adc = 0;
-    uint32_t pdigi = 0, rawid = 0;
-    d.clus[g] = int32_t(local + 1);  // count_modules: clus[i] = i
-    if (ww != 0) {
-      const uint32_t link = (ww >> 26) & 0x3Fu, roc = (ww >> 21) & 0x1Fu;
-      const uint32_t index = uint32_t(fed) * kMaxLink * kMaxRoc + (link - 1u) * kMaxRoc + roc + 1u;  // 1-based
-      // check_roc: only code 25 survives the reference's comparisons (SiPixelRawToClusterGPUKernel.jl:394-468)
-      const uint8_t etype = (roc == 25u) ? 25 : 0;
-      const bool skip_roc = roc < 8u ? false : (etype != 0);
-      bool keep = true;
-      if (d.include_errors && skip_roc) {
-        uint32_t pos = atomicAdd(&d.ev[e].n_errors, 1u);
-        uint32_t gp = atomicAdd(d.err_count, 1u);
-        if (gp < uint32_t(d.cap_words)) {
-          d.err[5 * size_t(gp) + 0] = uint32_t(e);
-          d.err[5 * size_t(gp) + 1] = local;
-          d.err[5 * size_t(gp) + 2] = 0xffffffffu;
-          d.err[5 * size_t(gp) + 3] = ww;
-          d.err[5 * size_t(gp) + 4] = 25u | (uint32_t(fed) << 8);
-        }
-        (void)pos;
-        keep = false;
-      }
-      uint64_t cab = 0;
-      if (keep) {
-        if (index < 1u || index > kCablingSize) { atomic_or_warn(&d.ev[e], kWarnModules); keep = false; }
-        else cab = c.cab[index - 1];
-      }
-      if (keep && d.use_quality && ((cab >> 56) & 1u)) keep = false;
-      if (keep) {
-        const uint32_t raw_id = uint32_t(cab);
-        const bool barrel = ((raw_id >> 25) & 0x7u) == 1u;
-        const uint32_t layer = barrel ? ((raw_id >> 20) & 0xFu) : 0u;
-        const uint32_t the_module = barrel ? ((raw_id >> 2) & 0x3FFu) : 0u;
-        const uint32_t panel = barrel ? 0u : ((raw_id >> 10) & 0x3u);
-        const int side = barrel ? ((the_module < 5u) ? -1 : 1) : ((panel == 1u) ? -1 : 1);
-        const uint32_t roc_in_det = uint32_t((cab >> 48) & 0xFFu);
-        int32_t row, col;
-        bool conv_err = false;
-        if (layer == 1u) {
-          col = int32_t((ww >> 15) & 0x3Fu);
-          row = int32_t((ww >> 8) & 0x7Fu);
-          if (d.include_errors && !(row < 80 && col < 52)) conv_err = true;
-        } else {
-          const int32_t dcol = int32_t((ww >> 16) & 0x1Fu), pxid = int32_t((ww >> 8) & 0xFFu);
-          row = 80 - pxid / 2;
-          col = dcol * 2 + pxid % 2;
-          if (row < 0) { atomic_or_warn(&d.ev[e], kWarnModules); keep = false; }
-          else if (d.include_errors && !((dcol < 26) & (2 <= pxid) & (pxid < 162))) conv_err = true;
-        }
-        if (keep && conv_err) {
-          atomicAdd(&d.ev[e].n_errors, 1u);
-          uint32_t gp = atomicAdd(d.err_count, 1u);
-          if (gp < uint32_t(d.cap_words)) {
-            d.err[5 * size_t(gp) + 0] = uint32_t(e);
-            d.err[5 * size_t(gp) + 1] = local;
-            d.err[5 * size_t(gp) + 2] = raw_id;
-            d.err[5 * size_t(gp) + 3] = ww;
-            d.err[5 * size_t(gp) + 4] = 37u | (uint32_t(fed) << 8);
-          }
-          keep = false;
-        }
-        if (keep) {
-          // frame_conversion, SiPixelRawToClusterGPUKernel.jl:271-350
-          int32_t sr, sc, ro, co;
-          const bool flip = barrel ? (side == -1 && layer != 1u) : true;
-          if (flip) {
-            if (roc_in_det < 8u) { sr = 1; sc = -1; ro = 0; co = (8 - int32_t(roc_in_det)) * 52 - 1; }
-            else { sr = -1; sc = 1; ro = 159; co = (int32_t(roc_in_det) - 8) * 52; }
-          } else {
-            if (roc_in_det < 8u) { sr = -1; sc = 1; ro = 159; co = int32_t(roc_in_det) * 52; }
-            else { sr = 1; sc = -1; ro = 0; co = (16 - int32_t(roc_in_det)) * 52 - 1; }
-          }
-          const int32_t grow = sr * row + ro, gcol = sc * col + co;
-          if (grow < 0 || gcol < 0) {
-            atomic_or_warn(&d.ev[e], kWarnModules);
-          } else {
-            xx = int16_t(grow);
-            yy = int16_t(gcol);
-            adc = int32_t(ww & 0xFFu);
-            const uint32_t a = uint32_t(adc) < 1023u ? uint32_t(adc) : 1023u;
-            pdigi = uint32_t(grow) | (uint32_t(gcol) << 11) | (a << 22);
-            mid = int16_t(uint32_t(cab >> 32) & 0xFFFFu);
-            rawid = raw_id;
-            // calib_digis, gpu_calib_pixel.jl:41-70, with get_ped_and_gain
-            if (mid != int16_t(kInvId) && (mid < 0 || mid >= kMaxNumModules)) {
-              atomic_or_warn(&d.ev[e], kWarnModules);  // the reference indexes its 2000-entry gain table out of range
-              mid = int16_t(kInvId);
-            }
-            if (mid != int16_t(kInvId)) {
-              const float cf = mid < 96 ? 50.f : 47.f;
-              const float off = mid < 96 ? -670.f : -60.f;
-              const int m = mid;
-              const uint32_t offset = c.gain_first[m] + uint32_t(int32_t(yy)) * c.gain_lcd[m] +
-                                      2u * (uint32_t(int32_t(xx)) / c.rows_avg);
-              const uint32_t kk = offset / 2;
-              if (kk >= c.n_gain_pairs) {
-                atomic_or_warn(&d.ev[e], kWarnModules);
-              } else {
-                const uint16_t pr = c.gain_pairs[kk];
-                const uint32_t sg = pr & 0xFFu, sp = pr >> 8;
-                const bool bad = sp == c.dead_flag || sp == c.noisy_flag;
-                const float ped = __fadd_rn(__fmul_rn(float(sp), c.ped_prec), c.min_ped);
-                const float gain = __fadd_rn(__fmul_rn(float(sg), c.gain_prec), c.min_gain);
-                if (bad) {
-                  mid = int16_t(kInvId);
-                  adc = 0;
-                } else {
-                  const float vcal = __fsub_rn(__fmul_rn(float(adc), gain), __fmul_rn(ped, gain));
-                  const float v = __fadd_rn(__fmul_rn(vcal, cf), off);
-                  const int32_t t = int32_t(truncf(v));
-                  adc = t > 100 ? t : 100;
-                }
-              }
-            }
-          }
-        }
-      }
+  // The reference stores one FED id per word pair (initialize_word_fed,
+  // SiPixelRawToClusterGPUKernel.jl:217-226): a FED ending on an odd word leaves its last word in
+  // a pair that the next non-empty FED writes (or none: id 0). Only FED sizes that are not whole
+  // 64-bit words, on which the reference raises, give odd word counts.
+  uint8_t fed_last = fed;
+  if ((wo + nw) & 1u) {
+    fed_last = 0;
+    for (int f2 = f + 1; f2 < NF; ++f2)
+      if (d.fed_nw[size_t(e) * NF + f2] > 0) { fed_last = uint8_t(d.c.fed_ids[f2] - 1200u); break; }
+  }
+  auto word = [&](uint32_t k, uint32_t ww) {
+    unpack_word(d, e, wo + k, gbase + k, k + 1 == nw ? fed_last : fed, ww);
+  };
+  if ((reinterpret_cast<uintptr_t>(src) & 3u) == 0) {
+    const uint32_t* src32 = reinterpret_cast<const uint32_t*>(src);
+    uint32_t head = uint32_t((16u - (reinterpret_cast<uintptr_t>(src) & 15u)) & 15u) >> 2;
+    head = head < nw ? head : nw;
+    if (threadIdx.x < head) word(threadIdx.x, __ldg(src32 + threadIdx.x));
+    const uint32_t nvec = (nw - head) >> 2;
+    const uint4* v = reinterpret_cast<const uint4*>(src32 + head);
+    for (uint32_t j = threadIdx.x; j < nvec; j += blockDim.x) {
+      const uint4 q = __ldg(v + j);
+      const uint32_t k = head + 4 * j;
+      word(k, q.x);
+      word(k + 1, q.y);
+      word(k + 2, q.z);
+      word(k + 3, q.w);
     }
-    d.xx[g] = xx; d.yy[g] = yy; d.adc[g] = adc; d.mid[g] = mid; d.pdigi[g] = pdigi; d.rawid[g] = rawid;
+    for (uint32_t k = head + 4 * nvec + threadIdx.x; k < nw; k += blockDim.x) word(k, __ldg(src32 + k));
+  } else {
+    for (uint32_t k = threadIdx.x; k < nw; k += blockDim.x) {
+      uint32_t ww;
+      memcpy(&ww, src + 4ull * k, 4);
+      word(k, ww);
+    }
   }
 }
 
@@ -287,7 +349,9 @@ __global__ void k_modstart_scan(Dev d) {
   }
   uint32_t* cim = d.clus_in_module + size_t(e) * kMaxNumModules;
   for (int i = threadIdx.x; i < kMaxNumModules; i += blockDim.x) cim[i] = 0;
+  for (int i = threadIdx.x; i < 64; i += blockDim.x) d.id_seen[size_t(e) * 64 + i] = 0;
   if (threadIdx.x == 0) {
+    d.ev[e].repeated_ids = 0;
     uint32_t nm = carry < uint32_t(kMaxNumModules) ? carry : uint32_t(kMaxNumModules);
     d.ev[e].n_modules = nm;
     d.module_start[size_t(e) * (kMaxNumModules + 1)] = nm;
@@ -315,6 +379,12 @@ __global__ void k_modstart_fill(Dev d) {
     if (fl) {
       uint32_t r = carry + ex;
       uint32_t i1 = wo + k + 1;  // 1-based digi index
+      // a module id starting a second run: the event's charge cut runs in serial order
+      const uint16_t id = uint16_t(d.mid[ebase + wo + k]);
+      if (id < 2048u) {
+        const uint32_t bit = 1u << (id & 31u);
+        if (atomicOr(&d.id_seen[size_t(e) * 64 + (id >> 5)], bit) & bit) d.ev[e].repeated_ids = 1;
+      }
       if (r < uint32_t(kMaxNumModules - 1)) ms[r + 1] = i1;
       else atomicMax(&ms[kMaxNumModules], i1);
     }

@@ -42,6 +42,7 @@ struct NoAllocScratch {
   uint32_t chunk_nmod[kMaxChunks];
   uint32_t clus_module_start[kMaxNumModules + 1];
   uint32_t big_list[kListHeader + kNumLists * kMaxNumModules];
+  uint32_t id_seen[64];
   uint32_t status;
 };
 
@@ -125,6 +126,7 @@ extern "C" int32_t pxl_clusterize_digis_noalloc(const uint16_t* id, const int16_
   d.fed_wo = s->chunk_wo;
   d.fed_nmod = s->chunk_nmod;
   d.status = &s->status;
+  d.id_seen = s->id_seen;
   d.mid = reinterpret_cast<int16_t*>(id_out);
   d.xx = const_cast<int16_t*>(x);
   d.yy = const_cast<int16_t*>(y);

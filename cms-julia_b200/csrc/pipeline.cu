@@ -218,7 +218,7 @@ int alloc_batch(PxlCtx* ctx) {
   A(fed_src, E * NF); A(fed_nw, E * NF); A(fed_wo, E * NF); A(fed_nmod, E * NF);
   A(xx, d.cap_words); A(yy, d.cap_words); A(adc, d.cap_words); A(mid, d.cap_words); A(clus, d.cap_words);
   A(pdigi, d.cap_words); A(rawid, d.cap_words);
-  A(err, 5 * d.cap_words); A(err_count, 1);
+  A(err, 5 * d.cap_words); A(err_count, 1); A(id_seen, E * 64);
   A(module_start, E * (kMaxNumModules + 1)); A(clus_in_module, E * kMaxNumModules); A(module_id, E * kMaxNumModules);
   A(clus_module_start, E * (kMaxNumModules + 1));
   A(xl, d.cap_hits); A(yl, d.cap_hits); A(xerr, d.cap_hits); A(yerr, d.cap_hits);

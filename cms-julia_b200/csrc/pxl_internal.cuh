@@ -39,6 +39,7 @@ enum : uint32_t {
   kWarnModules = 0x1u, kWarnPixels = 0x2u, kWarnClusters = 0x4u, kWarnHitsClamped = 0x8u,
   kWarnDoublets = 0x10u, kWarnColumns = 0x20u, kWarnTuples = 0x40u, kWarnFitDomain = 0x80u,
   kWarnFitsCapped = 0x100u, kWarnVertex = 0x200u, kWarnLists = 0x400u, kWarnBuffer = 0x800u,
+  kWarnFedFormat = 0x1000u,
 };
 
 struct DetParamsD {
@@ -91,6 +92,9 @@ struct EvInfo {
   uint32_t n_dup_cells, dup_cell_base;
   uint32_t n_cols_nb, n_cols_tr;    // non-empty neighbour / track lists (column store use)
   uint32_t n_fit3, n_fit4;          // tuples fitted with 3 and with 4 hits (fit5as4 included)
+  // 1 when a module id starts more than one module run (only corrupted data does that): the
+  // charge cut of such an event runs in the reference's serial order (k_charge_cut_serial)
+  uint32_t repeated_ids;
   // when the event found more tuples than it keeps: the hit offset where the last kept tuple's
   // hits really end (its visible size is 0, as the reference's overflowing bulk_finalize_fill
   // leaves it); 0 otherwise
@@ -137,6 +141,7 @@ struct Dev {
   // FED error records [cap_words]: raw_id, word, type | fed << 8
   uint32_t* err;
   uint32_t* err_count;  // per event
+  uint32_t* id_seen;    // [E][64] module ids that start a run (bit per id below 2048)
   // clusters, per event
   uint32_t* module_start;       // [E][2001]
   uint32_t* clus_in_module;     // [E][2000]

@@ -20,7 +20,7 @@ TUNE_STAGES = ("doublets", "hit_lists", "connect", "cell_lists", "fishbone", "nt
 WARN_BITS = {
     0x1: "modules", 0x2: "pixels_per_module", 0x4: "clusters_per_module", 0x8: "hits_clamped",
     0x10: "doublets", 0x20: "columns", 0x40: "tuples", 0x80: "fit_domain", 0x100: "fits_capped",
-    0x200: "vertex", 0x400: "lists", 0x800: "buffer",
+    0x200: "vertex", 0x400: "lists", 0x800: "buffer", 0x1000: "fed_format",
 }
 
 

@@ -48,6 +48,8 @@ extern "C" {
 #define PXL_WARN_VERTEX 0x200u         /* vertex finder assertion condition */
 #define PXL_WARN_LISTS 0x400u          /* a per-hit / per-cell list exceeded its row capacity */
 #define PXL_WARN_BUFFER 0x800u         /* batch buffer capacity exceeded: products incomplete */
+#define PXL_WARN_FED_FORMAT 0x1000u    /* a FED header / trailer / size on which the reference raises
+                                          (SiPixelRawToClusterCUDA.jl:104-128, ErrorChecker.jl:116-137) */
 
 /* stage mask for the producer boundary */
 #define PXL_STAGE_DIGIS 0x1u     /* SiPixelRawToClusterCUDA: digis + clusters */

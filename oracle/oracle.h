@@ -218,6 +218,7 @@ enum Flags : uint32_t {
   kFlagFitsCapped = 1u << 8,
   kFlagVertexAssert = 1u << 9,
   kFlagNeighbourOverflow = 1u << 10,
+  kFlagFedFormat = 1u << 12,  // a FED header / trailer condition on which the reference raises
 };
 
 struct Options {
@@ -231,7 +232,7 @@ void raw_to_clusters(const Conditions& c, const uint8_t* raw_event, size_t nbyte
 // reference's clustering test drives them (test/gpu_clustering_t.jl:245-280).
 void clusterize_digis(const uint16_t* id, const int16_t* x, const int16_t* y, const int32_t* adc, int n,
                       uint32_t* module_start, uint32_t* clus_in_module, uint32_t* module_id, int32_t* clus,
-                      uint16_t* id_out, int apply_charge_cut);
+                      uint16_t* id_out, int apply_charge_cut, uint32_t* flags = nullptr);
 void make_hits(const Conditions& c, EventOut& ev);
 void ca_tuples(const Conditions& c, EventOut& ev);
 void fit_tuples(const Conditions& c, EventOut& ev);

@@ -180,12 +180,30 @@ void raw_to_clusters(const Conditions& c, const uint8_t* raw, size_t nbytes, con
     uint32_t n_words = uint32_t(len) / 8;
     if (n_words == 0) continue;
     const uint8_t* d = raw + fd.first;
-    // header: check() = event_id >> 28 == 0x5; more_headers would make the reference
-    // index an undefined name, so a header announcing more headers is flagged.
+    // Header and trailer checks, SiPixelRawToClusterCUDA.jl:90-128 with ErrorChecker.jl:82-137.
+    // The reference's ErrorChecker is built with _includeErrors = false (ErrorChecker.jl:30-35),
+    // so these checks store no error record. A header that fails check() (event_id >> 28 != 0x5,
+    // fed_header.jl:182) ends the header loop silently; a source id other than the FED's only
+    // prints (ErrorChecker.jl:90). The other failures make the reference raise: a header announcing
+    // more headers or a trailer announcing more trailers indexes the undefined name rawData
+    // (SiPixelRawToClusterCUDA.jl:110, :120); a trailer failing check() (event_size >> 28 != 0xA,
+    // fed_trailer.jl:214) or whose fragment_length (event_size & 0xFFFFFF) differs from the FED's
+    // 64-bit word count prints the undefined name fedId (ErrorChecker.jl:125, :129); a FED size
+    // that is not a whole number of 64-bit words fails the payload assertions
+    // (SiPixelRawToClusterCUDA.jl:126-128). Those raise conditions are flagged and the payload
+    // [8, size - 8) is unpacked as on the valid path.
     uint32_t h0, h1, t0, t1;
     std::memcpy(&h0, d, 4); std::memcpy(&h1, d + 4, 4);
     std::memcpy(&t0, d + len - 8, 4); std::memcpy(&t1, d + len - 4, 4);
-    uint32_t num_word32 = uint32_t(len - 16) / 4;
+    {
+      bool raise = len % 8 != 0 || len < 16;
+      if ((h1 >> 28) == 0x5u && ((h0 >> 3) & 1u)) raise = true;  // more_headers
+      if ((t1 >> 28) != 0xAu) raise = true;                        // trailer check()
+      else if ((t1 & 0xFFFFFFu) != n_words) raise = true;          // fragment_length
+      else if ((t0 >> 3) & 1u) raise = true;                       // more_trailers
+      if (raise) ev.flags |= kFlagFedFormat;
+    }
+    uint32_t num_word32 = len >= 16 ? uint32_t(len - 16) / 4 : 0u;
     size_t base = ev.words.size();
     ev.words.resize(base + num_word32);
     std::memcpy(ev.words.data() + base, d + 8, size_t(num_word32) * 4);
@@ -196,6 +214,9 @@ void raw_to_clusters(const Conditions& c, const uint8_t* raw, size_t nbytes, con
     (void)h0; (void)h1; (void)t0; (void)t1;
   }
   ev.word_counter = wc;
+  // a pair no FED writes (after a last FED with an odd word count, a size on which the reference
+  // raises) reads as id 0 here; the reference reads what an earlier event left there
+  if (ev.fed_id_pairs.size() < (wc + 1) / 2) ev.fed_id_pairs.resize((wc + 1) / 2, 0);
   uint32_t n = wc;
   ev.xx.assign(n, 0); ev.yy.assign(n, 0); ev.adc.assign(n, 0); ev.pdigi.assign(n, 0); ev.raw_id_arr.assign(n, 0);
   ev.module_ind.assign(n, int16_t(kInvId)); ev.clus.assign(n, 0);
@@ -291,7 +312,7 @@ void raw_to_clusters(const Conditions& c, const uint8_t* raw, size_t nbytes, con
   std::vector<uint16_t> idv(n);
   for (uint32_t i = 0; i < n; ++i) idv[i] = uint16_t(ev.module_ind[i]);
   clusterize_digis(idv.data(), ev.xx.data(), ev.yy.data(), ev.adc.data(), int(n), ev.module_start, ev.clus_in_module,
-                   ev.module_id, ev.clus.data(), idv.data(), 1);
+                   ev.module_id, ev.clus.data(), idv.data(), 1, &ev.flags);
   for (uint32_t i = 0; i < n; ++i) ev.module_ind[i] = int16_t(idv[i]);
   ev.n_modules = ev.module_start[0];
 
@@ -310,7 +331,7 @@ void raw_to_clusters(const Conditions& c, const uint8_t* raw, size_t nbytes, con
 // reference's 1-based meaning (digi index i+1, cluster numbers from 1).
 void clusterize_digis(const uint16_t* id_in, const int16_t* x, const int16_t* y, const int32_t* adc, int n,
                       uint32_t* module_start, uint32_t* clus_in_module, uint32_t* module_id, int32_t* clus,
-                      uint16_t* id, int apply_charge_cut) {
+                      uint16_t* id, int apply_charge_cut, uint32_t* flags) {
   if (id != id_in) std::memcpy(id, id_in, sizeof(uint16_t) * size_t(n));
   // count_modules
   module_start[0] = 0;
@@ -441,7 +462,10 @@ void clusterize_digis(const uint16_t* id_in, const int16_t* x, const int16_t* y,
     for (int i = first_pixel; i <= n; ++i) {
       if (id[i - 1] != this_id) break;
       int32_t cl = clus[i - 1];
+      // an id past 1024 (a run with more clusters than the count its id's last run left)
+      // indexes the reference's charge buffer out of bounds: it raises
       if (cl >= 1 && cl <= kMaxClustersPerModule) charge[cl - 1] += adc[i - 1];
+      else if (flags) *flags |= kFlagClustersPerModule;
     }
     int32_t cut = this_id < 96 ? 2000 : 4000;
     for (uint32_t i = 0; i < nclus; ++i) { ok[i] = charge[i] > cut ? 1 : 0; newclus[i] = ok[i]; }
@@ -453,7 +477,13 @@ void clusterize_digis(const uint16_t* id_in, const int16_t* x, const int16_t* y,
       if (id[i - 1] == kInvId) continue;
       if (id[i - 1] != this_id) break;
       int32_t cl = clus[i - 1];
-      if (cl < 1 || cl > int32_t(nclus)) continue;
+      // newclus keeps the numbers of the module cut before this one beyond nclus: a run whose
+      // own clusters outnumber the count its id's last run left reads them, as the reference
+      // reads its per-event newclusId buffer; past 1024 the reference raises
+      if (cl < 1 || cl > kMaxClustersPerModule) {
+        if (flags) *flags |= kFlagClustersPerModule;
+        continue;
+      }
       clus[i - 1] = newclus[cl - 1];
       if (clus[i - 1] == kInvId) id[i - 1] = kInvId;
     }
