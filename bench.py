@@ -204,13 +204,18 @@ def bench_uneven(args, local: int, rank: int, world: int, plain_value: float) ->
     parity = {"events": E, "caps": "extended"}
     prod_err = {}
     orc = None
+    good = 0
     if not args.no_parity:
         from oracle import oracle
         from oracle.compare import compare_event
         orc = oracle.Oracle(conds, oracle.EXTENDED_CAPS)
+        _, ocnt = orc.run_batch(blob, offs, os.cpu_count() or 1, counts=True)
+        expected = validator_counts(ocnt)
     for k in range(2):
         chain.launch_slot(k, sh)
         warn |= chain.sync()
+        if orc is not None:
+            good += chain.validate_counts(expected[k * H:(k + 1) * H])[0]
         for e in range(H):
             counts.append(chain.counts(e))
             if orc is not None and k * H + e in big:
@@ -222,11 +227,10 @@ def bench_uneven(args, local: int, rank: int, world: int, plain_value: float) ->
     chain.close()
     if orc is not None:
         from oracle.compare import compare_counts
-        _, ocnt = orc.run_batch(blob, offs, os.cpu_count() or 1, counts=True)
         bad = compare_counts(counts, ocnt)
         parity.update({"count_mismatch_events": len(bad), "first_mismatch": bad[:5],
                        "product_sample": sorted(big), "product_mismatch_events": len(prod_err),
-                       "product_errors": prod_err})
+                       "product_errors": prod_err, "validator": {"validated_events": E, "good_events": good}})
     tot = {"digis_min": 10 ** 9, "digis_max": 0, "hits": 0, "cells": 0, "tuples": 0, "vertices": 0,
            "capped_events": 0, "buffer_overflow_events": 0}
     from pixeltrack._native import WARN_BITS
@@ -417,14 +421,28 @@ def bench_adjoint(args, local: int, rank: int, world: int) -> dict:
             "dtype": "f64 arithmetic, f32 outputs, f64 alignment accumulation"}
 
 
+def validator_counts(ocnt: np.ndarray) -> np.ndarray:
+    """The oracle's counts written to the reference's count files and read back: (n, 5)
+    modules, digis, clusters, tracks, vertices per event, the CountValidator's expectation."""
+    import tempfile
+    from oracle import oracle
+    from pixeltrack.formats import read_counts, write_counts
+    ix = [oracle.COUNT_NAMES.index(k) for k in ("n_modules", "n_words", "n_clusters", "n_tracks", "nv_final")]
+    with tempfile.TemporaryDirectory() as d:
+        write_counts(d, ocnt[:, ix])
+        return read_counts(d)
+
+
 def pu50_parity(chain, conds, blob, offs, E: int) -> dict:
     """Every event's counts against the oracle (all host threads), and every product of a few
-    events (first, middle, last and the three largest), on the chain's last run."""
+    events (first, middle, last and the three largest), on the chain's last run; the
+    CountValidator over the batch with the oracle's counts as its count files."""
     from oracle import oracle
     from oracle.compare import compare_counts, compare_event
     orc = oracle.Oracle(conds)
     _, ocnt = orc.run_batch(blob, offs, os.cpu_count() or 1, counts=True)
     bad = compare_counts([chain.counts(e) for e in range(E)], ocnt)
+    good, _ = chain.validate_counts(validator_counts(ocnt))
     sample = sorted({0, E // 2, E - 1, *np.argsort(np.diff(offs))[-3:].tolist()})
     prod_err = {}
     for e in sample:
@@ -433,7 +451,8 @@ def pu50_parity(chain, conds, blob, offs, E: int) -> dict:
         if errs:
             prod_err[e] = errs[:3]
     return {"events": E, "caps": "reference", "count_mismatch_events": len(bad), "first_mismatch": bad[:5],
-            "product_sample": sample, "product_mismatch_events": len(prod_err), "product_errors": prod_err}
+            "product_sample": sample, "product_mismatch_events": len(prod_err), "product_errors": prod_err,
+            "validator": {"validated_events": E, "good_events": good}}
 
 
 def oracle_fit_sample(w: dict, m: int):

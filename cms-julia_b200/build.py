@@ -32,6 +32,7 @@ CUDA_SOURCES = [
     "k_select.cu",
     "k_products.cu",
     "k_export.cu",
+    "k_validate.cu",
     "noalloc.cu",
     "pipeline.cu",
 ]

@@ -48,6 +48,9 @@ struct PxlCtx {
   // pxl_export_async: two alternating device export sets (allocated by the first call)
   pxl::ExportSet exp[2];
   int exp_next = 0;
+  // pxl_validate_counts: expected counts and per-event status (allocated by the first call)
+  uint32_t* val_expected = nullptr;
+  uint32_t* val_status = nullptr;
 };
 
 // reads the events' counters back (synchronises the context stream)

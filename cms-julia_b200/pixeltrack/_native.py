@@ -89,6 +89,7 @@ _SIGS = {
     "pxl_export_async": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(PxlExport), ctypes.c_void_p,
                                           ctypes.c_void_p]),
     "pxl_export_bytes": (ctypes.c_int64, [ctypes.POINTER(PxlExport), ctypes.c_int32]),
+    "pxl_validate_counts": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]),
     "pxl_results_async": (ctypes.c_int64, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]),
     "pxl_profile_enable": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_int32]),
     "pxl_profile_read": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_float),

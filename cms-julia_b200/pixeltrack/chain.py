@@ -173,6 +173,16 @@ class PixelChain:
         one copy per array (pxl_export_async); read `out` after copy_stream reaches the copies."""
         check(self._lib.pxl_export_async(self._h, ctypes.byref(out.desc), stream, copy_stream), "pxl_export_async")
 
+    def validate_counts(self, expected: np.ndarray) -> tuple[int, np.ndarray]:
+        """CountValidator over the last run's events (pxl_validate_counts): expected (n, 5) =
+        modules, digis, clusters, tracks, vertices per event (formats.read_counts layout).
+        Returns (good events, per-event status: failed-check bits | N(track) << 8)."""
+        x = np.ascontiguousarray(expected, dtype=np.uint32).reshape(-1, 5)
+        st = np.zeros(len(x), np.uint32)
+        good = check(self._lib.pxl_validate_counts(self._h, x.ctypes.data, len(x), st.ctypes.data),
+                     "pxl_validate_counts")
+        return good, st
+
     def sync(self) -> int:
         return check(self._lib.pxl_sync(self._h), "pxl_sync")
 

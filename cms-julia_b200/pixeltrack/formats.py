@@ -91,10 +91,27 @@ def write_conditions(data_dir: str | Path, conds: dict[str, bytes]) -> None:
         (d / name).write_bytes(conds[name])
 
 
-def read_counts(data_dir: str | Path) -> dict[str, np.ndarray]:
-    """Validation counts (CountValidator inputs): per event (nModules, nDigis, nClusters),
-    nTracks, nVertices."""
+COUNT_FILES = ("digicluster.bin", "tracks.bin", "vertices.bin")
+
+
+def read_counts(data_dir: str | Path) -> np.ndarray:
+    """Validation counts (the CountValidator's inputs, read as ReadRAW.jl:47-59 reads them, one
+    record per event in event order): (n_events, 5) uint32 = nModules, nDigis, nClusters (from
+    digicluster.bin), nTracks (tracks.bin), nVertices (vertices.bin)."""
     d = Path(data_dir)
-    dc = np.fromfile(d / "digicluster.bin", dtype=np.uint32).reshape(-1, 3)
-    return {"digicluster": dc, "tracks": np.fromfile(d / "tracks.bin", dtype=np.uint32),
-            "vertices": np.fromfile(d / "vertices.bin", dtype=np.uint32)}
+    dc = np.fromfile(d / "digicluster.bin", dtype="<u4").reshape(-1, 3)
+    tr = np.fromfile(d / "tracks.bin", dtype="<u4")
+    vx = np.fromfile(d / "vertices.bin", dtype="<u4")
+    if not (len(dc) == len(tr) == len(vx)):
+        raise ValueError(f"count files disagree on the event count: {len(dc)}, {len(tr)}, {len(vx)}")
+    return np.column_stack([dc, tr, vx]).astype(np.uint32)
+
+
+def write_counts(data_dir: str | Path, counts: np.ndarray) -> None:
+    """Writes the three count files for (n_events, 5) counts (the read_counts layout)."""
+    d = Path(data_dir)
+    d.mkdir(parents=True, exist_ok=True)
+    c = np.ascontiguousarray(counts, dtype="<u4").reshape(-1, 5)
+    np.ascontiguousarray(c[:, :3]).tofile(d / "digicluster.bin")
+    np.ascontiguousarray(c[:, 3]).tofile(d / "tracks.bin")
+    np.ascontiguousarray(c[:, 4]).tofile(d / "vertices.bin")

@@ -269,6 +269,16 @@ int32_t pxl_export_async(PxlCtx* ctx, const PxlExport* out, void* stream, void* 
 /* Bytes that pxl_export_async copies for `out` and a batch of n_events. */
 int64_t pxl_export_bytes(const PxlExport* out, int32_t n_events);
 
+/* CountValidator (plugin-Validation/count_to_validator.jl:18-84) on the device, over every
+ * event of the last run. expected[5 * n_events]: per event n_modules, n_digis, n_clusters
+ * (digicluster.bin), n_tracks (tracks.bin) and n_vertices (vertices.bin), the count files
+ * bin/ReadRAW.jl:47-59 reads. An event is good when its modules, digis and clusters are equal,
+ * its N(track) (tuples with hits, the TrackSOA loop of :50-55) is within a relative 0.012 and its
+ * vertex count is equal. status[n_events] (may be NULL) receives per event the failed checks (bit 0
+ * modules, 1 digis, 2 clusters, 3 tracks, 4 vertices) | N(track) << 8. Returns the number of good
+ * events, or < 0; synchronises. n_events must be the last run's event count. */
+int32_t pxl_validate_counts(PxlCtx* ctx, const uint32_t* expected, int32_t n_events, uint32_t* status);
+
 /* Number of kernel nodes in the captured graph (the kernels one replay launches). */
 int32_t pxl_graph_kernel_nodes(PxlCtx* ctx);
 

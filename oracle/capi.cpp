@@ -33,11 +33,15 @@ int64_t put_arr(const T* v, size_t n, void* dst, int64_t max_bytes) {
 
 // The per-event counts: the tuples are those the container keeps (at most the capacity, the
 // last one of an overflowing container holding no hits), not the raw counter.
+// The last count is the CountValidator's N(track): the TrackSOA's tuples with hits
+// (count_to_validator.jl:50-55).
 void event_counts(const EventOut& e, uint32_t* v) {
   const uint32_t nt = std::min(e.n_tuples, e.caps.tuples);
   const uint32_t nth = e.tuple_off.empty() ? 0u : e.tuple_off[nt] - 1;
-  const uint32_t c[11] = {e.word_counter, e.n_modules, e.n_clusters, e.n_hits, e.n_cells, nt, nth,
-                          e.nv_final, e.n_vtx_tracks, e.flags, uint32_t(e.errors.size())};
+  uint32_t with_hits = 0;
+  for (uint32_t t = 0; t < nt; ++t) with_hits += e.tuple_off[t + 1] > e.tuple_off[t];
+  const uint32_t c[12] = {e.word_counter, e.n_modules, e.n_clusters, e.n_hits, e.n_cells, nt, nth,
+                          e.nv_final, e.n_vtx_tracks, e.flags, uint32_t(e.errors.size()), with_hits};
   std::memcpy(v, c, sizeof(c));
 }
 
@@ -89,10 +93,10 @@ int32_t orc_run_event(OrcCtx* c, const uint8_t* raw, size_t nbytes, int32_t stag
 }
 
 // counts: word_counter, n_modules, n_clusters, n_hits, n_cells, n_tuples, n_tuple_hits,
-// nv_final, n_vtx_tracks, flags, n_errors
+// nv_final, n_vtx_tracks, flags, n_errors, n_tracks
 int32_t orc_counts(OrcCtx* c, uint32_t* out) {
   event_counts(c->ev, out);
-  return 11;
+  return 12;
 }
 
 // Copies a named product into dst (at most max_bytes); returns the element count, or -1.
@@ -226,7 +230,7 @@ int32_t orc_bl_fit(const double* hits, const float* ge, int32_t n, double B, dou
 
 // Runs the full chain over events with n_threads host threads (event-parallel, like the
 // reference's stream threads). Returns elapsed seconds; per-event counts go to
-// counts[n_events * 11] when non-null.
+// counts[n_events * 12] when non-null.
 double orc_run_batch(OrcCtx* c, const uint8_t* blob, const uint64_t* offsets, int32_t n_events, int32_t n_threads,
                      int32_t stage_mask, uint32_t* counts) {
   int nt = n_threads > 0 ? n_threads : 1;
@@ -239,7 +243,7 @@ double orc_run_batch(OrcCtx* c, const uint8_t* blob, const uint64_t* offsets, in
       EventOut ev;
       for (int e = t; e < n_events; e += nt) {
         run_event(c->cond, o, blob + offsets[e], size_t(offsets[e + 1] - offsets[e]), ev);
-        if (counts) event_counts(ev, counts + size_t(e) * 11);
+        if (counts) event_counts(ev, counts + size_t(e) * 12);
       }
     });
   }

@@ -30,7 +30,7 @@ DTYPES = {
     "ptv2": np.float32, "ndof": np.int32, "sort_ind": np.uint16, "errors": np.uint32,
 }
 COUNT_NAMES = ("n_words", "n_modules", "n_clusters", "n_hits", "n_cells", "n_tuples", "n_tuple_hits", "nv_final",
-               "n_vtx_tracks", "flags", "n_errors")
+               "n_vtx_tracks", "flags", "n_errors", "n_tracks")
 
 # Per-event capacities of the extended mode (hits, doublets, tuples, fits per multiplicity,
 # list columns): no pileup-200 event of the synthetic generator reaches them. The reference's
@@ -111,7 +111,7 @@ class Oracle:
         return self._l.orc_run_event(self._h, buf.ctypes.data, buf.nbytes, stages)
 
     def counts(self) -> dict[str, int]:
-        out = (ctypes.c_uint32 * 11)()
+        out = (ctypes.c_uint32 * len(COUNT_NAMES))()
         self._l.orc_counts(self._h, out)
         return dict(zip(COUNT_NAMES, list(out)))
 
@@ -129,7 +129,7 @@ class Oracle:
         blob = np.ascontiguousarray(blob, np.uint8)
         offsets = np.ascontiguousarray(offsets, np.uint64)
         n = len(offsets) - 1
-        cnt = np.zeros((n, 11), np.uint32) if counts else None
+        cnt = np.zeros((n, len(COUNT_NAMES)), np.uint32) if counts else None
         dt = self._l.orc_run_batch(self._h, blob.ctypes.data, offsets.ctypes.data, n, threads, stages,
                                    cnt.ctypes.data if counts else None)
         return (dt, cnt) if counts else dt

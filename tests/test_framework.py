@@ -54,3 +54,23 @@ def test_conditions_roundtrip(tmp_path, conditions):
         cls(str(tmp_path)).produce(es)
     assert es.get(producers.SiPixelFedIds).fed_ids[0] == 1200
     assert abs(es.get(producers.BeamSpotPOD).z - 0.3) < 1e-6
+
+
+def test_count_files_roundtrip(tmp_path, conditions, events_pu50):
+    """The count files (digicluster.bin, tracks.bin, vertices.bin, read as ReadRAW.jl:47-59 reads
+    them) written from the oracle's counts of the events read back record by record."""
+    import pytest
+    from oracle import oracle
+    from pixeltrack.formats import read_counts, write_counts
+    blob, offs = events_pu50
+    _, cnt = oracle.Oracle(conditions).run_batch(blob, offs, 2, counts=True)
+    ix = [oracle.COUNT_NAMES.index(k) for k in ("n_modules", "n_words", "n_clusters", "n_tracks", "nv_final")]
+    counts = cnt[:, ix]
+    write_counts(tmp_path, counts)
+    assert (tmp_path / "digicluster.bin").stat().st_size == 12 * len(counts)
+    assert (tmp_path / "tracks.bin").stat().st_size == 4 * len(counts)
+    assert np.array_equal(read_counts(tmp_path), counts)
+    assert np.all(counts[:, 3] > 0) and np.all(counts[:, 4] > 0)
+    (tmp_path / "vertices.bin").write_bytes(b"\0" * 4)
+    with pytest.raises(ValueError):
+        read_counts(tmp_path)
