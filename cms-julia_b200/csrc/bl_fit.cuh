@@ -436,8 +436,12 @@ BL_HD void line_fit(const float ge[6][N], const Geo<N, T>& G, T B, const Prep<N,
   L.chi2 = double(chi2);
 }
 
-// Karimaki translation of (phi, d, rho) and its covariance to a point (x0, y0) (broken_line.jl:85-127)
-BL_HD void translate_karimaki(CircleOut& c, double x0, double y0) {
+// Karimaki translation of (phi, d, rho) and its covariance to a point (x0, y0) (broken_line.jl:85-127).
+// With rot, the fit ran in a frame rotated by -theta (cos, sin = cr, sr): the direction vector
+// (C, BB) is turned back by theta before phi is taken, so phi comes out in the global frame and
+// on the reference's atan2 branch; d, rho and the covariance do not depend on the frame.
+BL_HD void translate_karimaki(CircleOut& c, double x0, double y0, bool rot = false, double cr = 1.0,
+                              double sr = 0.0) {
   const double p1 = c.par[0], p2 = c.par[1], p3 = c.par[2];
   double sn, cs;
   sincos(p1, &sn, &cs);
@@ -456,7 +460,8 @@ BL_HD void translate_karimaki(CircleOut& c, double x0, double y0) {
   const double J[3][3] = {{xi * uu * v, -xi * (p3 * p3) * DP, xi * DP},
                           {2.0 * mu * uu * DP, 2.0 * mu * v, mu * zeta - lambda * A},
                           {0.0, 0.0, 1.0}};
-  c.par[0] = bl_atan2<double>(BB, C);
+  if (rot) c.par[0] = bl_atan2<double>(C * sr + BB * cr, C * cr - BB * sr);
+  else c.par[0] = bl_atan2<double>(BB, C);
   c.par[1] = A / (1.0 + U);
   sandwich3(J, c.cov);
 }
@@ -510,10 +515,11 @@ BL_HD void circle_system(const float ge[6][N], const Geo<N, T>& G, const Prep<N,
   u[N] = ue[N];
 }
 
-// BL_Circle_fit (broken_line.jl:330-528); returns false where the reference raises
+// BL_Circle_fit (broken_line.jl:330-528); returns false where the reference raises. rot, cr,
+// sr: the frame rotation of the hits (fit_track), undone on phi.
 template <int N, class T>
 BL_HD bool circle_fit(const float ge[6][N], const Geo<N, T>& G, T B, const Prep<N, T>& P,
-                                           CircleOut& c) {
+                                           CircleOut& c, bool rot = false, double cr = 1.0, double sr = 0.0) {
   bool ok = true;
   c.q = P.q;
   const T ms_scale = T(1.0) + P.slope * P.slope;
@@ -553,7 +559,7 @@ BL_HD bool circle_fit(const float ge[6][N], const Geo<N, T>& G, T B, const Prep<
   sandwich3(J, c.cov);
   translate_karimaki(c, 0.5 * emd0, 0.5 * emd1);
   c.cov[0][0] += double(ms_scale * mult_scatt<T>(P.S[1] - P.S[0], B, P.R, P.slope));
-  translate_karimaki(c, G.h0[0] + dv0, G.h0[1] + dv1);
+  translate_karimaki(c, G.h0[0] + dv0, G.h0[1] + dv1, rot, cr, sr);
   T chi2 = 0;
 #pragma unroll
   for (int i = 0; i < N; ++i) {
@@ -575,15 +581,70 @@ struct TrackOut {
   double chi2_line, chi2_circle, pt, eta;
 };
 
-// full fit of one track of N hits: hits[3][N] (FP64 inputs), ge[6][N] (Float32)
+// The hits and their global covariances turned about the origin by -theta, the angle of the
+// chord from the first to the last hit in the transverse plane (cos, sin -> cr, sr), in FP64.
+// zero_tiny: global covariance entries below 1e-12 are zeroed first, as the broken-line fit
+// of the reference zeroes them.
+template <int N>
+BL_HD void chord_frame(const double hits[3][N], const float ge_in[6][N], bool zero_tiny, double hr[3][N],
+                       float ge[6][N], double& cr, double& sr) {
+  const double dx = hits[0][N - 1] - hits[0][0], dy = hits[1][N - 1] - hits[1][0];
+  const double l = sqrt(dx * dx + dy * dy);
+  cr = 1.0;
+  sr = 0.0;
+  if (l > 0) { cr = dx / l; sr = dy / l; }
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    hr[0][i] = cr * hits[0][i] + sr * hits[1][i];
+    hr[1][i] = cr * hits[1][i] - sr * hits[0][i];
+    hr[2][i] = hits[2][i];
+    auto z = [&](float v) { return zero_tiny && fabs(double(v)) < 1e-12 ? 0.0 : double(v); };
+    const double xx = z(ge_in[0][i]), xy = z(ge_in[1][i]), yy = z(ge_in[2][i]);
+    const double xz = z(ge_in[3][i]), yz = z(ge_in[4][i]);
+    ge[0][i] = float(cr * cr * xx + 2 * cr * sr * xy + sr * sr * yy);
+    ge[1][i] = float((cr * cr - sr * sr) * xy + cr * sr * (yy - xx));
+    ge[2][i] = float(sr * sr * xx - 2 * cr * sr * xy + cr * cr * yy);
+    ge[3][i] = float(cr * xz + sr * yz);
+    ge[4][i] = float(cr * yz - sr * xz);
+    ge[5][i] = ge_in[5][i];
+  }
+}
+
+// full fit of one track of N hits: hits[3][N] (FP64 inputs), ge[6][N] (Float32).
+// The FP32 fit (T = float) works in the chord frame: the transverse plane turned about the
+// origin so that the chord from the first to the last hit lies along x. A hit's offset from
+// hit 0 then has a large component along the chord but a small one across it, of the order of
+// the sagitta; rounding the offsets to FP32 costs the across component, which carries the
+// curvature, almost nothing (in the global frame a 30 cm offset rounds by 2e-6 cm, 3e-5 of a
+// 10 GeV track's sagitta). The rotation, the offsets and the hit covariances are turned in FP64
+// (global entries below 1e-12 zeroed first, as the reference zeroes them) and phi is turned back
+// in the last Karimaki translation; everything else is invariant under the rotation.
 template <int N, class T>
-BL_HD bool fit_track(const double hits[3][N], const float ge[6][N], double Bd, TrackOut& o) {
+BL_HD bool fit_track(const double hits[3][N], const float ge_in[6][N], double Bd, TrackOut& o) {
   Geo<N, T> G;
+  constexpr bool rot = sizeof(T) == 4;
+  double cr = 1.0, sr = 0.0;
+  float ge[6][N];
+  if constexpr (rot) {
+    double hr[3][N];
+    chord_frame<N>(hits, ge_in, true, hr, ge, cr, sr);
 #pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    G.h0[a] = hits[a][0];
+    for (int a = 0; a < 3; ++a) {
+      G.h0[a] = hr[a][0];
 #pragma unroll
-    for (int i = 0; i < N; ++i) G.p[a][i] = T(hits[a][i] - hits[a][0]);
+      for (int i = 0; i < N; ++i) G.p[a][i] = T(hr[a][i] - hr[a][0]);
+    }
+  } else {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      G.h0[a] = hits[a][0];
+#pragma unroll
+      for (int i = 0; i < N; ++i) G.p[a][i] = T(hits[a][i] - hits[a][0]);
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k)
+#pragma unroll
+      for (int i = 0; i < N; ++i) ge[k][i] = ge_in[k][i];
   }
   const T B = T(Bd);
   Prep<N, T> P;
@@ -592,7 +653,7 @@ BL_HD bool fit_track(const double hits[3][N], const float ge[6][N], double Bd, T
   LineOut L;
   line_fit<N, T>(ge, G, B, P, L);
   CircleOut C;
-  const bool ok = circle_fit<N, T>(ge, G, B, P, C);
+  const bool ok = circle_fit<N, T>(ge, G, B, P, C, rot, cr, sr);
   const double b = 1.0 / Bd;
   o.state[0] = C.par[0]; o.state[1] = C.par[1]; o.state[2] = C.par[2] * b; o.state[3] = L.par[0]; o.state[4] = L.par[1];
   const double cv[15] = {C.cov[0][0], C.cov[0][1], b * C.cov[0][2], 0.0, 0.0, C.cov[1][1], b * C.cov[1][2], 0.0, 0.0,

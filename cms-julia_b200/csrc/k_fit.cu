@@ -12,7 +12,7 @@ namespace pxl {
 
 namespace {
 
-template <int N>
+template <int N, class T>
 __device__ void fit_tuple(const Dev& d, uint64_t g, uint32_t hb, const uint32_t* hits_of_tuple, double B) {
   double h[3][N];
   float ge[6][N];
@@ -30,7 +30,7 @@ __device__ void fit_tuple(const Dev& d, uint64_t g, uint32_t hb, const uint32_t*
     h[2][i] = d.zg[hit];
   }
   bl::TrackOut o;
-  const bool ok = bl::fit_track<N, double>(h, ge, B, o);
+  const bool ok = bl::fit_track<N, T>(h, ge, B, o);
   float* st = d.t_state + 5 * g;
   float* cv = d.t_cov + 15 * g;
 #pragma unroll
@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(256) k_fit_list(Dev d) {
 // one hit count per launch, so that each instantiation keeps only its own registers.
 // Capped at 128 registers (four blocks per SM): the 4-hit fit spills a few hundred
 // bytes to L1 but runs twice the warps, which hides more of its FP64 latency.
-template <int N>
+template <int N, class T>
 __global__ void __launch_bounds__(128, 4) k_fit_tuples(Dev d) {
   const int e = blockIdx.y;
   const EvInfo& E = d.ev[e];
@@ -124,7 +124,7 @@ __global__ void __launch_bounds__(128, 4) k_fit_tuples(Dev d) {
   const double B = double(d.c.b_field);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nfit; i += gridDim.x * blockDim.x) {
     const uint64_t g = tb + d.fit_list[N == 3 ? tb + i : tb + nt - 1 - i];
-    fit_tuple<N>(d, g, hb, d.tuple_hits + d.tuple_off[g], B);
+    fit_tuple<N, T>(d, g, hb, d.tuple_hits + d.tuple_off[g], B);
   }
 }
 
@@ -222,10 +222,18 @@ void launch_fit(const Dev& d, const Launch& L) {
   // about 7000 fits per PU50 event: enough CTAs for every SM with few events
   const int bx = (L.tune && L.tune[kTuneFitTuples] > 0) ? L.tune[kTuneFitTuples]
                                                          : std::max(2, std::min(64, (148 * 16) / std::max(1, int(d.E))));
-  k_fit_tuples<3><<<dim3(bx, d.E), 128, 0, L.s>>>(d);
-  L.mark("broken_line_fit_3");
-  k_fit_tuples<4><<<dim3(bx, d.E), 128, 0, L.s>>>(d);
-  L.mark("broken_line_fit_4");
+  // FP64 as the reference fits (broken_line_fit_on_gpu.jl:28-30), or the mixed-precision fit
+  if (d.fit_precision == 1) {
+    k_fit_tuples<3, float><<<dim3(bx, d.E), 128, 0, L.s>>>(d);
+    L.mark("broken_line_fit_3");
+    k_fit_tuples<4, float><<<dim3(bx, d.E), 128, 0, L.s>>>(d);
+    L.mark("broken_line_fit_4");
+  } else {
+    k_fit_tuples<3, double><<<dim3(bx, d.E), 128, 0, L.s>>>(d);
+    L.mark("broken_line_fit_3");
+    k_fit_tuples<4, double><<<dim3(bx, d.E), 128, 0, L.s>>>(d);
+    L.mark("broken_line_fit_4");
+  }
 }
 
 int64_t fit_plan_bytes(int32_t n_tracks) {

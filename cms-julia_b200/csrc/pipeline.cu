@@ -208,6 +208,7 @@ int alloc_batch(PxlCtx* ctx) {
   d.tuples_per_event = uint32_t(p.tuples_per_event);
   d.fits_per_mult = uint32_t(p.fits_per_multiplicity);
   d.columns_per_event = uint32_t(p.columns_per_event);
+  d.fit_precision = p.fit_precision;
   d.include_errors = p.include_errors;
   d.use_quality = p.use_quality;
   d.apply_charge_cut = 1;
@@ -483,7 +484,7 @@ int32_t pxl_ctx_create(const PxlConditions* cond, const PxlParams* params, PxlCt
   const PxlParams& q = ctx->p;
   if (q.max_events <= 0 || q.hits_per_event <= 0 || uint32_t(q.hits_per_event) > kMaxHitsPerEvent ||
       q.doublets_per_event <= 0 || q.tuples_per_event <= 0 || q.fits_per_multiplicity <= 0 ||
-      q.columns_per_event <= 0) {
+      q.columns_per_event <= 0 || q.fit_precision < 0 || q.fit_precision > 1) {
     delete ctx;
     return PXL_ERR_ARG;
   }

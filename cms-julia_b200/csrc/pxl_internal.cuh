@@ -126,6 +126,7 @@ struct Dev {
   int64_t cap_words, cap_hits, cap_cells, cap_tuples, cap_tuple_hits, cap_items, cap_pairs, cap_long;
   uint32_t hits_per_event, doublets_per_event, tuples_per_event, fits_per_mult, columns_per_event;
   int32_t include_errors, use_quality;
+  int32_t fit_precision;     // 0 FP64 (the reference), 1 mixed precision
   int32_t apply_charge_cut;  // 1 in the chain; 0 only for the stand-alone clustering entry
   // inputs
   const uint8_t* raw;

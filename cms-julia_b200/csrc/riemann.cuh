@@ -112,8 +112,13 @@ struct RiemannOut {
   double chi2_circle, chi2_line, pt;
 };
 
+// The fit in a frame turned by -theta about the origin (rot; cos, sin = cr, sr): phi is taken
+// from the circle centre turned back. ge: the hits' covariances in that frame; ge_glob: in the
+// global frame, which cov_carttorad_prefit's projection reads (it takes the direction (1, tan a)
+// of a frame-independent angle a against the global axes, so it depends on the frame).
 template <int N, class T>
-BL_HD bool riemann_fit(const double hits[3][N], const float ge[6][N], double Bd, RiemannOut& o) {
+BL_HD bool riemann_fit_frame(const double hits[3][N], const float ge[6][N], const float ge_glob[6][N], double Bd,
+                             RiemannOut& o, bool rot, double cr, double sr) {
   // hits relative to hit 0 (FP64 subtraction), absolute hit 0 kept for the radii
   T px[N], py[N], pz[N];
 #pragma unroll
@@ -162,7 +167,9 @@ BL_HD bool riemann_fit(const double hits[3][N], const float ge[6][N], double Bd,
     for (int i = 0; i < N; ++i) {
       // angle at the centre between the origin and hit i: -o x p, -o . p with o the centre
       const T qx = T(hits[0][i]) - gcx, qy = T(hits[1][i]) - gcy;
-      sv[i] = s_abs(bl_atan2<T>(-gcx * qy + gcy * qx, -gcx * qx - gcy * qy) * fR);
+      // the cross product of two vectors a radius long is small against its terms: its two
+      // products are compensated in FP32
+      sv[i] = s_abs(bl_atan2<T>(bl::diff_of_products<T>(gcy, qx, gcx, qy), -gcx * qx - gcy * qy) * fR);
     }
     const T st = T(sin(double(theta)));
 #pragma unroll
@@ -186,7 +193,7 @@ BL_HD bool riemann_fit(const double hits[3][N], const float ge[6][N], double Bd,
     for (int i = 0; i < N; ++i) {
       // projected variance (cov_carttorad_prefit): its three terms cancel almost exactly
       // for hits near the coordinate axes, so it is evaluated in FP64 in both modes
-      const double vxx = ge[0][i], vxy = ge[1][i], vyy = ge[2][i];
+      const double vxx = ge_glob[0][i], vxy = ge_glob[1][i], vyy = ge_glob[2][i];
       double d;
       if (rad[i] < T(1e-4)) {
         d = vxx;
@@ -287,7 +294,7 @@ BL_HD bool riemann_fit(const double hits[3][N], const float ge[6][N], double Bd,
 #pragma unroll
   for (int i = 0; i < N; ++i) {
     const T qx = px[i] - ox, qy = py[i] - oy;  // hit - centre
-    const T cr = -gox * qy + goy * qx, dt = -gox * qx - goy * qy;
+    const T cr = bl::diff_of_products<T>(goy, qx, gox, qy), dt = -gox * qx - goy * qy;
     const T at = -T(q) * bl_atan2<T>(cr, dt);
     sarc[i] = at * Rt;
     const T temp0 = -T(q) * Rt / (dt * dt + cr * cr);
@@ -363,8 +370,13 @@ BL_HD bool riemann_fit(const double hits[3][N], const float ge[6][N], double Bd,
   }
   o.chi2_line = chi2l;
   // ---------------------------------------------------------------- (phi, d0, q/pT, cot(theta), zip)
-  const double gx = hits[0][0] + cx, gy = hits[1][0] + cy;
+  double gx = hits[0][0] + cx, gy = hits[1][0] + cy;
   const double rc = sqrt(gx * gx + gy * gy);
+  if (rot) {
+    const double tx = cr * gx - sr * gy;
+    gy = sr * gx + cr * gy;
+    gx = tx;
+  }
   o.state[0] = atan2(q * gx, -q * gy);
   o.state[1] = q * (rc - R);
   o.pt = R * Bd;
@@ -372,6 +384,21 @@ BL_HD bool riemann_fit(const double hits[3][N], const float ge[6][N], double Bd,
   o.state[3] = cf * (sol1 * sn + cs);
   o.state[4] = cf * sol0;
   return isfinite(o.state[0]) && isfinite(o.state[2]);
+}
+
+// The FP32 fit (T = float) runs in the chord frame of the hits (bl::chord_frame): their
+// offsets from hit 0, rounded to FP32, then keep the small component across the chord, which
+// carries the curvature, almost exactly. Every quantity but phi is invariant under the turn.
+template <int N, class T>
+BL_HD bool riemann_fit(const double hits[3][N], const float ge[6][N], double Bd, RiemannOut& o) {
+  if constexpr (sizeof(T) == 4) {
+    double hr[3][N], cr, sr;
+    float gr[6][N];
+    bl::chord_frame<N>(hits, ge, false, hr, gr, cr, sr);
+    return riemann_fit_frame<N, T>(hr, gr, ge, Bd, o, true, cr, sr);
+  } else {
+    return riemann_fit_frame<N, T>(hits, ge, ge, Bd, o, false, 1.0, 0.0);
+  }
 }
 
 }  // namespace rm

@@ -43,7 +43,7 @@ class PxlParams(ctypes.Structure):
         ("tuples_per_event", ctypes.c_int32), ("fits_per_multiplicity", ctypes.c_int32),
         ("include_errors", ctypes.c_int32), ("use_quality", ctypes.c_int32),
         ("blocks_per_event", ctypes.c_int32), ("threads_per_block", ctypes.c_int32),
-        ("columns_per_event", ctypes.c_int32),
+        ("columns_per_event", ctypes.c_int32), ("fit_precision", ctypes.c_int32),
     ]
 
 

@@ -95,6 +95,10 @@ typedef struct PxlParams {
   int32_t threads_per_block;         /* launch shape; 0 = chosen by the autotuner */
   int32_t columns_per_event;         /* 65536 (MAX_NUM_OF_ACTIVE_DOUBLETS): cells with a neighbour or
                                         track list; a warning (PXL_WARN_COLUMNS) above it */
+  int32_t fit_precision;             /* broken-line fits of the chain: 0 = FP64 as the reference
+                                        (broken_line_fit_on_gpu.jl:28-30); 1 = FP32 arithmetic with
+                                        the band solve, transport and covariance in FP64 (pxl_bl_fit
+                                        precision 1) */
 } PxlParams;
 
 typedef struct PxlEventCounts {

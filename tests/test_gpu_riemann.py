@@ -37,16 +37,18 @@ def test_riemann_fp64_matches_oracle():
 
 
 def test_riemann_mixed_precision_bounds():
+    """FP32 mode against FP64 on the 2^20 workload tracks: q/pT and cot(theta) within 1e-5
+    relative on every track."""
     from pixeltrack import gen
-    w = gen.fit_tracks(20000, seed=52)
+    w = gen.fit_tracks(1 << 20, seed=52)
     f64 = _run(w, 0)["state"].astype(np.float64)
     f32 = _run(w, 1)["state"].astype(np.float64)
     ok = np.all(np.isfinite(f64), axis=1)
     d = np.abs(f32[ok] - f64[ok])
     qpt = d[:, 2] / np.abs(f64[ok, 2])
-    assert np.percentile(qpt, 99) < 1e-5 and qpt.max() < 1e-4
-    assert (d[:, 3] / np.maximum(np.abs(f64[ok, 3]), 1e-3)).max() < 2e-5
-    assert d[:, 0].max() < 2e-6 and d[:, 1].max() < 5e-6 and d[:, 4].max() < 2e-4
+    assert qpt.max() < 1e-5
+    assert (d[:, 3] / np.maximum(np.abs(f64[ok, 3]), 1e-3)).max() < 1e-5
+    assert d[:, 0].max() < 1e-6 and d[:, 1].max() < 1e-6 and d[:, 4].max() < 1e-5
 
 
 def test_riemann_exact_helix():
