@@ -455,6 +455,47 @@ def pu50_parity(chain, conds, blob, offs, E: int) -> dict:
             "validator": {"validated_events": E, "good_events": good}}
 
 
+def chain_fit_precision(chain, conds, blob, offs, E: int, params, n_check: int = 200) -> dict:
+    """The chain run again with its fits in mixed precision (fit_precision = 1): per-parameter
+    error of the fitted tuples of n_check events against the FP64 chain's (the same tuples), and
+    the live time of the fit segments in both modes (non-graph runs)."""
+    import ctypes
+    from pixeltrack import PixelChain
+    p = type(params)()
+    ctypes.memmove(ctypes.byref(p), ctypes.byref(params), ctypes.sizeof(params))
+    p.fit_precision = 1
+    mixed = PixelChain(conds, p)
+    fit_ms = {}
+    for name, ch in (("fp64", chain), ("mixed", mixed)):
+        ch.profile(True)
+        for _ in range(2):
+            ch.run_batch(blob, offs)
+            segs = dict(ch.profile_read())
+        ch.profile(False)
+        fit_ms[name] = segs.get("broken_line_fit_3", 0.0) + segs.get("broken_line_fit_4", 0.0)
+    chain.run_batch(blob, offs)
+    rows = {"q_over_pt_rel": [], "phi_abs_rad": [], "cot_theta_rel": [], "d0_abs_cm": [], "z0_abs_cm": []}
+    for e in np.linspace(0, E - 1, min(n_check, E)).astype(int):
+        nt = chain.counts(e).n_tuples
+        sel = chain.product("fitted", e)[:nt].astype(bool)
+        a = mixed.product("state", e).reshape(-1, 5)[:nt][sel].astype(np.float64)
+        b = chain.product("state", e).reshape(-1, 5)[:nt][sel].astype(np.float64)
+        ok = np.all(np.isfinite(b), axis=1)
+        a, b = a[ok], b[ok]
+        rows["q_over_pt_rel"].append(np.abs(a[:, 2] - b[:, 2]) / np.abs(b[:, 2]))
+        rows["phi_abs_rad"].append(np.abs(a[:, 0] - b[:, 0]))
+        rows["cot_theta_rel"].append(np.abs(a[:, 3] - b[:, 3]) / np.maximum(np.abs(b[:, 3]), 1e-3))
+        rows["d0_abs_cm"].append(np.abs(a[:, 1] - b[:, 1]))
+        rows["z0_abs_cm"].append(np.abs(a[:, 4] - b[:, 4]))
+    mixed.close()
+    out = {k: {"median": float(np.median(np.concatenate(v))), "p99": float(np.percentile(np.concatenate(v), 99)),
+               "max": float(np.concatenate(v).max())} for k, v in rows.items()}
+    out["tracks"] = int(sum(len(v) for v in rows["q_over_pt_rel"]))
+    out["events"] = int(min(n_check, E))
+    out["fit_segments_ms"] = fit_ms
+    return out
+
+
 def oracle_fit_sample(w: dict, m: int):
     from oracle import oracle
     return oracle.bl_fit_batch(w["hits"][: w["offsets"][m]], w["ge"][: w["offsets"][m]], w["offsets"][: m + 1], FIT_B, 1)
@@ -574,6 +615,8 @@ def main():
         return
     # parity of the batch with the oracle (outside every timed region)
     parity = None if args.no_parity else pu50_parity(chain, conds, blob, offs, E)
+    # the chain's fits in mixed precision against its FP64 fits
+    chain_mixed = chain_fit_precision(chain, conds, blob, offs, E, params)
 
     # batched graph: input in HBM, one replay per step
     chain.stage_batch(blob, offs, sh)
@@ -710,6 +753,7 @@ def main():
             "roofline": roofline, "cpu_baseline": cpu, "gpu_launches": kernels_per_step * args.steps,
             "clocks": clk.summary(), "segments_ms": seg_ms, "totals": totals, "warnings": warn, "fits": fits,
             "adjoint": adjoint, "uneven_pu0_200": uneven, "parity": parity,
+            "chain_fit_mixed_vs_fp64": chain_mixed,
             "vertices_per_event": nv_check / E,
         }
         print(json.dumps(line), flush=True)
