@@ -179,25 +179,35 @@ def bench_uneven(args, local: int, rank: int, world: int, plain_value: float) ->
               for k in range(2)]
     chain.stage_batch(*halves[0], sh)
     stream.synchronize()
-    tuned = chain.autotune()
-    # both halves resident in the context's two input slots, one graph per slot
-    chain.stage_batch(*halves[0], sh)
-    stream.synchronize()
-    chain.capture_graph()
-    chain.stage_slot(1, *halves[1], sh)
-    stream.synchronize()
-    for _ in range(args.warmup):
-        chain.launch_slot(0, sh)
-        chain.launch_slot(1, sh)
-    warn = chain.sync()
-    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    t0.record(stream)
-    for _ in range(args.uneven_steps):
-        chain.launch_slot(0, sh)
-        chain.launch_slot(1, sh)
-    t1.record(stream)
-    t1.synchronize()
-    ms = pdist.max_over_ranks(t0.elapsed_time(t1), device=torch.device("cuda", local)) / args.uneven_steps
+
+    def timed_step(candidates):
+        """Tunes the launch shapes among candidates on the first half, captures both halves'
+        graphs (resident in the context's two input slots) and times the step."""
+        chain.stage_batch(*halves[0], sh)
+        stream.synchronize()
+        tuned = chain.autotune(candidates=candidates)
+        chain.stage_batch(*halves[0], sh)
+        stream.synchronize()
+        chain.capture_graph()
+        chain.stage_slot(1, *halves[1], sh)
+        stream.synchronize()
+        for _ in range(args.warmup):
+            chain.launch_slot(0, sh)
+            chain.launch_slot(1, sh)
+        warn = chain.sync()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(args.uneven_steps):
+            chain.launch_slot(0, sh)
+            chain.launch_slot(1, sh)
+        t1.record(stream)
+        t1.synchronize()
+        return pdist.max_over_ranks(t0.elapsed_time(t1), device=torch.device("cuda", local)) / args.uneven_steps, \
+            tuned, warn
+
+    # static grids only, then with the persistent work queues among the candidates (kept)
+    ms_static, tuned_static, _ = timed_step((4, 8, 16, 32, 64, 128))
+    ms, tuned, warn = timed_step((4, 8, 16, 32, 64, 128, -2, -8))
     # per-event counts of each half, and the full products of the largest events
     counts = []
     big = set(np.argsort(np.diff(offs))[-10:].tolist())
@@ -250,6 +260,9 @@ def bench_uneven(args, local: int, rank: int, world: int, plain_value: float) ->
             "unit": "events/s", "ms_per_step": ms, "steps": args.uneven_steps, "raw_bytes_per_step": int(offs[-1]),
             "over_plain_per_event_pu50": value / world / plain_value if plain_value else None,
             "blocks_per_event": tuned, "totals": tot, "warnings": [n for b, n in WARN_BITS.items() if warn & b],
+            "static_grid": {"value": world * E / (ms_static / 1e3), "ms_per_step": ms_static,
+                            "blocks_per_event": tuned_static,
+                            "note": "the same batch with every stage on a static grid (no work queue)"},
             "parity": parity}
 
 

@@ -22,6 +22,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # The stand-alone fit library enables contraction for its FP32 mode.
 CUDA_SOURCES = [
     "scan.cu",
+    "workqueue.cu",
     "k_raw.cu",
     "k_cluster.cu",
     "k_rechits.cu",

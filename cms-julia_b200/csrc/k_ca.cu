@@ -14,6 +14,7 @@
 // tests lay their (item, candidate) and (cell, candidate) pairs end to end over the
 // lanes of a warp, so that lanes stay busy whatever the candidate counts; the tuple
 // walks run from per-warp queues of the start cells that walk, one tree per lane.
+#include <algorithm>
 #include <cstddef>
 
 #include "pxl_internal.cuh"
@@ -216,11 +217,8 @@ constexpr int kGroupCells = 768;  // outer hits one 32-item group stages in shar
 // doublets, or that finds the pool full, records kNoPool and the fill pass searches again.
 constexpr int kDblQueue = 64;
 
-__global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* __restrict__ pair_cum) {
-  const int e = blockIdx.y;
-  const EvInfo& E = d.ev[e];
-  const uint32_t n = E.n_items;
-  if (n == 0) return;
+template <bool kQ>
+__global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* __restrict__ pair_cum, WorkQueue q) {
   __shared__ uint32_t s_cum[kNPairs];
   __shared__ uint32_t s_hls[11];
   __shared__ uint4 s_rng[8][32];   // per compacted item: lo0, n0, lo1, first candidate
@@ -229,6 +227,10 @@ __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* _
   __shared__ uint32_t s_q[8][kDblQueue];  // owner << kHitIdBits | candidate
   __shared__ uint32_t s_out[8][kGroupCells];
   __shared__ uint8_t s_own[8][kGroupCells];
+  for_each_vblock<kQ>(q, [&](int e, uint32_t bx, uint32_t nbx) {
+  const EvInfo& E = d.ev[e];
+  const uint32_t n = E.n_items;
+  if (n == 0) return;
   if (threadIdx.x < kNPairs) s_cum[threadIdx.x] = pair_cum[size_t(e) * kNPairs + threadIdx.x];
   if (threadIdx.x < 11) s_hls[threadIdx.x] = d.hits_layer_start[size_t(e) * 11 + threadIdx.x];
   __syncthreads();
@@ -239,7 +241,7 @@ __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* _
   const uint32_t ib = E.item_base;
   const unsigned lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
-  for (uint32_t j0 = blockIdx.x * blockDim.x + 32u * w; j0 < n; j0 += gridDim.x * blockDim.x) {
+  for (uint32_t j0 = bx * blockDim.x + 32u * w; j0 < n; j0 += nbx * blockDim.x) {
     const uint32_t j = j0 + lane;
     ItemHead h{};
     if (j < n) h = item_head(j, s_cum, s_hls, hv, poff);
@@ -331,21 +333,23 @@ __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* _
     if (j < n) d.item_pool[ib + j] = off == kNoPool ? kNoPool : off + ex;
     __syncwarp();
   }
+  });
 }
 
 // Fill pass over the same 32-item groups: cells of a group are contiguous, so the warp
 // writes them with consecutive lanes on consecutive cells, outer hits from the pool and the
 // inner hit, pair and inner z / r of each cell's item from shared memory.
-__global__ void __launch_bounds__(256) k_doublets_fill(Dev d, const uint32_t* __restrict__ pair_cum) {
-  const int e = blockIdx.y;
-  const EvInfo& E = d.ev[e];
-  const uint32_t n = E.n_items;
-  if (n == 0) return;
+template <bool kQ>
+__global__ void __launch_bounds__(256) k_doublets_fill(Dev d, const uint32_t* __restrict__ pair_cum, WorkQueue q) {
   __shared__ uint32_t s_cum[kNPairs];
   __shared__ uint32_t s_hls[11];
   __shared__ uint32_t s_pos[8][33];
   __shared__ uint32_t s_hit[8][32];
   __shared__ uint8_t s_pid[8][32];
+  for_each_vblock<kQ>(q, [&](int e, uint32_t bx, uint32_t nbx) {
+  const EvInfo& E = d.ev[e];
+  const uint32_t n = E.n_items;
+  if (n == 0) return;
   if (threadIdx.x < kNPairs) s_cum[threadIdx.x] = pair_cum[size_t(e) * kNPairs + threadIdx.x];
   if (threadIdx.x < 11) s_hls[threadIdx.x] = d.hits_layer_start[size_t(e) * 11 + threadIdx.x];
   __syncthreads();
@@ -360,7 +364,7 @@ __global__ void __launch_bounds__(256) k_doublets_fill(Dev d, const uint32_t* __
   const uint64_t cell_lo = E.cell_base;
   const uint32_t keep = E.n_cells;
   const unsigned lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
-  for (uint32_t j0 = blockIdx.x * blockDim.x + 32u * w; j0 < n; j0 += gridDim.x * blockDim.x) {
+  for (uint32_t j0 = bx * blockDim.x + 32u * w; j0 < n; j0 += nbx * blockDim.x) {
     const uint32_t j = j0 + lane;
     const bool valid = j < n;
     const uint32_t pos = valid ? d.item_cnt[ib + j] - raw_lo : 0u;
@@ -404,6 +408,7 @@ __global__ void __launch_bounds__(256) k_doublets_fill(Dev d, const uint32_t* __
     }
     __syncwarp();
   }
+  });
 }
 
 // per event: cell base, raw and capped counts
@@ -594,18 +599,19 @@ __global__ void __launch_bounds__(256) k_ohc_records(Dev d) {
 constexpr int kConnWarps = 8;
 constexpr int kConnQueue = 64;
 
-__global__ void __launch_bounds__(256) k_connect_test(Dev d) {
-  const int e = blockIdx.y;
-  const EvInfo& E = d.ev[e];
-  const uint64_t cb = E.cell_base;
-  const uint32_t hb = E.hit_base;
-  const float4* hxyzr = d.hit_xyzr + hb;
+template <bool kQ>
+__global__ void __launch_bounds__(256) k_connect_test(Dev d, WorkQueue q) {
   __shared__ float4 s_rz[kConnWarps][32];  // inner r, z and outer r, z of each cell
   __shared__ float4 s_xy[kConnWarps][32];  // inner x, y and outer x, y
   __shared__ uint32_t s_lo[kConnWarps][32];
   __shared__ uint32_t s_ex[kConnWarps][32];
   __shared__ uint8_t s_barrel[kConnWarps][32];
   __shared__ uint16_t s_queue[kConnWarps][kConnQueue];  // pair: owner lane << 8 | candidate
+  for_each_vblock<kQ>(q, [&](int e, uint32_t bx, uint32_t nbx) {
+  const EvInfo& E = d.ev[e];
+  const uint64_t cb = E.cell_base;
+  const uint32_t hb = E.hit_base;
+  const float4* hxyzr = d.hit_xyzr + hb;
   const unsigned lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
   uint64_t c0 = 0;
@@ -646,7 +652,7 @@ __global__ void __launch_bounds__(256) k_connect_test(Dev d) {
       }
     }
   };
-  for (uint32_t k0 = blockIdx.x * blockDim.x + 32u * w; k0 < E.n_cells; k0 += gridDim.x * blockDim.x) {
+  for (uint32_t k0 = bx * blockDim.x + 32u * w; k0 < E.n_cells; k0 += nbx * blockDim.x) {
     const uint32_t k = k0 + lane;
     c0 = cb + k0;
     const uint64_t c = cb + k;
@@ -695,6 +701,7 @@ __global__ void __launch_bounds__(256) k_connect_test(Dev d) {
     circle_step(0, qn);
     __syncwarp();
   }
+  });
 }
 
 // neighbour lists from the pair list: each passing (candidate o, cell c) appends c to o's list
@@ -744,8 +751,9 @@ __global__ void k_sort_cell_lists(Dev d) {
 }
 
 // ---------------------------------------------------------------- fishbone
-__global__ void __launch_bounds__(128) k_fishbone(Dev d) {
-  const int e = blockIdx.y;
+template <bool kQ>
+__global__ void __launch_bounds__(128) k_fishbone(Dev d, WorkQueue q) {
+  for_each_vblock<kQ>(q, [&](int e, uint32_t bx, uint32_t nbx) {
   const EvInfo& E = d.ev[e];
   if (E.n_hits <= 1) return;
   const uint32_t hb = E.hit_base;
@@ -753,7 +761,7 @@ __global__ void __launch_bounds__(128) k_fishbone(Dev d) {
   const float* yg = d.yg + hb;
   const float* zg = d.zg + hb;
   const int16_t* det = d.detind + hb;
-  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < E.n_hits; k += gridDim.x * blockDim.x) {
+  for (uint32_t k = bx * blockDim.x + threadIdx.x; k < E.n_hits; k += nbx * blockDim.x) {
     const uint32_t lo = d.ohc_cnt[hb + k];
     uint32_t n = d.ohc_cnt[hb + k + 1] - lo;
     if (n < 2) continue;
@@ -804,6 +812,7 @@ __global__ void __launch_bounds__(128) k_fishbone(Dev d) {
       }
     }
   }
+  });
 }
 
 // ---------------------------------------------------------------- ntuplets
@@ -901,12 +910,12 @@ __device__ __forceinline__ bool is_start(const Dev& d, uint64_t c) {
 constexpr int kNtupWarps = 4;
 constexpr int kNtupQueue = 64;
 
-template <bool kFill>
-__global__ void __launch_bounds__(32 * kNtupWarps) k_ntuplets(Dev d) {
-  const int e = blockIdx.y;
+template <bool kFill, bool kQ>
+__global__ void __launch_bounds__(32 * kNtupWarps) k_ntuplets(Dev d, WorkQueue q) {
+  __shared__ uint32_t s_queue[kNtupWarps][kNtupQueue];
+  for_each_vblock<kQ>(q, [&](int e, uint32_t bx, uint32_t nbx) {
   const EvInfo& E = d.ev[e];
   const uint64_t cb = E.cell_base;
-  __shared__ uint32_t s_queue[kNtupWarps][kNtupQueue];
   const unsigned lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
   const uint32_t ncell = E.n_cells;
@@ -926,7 +935,7 @@ __global__ void __launch_bounds__(32 * kNtupWarps) k_ntuplets(Dev d) {
     }
   };
   uint32_t qn = 0;
-  for (uint32_t k0 = blockIdx.x * blockDim.x + 32u * w; k0 < ncell; k0 += gridDim.x * blockDim.x) {
+  for (uint32_t k0 = bx * blockDim.x + 32u * w; k0 < ncell; k0 += nbx * blockDim.x) {
     const uint32_t k = k0 + lane;
     bool walker = false;
     if (k < ncell) {
@@ -948,6 +957,8 @@ __global__ void __launch_bounds__(32 * kNtupWarps) k_ntuplets(Dev d) {
     }
   }
   walk_queued(0, qn);
+  __syncwarp();
+  });
 }
 
 __global__ void k_tuple_bases(Dev d) {
@@ -1076,6 +1087,25 @@ __global__ void k_multiplicity(Dev d) {
 
 }  // namespace
 
+// CTAs of one persistent wave per tunable stage (SMs x resident CTAs of the stage's
+// work-queue kernels, the smaller where a stage has two); 0 for the stages without one
+int prepare_ca_kernels(int ctas[kTuneCount]) {
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return -1;
+  auto occ = [&](auto kernel, int threads) {
+    int n = 0;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, 0) == cudaSuccess ? n : 0;
+  };
+  for (int s = 0; s < kTuneCount; ++s) ctas[s] = 0;
+  ctas[kTuneDoublets] = sms * std::min(occ(k_doublets_count<true>, 256), occ(k_doublets_fill<true>, 256));
+  ctas[kTuneConnect] = sms * occ(k_connect_test<true>, 256);
+  ctas[kTuneFishbone] = sms * occ(k_fishbone<true>, 128);
+  ctas[kTuneNtuplets] = sms * std::min(occ(k_ntuplets<false, true>, 32 * kNtupWarps),
+                                       occ(k_ntuplets<true, true>, 32 * kNtupWarps));
+  return 0;
+}
+
 // a list-sorting kernel followed by the sort of the lists it left long
 template <class F>
 void launch_sorted(const Dev& d, const Launch& L, uint32_t* list, F&& sort_kernel) {
@@ -1095,7 +1125,19 @@ void launch_ca(const Dev& d, const Launch& L) {
   launch_ev_scan(d, L.s, int(offsetof(EvInfo, n_items)), int(offsetof(EvInfo, item_base)));
   L.mark("doublet_items");
   cudaMemsetAsync(d.dbl_pool_ctr, 0, sizeof(uint32_t), L.s);
-  k_doublets_count<<<g(kTuneDoublets), 256, 0, L.s>>>(d, pair_cum);
+  // the per-event stages run on their static grid or from a work queue (Launch::queue_of):
+  // virtual blocks of (strides x block size) work units, events by decreasing hit count
+  launch_wq_order(d, L.s);
+  auto plan = [&](int seg, int count_off, int threads) {
+    return launch_wq_plan(d, L, count_off, uint32_t(L.queue_of(seg)) * uint32_t(threads));
+  };
+  const int ctas_dbl = L.queue_of(kTuneDoublets) ? L.wq_ctas[kTuneDoublets] : 0;
+  if (ctas_dbl) {
+    const WorkQueue q = plan(kTuneDoublets, int(offsetof(EvInfo, n_items)), 256);
+    k_doublets_count<true><<<ctas_dbl, 256, 0, L.s>>>(d, pair_cum, q);
+  } else {
+    k_doublets_count<false><<<g(kTuneDoublets), 256, 0, L.s>>>(d, pair_cum, WorkQueue{});
+  }
   L.mark("doublets_count");
   excl_scan_u32(d.item_cnt, d.cap_items, &d.ev[d.E].n_items, d.scan_tmp, L.s);
   k_cell_bases<<<eb, 128, 0, L.s>>>(d);
@@ -1103,7 +1145,12 @@ void launch_ca(const Dev& d, const Launch& L) {
   launch_ev_clamp(d, L.s, int(offsetof(EvInfo, n_cells)), int(offsetof(EvInfo, cell_base)), d.cap_cells);
   k_cell_regions<<<eb, 128, 0, L.s>>>(d);
   L.mark("doublets_scan");
-  k_doublets_fill<<<g(kTuneDoublets), 256, 0, L.s>>>(d, pair_cum);
+  if (ctas_dbl) {
+    const WorkQueue q = plan(kTuneDoublets, int(offsetof(EvInfo, n_items)), 256);
+    k_doublets_fill<true><<<ctas_dbl, 256, 0, L.s>>>(d, pair_cum, q);
+  } else {
+    k_doublets_fill<false><<<g(kTuneDoublets), 256, 0, L.s>>>(d, pair_cum, WorkQueue{});
+  }
   L.mark("doublets_fill");
   // cells ending on each hit (counted by the doublet fill)
   excl_scan_shift_u32(d.ohc_cur, d.ohc_cnt, d.cap_hits, &d.ev[d.E].n_hits, d.scan_tmp, L.s);
@@ -1113,20 +1160,41 @@ void launch_ca(const Dev& d, const Launch& L) {
   L.mark("outer_hit_lists");
   // connection and neighbour lists
   cudaMemsetAsync(d.cn_pair_ctr, 0, sizeof(uint32_t), L.s);
-  k_connect_test<<<g(kTuneConnect), 256, 0, L.s>>>(d);
+  if (L.queue_of(kTuneConnect)) {
+    const WorkQueue q = plan(kTuneConnect, int(offsetof(EvInfo, n_cells)), 256);
+    k_connect_test<true><<<L.wq_ctas[kTuneConnect], 256, 0, L.s>>>(d, q);
+  } else {
+    k_connect_test<false><<<g(kTuneConnect), 256, 0, L.s>>>(d, WorkQueue{});
+  }
   L.mark("connect");
   excl_scan_shift_u32(d.cn_cur, d.cn_cnt, d.cap_cells, &d.ev[d.E].n_cells_raw, d.scan_tmp, L.s);
   k_connect_fill<<<148 * 8, 256, 0, L.s>>>(d);
   launch_sorted(d, L, d.cn_list, [&](cudaStream_t s) { k_sort_cell_lists<0><<<g(kTuneCellLists), 256, 0, s>>>(d); });
   L.mark("neighbour_lists");
-  k_fishbone<<<g(kTuneFishbone), 128, 0, L.s>>>(d);
+  if (L.queue_of(kTuneFishbone)) {
+    const WorkQueue q = plan(kTuneFishbone, int(offsetof(EvInfo, n_hits)), 128);
+    k_fishbone<true><<<L.wq_ctas[kTuneFishbone], 128, 0, L.s>>>(d, q);
+  } else {
+    k_fishbone<false><<<g(kTuneFishbone), 128, 0, L.s>>>(d, WorkQueue{});
+  }
   L.mark("fishbone");
   // ntuplets
-  k_ntuplets<false><<<g(kTuneNtuplets), 32 * kNtupWarps, 0, L.s>>>(d);
+  const int ctas_nt = L.queue_of(kTuneNtuplets) ? L.wq_ctas[kTuneNtuplets] : 0;
+  if (ctas_nt) {
+    const WorkQueue q = plan(kTuneNtuplets, int(offsetof(EvInfo, n_cells)), 32 * kNtupWarps);
+    k_ntuplets<false, true><<<ctas_nt, 32 * kNtupWarps, 0, L.s>>>(d, q);
+  } else {
+    k_ntuplets<false, false><<<g(kTuneNtuplets), 32 * kNtupWarps, 0, L.s>>>(d, WorkQueue{});
+  }
   L.mark("ntuplets_count");
   excl_scan_u64(d.tstart_cnt, d.cap_cells, &d.ev[d.E].n_cells_raw, d.scan_tmp64, L.s);
   k_tuple_bases<<<eb, 128, 0, L.s>>>(d);
-  k_ntuplets<true><<<g(kTuneNtuplets), 32 * kNtupWarps, 0, L.s>>>(d);
+  if (ctas_nt) {
+    const WorkQueue q = plan(kTuneNtuplets, int(offsetof(EvInfo, n_cells)), 32 * kNtupWarps);
+    k_ntuplets<true, true><<<ctas_nt, 32 * kNtupWarps, 0, L.s>>>(d, q);
+  } else {
+    k_ntuplets<true, false><<<g(kTuneNtuplets), 32 * kNtupWarps, 0, L.s>>>(d, WorkQueue{});
+  }
   k_tuple_ends<<<div_up(d.E, 128), 128, 0, L.s>>>(d);
   L.mark("ntuplets_fill");
   excl_scan_shift_u32(d.ct_cur, d.ct_cnt, d.cap_cells, &d.ev[d.E].n_cells_raw, d.scan_tmp, L.s);

@@ -220,6 +220,7 @@ int alloc_batch(PxlCtx* ctx) {
   A(xx, d.cap_words); A(yy, d.cap_words); A(adc, d.cap_words); A(mid, d.cap_words); A(clus, d.cap_words);
   A(pdigi, d.cap_words); A(rawid, d.cap_words);
   A(err, 5 * d.cap_words); A(err_count, 1); A(id_seen, E * 64);
+  A(wq_order, E); A(wq_head, kWqSlots); A(wq_prefix, kWqSlots * (E + 1));
   A(module_start, E * (kMaxNumModules + 1)); A(clus_in_module, E * kMaxNumModules); A(module_id, E * kMaxNumModules);
   A(clus_module_start, E * (kMaxNumModules + 1));
   A(xl, d.cap_hits); A(yl, d.cap_hits); A(xerr, d.cap_hits); A(yerr, d.cap_hits);
@@ -275,6 +276,7 @@ int run_chain(PxlCtx* ctx, uint32_t mask, cudaStream_t s) {
   if (d.E <= 0) return 0;
   Launch L{s, d.bpe, 256, (ctx->prof.on && !ctx->capturing) ? &ctx->prof : nullptr};
   L.tune = ctx->tune;
+  L.wq_ctas = ctx->wq_ctas;
   if ((mask & PXL_STAGE_DIGIS) && L.prof) ctx->prof.n = 0;
   // stages run in chain order; a producer boundary may stop after any of them and a
   // later call (pxl_event_continue) resumes from the products already on the device
@@ -494,7 +496,7 @@ int32_t pxl_ctx_create(const PxlConditions* cond, const PxlParams* params, PxlCt
     pxl_ctx_destroy(ctx);
     return PXL_ERR_CUDA;
   }
-  int rc = prepare_select_kernels() ? PXL_ERR_CUDA : 0;
+  int rc = (prepare_select_kernels() || prepare_ca_kernels(ctx->wq_ctas)) ? PXL_ERR_CUDA : 0;
   if (!rc) rc = load_conditions(ctx, cond);
   if (!rc) rc = alloc_batch(ctx);
   if (rc) { pxl_ctx_destroy(ctx); return rc; }
@@ -676,7 +678,7 @@ int32_t pxl_autotune(PxlCtx* ctx, const int32_t* candidates, int32_t n_candidate
   if (!ctx || !candidates || n_candidates <= 0 || n_candidates > 32 || reps <= 0) return PXL_ERR_ARG;
   if (ctx->d.E <= 0) return PXL_ERR_STATE;
   for (int i = 0; i < n_candidates; ++i)
-    if (candidates[i] <= 0 || candidates[i] > 4096) return PXL_ERR_ARG;
+    if (candidates[i] == 0 || candidates[i] > 4096 || candidates[i] < -64) return PXL_ERR_ARG;
   // timed segments (names given by the launchers) and the stage each one tunes
   static const struct { const char* name; int seg; } kMap[] = {
       {"doublets_count", kTuneDoublets}, {"doublets_fill", kTuneDoublets}, {"outer_hit_lists", kTuneHitLists},

@@ -45,6 +45,8 @@ struct PxlCtx {
   bool capturing = false;
   // blocks per event of the tunable stages (0 = the default shape), set by pxl_autotune
   int tune[pxl::kTuneCount] = {};
+  // CTAs of one persistent work-queue wave per stage (0: the stage has no work-queue form)
+  int wq_ctas[pxl::kTuneCount] = {};
   // pxl_export_async: two alternating device export sets (allocated by the first call)
   pxl::ExportSet exp[2];
   int exp_next = 0;

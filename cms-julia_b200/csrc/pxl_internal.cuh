@@ -224,6 +224,11 @@ struct Dev {
   int64_t cap_big;
   // launch shape
   int32_t bpe;             // blocks per event for per-event kernels
+  // persistent work-queue launches (workqueue.cu): events by decreasing hit count, and per
+  // launch slot a pulled-block counter and the virtual-block prefix over that order
+  uint32_t* wq_order;      // [E]
+  uint32_t* wq_head;       // [kWqSlots]
+  uint32_t* wq_prefix;     // [kWqSlots][E + 1]
 };
 
 // One set of device export buffers of pxl_export_async: the batch's loose tracks and vertices
@@ -236,6 +241,46 @@ struct ExportSet {
   uint32_t cap_tracks = 0, cap_vertices = 0;
   cudaEvent_t ready = nullptr, copied = nullptr;  // kernels done (compute stream), copies done (copy stream)
 };
+
+// ---------------------------------------------------------------- persistent work queues
+// A per-event kernel runs either on a static grid (blocks per event x events; the hardware
+// hands the blocks out in event order) or as a persistent grid of one wave of CTAs that pull
+// virtual blocks from a device counter. An event gets as many virtual blocks as its work needs
+// (its count of the stage's work units over the units one block takes), and the events come
+// most work first, so that the longest events start early and the short ones fill the tail.
+// Either way the kernel body sees (event, block, blocks of the event).
+constexpr int kWqSlots = 16;  // persistent launches per chain run (each its own counter)
+
+struct WorkQueue {
+  const uint32_t* order = nullptr;   // [n] events, most work first
+  const uint32_t* prefix = nullptr;  // [n + 1] virtual blocks before each order slot
+  uint32_t* head = nullptr;          // pulled virtual blocks
+  uint32_t n = 0;
+};
+
+template <bool kQ, class F>
+__device__ __forceinline__ void for_each_vblock(const WorkQueue& q, F&& body) {
+  if constexpr (!kQ) {
+    body(int(blockIdx.y), uint32_t(blockIdx.x), uint32_t(gridDim.x));
+  } else {
+    __shared__ uint32_t s_v;
+    const uint32_t total = q.prefix[q.n];
+    for (;;) {
+      __syncthreads();  // the previous block's shared memory and s_v are free again
+      if (threadIdx.x == 0) s_v = atomicAdd(q.head, 1u);
+      __syncthreads();
+      const uint32_t v = s_v;
+      if (v >= total) return;
+      // the order slot i with prefix[i] <= v < prefix[i + 1] (slots without work are skipped)
+      uint32_t lo = 0, hi = q.n;
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (q.prefix[mid] <= v) lo = mid; else hi = mid;
+      }
+      body(int(q.order[lo]), v - q.prefix[lo], q.prefix[lo + 1] - q.prefix[lo]);
+    }
+  }
+}
 
 // Track lists by hit count for the stand-alone fits (workspace layout).
 constexpr int kFitMaxN = 8;
@@ -348,11 +393,17 @@ struct Launch {
   int bpe;        // blocks per event
   int tpb;        // threads per block
   Prof* prof = nullptr;
-  const int* tune = nullptr;  // [kTuneCount] blocks per event per stage, 0 = bpe
+  // [kTuneCount] launch shape per stage: > 0 blocks per event (static grid), < 0 persistent
+  // work queue with -value loop strides per virtual block, 0 the default
+  const int* tune = nullptr;
+  const int* wq_ctas = nullptr;  // [kTuneCount] CTAs of one persistent wave per stage (0: none)
+  mutable int wq_slot = 0;       // next work-queue slot of the run
   int bpe_of(int seg) const {
     const int b = (tune && tune[seg] > 0) ? tune[seg] : bpe;
     return b > 0 ? b : 64;
   }
+  // loop strides per virtual block when the stage runs from a work queue, else 0
+  int queue_of(int seg) const { return (tune && tune[seg] < 0 && wq_ctas && wq_ctas[seg] > 0) ? -tune[seg] : 0; }
   void mark(const char* nm) const {
     if (prof && prof->on && prof->n < Prof::kMax) {
       cudaEventRecord(prof->ev[prof->n], s);
@@ -362,6 +413,12 @@ struct Launch {
   }
 };
 
+// workqueue.cu: the event order of the run (most hits first, once the hits are known), and the
+// plan of one persistent launch: virtual blocks per event = ceil(count / units_per_block) with
+// count the EvInfo field at count_off
+void launch_wq_order(const Dev& d, cudaStream_t s);
+WorkQueue launch_wq_plan(const Dev& d, const Launch& L, int count_off, uint32_t units_per_block);
+
 void launch_raw(const Dev& d, const Launch& L, const int16_t* fed_slot_of);  // a1-a4
 void launch_modstart(const Dev& d, const Launch& L);  // a4 only (digis already in place)
 void launch_ev_scan(const Dev& d, cudaStream_t s, int count_off, int base_off);
@@ -369,6 +426,7 @@ void launch_ev_clamp(const Dev& d, cudaStream_t s, int count_off, int base_off, 
 void launch_cluster(const Dev& d, const Launch& L);   // a5-a7
 void launch_rechits(const Dev& d, const Launch& L);   // a8-a9
 void launch_ca(const Dev& d, const Launch& L);        // a10-a14
+int prepare_ca_kernels(int ctas[kTuneCount]);         // CTAs of one persistent wave per stage (current device)
 void launch_fit(const Dev& d, const Launch& L);       // a15-a16
 void launch_classify(const Dev& d, const Launch& L);  // a17
 int prepare_select_kernels();  // kernel attributes (dynamic shared memory) on the current device

@@ -198,8 +198,10 @@ class PixelChain:
         n = check(self._lib.pxl_profile_read(self._h, ms, names, 128), "pxl_profile_read")
         return [(names[i].decode(), ms[i]) for i in range(n)]
 
-    def autotune(self, candidates=(4, 8, 16, 32, 64, 128), reps: int = 2) -> dict[str, int]:
-        """Chooses the blocks per event of each tunable stage on the staged batch (pxl_autotune)."""
+    def autotune(self, candidates=(4, 8, 16, 32, 64, 128, -2, -8), reps: int = 2) -> dict[str, int]:
+        """Chooses the launch shape of each tunable stage on the staged batch (pxl_autotune):
+        c > 0 a static grid of c blocks per event, c < 0 a persistent work queue of virtual
+        blocks of -c loop strides."""
         cand = (ctypes.c_int32 * len(candidates))(*candidates)
         out = (ctypes.c_int32 * len(_native.TUNE_STAGES))()
         check(self._lib.pxl_autotune(self._h, cand, len(candidates), reps, out), "pxl_autotune")

@@ -293,11 +293,14 @@ int32_t pxl_profile_enable(PxlCtx* ctx, int32_t on);
 int32_t pxl_profile_read(PxlCtx* ctx, float* ms, const char** names, int32_t max);
 
 /* Launch-shape autotuner. Runs the whole chain on the batch staged last (pxl_batch_stage or
- * pxl_batch_run) once per candidate blocks-per-event value (each shape warmed up once, then
- * timed reps times with per-stage CUDA events) and keeps, for each tunable stage (doublets,
- * hit lists, connect, cell lists, fishbone, ntuplets, cell tracks, early duplicates,
- * classification, hit-to-tuple, fits), the fastest value. The choice holds for later runs
- * and graph captures of this context. chosen[PXL_TUNE_STAGES] (may be NULL) receives it.
+ * pxl_batch_run) once per candidate shape (each shape warmed up once, then timed reps times
+ * with per-stage CUDA events) and keeps, for each tunable stage (doublets, hit lists, connect,
+ * cell lists, fishbone, ntuplets, cell tracks, early duplicates, classification, hit-to-tuple,
+ * fits), the fastest. A candidate c > 0 (at most 4096) is a static grid of c blocks per event;
+ * c < 0 (at least -64) a persistent work queue: the doublet, connect, fishbone and ntuplet
+ * stages run as one wave of CTAs that pull virtual blocks of -c loop strides, events with the
+ * most hits first (the other stages run their default grid for it). The choice holds for later
+ * runs and graph captures of this context. chosen[PXL_TUNE_STAGES] (may be NULL) receives it.
  * Products of the staged batch are recomputed. No counterpart in the reference, whose
  * serial loops have no launch shape. */
 #define PXL_TUNE_STAGES 11

@@ -203,3 +203,27 @@ def test_chain_mixed_precision_fit(conditions, events_pu50):
         assert ok.sum() > 1000
         assert (np.abs(a[ok, 2] - b[ok, 2]) / np.abs(b[ok, 2])).max() < 1e-5
         assert (np.abs(a[ok, 3] - b[ok, 3]) / np.maximum(np.abs(b[ok, 3]), 1e-3)).max() < 1e-5
+
+
+@pytest.mark.parametrize("strides", [-1, -8])
+def test_work_queue_launches_keep_results(conditions, events_pu50, strides):
+    """The doublet, connect, fishbone and ntuplet stages launched as persistent work queues
+    (virtual blocks pulled from a device counter, events with the most hits first) give the
+    oracle's results, as the static grids do."""
+    from pixeltrack import PixelChain, batch_params
+    blob, offs = events_pu50
+    n = len(offs) - 1
+    with PixelChain(conditions, batch_params(n)) as bc:
+        bc.stage_batch(blob, offs)
+        chosen = bc.autotune(candidates=(strides,), reps=1)
+        assert chosen["doublets"] == strides and chosen["ntuplets"] == strides
+        bc.stage_batch(blob, offs)
+        bc.capture_graph()
+        bc.launch_graph()
+        assert bc.sync() == 0
+        orc = oracle.Oracle(conditions)
+        for e in range(n):
+            orc.run_event(blob[offs[e]:offs[e + 1]], 63)
+            errs = compare_ca(bc, orc, e, classified=True) + compare_fits(bc, orc, e) + compare_quality(bc, orc, e) \
+                + compare_vertices(bc, orc, e)
+            assert not errs, (e, errs)
