@@ -377,10 +377,14 @@ BL_HD void line_weights(const float ge[6][N], const Prep<N, T>& P, T w[N]) {
 template <int N, class T>
 BL_HD void line_system(const float ge[6][N], const Prep<N, T>& P, T w[N], Band<N, false>& f, double u[N]) {
   line_weights<N, T>(ge, P, w);
-  double d[N], e1[N], e2[N], r[N];
-  band_entries<N, T>(w, P.S, P.VB, d, e1, e2);
+  // assembled in FP64, as the circle system (circle_system)
+  double wd[N], Sd[N], VBd[N];
 #pragma unroll
-  for (int i = 0; i < N; ++i) r[N - 1 - i] = double(w[i] * P.Z[i]);
+  for (int i = 0; i < N; ++i) { wd[i] = double(w[i]); Sd[i] = double(P.S[i]); VBd[i] = double(P.VB[i]); }
+  double d[N], e1[N], e2[N], r[N];
+  band_entries<N, double>(wd, Sd, VBd, d, e1, e2);
+#pragma unroll
+  for (int i = 0; i < N; ++i) r[N - 1 - i] = wd[i] * double(P.Z[i]);
   band_factor<N, false>(d, e1, e2, nullptr, 0.0, f);
   double ue[N];
   band_solve<N, false>(f, r, ue);
@@ -493,21 +497,28 @@ BL_HD void circle_system(const float ge[6][N], const Geo<N, T>& G, const Prep<N,
     const T t1 = RR[1][0] * V[0][1] + RR[1][1] * V[1][1];
     w[i] = T(1.0) / (t0 * RR[1][0] + t1 * RR[1][1]);
   }
+  // The system is assembled in FP64 from the FP32 weights, arc lengths, scattering variances
+  // and residuals: for a stiff track the scattering terms are large and nearly cancel against
+  // each other in the elimination, and FP32 entries would cost the curvature correction digits
+  // (which the fast-fit curvature then cancels further when the fast fit is far off).
+  double wd[N], sd[N], VBd[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) { wd[i] = double(w[i]); sd[i] = double(P.s[i]); VBd[i] = double(VB[i]); }
   double d[N], e1[N], e2[N], b[N], r[N];
-  band_entries<N, T>(w, P.s, VB, d, e1, e2);
-  const T* s = P.s;
-  T cnn = 0;
+  band_entries<N, double>(wd, sd, VBd, d, e1, e2);
+  const double* s = sd;
+  double cnn = 0;
 #pragma unroll
   for (int i = 0; i < N; ++i) {
-    T v = 0;
-    if (i > 0 && i < N - 1) v += -(s[i + 1] - s[i - 1]) * (s[i + 1] - s[i - 1]) / (T(2.0) * VB[i] * (s[i + 1] - s[i]) * (s[i] - s[i - 1]));
-    if (i > 1) v += (s[i] - s[i - 2]) / (T(2.0) * VB[i - 1] * (s[i] - s[i - 1]));
-    if (i < N - 2) v += (s[i + 2] - s[i]) / (T(2.0) * VB[i + 1] * (s[i + 1] - s[i]));
-    b[N - 1 - i] = double(v);
-    r[N - 1 - i] = double(w[i] * Z[i]);
-    if (i > 0 && i < N - 1) cnn += ((s[i + 1] - s[i - 1]) * (s[i + 1] - s[i - 1])) / (T(4.0) * VB[i]);
+    double v = 0;
+    if (i > 0 && i < N - 1) v += -(s[i + 1] - s[i - 1]) * (s[i + 1] - s[i - 1]) / (2.0 * VBd[i] * (s[i + 1] - s[i]) * (s[i] - s[i - 1]));
+    if (i > 1) v += (s[i] - s[i - 2]) / (2.0 * VBd[i - 1] * (s[i] - s[i - 1]));
+    if (i < N - 2) v += (s[i + 2] - s[i]) / (2.0 * VBd[i + 1] * (s[i + 1] - s[i]));
+    b[N - 1 - i] = v;
+    r[N - 1 - i] = wd[i] * double(Z[i]);
+    if (i > 0 && i < N - 1) cnn += ((s[i + 1] - s[i - 1]) * (s[i + 1] - s[i - 1])) / (4.0 * VBd[i]);
   }
-  band_factor<N, true>(d, e1, e2, b, double(cnn), f);
+  band_factor<N, true>(d, e1, e2, b, cnn, f);
   double ue[N + 1];
   band_solve<N, true>(f, r, ue);
 #pragma unroll

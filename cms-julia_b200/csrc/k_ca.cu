@@ -123,6 +123,44 @@ __device__ __forceinline__ ItemHead item_head(uint32_t j, const uint32_t* cum, c
   return h;
 }
 
+// The same item for the count pass, over the binned records sorted by iphi (as uint16) within
+// each bin: its candidates are exactly the outer hits that pass the reference's dphi cut
+// (|int16(iphi_o - iphi_i)| <= cut), i.e. the part of bin kl from iphi - cut on, the bins
+// between, and the part of the last bin up to iphi + cut (two binary searches in the edge bins),
+// as at most two ranges when the window wraps past bin 128. The window (2 cut + 1 < 2^15) never
+// covers all 128 bins, the reference's kl == kh case.
+__device__ __forceinline__ ItemHead item_head_s(uint32_t j, const uint32_t* cum, const uint32_t* hls,
+                                                const HitView& hv, const uint32_t* poff, const uint16_t* __restrict__ us) {
+  ItemHead h = item_head(j, cum, hls, hv, poff);
+  if (!h.ok || h.n == 0) return h;
+  const int outer = c_layer_pairs[2 * h.pid + 1];
+  const uint32_t h_off = 128u * uint32_t(outer);
+  const uint16_t lo_u = uint16_t(h.iphi - h.cut), hi_u = uint16_t(h.iphi + h.cut);
+  const uint32_t kl = (uint32_t(lo_u) >> 9) + 1u, km = (uint32_t(hi_u) >> 9) + 1u;  // first, last bin
+  uint32_t a = poff[kl - 1 + h_off], ae = poff[kl + h_off];
+  while (a < ae) {  // first entry of bin kl at or above lo_u
+    const uint32_t m = (a + ae) >> 1;
+    if (us[m] < lo_u) a = m + 1; else ae = m;
+  }
+  uint32_t b = poff[km - 1 + h_off], be = poff[km + h_off];
+  while (b < be) {  // one past the last entry of bin km at or below hi_u
+    const uint32_t m = (b + be) >> 1;
+    if (us[m] <= hi_u) b = m + 1; else be = m;
+  }
+  if (kl <= km) {
+    h.lo0 = a;
+    h.n0 = b - a;
+    h.lo1 = 0;
+    h.n = h.n0;
+  } else {
+    h.lo0 = a;
+    h.n0 = poff[128 + h_off] - a;
+    h.lo1 = poff[h_off];
+    h.n = h.n0 + (b - h.lo1);
+  }
+  return h;
+}
+
 // The outer-hit cuts of one candidate (gpu_pixel_doublets.jl), in the reference's order:
 // doublet_pass_a takes the module, z0 and dphi cuts (about a quarter of the candidates pass),
 // doublet_pass_b the cluster-size and pt cuts. c_max_r holds small integers, so the float
@@ -171,6 +209,23 @@ __device__ __forceinline__ bool doublet_pass_b(int pid, float me_z, float me_r, 
   }
   return true;
 }
+
+// doublet_pass_a without the dphi cut, for candidates that pass it by construction
+__device__ __forceinline__ bool doublet_pass_z(int pid, float me_z, float me_r, const HitRec& hr) {
+  if (hr.det() > 2000) return false;
+  const float dr = __fsub_rn(hr.r, me_r);
+  return !(dr > c_max_rf[pid] || dr < 0 ||
+           fabsf(__fsub_rn(__fmul_rn(me_z, hr.r), __fmul_rn(me_r, hr.z))) > __fmul_rn(12.f, dr));
+}
+
+// Reference order of a passing outer hit among its item's cells: the window's bins in order
+// (bin offset from the item's first bin kl), then decreasing hit id within a bin.
+__device__ __forceinline__ uint32_t cell_order_key(int16_t me_p, int16_t cut, const HitRec& hr) {
+  const uint32_t kl = (uint32_t(uint16_t(me_p - cut)) >> 9) + 1u;
+  const uint32_t bo = (((uint32_t(uint16_t(hr.iphi)) >> 9) + 1u - kl) & 127u);
+  return (bo << kHitIdBits) | ((kMaxHitsPerEvent - 1u) - hr.id());
+}
+__device__ __forceinline__ uint32_t key_hit(uint32_t key) { return (kMaxHitsPerEvent - 1u) - (key & (kMaxHitsPerEvent - 1u)); }
 
 __device__ __forceinline__ bool doublet_pass(const ItemHead& h, const HitRec& hr) {
   return doublet_pass_a(h.pid, h.z, h.r, h.iphi, h.cut, hr) && doublet_pass_b(h.pid, h.z, h.r, h.iphi, h.ysize, hr);
@@ -237,14 +292,15 @@ __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* _
   const uint32_t hb = E.hit_base;
   HitView hv{d.xg + hb, d.yg + hb, d.zg + hb, d.rg + hb, d.iphi + hb, d.ysize + hb, d.detind + hb};
   const uint32_t* poff = d.phi_off + size_t(e) * kPhiTotBins;
-  const HitRec* hrec = d.hit_rec + hb;
+  const HitRec* hrec = d.hit_rec_s + hb;  // sorted by iphi within each bin
+  const uint16_t* us = d.hit_u_s + hb;
   const uint32_t ib = E.item_base;
   const unsigned lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
   const unsigned lt = (1u << lane) - 1u;
   for (uint32_t j0 = bx * blockDim.x + 32u * w; j0 < n; j0 += nbx * blockDim.x) {
     const uint32_t j = j0 + lane;
     ItemHead h{};
-    if (j < n) h = item_head(j, s_cum, s_hls, hv, poff);
+    if (j < n) h = item_head_s(j, s_cum, s_hls, hv, poff, us);
     const uint32_t nc = h.ok ? h.n : 0u;
     // items with candidates, compacted (compact index = rank among them); the candidates
     // of compacted item c start at position ctex
@@ -272,7 +328,7 @@ __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* _
         const HitRec hr = hrec[v & (kMaxHitsPerEvent - 1u)];
         pass = doublet_pass_b(int(g.w & 0xffu), __uint_as_float(g.x), __uint_as_float(g.y), int16_t(g.z & 0xffffu),
                               int16_t(g.w >> 16), hr);
-        oi = hr.id();
+        oi = cell_order_key(int16_t(g.z & 0xffffu), int16_t(g.z >> 16), hr);
       }
       const uint32_t bal = __ballot_sync(0xffffffffu, pass);
       if (pass) {
@@ -296,8 +352,7 @@ __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* _
         const uint4 g = s_geo[w][o];
         const uint32_t k = t - rg.w;
         p = k < rg.y ? rg.x + k : rg.z + (k - rg.y);
-        pass = doublet_pass_a(int(g.w & 0xffu), __uint_as_float(g.x), __uint_as_float(g.y), int16_t(g.z & 0xffffu),
-                              int16_t(g.z >> 16), hrec[p]);
+        pass = doublet_pass_z(int(g.w & 0xffu), __uint_as_float(g.x), __uint_as_float(g.y), hrec[p]);
       }
       const uint32_t bal = __ballot_sync(0xffffffffu, pass);
       if (pass) s_q[w][(qtail + __popc(bal & lt)) % kDblQueue] = (o << kHitIdBits) | p;
@@ -318,6 +373,19 @@ __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* _
       if (x + 1 == nst || s_own[w][x + 1] != o) s_end[w][o] = x + 1;
     }
     __syncwarp();
+    // each item's passing outer hits into the reference's cell order (they came in iphi order
+    // within each bin); a few per item, one lane each
+    if (nc > 0 && nout <= uint32_t(kGroupCells)) {
+      uint32_t* r = s_out[w];
+      const uint32_t b0 = s_beg[w][ci], b1 = s_end[w][ci];
+      for (uint32_t x = b0 + 1; x < b1; ++x) {
+        const uint32_t v = r[x];
+        uint32_t y = x;
+        while (y > b0 && r[y - 1] > v) { r[y] = r[y - 1]; --y; }
+        r[y] = v;
+      }
+    }
+    __syncwarp();
     const uint32_t cnt = nc > 0 ? s_end[w][ci] - s_beg[w][ci] + s_over[w][ci] : 0u;
     if (j < n) d.item_cnt[ib + j] = cnt;
     uint32_t off = kNoPool;
@@ -328,7 +396,7 @@ __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* _
       if (uint64_t(o) + nout <= uint64_t(d.cap_cells)) off = o;
     }
     if (off != kNoPool)
-      for (uint32_t x = lane; x < nout; x += 32) d.dbl_pool[off + x] = s_out[w][x];
+      for (uint32_t x = lane; x < nout; x += 32) d.dbl_pool[off + x] = key_hit(s_out[w][x]);
     const uint32_t ex = warp_incl_scan(cnt) - cnt;
     if (j < n) d.item_pool[ib + j] = off == kNoPool ? kNoPool : off + ex;
     __syncwarp();

@@ -168,6 +168,14 @@ __device__ __forceinline__ bool hit_module(const Dev& d, int e, uint32_t m, HitM
   const uint32_t e1 = module_end1(d.mid, eb, ms, m, nmod, n_el, ms[m + 1], int16_t(hm.me));
   hm.end0 = (m + 1 < nmod) ? e1 - 1 : n_el;
   if (hm.end0 < hm.first0 || hm.end0 > n_el) return false;
+  // A module id with several runs (corrupt or repeated FED data): the reference's serial
+  // getHits writes the same nclus hit slots once per run, so the last run's values are the
+  // ones left. Only that run writes here; the others would race with it.
+  if (E.repeated_ids) {
+    const uint32_t* mid = d.module_id + size_t(e) * kMaxNumModules;
+    for (uint32_t k = m + 1; k < nmod; ++k)
+      if (mid[k] == hm.me) return false;
+  }
   return true;
 }
 
@@ -414,6 +422,22 @@ __global__ void __launch_bounds__(1024) k_phi_binner(Dev d) {
     // hits sit on modules below 2000, so the detector index fits the record's 11 bits
     r.det_id = (uint32_t(d.detind[hb + i]) << kHitIdBits) | i;
     rec[p] = r;
+  }
+  __syncthreads();
+  // the same records sorted by iphi (as uint16) within each bin, for the doublet search's exact
+  // phi windows (one thread per bin; equal iphi keep the bin's order)
+  HitRec* rs = d.hit_rec_s + hb;
+  uint16_t* us = d.hit_u_s + hb;
+  for (int b = threadIdx.x; b < kPhiTotBins - 1; b += blockDim.x) {
+    const uint32_t lo = s_off[b], hi = s_off[b + 1];
+    for (uint32_t p = lo; p < hi; ++p) {
+      const HitRec r = rec[p];
+      const uint16_t u = uint16_t(r.iphi);
+      uint32_t q = p;
+      while (q > lo && us[q - 1] > u) { rs[q] = rs[q - 1]; us[q] = us[q - 1]; --q; }
+      rs[q] = r;
+      us[q] = u;
+    }
   }
 }
 

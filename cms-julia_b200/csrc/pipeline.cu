@@ -226,7 +226,7 @@ int alloc_batch(PxlCtx* ctx) {
   A(xl, d.cap_hits); A(yl, d.cap_hits); A(xerr, d.cap_hits); A(yerr, d.cap_hits);
   A(xg, d.cap_hits); A(yg, d.cap_hits); A(zg, d.cap_hits); A(rg, d.cap_hits);
   A(iphi, d.cap_hits); A(xsize, d.cap_hits); A(ysize, d.cap_hits); A(detind, d.cap_hits); A(charge, d.cap_hits);
-  A(hits_layer_start, E * 11); A(phi_off, E * kPhiTotBins); A(phi_bins, d.cap_hits); A(hit_rec, d.cap_hits); A(hit_sum, d.cap_hits); A(hit_me, d.cap_hits); A(hit_xyzr, d.cap_hits);
+  A(hits_layer_start, E * 11); A(phi_off, E * kPhiTotBins); A(phi_bins, d.cap_hits); A(hit_rec, d.cap_hits); A(hit_rec_s, d.cap_hits); A(hit_u_s, d.cap_hits); A(hit_sum, d.cap_hits); A(hit_me, d.cap_hits); A(hit_xyzr, d.cap_hits);
   A(pair_cum, E * kNPairs);
   A(item_cnt, d.cap_items + 1);
   A(item_pool, d.cap_items); A(dbl_pool, d.cap_cells); A(dbl_pool_ctr, 1);

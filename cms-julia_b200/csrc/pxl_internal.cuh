@@ -155,6 +155,8 @@ struct Dev {
   uint32_t* phi_off;           // [E][1281]
   uint32_t* phi_bins;          // [cap_hits], 1-based hit ids
   struct HitRec* hit_rec;      // [cap_hits] the binned hits' doublet fields, in bin order
+  struct HitRec* hit_rec_s;    // [cap_hits] the same, sorted by iphi (as uint16) within each bin
+  uint16_t* hit_u_s;           // [cap_hits] their iphi (as uint16), for the phi-window searches
   struct ClusSumRec* hit_sum;  // [cap_hits] per-cluster sums of getHits, input of the CPE
   uint32_t* hit_me;            // [cap_hits] module of the hit's record, 0xFFFFFFFF when none
   float4* hit_xyzr;            // [cap_hits] global x, y, z, r of each hit

@@ -1,4 +1,4 @@
-"""Extended-capacity mode on high-pileup events (PU 150-200) above the reference's per-event
+"""Extended-capacity mode on high-pileup events (PU up to 260) above the reference's per-event
 capacities: the CUDA chain with pxl_params_extended must equal the oracle run with the same
 enlarged capacities on every product, and with the reference's capacities both must
 truncate the same way (ca_hit_ntuplet_generator.jl:40 doublets, PixelTrackHeterogeneous.jl:55
@@ -17,7 +17,7 @@ E = 4
 @pytest.fixture(scope="module")
 def high_pu():
     from pixeltrack import gen
-    blob, offs = gen.events(E, gen.MODE_UNIFORM, pu=200, seed=4242)
+    blob, offs = gen.events(E, gen.MODE_UNIFORM, pu=260, seed=4242)
     return blob, offs
 
 
