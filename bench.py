@@ -485,7 +485,10 @@ def chain_fit_precision(chain, conds, blob, offs, E: int, params, n_check: int =
             ch.run_batch(blob, offs)
             segs = dict(ch.profile_read())
         ch.profile(False)
-        fit_ms[name] = segs.get("broken_line_fit_3", 0.0) + segs.get("broken_line_fit_4", 0.0)
+        fit_ms[name] = (segs.get("broken_line_fit_3", 0.0) + segs.get("broken_line_fit_4", 0.0) +
+                        segs.get("broken_line_refit_fp64", 0.0))
+    n_refit = sum(mixed.counts(e).n_fits_fp64 for e in range(E))
+    n_fits = sum(int(mixed.product("fitted", e)[:mixed.counts(e).n_tuples].sum()) for e in range(E))
     chain.run_batch(blob, offs)
     rows = {"q_over_pt_rel": [], "phi_abs_rad": [], "cot_theta_rel": [], "d0_abs_cm": [], "z0_abs_cm": []}
     for e in np.linspace(0, E - 1, min(n_check, E)).astype(int):
@@ -506,6 +509,7 @@ def chain_fit_precision(chain, conds, blob, offs, E: int, params, n_check: int =
     out["tracks"] = int(sum(len(v) for v in rows["q_over_pt_rel"]))
     out["events"] = int(min(n_check, E))
     out["fit_segments_ms"] = fit_ms
+    out["refits_fp64"] = {"tuples": int(n_refit), "of_fitted": int(n_fits), "rule": "mixed fit pT >= 50 GeV"}
     return out
 
 

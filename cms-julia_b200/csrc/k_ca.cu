@@ -373,19 +373,6 @@ __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* _
       if (x + 1 == nst || s_own[w][x + 1] != o) s_end[w][o] = x + 1;
     }
     __syncwarp();
-    // each item's passing outer hits into the reference's cell order (they came in iphi order
-    // within each bin); a few per item, one lane each
-    if (nc > 0 && nout <= uint32_t(kGroupCells)) {
-      uint32_t* r = s_out[w];
-      const uint32_t b0 = s_beg[w][ci], b1 = s_end[w][ci];
-      for (uint32_t x = b0 + 1; x < b1; ++x) {
-        const uint32_t v = r[x];
-        uint32_t y = x;
-        while (y > b0 && r[y - 1] > v) { r[y] = r[y - 1]; --y; }
-        r[y] = v;
-      }
-    }
-    __syncwarp();
     const uint32_t cnt = nc > 0 ? s_end[w][ci] - s_beg[w][ci] + s_over[w][ci] : 0u;
     if (j < n) d.item_cnt[ib + j] = cnt;
     uint32_t off = kNoPool;
@@ -395,8 +382,16 @@ __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* _
       o = __shfl_sync(0xffffffffu, o, 0);
       if (uint64_t(o) + nout <= uint64_t(d.cap_cells)) off = o;
     }
+    // each staged outer hit goes to its place in the reference's cell order, its rank by
+    // cell_order_key among its item's (they came in iphi order within each bin)
     if (off != kNoPool)
-      for (uint32_t x = lane; x < nout; x += 32) d.dbl_pool[off + x] = key_hit(s_out[w][x]);
+      for (uint32_t x = lane; x < nout; x += 32) {
+        const uint32_t v = s_out[w][x], o = s_own[w][x];
+        const uint32_t b0 = s_beg[w][o], b1 = s_end[w][o];
+        uint32_t rank = 0;
+        for (uint32_t y = b0; y < b1; ++y) rank += s_out[w][y] < v;
+        d.dbl_pool[off + b0 + rank] = key_hit(v);
+      }
     const uint32_t ex = warp_incl_scan(cnt) - cnt;
     if (j < n) d.item_pool[ib + j] = off == kNoPool ? kNoPool : off + ex;
     __syncwarp();

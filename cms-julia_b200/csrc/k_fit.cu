@@ -12,8 +12,13 @@ namespace pxl {
 
 namespace {
 
+// Mixed precision keeps q/pT within 1e-5 of FP64 up to pT of about 100 GeV; the few stiffer
+// tuples (about 1 % of a PU50 event's tuples are above 50 GeV) are fitted again in FP64.
+constexpr double kRefitPt = 50.0;
+
+// Returns false, writing nothing, for a mixed-precision fit that needs the FP64 refit.
 template <int N, class T>
-__device__ void fit_tuple(const Dev& d, uint64_t g, uint32_t hb, const uint32_t* hits_of_tuple, double B) {
+__device__ bool fit_tuple(const Dev& d, uint64_t g, uint32_t hb, const uint32_t* hits_of_tuple, double B) {
   double h[3][N];
   float ge[6][N];
 #pragma unroll
@@ -31,6 +36,7 @@ __device__ void fit_tuple(const Dev& d, uint64_t g, uint32_t hb, const uint32_t*
   }
   bl::TrackOut o;
   const bool ok = bl::fit_track<N, T>(h, ge, B, o);
+  if (sizeof(T) == 4 && !(o.pt < kRefitPt)) return false;
   float* st = d.t_state + 5 * g;
   float* cv = d.t_cov + 15 * g;
 #pragma unroll
@@ -42,6 +48,7 @@ __device__ void fit_tuple(const Dev& d, uint64_t g, uint32_t hb, const uint32_t*
   d.t_chi2[g] = float((o.chi2_line + o.chi2_circle) / double(2 * N - 5));
   d.t_fitted[g] = 1;
   (void)ok;
+  return true;
 }
 
 // Which tuples are fitted, and with how many hits: 3-hit tuples with 3, 4- and
@@ -107,7 +114,7 @@ __global__ void __launch_bounds__(256) k_fit_list(Dev d) {
     if (!d.t_fitted[tb + w / 5]) d.t_state[5 * tb + w] = 0.f;
   for (uint32_t w = threadIdx.x; w < 15 * nt; w += blockDim.x)
     if (!d.t_fitted[tb + w / 15]) d.t_cov[15 * tb + w] = 0.f;
-  if (threadIdx.x == 0) { E.n_fit3 = s_n3; E.n_fit4 = s_n4; }
+  if (threadIdx.x == 0) { E.n_fit3 = s_n3; E.n_fit4 = s_n4; E.n_refit3 = 0; E.n_refit4 = 0; }
 }
 
 // one hit count per launch, so that each instantiation keeps only its own registers.
@@ -123,8 +130,28 @@ __global__ void __launch_bounds__(128, 4) k_fit_tuples(Dev d) {
   // B = Float64(Float32(bf)) as HelixFitOnGPU stores the field (ca_hit_ntuplet_generator.jl:83)
   const double B = double(d.c.b_field);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nfit; i += gridDim.x * blockDim.x) {
-    const uint64_t g = tb + d.fit_list[N == 3 ? tb + i : tb + nt - 1 - i];
-    fit_tuple<N, T>(d, g, hb, d.tuple_hits + d.tuple_off[g], B);
+    const uint32_t t = d.fit_list[N == 3 ? tb + i : tb + nt - 1 - i];
+    const uint64_t g = tb + t;
+    if (!fit_tuple<N, T>(d, g, hb, d.tuple_hits + d.tuple_off[g], B)) {
+      EvInfo& Ew = d.ev[e];
+      const uint32_t k = atomicAdd(N == 3 ? &Ew.n_refit3 : &Ew.n_refit4, 1u);
+      d.refit_list[N == 3 ? tb + k : tb + nt - 1 - k] = t;
+    }
+  }
+}
+
+// FP64 refits of the mixed-precision fits that asked for one (same list layout as fit_list)
+template <int N>
+__global__ void __launch_bounds__(128, 4) k_refit_tuples(Dev d) {
+  const int e = blockIdx.y;
+  const EvInfo& E = d.ev[e];
+  const uint64_t tb = E.tuple_base;
+  const uint32_t hb = E.hit_base;
+  const uint32_t nt = E.n_tuples, nfit = N == 3 ? E.n_refit3 : E.n_refit4;
+  const double B = double(d.c.b_field);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nfit; i += gridDim.x * blockDim.x) {
+    const uint64_t g = tb + d.refit_list[N == 3 ? tb + i : tb + nt - 1 - i];
+    fit_tuple<N, double>(d, g, hb, d.tuple_hits + d.tuple_off[g], B);
   }
 }
 
@@ -228,6 +255,10 @@ void launch_fit(const Dev& d, const Launch& L) {
     L.mark("broken_line_fit_3");
     k_fit_tuples<4, float><<<dim3(bx, d.E), 128, 0, L.s>>>(d);
     L.mark("broken_line_fit_4");
+    // about 1 % of the fits: one block per event and hit count
+    k_refit_tuples<3><<<dim3(1, d.E), 128, 0, L.s>>>(d);
+    k_refit_tuples<4><<<dim3(1, d.E), 128, 0, L.s>>>(d);
+    L.mark("broken_line_refit_fp64");
   } else {
     k_fit_tuples<3, double><<<dim3(bx, d.E), 128, 0, L.s>>>(d);
     L.mark("broken_line_fit_3");

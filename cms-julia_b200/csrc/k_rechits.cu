@@ -399,46 +399,40 @@ __global__ void __launch_bounds__(1024) k_phi_binner(Dev d) {
     bins[w - 1] = i + 1;
   }
   __syncthreads();
-  // order each bin by decreasing hit id
-  for (int b = threadIdx.x; b < kPhiTotBins - 1; b += blockDim.x) {
-    const uint32_t lo = s_off[b], hi = s_off[b + 1];
-    for (uint32_t p = lo + 1; p < hi; ++p) {
-      const uint32_t v = bins[p];
-      uint32_t q = p;
-      while (q > lo && bins[q - 1] < v) { bins[q] = bins[q - 1]; --q; }
-      bins[q] = v;
-    }
-  }
   for (int b = threadIdx.x; b < kPhiTotBins; b += blockDim.x) poff[b] = s_off[b];
-  __syncthreads();
+  // Each binned hit's place in two orders of its bin, by its rank among the bin's hits (a
+  // bin holds a few tens of hits): decreasing hit id, the reference's order (its fill
+  // decrements the bin cursor), for the doublet records and the bins; and increasing iphi
+  // (as uint16, ties by decreasing id) for the records of the doublet search's exact phi
+  // windows.
   HitRec* rec = d.hit_rec + hb;
+  HitRec* rs = d.hit_rec_s + hb;
+  uint16_t* us = d.hit_u_s + hb;
   for (uint32_t p = threadIdx.x; p < ntot; p += blockDim.x) {
-    const uint32_t i = bins[p] - 1u;
+    const uint32_t v = bins[p], i = v - 1u;
+    const uint32_t b = bin_of(i) - 1u;
+    const uint32_t lo = s_off[b], hi = s_off[b + 1];
+    const uint16_t u = uint16_t(d.iphi[hb + i]);
+    uint32_t rid = 0, ru = 0;
+    for (uint32_t q = lo; q < hi; ++q) {
+      const uint32_t w = bins[q];
+      const uint16_t uq = uint16_t(d.iphi[hb + w - 1u]);
+      rid += w > v;
+      ru += uq < u || (uq == u && w > v);
+    }
     HitRec r;
     r.z = d.zg[hb + i];
     r.r = d.rg[hb + i];
-    r.iphi = d.iphi[hb + i];
+    r.iphi = int16_t(u);
     r.ysize = d.ysize[hb + i];
     // hits sit on modules below 2000, so the detector index fits the record's 11 bits
     r.det_id = (uint32_t(d.detind[hb + i]) << kHitIdBits) | i;
-    rec[p] = r;
+    rec[lo + rid] = r;
+    rs[lo + ru] = r;
+    us[lo + ru] = u;
   }
   __syncthreads();
-  // the same records sorted by iphi (as uint16) within each bin, for the doublet search's exact
-  // phi windows (one thread per bin; equal iphi keep the bin's order)
-  HitRec* rs = d.hit_rec_s + hb;
-  uint16_t* us = d.hit_u_s + hb;
-  for (int b = threadIdx.x; b < kPhiTotBins - 1; b += blockDim.x) {
-    const uint32_t lo = s_off[b], hi = s_off[b + 1];
-    for (uint32_t p = lo; p < hi; ++p) {
-      const HitRec r = rec[p];
-      const uint16_t u = uint16_t(r.iphi);
-      uint32_t q = p;
-      while (q > lo && us[q - 1] > u) { rs[q] = rs[q - 1]; us[q] = us[q - 1]; --q; }
-      rs[q] = r;
-      us[q] = u;
-    }
-  }
+  for (uint32_t p = threadIdx.x; p < ntot; p += blockDim.x) bins[p] = (rec[p].det_id & (kMaxHitsPerEvent - 1u)) + 1u;
 }
 
 }  // namespace

@@ -243,7 +243,7 @@ int alloc_batch(PxlCtx* ctx) {
   A(tm_bins, d.cap_tuples);
   A(t_state, 5 * d.cap_tuples); A(t_cov, 15 * d.cap_tuples); A(t_pt, d.cap_tuples); A(t_eta, d.cap_tuples);
   A(t_chi2, d.cap_tuples); A(t_fitted, d.cap_tuples);
-  A(fit_list, d.cap_tuples);
+  A(fit_list, d.cap_tuples); A(refit_list, d.cap_tuples);
   A(htt_cnt, d.cap_hits + 1); A(htt_cur, d.cap_hits); A(htt_list, d.cap_tuple_hits);
   A(dup_bits, d.cap_cells / 32 + 2); A(dup_list, d.cap_cells); A(dup_eoff, d.cap_cells + E + 1);
   A(dup_et, d.cap_tuple_hits); A(dup_ek, d.cap_tuple_hits);
@@ -758,6 +758,7 @@ int32_t pxl_event_counts(PxlCtx* ctx, int32_t e, PxlEventCounts* out) {
   out->n_vertex_tracks = E.n_vtx_tracks;
   out->warnings = E.warnings;
   out->n_errors = E.n_errors;
+  out->n_fits_fp64 = E.n_refit3 + E.n_refit4;
   return 0;
 }
 

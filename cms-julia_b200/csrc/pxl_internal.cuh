@@ -92,6 +92,7 @@ struct EvInfo {
   uint32_t n_dup_cells, dup_cell_base;
   uint32_t n_cols_nb, n_cols_tr;    // non-empty neighbour / track lists (column store use)
   uint32_t n_fit3, n_fit4;          // tuples fitted with 3 and with 4 hits (fit5as4 included)
+  uint32_t n_refit3, n_refit4;      // of those, mixed-precision fits redone in FP64
   // 1 when a module id starts more than one module run (only corrupted data does that): the
   // charge cut of such an event runs in the reference's serial order (k_charge_cut_serial)
   uint32_t repeated_ids;
@@ -199,6 +200,7 @@ struct Dev {
   // fit results [cap_tuples]
   float* t_state; float* t_cov; float* t_pt; float* t_eta; float* t_chi2; uint8_t* t_fitted;
   uint32_t* fit_list;      // [cap_tuples] per event: 3-hit fits from the front, 4-hit fits from the back
+  uint32_t* refit_list;    // [cap_tuples] per event, the same way: mixed-precision fits redone in FP64
   // hit -> tuple lists
   uint32_t* htt_cnt;       // [cap_hits + 1]
   uint32_t* htt_cur;

@@ -50,7 +50,7 @@ class PxlParams(ctypes.Structure):
 class PxlEventCounts(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint32) for n in (
         "n_words", "n_modules", "n_clusters", "n_hits", "n_doublets", "n_tuples", "n_tuple_hits",
-        "n_vertices", "n_vertex_tracks", "warnings", "n_errors")]
+        "n_vertices", "n_vertex_tracks", "warnings", "n_errors", "n_fits_fp64")]
 
 
 class PxlExport(ctypes.Structure):

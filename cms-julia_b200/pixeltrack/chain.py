@@ -47,6 +47,7 @@ class EventCounts:
     n_vertex_tracks: int
     warnings: int
     n_errors: int
+    n_fits_fp64: int
 
 
 def default_params(**kw) -> PxlParams:

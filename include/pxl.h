@@ -98,7 +98,8 @@ typedef struct PxlParams {
   int32_t fit_precision;             /* broken-line fits of the chain: 0 = FP64 as the reference
                                         (broken_line_fit_on_gpu.jl:28-30); 1 = FP32 arithmetic with
                                         the band solve, transport and covariance in FP64 (pxl_bl_fit
-                                        precision 1) */
+                                        precision 1); a tuple whose FP32 fit gives pT >= 50 GeV (or
+                                        no finite pT) is fitted again in FP64 (n_fits_fp64) */
 } PxlParams;
 
 typedef struct PxlEventCounts {
@@ -113,6 +114,7 @@ typedef struct PxlEventCounts {
   uint32_t n_vertex_tracks;
   uint32_t warnings;     /* PXL_WARN_* */
   uint32_t n_errors;     /* FED error records */
+  uint32_t n_fits_fp64;  /* fit_precision 1: tuples fitted again in FP64 (stiff tracks) */
 } PxlEventCounts;
 
 /* Products in the reference's layout, for pxl_copy_product (element type in brackets,
