@@ -256,7 +256,8 @@ __device__ __forceinline__ void unpack_word(const Dev& d, int e, uint32_t local,
 // is read with 128-bit loads where it sits on 4-byte boundaries (always, for FED sizes in whole
 // 64-bit words): the words before the first 16-byte boundary and after the last one are read
 // singly, the rest four per thread.
-__global__ void k_unpack(Dev d) {
+__global__ void __launch_bounds__(256) k_unpack(Dev d) {
+  __shared__ __align__(16) uint32_t s_words[8][128];
   const int f = blockIdx.x, e = blockIdx.y;
   const int NF = d.n_fed_slots;
   const size_t fs = size_t(e) * NF + f;
@@ -291,13 +292,21 @@ __global__ void k_unpack(Dev d) {
     if (threadIdx.x < head) word(threadIdx.x, __ldg(src32 + threadIdx.x));
     const uint32_t nvec = (nw - head) >> 2;
     const uint4* v = reinterpret_cast<const uint4*>(src32 + head);
-    for (uint32_t j = threadIdx.x; j < nvec; j += blockDim.x) {
-      const uint4 q = __ldg(v + j);
-      const uint32_t k = head + 4 * j;
-      word(k, q.x);
-      word(k + 1, q.y);
-      word(k + 2, q.z);
-      word(k + 3, q.w);
+    // a warp loads 32 aligned 16-byte vectors (128 words) and decodes them word by word through
+    // shared memory, lane l taking words l, l + 32, l + 64, l + 96, so that the per-digi stores
+    // of consecutive lanes stay consecutive
+    const unsigned lane = threadIdx.x & 31u, wq = threadIdx.x >> 5;
+    uint32_t* sw = s_words[wq];
+    for (uint32_t j0 = 32u * wq; j0 < nvec; j0 += blockDim.x) {
+      if (j0 + lane < nvec) reinterpret_cast<uint4*>(sw)[lane] = __ldg(v + j0 + lane);
+      __syncwarp();
+      const uint32_t nwords = 4u * min(32u, nvec - j0);
+#pragma unroll
+      for (uint32_t i = 0; i < 4; ++i) {
+        const uint32_t wi = 32u * i + lane;
+        if (wi < nwords) word(head + 4u * j0 + wi, sw[wi]);
+      }
+      __syncwarp();
     }
     for (uint32_t k = head + 4 * nvec + threadIdx.x; k < nw; k += blockDim.x) word(k, __ldg(src32 + k));
   } else {
