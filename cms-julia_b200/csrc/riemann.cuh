@@ -10,10 +10,10 @@
 // and tan(theta) in the line's scattering term, and (phi, d0, pT) from the circle
 // geometry (pT = R B).
 //
-// Precision: T is the type of the per-hit geometry and the scattering models;
-// the per-hit projected variances, the inverses of the N x N covariance matrices
-// (Cholesky), the scatter matrix, its 3x3 eigenproblem and the final parameters
-// are FP64.
+// Precision: T is the type of the per-hit geometry and the circle's scattering model;
+// the per-hit projected variances, the line's arc lengths and scattering covariance, the
+// inverses of the N x N covariance matrices (Cholesky), the scatter matrix, its 3x3
+// eigenproblem and the final parameters are FP64.
 #pragma once
 #include "bl_fit.cuh"
 
@@ -295,8 +295,16 @@ BL_HD bool riemann_fit_frame(const double hits[3][N], const float ge[6][N], cons
   for (int i = 0; i < N; ++i) {
     const T qx = px[i] - ox, qy = py[i] - oy;  // hit - centre
     const T cr = bl::diff_of_products<T>(goy, qx, gox, qy), dt = -gox * qx - goy * qy;
-    const T at = -T(q) * bl_atan2<T>(cr, dt);
-    sarc[i] = at * Rt;
+    if constexpr (sizeof(T) == 4) {
+      // the arc lengths in FP64: the line of a nearly flat track (cot(theta) ~ 1e-3) with a
+      // large chi2 moves with them by more than their FP32 rounding allows
+      const double hx = double(px[i]) - cx, hy = double(py[i]) - cy;
+      const double gx = hits[0][0] + cx, gy = hits[1][0] + cy;
+      sarc[i] = T(-double(q) * atan2(gy * hx - gx * hy, -gx * hx - gy * hy) * R);
+    } else {
+      const T at = -T(q) * bl_atan2<T>(cr, dt);
+      sarc[i] = at * Rt;
+    }
     const T temp0 = -T(q) * Rt / (dt * dt + cr * cr);
     const T d_x = temp0 * (goy * dt + gox * cr), d_y = temp0 * (-gox * dt + goy * cr);
     // Jx (V) Jx^T for the (s, z) pair, then the Z' variance after the rotation
@@ -310,29 +318,34 @@ BL_HD bool riemann_fit_frame(const double hits[3][N], const float ge[6][N], cons
   }
   double Cz[N][N];
   {
-    const T p_t = fR * B < T(20) ? fR * B : T(20);
-    const T p_2 = p_t * p_t * (T(1) + T(1) / (ftan * ftan));
-    T S3[N], sig2[N];
-    const T x0inv = T(0.06 / 16.0);
+    // The line's scattering covariance is built in FP64 in both modes: its path lengths S3
+    // run from the origin with the absolute z (the reference's choice), so they are large
+    // against their differences, and a nearly flat line (cot(theta) ~ 1e-3) through hits with
+    // a large chi2 moves with the relative weights by more than the FP32 rounding allows.
+    const double ft = double(ftan);
+    const double p_t = double(fR * B < T(20) ? fR * B : T(20));
+    const double p_2 = p_t * p_t * (1.0 + 1.0 / (ft * ft));
+    double S3[N], sig2[N];
+    const double x0inv = 0.06 / 16.0;
 #pragma unroll
     for (int i = 0; i < N; ++i) {
-      const T zi = T(hits[2][i]);
-      S3[i] = s_sqrt<T>(sarc[i] * sarc[i] + zi * zi);
+      const double si = double(sarc[i]), zi = hits[2][i];
+      S3[i] = sqrt(si * si + zi * zi);
     }
 #pragma unroll
     for (int i = 0; i < N; ++i) {
-      const T rl = (i == 0 ? S3[0] : s_abs(S3[i] - S3[i - 1])) * x0inv;
-      const T l = rl > T(0) ? T(1) + T(0.038) * s_log<T>(rl) : T(0);
-      sig2[i] = T(0.000225) / p_2 * (l * l) * rl;
+      const double rl = (i == 0 ? S3[0] : fabs(S3[i] - S3[i - 1])) * x0inv;
+      const double l = rl > 0.0 ? 1.0 + 0.038 * log(rl) : 0.0;
+      sig2[i] = 0.000225 / p_2 * (l * l) * rl;
     }
 #pragma unroll
     for (int k = 0; k < N; ++k)
 #pragma unroll
       for (int l = k; l < N; ++l) {
-        T v2 = T(0);
+        double v2 = 0.0;
 #pragma unroll
-        for (int i = 0; i <= (k < l ? k : l); ++i) v2 += s_abs(S3[k] - S3[i]) * s_abs(S3[l] - S3[i]) * sig2[i];
-        Cz[k][l] = double(v2) + (k == l ? double(cov_zz[k]) : 0.0);
+        for (int i = 0; i <= (k < l ? k : l); ++i) v2 += fabs(S3[k] - S3[i]) * fabs(S3[l] - S3[i]) * sig2[i];
+        Cz[k][l] = v2 + (k == l ? double(cov_zz[k]) : 0.0);
         Cz[l][k] = Cz[k][l];
       }
   }
