@@ -219,7 +219,11 @@ __device__ __forceinline__ bool doublet_pass_z(int pid, float me_z, float me_r, 
 }
 
 // Reference order of a passing outer hit among its item's cells: the window's bins in order
-// (bin offset from the item's first bin kl), then decreasing hit id within a bin.
+// (bin offset from the item's first bin kl), then decreasing hit id within a bin. A window of
+// at most 2 * 730 + 1 iphi units touches at most four 512-unit bins, so the bin offset takes
+// bits 21-26 and bits 27-31 stay free for the item's slot in its warp group (kOwnerShift).
+constexpr uint32_t kOwnerShift = 27;
+static_assert(kHitIdBits + 6 <= kOwnerShift, "bin offset bits");
 __device__ __forceinline__ uint32_t cell_order_key(int16_t me_p, int16_t cut, const HitRec& hr) {
   const uint32_t kl = (uint32_t(uint16_t(me_p - cut)) >> 9) + 1u;
   const uint32_t bo = (((uint32_t(uint16_t(hr.iphi)) >> 9) + 1u - kl) & 127u);
@@ -278,10 +282,10 @@ __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* _
   __shared__ uint32_t s_hls[11];
   __shared__ uint4 s_rng[8][32];   // per compacted item: lo0, n0, lo1, first candidate
   __shared__ uint4 s_geo[8][32];   // per compacted item: z, r (float bits), iphi | cut << 16, pid | ysize << 16
-  __shared__ uint32_t s_beg[8][32], s_end[8][32], s_over[8][32];
+  __shared__ uint16_t s_beg[8][32], s_end[8][32];
+  __shared__ uint32_t s_over[8][32];
   __shared__ uint32_t s_q[8][kDblQueue];  // owner << kHitIdBits | candidate
-  __shared__ uint32_t s_out[8][kGroupCells];
-  __shared__ uint8_t s_own[8][kGroupCells];
+  __shared__ uint32_t s_out[8][kGroupCells];  // owner << kOwnerShift | cell_order_key
   for_each_vblock<kQ>(q, [&](int e, uint32_t bx, uint32_t nbx) {
   const EvInfo& E = d.ev[e];
   const uint32_t n = E.n_items;
@@ -328,12 +332,12 @@ __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* _
         const HitRec hr = hrec[v & (kMaxHitsPerEvent - 1u)];
         pass = doublet_pass_b(int(g.w & 0xffu), __uint_as_float(g.x), __uint_as_float(g.y), int16_t(g.z & 0xffffu),
                               int16_t(g.w >> 16), hr);
-        oi = cell_order_key(int16_t(g.z & 0xffffu), int16_t(g.z >> 16), hr);
+        oi = (o << kOwnerShift) | cell_order_key(int16_t(g.z & 0xffffu), int16_t(g.z >> 16), hr);
       }
       const uint32_t bal = __ballot_sync(0xffffffffu, pass);
       if (pass) {
         const uint32_t pos = nout + __popc(bal & lt);
-        if (pos < uint32_t(kGroupCells)) { s_out[w][pos] = oi; s_own[w][pos] = uint8_t(o); }
+        if (pos < uint32_t(kGroupCells)) s_out[w][pos] = oi;
         else atomicAdd(&s_over[w][o], 1u);
       }
       nout += __popc(bal);
@@ -368,9 +372,9 @@ __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* _
     // doublets per item: the staged outputs are in item order, so each item's are one run
     const uint32_t nst = nout < uint32_t(kGroupCells) ? nout : uint32_t(kGroupCells);
     for (uint32_t x = lane; x < nst; x += 32) {
-      const uint32_t o = s_own[w][x];
-      if (x == 0 || s_own[w][x - 1] != o) s_beg[w][o] = x;
-      if (x + 1 == nst || s_own[w][x + 1] != o) s_end[w][o] = x + 1;
+      const uint32_t o = s_out[w][x] >> kOwnerShift;
+      if (x == 0 || (s_out[w][x - 1] >> kOwnerShift) != o) s_beg[w][o] = uint16_t(x);
+      if (x + 1 == nst || (s_out[w][x + 1] >> kOwnerShift) != o) s_end[w][o] = uint16_t(x + 1);
     }
     __syncwarp();
     const uint32_t cnt = nc > 0 ? s_end[w][ci] - s_beg[w][ci] + s_over[w][ci] : 0u;
@@ -382,12 +386,12 @@ __global__ void __launch_bounds__(256) k_doublets_count(Dev d, const uint32_t* _
       o = __shfl_sync(0xffffffffu, o, 0);
       if (uint64_t(o) + nout <= uint64_t(d.cap_cells)) off = o;
     }
-    // each staged outer hit goes to its place in the reference's cell order, its rank by
-    // cell_order_key among its item's (they came in iphi order within each bin)
+    // each staged outer hit goes to its place in the reference's cell order, its rank by key
+    // among its item's (they came in iphi order within each bin)
     if (off != kNoPool)
       for (uint32_t x = lane; x < nout; x += 32) {
-        const uint32_t v = s_out[w][x], o = s_own[w][x];
-        const uint32_t b0 = s_beg[w][o], b1 = s_end[w][o];
+        const uint32_t v = s_out[w][x];
+        const uint32_t b0 = s_beg[w][v >> kOwnerShift], b1 = s_end[w][v >> kOwnerShift];
         uint32_t rank = 0;
         for (uint32_t y = b0; y < b1; ++y) rank += s_out[w][y] < v;
         d.dbl_pool[off + b0 + rank] = key_hit(v);
