@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define PXL_ABI_VERSION 2
+#define PXL_ABI_VERSION 3  /* 3: PxlEventCounts.n_fits_fp64 */
 
 /* fatal status codes */
 #define PXL_ERR_ARG (-1)

@@ -31,7 +31,7 @@ def test_bindings_cover_the_header():
 
 def test_version_without_gpu():
     from pixeltrack import _native
-    assert _native.lib().pxl_version() == 2
+    assert _native.lib().pxl_version() == 3
 
 
 def test_params_default_are_the_reference_capacities():
