@@ -100,7 +100,7 @@ def test_standalone_fit_fixtures(precision):
     data, hits, ge, offs = _fixture_tracks()
     out = bl_fit(torch.as_tensor(hits).cuda(), torch.as_tensor(ge).cuda(), torch.as_tensor(offs).cuda(), data["B"],
                  precision=precision)
-    # FP64 fit: outputs stored as FP32; mixed precision: the north-star bound, 1e-5
+    # FP64 fit: outputs stored as FP32; mixed precision: within 1e-5 of FP64
     tol = 1e-6 if precision == 0 else 1e-5
     for k, n in enumerate(("3", "4", "5")):
         ref = data["fits"][n]["oracle"]
