@@ -3,7 +3,8 @@
 One step = the whole chain (raw FED words -> digis -> clusters -> rechits -> CA
 ntuplets -> broken-line fits -> classification -> vertices) over one batch of
 synthetic PU50 events (1000 by default), replayed as one CUDA graph with the input
-already in HBM. Also measured: the same metric end to end through the public API
+already in HBM; two contexts on two streams take alternate steps, so that two batches are
+in flight. Also measured: the same metric end to end through the public API
 (host->device copy of the raw events from pinned memory and device->host copy of the
 batch's track and vertex collections inside the timed region), the plain per-event launch sequence,
 per-kernel times (live CUDA events) for the roofline of the dominant kernel, and the
@@ -32,7 +33,8 @@ for p in (ROOT, ROOT / "cms-julia_b200"):
 
 METRIC = "PU50 events/s on 1 B200 batched vs plain; BL fits/s and err vs FP64"
 WORKLOAD = ("synthetic PU50 events (50 vertices x Poisson(30) helix tracks, |eta|<2.5, pT 0.5-10 GeV, 1e-4 noise, "
-            "1% inefficiency) on a seeded Phase-1-like geometry, batched by prefix offsets, one CUDA graph per step")
+            "1% inefficiency) on a seeded Phase-1-like geometry, batched by prefix offsets, one CUDA graph per step; "
+            "two contexts on two streams take alternate steps, so that two batches are in flight")
 
 
 def parse():
@@ -635,22 +637,36 @@ def main():
     # the chain's fits in mixed precision against its FP64 fits
     chain_mixed = chain_fit_precision(chain, conds, blob, offs, E, params)
 
-    # batched graph: input in HBM, one replay per step
-    chain.stage_batch(blob, offs, sh)
-    stream.synchronize()
-    chain.capture_graph()
+    # batched graph: input in HBM, one replay per step. A second context on its own stream
+    # takes every other step, so that two batches are in flight: one batch's kernels fill the
+    # SMs that the other's last waves and per-event stages leave idle (the reference's
+    # analogue is its several stream threads, each with its own producers).
+    chain2 = PixelChain(conds, params)
+    stream2 = torch.cuda.Stream(device=local)
+    sh2 = stream2.cuda_stream
+    chain2.stage_batch(blob, offs, sh2)
+    stream2.synchronize()
+    if args.bpe == 0:
+        chain2.autotune()
+    chains, streams, shs = [chain, chain2], [stream, stream2], [sh, sh2]
+    for c, s_, h_ in zip(chains, streams, shs):
+        c.stage_batch(blob, offs, h_)
+        s_.synchronize()
+        c.capture_graph()
     kernels_per_step = chain.graph_kernel_nodes()
-    for _ in range(args.warmup):
-        chain.launch_graph(sh)
-    stream.synchronize()
+    for k in range(max(args.warmup, 2)):
+        chains[k % 2].launch_graph(shs[k % 2])
+    torch.cuda.synchronize()
     if dist:
         dist.barrier()
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
         t0.record(stream)
-        for _ in range(args.steps):
-            chain.launch_graph(sh)
+        stream2.wait_event(t0)
+        for k in range(args.steps):
+            chains[k % 2].launch_graph(shs[k % 2])
+        stream.wait_stream(stream2)
         t1.record(stream)
         t1.synchronize()
     ms = pdist.max_over_ranks(t0.elapsed_time(t1), device="cuda")
@@ -659,9 +675,10 @@ def main():
 
     # end to end through the public API: pinned host raw events in; the batch's track and vertex
     # collections out (pxl_export_async: the loose tracks' parameters, hit counts and vertex
-    # ids, the vertices, and the per-event index, one copy per array). Batch i+1 is copied into
-    # the other input slot on a copy stream while batch i runs, and batch i's collections go
-    # to host memory on a third stream while batch i+1 runs.
+    # ids, the vertices, and the per-event index, one copy per array). The two contexts take
+    # alternate steps on their own streams; batch i+1 is copied into its context's next input
+    # slot on a copy stream while batch i runs, and batch i's collections go to host memory on
+    # a third stream.
     from pixeltrack import TrackExport
     pinned = torch.empty(len(blob), dtype=torch.uint8, pin_memory=True)
     pinned.numpy()[:] = blob
@@ -679,24 +696,25 @@ def main():
     d2h_stream = torch.cuda.Stream(device=local)
 
     def e2e_steps(n):
-        chain.stage_slot(0, pinned_np, offs, copy.cuda_stream)
-        for i in range(n):
-            chain.launch_slot(i % 2, sh)
-            chain.export_async(outs[i % 2], sh, d2h_stream.cuda_stream)
-            if i + 1 < n:
-                chain.stage_slot((i + 1) % 2, pinned_np, offs, copy.cuda_stream)
+        chains[0].stage_slot(0, pinned_np, offs, copy.cuda_stream)
+        for k in range(n):
+            i, slot = k % 2, (k // 2) % 2
+            chains[i].launch_slot(slot, shs[i])
+            chains[i].export_async(outs[k % 2], shs[i], d2h_stream.cuda_stream)
+            if k + 1 < n:
+                chains[(k + 1) % 2].stage_slot(((k + 1) // 2) % 2, pinned_np, offs, copy.cuda_stream)
 
-    e2e_steps(args.warmup)
-    stream.synchronize()
-    d2h_stream.synchronize()
+    e2e_steps(max(args.warmup, 2))
+    torch.cuda.synchronize()
     if dist:
         dist.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     e0.record(stream)
-    copy.wait_event(e0)
-    d2h_stream.wait_event(e0)
+    for s_ in (copy, d2h_stream, stream2):
+        s_.wait_event(e0)
     e2e_steps(args.steps)
+    stream.wait_stream(stream2)
     stream.wait_stream(d2h_stream)
     e1.record(stream)
     e1.synchronize()
@@ -759,7 +777,7 @@ def main():
             "metric": METRIC, "value": value, "unit": "events/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32/f32/f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "events_per_step": E, "pileup": args.pu,
+            "config": {"workload": WORKLOAD, "events_per_step": E, "pileup": args.pu, "contexts_in_flight": 2,
                        "raw_bytes_per_step": int(offs[-1]), "l2": "inputs and intermediates larger than L2",
                        "parallelism": f"events sharded over {world} GPU(s), no data-path collective",
                        "blocks_per_event": tuned or args.bpe},
@@ -774,6 +792,7 @@ def main():
             "vertices_per_event": nv_check / E,
         }
         print(json.dumps(line), flush=True)
+    chain2.close()
     chain.close()
     if dist:
         dist.barrier()
