@@ -158,51 +158,63 @@ FIT_B = 0.0114256972711507  # 1/(pT R) at 3.8 T, GeV^-1 cm^-1
 
 def bench_uneven(args, local: int, rank: int, world: int, plain_value: float) -> dict:
     """Batched uneven events: 4096 events with pileup drawn uniformly from [0, 200] (about
-    12k-130k digis each), in the extended-capacity mode (no event truncated), run as two
-    resident 2048-event halves, each one captured CUDA graph over prefix-offset packed input,
-    launch shapes from the autotuner. The parity check (outside the timed region) compares
-    every event's counts with the oracle run with the same capacities, and every product of
-    the ten largest events."""
+    1k-130k digis per event), extended per-event capacities so that no event is truncated, as
+    four resident 1024-event quarters on two contexts (each holding two quarters in its two
+    input slots, each slot one captured CUDA graph over prefix-offset packed input) that run
+    on two streams, so that two quarters are in flight; launch shapes from the autotuner. The
+    parity check (outside the timed region) compares every event's counts with the oracle run
+    with the same capacities, and every product of the ten largest events."""
     import torch
     from pixeltrack import dist as pdist
     from pixeltrack import PixelChain, batch_params, gen
     E = args.uneven_events
-    H = E // 2
+    NQ = 4
+    H = E // NQ
     conds = gen.conditions()
     blob, offs = gen.events(E, gen.MODE_UNIFORM, pu=200.0, seed=args.seed + 31 + 7919 * rank)
     words = int(np.diff(offs).sum() // 4)
     params = batch_params(H, words_per_event=int(words / E * 1.4) + 4096, hits_per_event_avg=24_000,
                           doublets_per_event_avg=360_000, tuples_per_event_avg=36_000, device=local,
                           extended=True)
-    chain = PixelChain(conds, params)
-    stream = torch.cuda.Stream(device=local)
-    sh = stream.cuda_stream
-    halves = [(blob[int(offs[k * H]):int(offs[(k + 1) * H])], offs[k * H:(k + 1) * H + 1] - offs[k * H])
-              for k in range(2)]
-    chain.stage_batch(*halves[0], sh)
-    stream.synchronize()
+    chains = [PixelChain(conds, params) for _ in range(2)]
+    streams = [torch.cuda.Stream(device=local) for _ in range(2)]
+    shs = [s_.cuda_stream for s_ in streams]
+    quarters = [(blob[int(offs[k * H]):int(offs[(k + 1) * H])], offs[k * H:(k + 1) * H + 1] - offs[k * H])
+                for k in range(NQ)]
+    # quarter k runs on context k % 2 from its input slot k // 2
 
     def timed_step(candidates):
-        """Tunes the launch shapes among candidates on the first half, captures both halves'
-        graphs (resident in the context's two input slots) and times the step."""
-        chain.stage_batch(*halves[0], sh)
-        stream.synchronize()
-        tuned = chain.autotune(candidates=candidates)
-        chain.stage_batch(*halves[0], sh)
-        stream.synchronize()
-        chain.capture_graph()
-        chain.stage_slot(1, *halves[1], sh)
-        stream.synchronize()
+        """Tunes the launch shapes among candidates on each context's first quarter, captures
+        the quarters' graphs (resident in the contexts' input slots) and times the step."""
+        tuned = {}
+        for i, c in enumerate(chains):
+            c.stage_batch(*quarters[i], shs[i])
+            streams[i].synchronize()
+            t = c.autotune(candidates=candidates)
+            tuned = tuned or t
+            c.stage_batch(*quarters[i], shs[i])
+            streams[i].synchronize()
+            c.capture_graph()
+            c.stage_slot(1, *quarters[i + 2], shs[i])
+            streams[i].synchronize()
+
+        def step():
+            for k in range(NQ):
+                chains[k % 2].launch_slot(k // 2, shs[k % 2])
+
         for _ in range(args.warmup):
-            chain.launch_slot(0, sh)
-            chain.launch_slot(1, sh)
-        warn = chain.sync()
+            step()
+        warn = 0
+        for c in chains:
+            warn |= c.sync()
+        torch.cuda.synchronize()
         t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        t0.record(stream)
+        t0.record(streams[0])
+        streams[1].wait_event(t0)
         for _ in range(args.uneven_steps):
-            chain.launch_slot(0, sh)
-            chain.launch_slot(1, sh)
-        t1.record(stream)
+            step()
+        streams[0].wait_stream(streams[1])
+        t1.record(streams[0])
         t1.synchronize()
         return pdist.max_over_ranks(t0.elapsed_time(t1), device=torch.device("cuda", local)) / args.uneven_steps, \
             tuned, warn
@@ -223,8 +235,9 @@ def bench_uneven(args, local: int, rank: int, world: int, plain_value: float) ->
         orc = oracle.Oracle(conds, oracle.EXTENDED_CAPS)
         _, ocnt = orc.run_batch(blob, offs, os.cpu_count() or 1, counts=True)
         expected = validator_counts(ocnt)
-    for k in range(2):
-        chain.launch_slot(k, sh)
+    for k in range(NQ):
+        chain = chains[k % 2]
+        chain.launch_slot(k // 2, shs[k % 2])
         warn |= chain.sync()
         if orc is not None:
             good += chain.validate_counts(expected[k * H:(k + 1) * H])[0]
@@ -236,7 +249,8 @@ def bench_uneven(args, local: int, rank: int, world: int, plain_value: float) ->
                 errs = compare_event(chain, orc, e)
                 if errs:
                     prod_err[g] = errs[:3]
-    chain.close()
+    for c in chains:
+        c.close()
     if orc is not None:
         from oracle.compare import compare_counts
         bad = compare_counts(counts, ocnt)
@@ -256,9 +270,10 @@ def bench_uneven(args, local: int, rank: int, world: int, plain_value: float) ->
         tot["capped_events"] += int(bool(c.warnings & 0x5D))
         tot["buffer_overflow_events"] += int(bool(c.warnings & 0x800))
     value = world * E / (ms / 1e3)
-    return {"workload": f"{E} synthetic events, pileup uniform in [0, 200], extended per-event capacities, two "
-                        f"resident {H}-event halves per step, each one CUDA graph over prefix-offset packed input, "
-                        "autotuned launch shapes", "events_per_step": E, "value": value,
+    return {"workload": f"{E} synthetic events, pileup uniform in [0, 200], extended per-event capacities, "
+                        f"{NQ} resident {H}-event quarters per step on two contexts and two streams (two quarters "
+                        "in flight), each one CUDA graph over prefix-offset packed input, autotuned launch shapes",
+            "events_per_step": E, "value": value,
             "unit": "events/s", "ms_per_step": ms, "steps": args.uneven_steps, "raw_bytes_per_step": int(offs[-1]),
             "over_plain_per_event_pu50": value / world / plain_value if plain_value else None,
             "blocks_per_event": tuned, "totals": tot, "warnings": [n for b, n in WARN_BITS.items() if warn & b],
