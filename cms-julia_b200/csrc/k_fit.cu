@@ -3,6 +3,7 @@
 // with their first 4 hits, at most 24576 per multiplicity) and the stand-alone
 // fit entry point pxl_bl_fit (3..8 hits, FP64 or mixed precision).
 #include <algorithm>
+#include <mutex>
 
 #include "../../include/pxl.h"
 #include "bl_fit.cuh"
@@ -230,15 +231,19 @@ __global__ void __launch_bounds__(128, 4) k_fit_bucket(const double* __restrict_
 }
 
 template <class T>
-void launch_bucket_fits(const double* hits, const float* ge, const int32_t* offs, const FitPlan* plan, double B,
-                        float* state, float* cov, float* chi2, float* pt, float* eta, int32_t* status, cudaStream_t s) {
+int launch_bucket_fits(const double* hits, const float* ge, const int32_t* offs, const FitPlan* plan, double B,
+                       float* state, float* cov, float* chi2, float* pt, float* eta, int32_t* status, cudaStream_t s) {
   const int g = 148 * 4;
-  k_fit_bucket<3, T><<<g, 128, 0, s>>>(hits, ge, offs, plan, B, state, cov, chi2, pt, eta, status);
-  k_fit_bucket<4, T><<<g, 128, 0, s>>>(hits, ge, offs, plan, B, state, cov, chi2, pt, eta, status);
-  k_fit_bucket<5, T><<<g, 128, 0, s>>>(hits, ge, offs, plan, B, state, cov, chi2, pt, eta, status);
-  k_fit_bucket<6, T><<<g, 128, 0, s>>>(hits, ge, offs, plan, B, state, cov, chi2, pt, eta, status);
-  k_fit_bucket<7, T><<<g, 128, 0, s>>>(hits, ge, offs, plan, B, state, cov, chi2, pt, eta, status);
-  k_fit_bucket<8, T><<<g, 128, 0, s>>>(hits, ge, offs, plan, B, state, cov, chi2, pt, eta, status);
+  return fan_out(s, 6, [&](int k, cudaStream_t st) {
+    switch (k) {
+      case 0: k_fit_bucket<3, T><<<g, 128, 0, st>>>(hits, ge, offs, plan, B, state, cov, chi2, pt, eta, status); break;
+      case 1: k_fit_bucket<4, T><<<g, 128, 0, st>>>(hits, ge, offs, plan, B, state, cov, chi2, pt, eta, status); break;
+      case 2: k_fit_bucket<5, T><<<g, 128, 0, st>>>(hits, ge, offs, plan, B, state, cov, chi2, pt, eta, status); break;
+      case 3: k_fit_bucket<6, T><<<g, 128, 0, st>>>(hits, ge, offs, plan, B, state, cov, chi2, pt, eta, status); break;
+      case 4: k_fit_bucket<7, T><<<g, 128, 0, st>>>(hits, ge, offs, plan, B, state, cov, chi2, pt, eta, status); break;
+      default: k_fit_bucket<8, T><<<g, 128, 0, st>>>(hits, ge, offs, plan, B, state, cov, chi2, pt, eta, status); break;
+    }
+  });
 }
 
 }  // namespace
@@ -271,6 +276,37 @@ int64_t fit_plan_bytes(int32_t n_tracks) {
   return (int64_t(sizeof(FitPlan)) + 4 * int64_t(n_tracks > 0 ? n_tracks : 0) + 255) / 256 * 256;
 }
 
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_side_mu;
+SideStreams g_side[kMaxDevices];
+bool g_side_made[kMaxDevices];
+}  // namespace
+
+SideStreams* side_streams_lock() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+  g_side_mu.lock();
+  if (!g_side_made[dev]) {
+    SideStreams& ss = g_side[dev];
+    bool ok = true;
+    for (int j = 0; j < 2; ++j) {
+      ok = ok && cudaStreamCreateWithFlags(&ss.st[j], cudaStreamNonBlocking) == cudaSuccess;
+      ok = ok && cudaEventCreateWithFlags(&ss.join[j], cudaEventDisableTiming) == cudaSuccess;
+    }
+    ok = ok && cudaEventCreateWithFlags(&ss.fork, cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
+      cudaGetLastError();
+      g_side_mu.unlock();
+      return nullptr;
+    }
+    g_side_made[dev] = true;
+  }
+  return &g_side[dev];
+}
+
+void side_streams_unlock() { g_side_mu.unlock(); }
+
 int fit_plan_build(const int32_t* offs, int32_t n, FitPlan* plan, int32_t* status, cudaStream_t s) {
   if (cudaMemsetAsync(plan, 0, sizeof(FitPlan) - sizeof(plan->list), s) != cudaSuccess) return PXL_ERR_CUDA;
   const int blocks = std::max(1, std::min(148 * 8, int((n + 255) / 256)));
@@ -295,9 +331,8 @@ extern "C" int32_t pxl_bl_fit(const double* hits, const float* hits_ge, const in
   auto* plan = static_cast<pxl::FitPlan*>(workspace);
   int rc = pxl::fit_plan_build(offs, n, plan, status, s);
   if (rc) return rc;
-  if (precision == 0)
-    pxl::launch_bucket_fits<double>(hits, hits_ge, offs, plan, b_field, state, cov, chi2, pt, eta, status, s);
-  else
-    pxl::launch_bucket_fits<float>(hits, hits_ge, offs, plan, b_field, state, cov, chi2, pt, eta, status, s);
-  return cudaGetLastError() == cudaSuccess ? 0 : PXL_ERR_CUDA;
+  rc = precision == 0
+           ? pxl::launch_bucket_fits<double>(hits, hits_ge, offs, plan, b_field, state, cov, chi2, pt, eta, status, s)
+           : pxl::launch_bucket_fits<float>(hits, hits_ge, offs, plan, b_field, state, cov, chi2, pt, eta, status, s);
+  return rc == 0 ? 0 : PXL_ERR_CUDA;
 }

@@ -50,14 +50,18 @@ __global__ void __launch_bounds__(128) k_riemann(RmArgs A) {
 }
 
 template <class T>
-void launch_riemann(const RmArgs& A, cudaStream_t s) {
+int launch_riemann(const RmArgs& A, cudaStream_t s) {
   const int g = 148 * 4;
-  k_riemann<3, T><<<g, 128, 0, s>>>(A);
-  k_riemann<4, T><<<g, 128, 0, s>>>(A);
-  k_riemann<5, T><<<g, 128, 0, s>>>(A);
-  k_riemann<6, T><<<g, 128, 0, s>>>(A);
-  k_riemann<7, T><<<g, 128, 0, s>>>(A);
-  k_riemann<8, T><<<g, 128, 0, s>>>(A);
+  return fan_out(s, 6, [&](int k, cudaStream_t st) {
+    switch (k) {
+      case 0: k_riemann<3, T><<<g, 128, 0, st>>>(A); break;
+      case 1: k_riemann<4, T><<<g, 128, 0, st>>>(A); break;
+      case 2: k_riemann<5, T><<<g, 128, 0, st>>>(A); break;
+      case 3: k_riemann<6, T><<<g, 128, 0, st>>>(A); break;
+      case 4: k_riemann<7, T><<<g, 128, 0, st>>>(A); break;
+      default: k_riemann<8, T><<<g, 128, 0, st>>>(A); break;
+    }
+  });
 }
 
 }  // namespace
@@ -77,7 +81,6 @@ extern "C" int32_t pxl_riemann_fit(const double* hits, const float* hits_ge, con
   int rc = fit_plan_build(offs, n, plan, status, s);
   if (rc) return rc;
   RmArgs A{hits, hits_ge, offs, plan, b_field, state, chi2, pt, status};
-  if (precision == 0) launch_riemann<double>(A, s);
-  else launch_riemann<float>(A, s);
-  return cudaGetLastError() == cudaSuccess ? 0 : PXL_ERR_CUDA;
+  rc = precision == 0 ? launch_riemann<double>(A, s) : launch_riemann<float>(A, s);
+  return rc == 0 ? 0 : PXL_ERR_CUDA;
 }

@@ -299,6 +299,35 @@ struct FitPlan {
 int64_t fit_plan_bytes(int32_t n_tracks);
 int fit_plan_build(const int32_t* offs, int32_t n, FitPlan* plan, int32_t* status, cudaStream_t s);
 
+// Two side streams of the current device with a fork event and two join events, created on
+// first use; side_streams_lock returns them held by the caller until side_streams_unlock
+// (nullptr, and nothing held, when they could not be created).
+struct SideStreams {
+  cudaStream_t st[2];
+  cudaEvent_t fork, join[2];
+};
+SideStreams* side_streams_lock();
+void side_streams_unlock();
+
+// Enqueues launch(k, stream) for k = 0 .. n-1 round robin on s and the two side streams,
+// forked from s and joined back into it: the per-hit-count fit kernels then overlap where an
+// earlier one's last blocks leave SMs idle. Without side streams every launch goes on s.
+template <class F>
+int fan_out(cudaStream_t s, int n, F&& launch) {
+  SideStreams* ss = side_streams_lock();
+  if (!ss) {
+    for (int k = 0; k < n; ++k) launch(k, s);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+  }
+  bool ok = cudaEventRecord(ss->fork, s) == cudaSuccess && cudaStreamWaitEvent(ss->st[0], ss->fork, 0) == cudaSuccess &&
+            cudaStreamWaitEvent(ss->st[1], ss->fork, 0) == cudaSuccess;
+  for (int k = 0; ok && k < n; ++k) launch(k, k % 3 == 0 ? s : ss->st[k % 3 - 1]);
+  for (int j = 0; ok && j < 2; ++j)
+    ok = cudaEventRecord(ss->join[j], ss->st[j]) == cudaSuccess && cudaStreamWaitEvent(s, ss->join[j], 0) == cudaSuccess;
+  side_streams_unlock();
+  return ok && cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
 // ---------------------------------------------------------------- helpers
 __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v) {
   const unsigned lane = threadIdx.x & 31u;
