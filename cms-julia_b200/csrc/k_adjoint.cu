@@ -124,12 +124,17 @@ extern "C" int32_t pxl_bl_fit_adjoint(const double* hits, const float* hits_ge, 
     AdjArgs A{hits, hits_ge, offs, plan, b_field, hit_module, module_pos, align, n_modules, chi2, grad_hits,
               want_align ? acc : nullptr};
     const int g = 148 * 4;
-    k_bl_adjoint<3><<<g, 128, 0, s>>>(A);
-    k_bl_adjoint<4><<<g, 128, 0, s>>>(A);
-    k_bl_adjoint<5><<<g, 128, 0, s>>>(A);
-    k_bl_adjoint<6><<<g, 128, 0, s>>>(A);
-    k_bl_adjoint<7><<<g, 128, 0, s>>>(A);
-    k_bl_adjoint<8><<<g, 128, 0, s>>>(A);
+    rc = fan_out(s, 6, [&](int k, cudaStream_t st) {
+      switch (k) {
+        case 0: k_bl_adjoint<3><<<g, 128, 0, st>>>(A); break;
+        case 1: k_bl_adjoint<4><<<g, 128, 0, st>>>(A); break;
+        case 2: k_bl_adjoint<5><<<g, 128, 0, st>>>(A); break;
+        case 3: k_bl_adjoint<6><<<g, 128, 0, st>>>(A); break;
+        case 4: k_bl_adjoint<7><<<g, 128, 0, st>>>(A); break;
+        default: k_bl_adjoint<8><<<g, 128, 0, st>>>(A); break;
+      }
+    });
+    if (rc) return PXL_ERR_CUDA;
   }
   if (want_align) k_align_out<<<std::max(1, (6 * n_modules + 255) / 256), 256, 0, s>>>(acc, 6 * n_modules, grad_align, grad_align64);
   return cudaGetLastError() == cudaSuccess ? 0 : PXL_ERR_CUDA;
