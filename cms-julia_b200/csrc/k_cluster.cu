@@ -743,6 +743,26 @@ __global__ void k_hits_module_start(Dev d) {
 
 }  // namespace
 
+// Blocks of k_find_clus_mid that fit on the current device at once: the kernel takes the
+// mid-size modules of the work list in one persistent wave (grid-stride), so that no partial
+// last wave of long-running blocks is left (1.48 instead of 1.69 ms per 1000 PU50 events with
+// 2.3 waves).
+static int mid_wave_ctas() {
+  static int cached[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148 * 7;
+  if (!cached[dev]) {
+    int occ = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_find_clus_mid, 32 * kMidWarps, 0) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || occ < 1 || sms < 1) {
+      cudaGetLastError();
+      return 148 * 7;
+    }
+    cached[dev] = occ * sms;
+  }
+  return cached[dev];
+}
+
 void launch_cluster(const Dev& d, const Launch& L) {
   cudaMemsetAsync(d.big_list, 0, kListHeader * sizeof(uint32_t), L.s);
   // enough warps that a few events fill the GPU, at least 8 modules per warp otherwise
@@ -751,7 +771,7 @@ void launch_cluster(const Dev& d, const Launch& L) {
   L.mark("find_clus_tiny");
   k_find_clus_small<<<148 * 64, 32 * kWarpsPerBlock, 0, L.s>>>(d);
   L.mark("find_clus_small");
-  k_find_clus_mid<<<148 * 16, 32 * kMidWarps, 0, L.s>>>(d);
+  k_find_clus_mid<<<mid_wave_ctas(), 32 * kMidWarps, 0, L.s>>>(d);
   L.mark("find_clus_mid");
   k_find_clus_block<<<148 * 2, 256, 0, L.s>>>(d);
   L.mark("find_clus_block");
