@@ -886,10 +886,12 @@ __global__ void __launch_bounds__(128) k_fishbone(Dev d, WorkQueue q) {
 constexpr int kMaxDepth = 8;
 
 // Depth-first walk of find_ntuplets from one start cell. kFill == false counts tuples and
-// hits; kFill == true writes them from the given global tuple / hit positions.
+// hits and appends each tuple's record (its doublets, and its ordinal and hit offset among the
+// start cell's tuples) to part `part` of the record pool; kFill == true writes the tuples from
+// the given global tuple / hit positions (run only when the pool overflowed).
 template <bool kFill>
 __device__ void walk(const Dev& d, uint64_t cb, uint64_t start, uint64_t* tuple_pos, uint64_t* hit_pos,
-                     uint32_t* ntup, uint32_t* nhit, uint64_t tuple_lo, uint32_t tcap, int e) {
+                     uint32_t* ntup, uint32_t* nhit, uint64_t tuple_lo, uint32_t tcap, int e, uint32_t part) {
   uint32_t stack_c[kMaxDepth];
   uint32_t stack_k[kMaxDepth];
   int depth = 0;
@@ -953,6 +955,19 @@ __device__ void walk(const Dev& d, uint64_t cb, uint64_t start, uint64_t* tuple_
         *tuple_pos = g + 1;
         *hit_pos = hp + nh;
       } else {
+        // the tuple's record, appended to the warp's part of the pool
+        const uint32_t slot = atomicAdd(&d.tp_ctr[part * kTpStride], 1u);
+        if (slot < d.tp_part) {
+          const uint64_t r = uint64_t(part) * d.tp_part + slot;
+          uint32_t cc[kMaxDepth];
+#pragma unroll
+          for (int k = 0; k < kMaxDepth; ++k) cc[k] = k <= depth ? stack_c[k] : 0u;
+          d.tp_hdr[r] = make_uint4(uint32_t(start), *ntup, *nhit, (uint32_t(e) << 4) | nh);
+          d.tp_cells[2 * r] = make_uint4(cc[0], cc[1], cc[2], cc[3]);
+          d.tp_cells[2 * r + 1] = make_uint4(cc[4], cc[5], cc[6], cc[7]);
+        } else {
+          d.tp_ctr[kTpParts * kTpStride] = 1u;  // the fill walks again
+        }
         *ntup += 1;
         *nhit += nh;
       }
@@ -980,6 +995,9 @@ constexpr int kNtupQueue = 64;
 template <bool kFill, bool kQ>
 __global__ void __launch_bounds__(32 * kNtupWarps) k_ntuplets(Dev d, WorkQueue q) {
   __shared__ uint32_t s_queue[kNtupWarps][kNtupQueue];
+  // the fill walks only when the count pass could not keep every tuple's record
+  if (kFill && d.tp_ctr[kTpParts * kTpStride] == 0) return;
+  const uint32_t part = ((blockIdx.y * gridDim.x + blockIdx.x) * kNtupWarps + (threadIdx.x >> 5)) % kTpParts;
   for_each_vblock<kQ>(q, [&](int e, uint32_t bx, uint32_t nbx) {
   const EvInfo& E = d.ev[e];
   const uint64_t cb = E.cell_base;
@@ -993,12 +1011,12 @@ __global__ void __launch_bounds__(32 * kNtupWarps) k_ntuplets(Dev d, WorkQueue q
     const uint64_t c = cb + s_queue[w][q0 + lane];
     if (!kFill) {
       uint32_t nt = 0, nh = 0;
-      walk<false>(d, cb, c, nullptr, nullptr, &nt, &nh, 0, 0, e);
+      walk<false>(d, cb, c, nullptr, nullptr, &nt, &nh, 0, 0, e, part);
       d.tstart_cnt[c] = (uint64_t(nt) << 32) | nh;
     } else {
       const uint64_t v = d.tstart_cnt[c];
       uint64_t tp = v >> 32, hp = v & 0xFFFFFFFFull;
-      walk<true>(d, cb, c, &tp, &hp, nullptr, nullptr, tuple_lo, E.n_tuples, e);
+      walk<true>(d, cb, c, &tp, &hp, nullptr, nullptr, tuple_lo, E.n_tuples, e, 0u);
     }
   };
   uint32_t qn = 0;
@@ -1026,6 +1044,65 @@ __global__ void __launch_bounds__(32 * kNtupWarps) k_ntuplets(Dev d, WorkQueue q
   walk_queued(0, qn);
   __syncwarp();
   });
+}
+
+// The fill from the pool: block r moves the records of part r to their tuple and hit
+// positions (the start cell's scanned positions plus the record's ordinal and hit offset) and
+// writes what the walking fill writes at a leaf. Independent records, one thread each, so the
+// gathers of the tuples' hits overlap; nothing is walked again.
+__global__ void __launch_bounds__(256) k_tuples_from_pool(Dev d) {
+  if (d.tp_ctr[kTpParts * kTpStride]) return;  // a part overflowed: k_ntuplets<true> walks
+  const uint32_t r = blockIdx.x;
+  uint32_t n = d.tp_ctr[r * kTpStride];
+  if (n > d.tp_part) n = d.tp_part;
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const uint64_t s = uint64_t(r) * d.tp_part + i;
+    const uint4 h = d.tp_hdr[s];
+    const uint4 c0 = d.tp_cells[2 * s], c1 = d.tp_cells[2 * s + 1];
+    const uint32_t cells[kMaxDepth] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+    const int e = int(h.w >> 4);
+    const uint32_t nh = h.w & 15u;
+    const int depth = int(nh) - 2;  // index of the tuple's last doublet
+    const uint64_t v = d.tstart_cnt[h.x];
+    const uint64_t g = (v >> 32) + h.y;
+    const uint64_t hp = (v & 0xFFFFFFFFull) + h.z;
+    if (!(g < uint64_t(d.cap_tuples) && hp + nh <= uint64_t(d.cap_tuple_hits))) continue;
+    const EvInfo& E = d.ev[e];
+    const uint32_t hbase = E.hit_base;
+    uint32_t ih[kMaxDepth];
+    uint32_t top = 0;
+#pragma unroll
+    for (int k = 0; k < kMaxDepth; ++k) {
+      ih[k] = k <= depth ? d.cell_inner[cells[k]] : 0u;
+      if (k == depth) top = cells[k];
+    }
+    const uint32_t oh = d.cell_outer[top];
+    int16_t det[kMaxDepth];
+#pragma unroll
+    for (int k = 0; k < kMaxDepth; ++k)
+      if (k <= depth) det[k] = d.detind[hbase + ih[k]];
+    const int16_t det_o = d.detind[hbase + oh];
+    d.tuple_off[g] = uint32_t(hp);
+#pragma unroll
+    for (int k = 0; k < kMaxDepth; ++k)
+      if (k <= depth) {
+        d.tuple_hits[hp + k] = ih[k];
+        d.tuple_det[hp + k] = uint16_t(det[k]);
+      }
+    d.tuple_hits[hp + depth + 1] = oh;
+    d.tuple_det[hp + depth + 1] = uint16_t(det_o);
+    d.quality[g] = 0;
+    // cell -> track pairs only for the tuples the event keeps (as the walking fill)
+    if (g - E.tuple_base < E.n_tuples) {
+      const uint64_t pp = hp - g;
+#pragma unroll
+      for (int k = 0; k < kMaxDepth; ++k)
+        if (k <= depth) {
+          d.tuple_cell[pp + k] = cells[k];
+          atomicAdd(&d.ct_cur[cells[k]], 1u);
+        }
+    }
+  }
 }
 
 __global__ void k_tuple_bases(Dev d) {
@@ -1245,7 +1322,9 @@ void launch_ca(const Dev& d, const Launch& L) {
     k_fishbone<false><<<g(kTuneFishbone), 128, 0, L.s>>>(d, WorkQueue{});
   }
   L.mark("fishbone");
-  // ntuplets
+  // ntuplets: the count pass keeps each tuple's record in the pool; the fill moves the records
+  // into place, or walks again when the pool overflowed
+  cudaMemsetAsync(d.tp_ctr, 0, size_t(kTpParts * kTpStride + 1) * sizeof(uint32_t), L.s);
   const int ctas_nt = L.queue_of(kTuneNtuplets) ? L.wq_ctas[kTuneNtuplets] : 0;
   if (ctas_nt) {
     const WorkQueue q = plan(kTuneNtuplets, int(offsetof(EvInfo, n_cells)), 32 * kNtupWarps);
@@ -1256,6 +1335,7 @@ void launch_ca(const Dev& d, const Launch& L) {
   L.mark("ntuplets_count");
   excl_scan_u64(d.tstart_cnt, d.cap_cells, &d.ev[d.E].n_cells_raw, d.scan_tmp64, L.s);
   k_tuple_bases<<<eb, 128, 0, L.s>>>(d);
+  k_tuples_from_pool<<<kTpParts, 256, 0, L.s>>>(d);
   if (ctas_nt) {
     const WorkQueue q = plan(kTuneNtuplets, int(offsetof(EvInfo, n_cells)), 32 * kNtupWarps);
     k_ntuplets<true, true><<<ctas_nt, 32 * kNtupWarps, 0, L.s>>>(d, q);

@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstddef>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -237,6 +238,13 @@ int alloc_batch(PxlCtx* ctx) {
   A(cn_pairs, d.cap_pairs); A(cn_pair_ctr, 1); d.cap_long = std::max({d.cap_cells, d.cap_pairs, d.cap_tuple_hits}) / 9 + 1;
   A(long_lists, d.cap_long); A(long_ctr, 1); A(cn_cnt, d.cap_cells + 1); A(cn_cur, d.cap_cells); A(cn_list, d.cap_pairs);
   A(tstart_cnt, d.cap_cells + 1);
+  // tuple record pool: the batch's tuples plus a quarter for uneven parts
+  d.tp_part = uint32_t((d.cap_tuples + d.cap_tuples / 4) / kTpParts + 64);
+  // PXL_TUPLE_POOL_PART (records per part) shrinks the pool, so that tests can make it overflow
+  // and check the walking fill that then runs
+  if (const char* v = std::getenv("PXL_TUPLE_POOL_PART")) d.tp_part = uint32_t(std::max(1, std::atoi(v)));
+  A(tp_hdr, int64_t(kTpParts) * d.tp_part); A(tp_cells, 2 * int64_t(kTpParts) * d.tp_part);
+  A(tp_ctr, kTpParts * kTpStride + 1);
   A(tuple_off, d.cap_tuples + 1); A(tuple_hits, d.cap_tuple_hits); A(quality, d.cap_tuples);
   A(tuple_cell, d.cap_tuple_hits);
   A(ct_cnt, d.cap_cells + 1); A(ct_cur, d.cap_cells); A(ct_list, d.cap_tuple_hits);

@@ -28,6 +28,8 @@ constexpr int kNPairs = 19;
 constexpr int kTupleStride = 32 * 1024;
 constexpr int kMaxCellsPerHit = 128;
 constexpr int kCellRows = 64;
+constexpr int kTpParts = 1024;  // parts of the tuple record pool
+constexpr int kTpStride = 32;   // words between the parts' counters
 constexpr int kMaxActiveColumns = 512 * 1024 / 8;  // MAX_NUM_OF_ACTIVE_DOUBLETS, the default column cap
 constexpr uint32_t kHitIdBits = 21;                // event-local hit ids are below 2^21
 constexpr uint32_t kMaxHitsPerEvent = 1u << kHitIdBits;
@@ -188,6 +190,13 @@ struct Dev {
   uint32_t* long_ctr;      // [1]
   // tuples
   uint64_t* tstart_cnt;    // [cap_cells + 1] (tuples << 32 | hits) per start cell -> exclusive positions
+  // tuples found by the count pass, in kTpParts parts of tp_part records each (a warp appends to
+  // part (warp id mod kTpParts)): header (start cell, tuple ordinal and hit offset within the start
+  // cell's tuples, event << 4 | hits) and the tuple's doublets (two uint4, unused entries 0)
+  uint4* tp_hdr;           // [kTpParts * tp_part]
+  uint4* tp_cells;         // [2 * kTpParts * tp_part]
+  uint32_t* tp_ctr;        // [kTpParts * kTpStride + 1] records per part; last word: a part overflowed
+  uint32_t tp_part;
   uint32_t* tuple_off;     // [cap_tuples + 1] global hit offsets (0-based, packed)
   uint32_t* tuple_hits;    // [cap_tuple_hits] event-local 0-based hit index
   uint16_t* tuple_det;     // [cap_tuple_hits] detector index of each tuple hit (det_indices)

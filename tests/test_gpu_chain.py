@@ -98,6 +98,24 @@ def test_batch_ca_matches_oracle(conditions, orc, events_pu50):
             assert not errs, (e, errs)
 
 
+def test_batch_ca_with_overflowing_tuple_pool(conditions, orc, events_pu50, monkeypatch):
+    """The count pass keeps each tuple's record in a pool of 1024 parts, from which the fill
+    moves the tuples into place. With one record per part (PXL_TUPLE_POOL_PART, read when the
+    context is created) a PU50 batch overflows the pool, and the fill walks the tuples again:
+    the products must be the same."""
+    from pixeltrack import PixelChain, batch_params
+    blob, offs = events_pu50
+    n = len(offs) - 1
+    monkeypatch.setenv("PXL_TUPLE_POOL_PART", "1")
+    with PixelChain(conditions, batch_params(n)) as bc:
+        monkeypatch.delenv("PXL_TUPLE_POOL_PART")
+        bc.run_batch(blob, offs, stages=7)
+        for e in range(n):
+            orc.run_event(blob[offs[e]:offs[e + 1]], 7)
+            errs = compare_ca(bc, orc, e)
+            assert not errs, (e, errs)
+
+
 def test_batch_matches_oracle(conditions, orc, events_pu50):
     from pixeltrack import PixelChain, batch_params
     blob, offs = events_pu50
