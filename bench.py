@@ -60,6 +60,7 @@ def parse():
     ap.add_argument("--no-parity", action="store_true", help="skip the per-event comparison with the oracle")
     ap.add_argument("--adjoint-sample", type=int, default=500)
     ap.add_argument("--bpe", type=int, default=0, help="blocks per event for the per-event kernels (0: automatic)")
+    ap.add_argument("--contexts", type=int, default=2, help="contexts (each on its own stream) taking turns")
     return ap.parse_args()
 
 
@@ -656,21 +657,25 @@ def main():
     # takes every other step, so that two batches are in flight: one batch's kernels fill the
     # SMs that the other's last waves and per-event stages leave idle (the reference's
     # analogue is its several stream threads, each with its own producers).
-    chain2 = PixelChain(conds, params)
-    stream2 = torch.cuda.Stream(device=local)
-    sh2 = stream2.cuda_stream
-    chain2.stage_batch(blob, offs, sh2)
-    stream2.synchronize()
-    if args.bpe == 0:
-        chain2.autotune()
-    chains, streams, shs = [chain, chain2], [stream, stream2], [sh, sh2]
+    nctx = max(1, args.contexts)
+    chains, streams, shs = [chain], [stream], [sh]
+    for _ in range(nctx - 1):
+        c = PixelChain(conds, params)
+        s_ = torch.cuda.Stream(device=local)
+        c.stage_batch(blob, offs, s_.cuda_stream)
+        s_.synchronize()
+        if args.bpe == 0:
+            c.autotune()
+        chains.append(c)
+        streams.append(s_)
+        shs.append(s_.cuda_stream)
     for c, s_, h_ in zip(chains, streams, shs):
         c.stage_batch(blob, offs, h_)
         s_.synchronize()
         c.capture_graph()
     kernels_per_step = chain.graph_kernel_nodes()
-    for k in range(max(args.warmup, 2)):
-        chains[k % 2].launch_graph(shs[k % 2])
+    for k in range(max(args.warmup, nctx)):
+        chains[k % nctx].launch_graph(shs[k % nctx])
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -678,10 +683,12 @@ def main():
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
         t0.record(stream)
-        stream2.wait_event(t0)
+        for s_ in streams[1:]:
+            s_.wait_event(t0)
         for k in range(args.steps):
-            chains[k % 2].launch_graph(shs[k % 2])
-        stream.wait_stream(stream2)
+            chains[k % nctx].launch_graph(shs[k % nctx])
+        for s_ in streams[1:]:
+            stream.wait_stream(s_)
         t1.record(stream)
         t1.synchronize()
     ms = pdist.max_over_ranks(t0.elapsed_time(t1), device="cuda")
@@ -713,24 +720,24 @@ def main():
     def e2e_steps(n):
         chains[0].stage_slot(0, pinned_np, offs, copy.cuda_stream)
         for k in range(n):
-            i, slot = k % 2, (k // 2) % 2
+            i, slot = k % nctx, (k // nctx) % 2
             chains[i].launch_slot(slot, shs[i])
             chains[i].export_async(outs[k % 2], shs[i], d2h_stream.cuda_stream)
             if k + 1 < n:
-                chains[(k + 1) % 2].stage_slot(((k + 1) // 2) % 2, pinned_np, offs, copy.cuda_stream)
+                chains[(k + 1) % nctx].stage_slot(((k + 1) // nctx) % 2, pinned_np, offs, copy.cuda_stream)
 
-    e2e_steps(max(args.warmup, 2))
+    e2e_steps(max(args.warmup, nctx))
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     e0.record(stream)
-    for s_ in (copy, d2h_stream, stream2):
+    for s_ in [copy, d2h_stream] + streams[1:]:
         s_.wait_event(e0)
     e2e_steps(args.steps)
-    stream.wait_stream(stream2)
-    stream.wait_stream(d2h_stream)
+    for s_ in streams[1:] + [d2h_stream]:
+        stream.wait_stream(s_)
     e1.record(stream)
     e1.synchronize()
     ems = pdist.max_over_ranks(e0.elapsed_time(e1), device="cuda")
@@ -792,7 +799,7 @@ def main():
             "metric": METRIC, "value": value, "unit": "events/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32/f32/f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "events_per_step": E, "pileup": args.pu, "contexts_in_flight": 2,
+            "config": {"workload": WORKLOAD, "events_per_step": E, "pileup": args.pu, "contexts_in_flight": nctx,
                        "raw_bytes_per_step": int(offs[-1]), "l2": "inputs and intermediates larger than L2",
                        "parallelism": f"events sharded over {world} GPU(s), no data-path collective",
                        "blocks_per_event": tuned or args.bpe},
@@ -807,8 +814,8 @@ def main():
             "vertices_per_event": nv_check / E,
         }
         print(json.dumps(line), flush=True)
-    chain2.close()
-    chain.close()
+    for c in chains:
+        c.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
