@@ -1046,16 +1046,19 @@ __global__ void __launch_bounds__(32 * kNtupWarps) k_ntuplets(Dev d, WorkQueue q
   });
 }
 
-// The fill from the pool: block r moves the records of part r to their tuple and hit
+// The fill from the pool: two blocks per part r move its records to their tuple and hit
 // positions (the start cell's scanned positions plus the record's ordinal and hit offset) and
-// writes what the walking fill writes at a leaf. Independent records, one thread each, so the
+// write what the walking fill writes at a leaf. Independent records, one thread each, so the
 // gathers of the tuples' hits overlap; nothing is walked again.
+constexpr int kPoolBlocksPerPart = 2;  // measured faster than one (1000 PU50 events: 1.01 / 1.05 ms)
+
 __global__ void __launch_bounds__(256) k_tuples_from_pool(Dev d) {
   if (d.tp_ctr[kTpParts * kTpStride]) return;  // a part overflowed: k_ntuplets<true> walks
-  const uint32_t r = blockIdx.x;
+  const uint32_t r = blockIdx.x / kPoolBlocksPerPart;
   uint32_t n = d.tp_ctr[r * kTpStride];
   if (n > d.tp_part) n = d.tp_part;
-  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+  for (uint32_t i = threadIdx.x + (blockIdx.x % kPoolBlocksPerPart) * blockDim.x; i < n;
+       i += kPoolBlocksPerPart * blockDim.x) {
     const uint64_t s = uint64_t(r) * d.tp_part + i;
     const uint4 h = d.tp_hdr[s];
     const uint4 c0 = d.tp_cells[2 * s], c1 = d.tp_cells[2 * s + 1];
@@ -1335,7 +1338,7 @@ void launch_ca(const Dev& d, const Launch& L) {
   L.mark("ntuplets_count");
   excl_scan_u64(d.tstart_cnt, d.cap_cells, &d.ev[d.E].n_cells_raw, d.scan_tmp64, L.s);
   k_tuple_bases<<<eb, 128, 0, L.s>>>(d);
-  k_tuples_from_pool<<<kTpParts, 256, 0, L.s>>>(d);
+  k_tuples_from_pool<<<kTpParts * kPoolBlocksPerPart, 256, 0, L.s>>>(d);
   if (ctas_nt) {
     const WorkQueue q = plan(kTuneNtuplets, int(offsetof(EvInfo, n_cells)), 32 * kNtupWarps);
     k_ntuplets<true, true><<<ctas_nt, 32 * kNtupWarps, 0, L.s>>>(d, q);

@@ -327,19 +327,25 @@ __device__ __forceinline__ bool module_start_flag(const Dev& d, uint64_t ebase, 
   return j < 0 || d.mid[ebase + j] != id;
 }
 
-__global__ void k_modstart_count(Dev d) {
-  const int f = blockIdx.x, e = blockIdx.y;
+// Module starts per FED slot, one warp per slot (kModWarps slots per block): the flags of 32
+// words per step, counted with a ballot.
+constexpr int kModWarps = 8;
+
+__global__ void __launch_bounds__(32 * kModWarps) k_modstart_count(Dev d) {
+  const int f = blockIdx.x * kModWarps + int(threadIdx.x >> 5), e = blockIdx.y;
   const int NF = d.n_fed_slots;
+  if (f >= NF) return;
+  const unsigned lane = threadIdx.x & 31u;
   const size_t fs = size_t(e) * NF + f;
   const uint32_t nw = d.fed_nw[fs], wo = d.fed_wo[fs];
-  __shared__ uint32_t sh[33];
   uint32_t cnt = 0;
   const uint64_t ebase = d.ev[e].word_base;
   if (ebase + wo + nw <= uint64_t(d.cap_words))
-    for (uint32_t k = threadIdx.x; k < nw; k += blockDim.x) cnt += module_start_flag(d, ebase, wo + k) ? 1u : 0u;
-  uint32_t tot;
-  block_excl_scan(cnt, sh, &tot);
-  if (threadIdx.x == 0) d.fed_nmod[fs] = tot;
+    for (uint32_t k0 = 0; k0 < nw; k0 += 32) {
+      const uint32_t k = k0 + lane;
+      cnt += __popc(__ballot_sync(0xffffffffu, k < nw && module_start_flag(d, ebase, wo + k)));
+    }
+  if (lane == 0) d.fed_nmod[fs] = cnt;
 }
 
 // per event: module-start offsets per FED slot, n_modules; zero the cluster counters
@@ -370,24 +376,27 @@ __global__ void k_modstart_scan(Dev d) {
   }
 }
 
-__global__ void k_modstart_fill(Dev d) {
-  const int f = blockIdx.x, e = blockIdx.y;
+// The module starts of each FED slot at the slot's offset, one warp per slot, in word order
+// (rank of a flag = flags of the earlier lanes plus those of the earlier steps).
+__global__ void __launch_bounds__(32 * kModWarps) k_modstart_fill(Dev d) {
+  const int f = blockIdx.x * kModWarps + int(threadIdx.x >> 5), e = blockIdx.y;
   const int NF = d.n_fed_slots;
+  if (f >= NF) return;
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned lt = (1u << lane) - 1u;
   const size_t fs = size_t(e) * NF + f;
   const uint32_t nw = d.fed_nw[fs], wo = d.fed_wo[fs];
   const uint64_t ebase = d.ev[e].word_base;
   if (ebase + wo + nw > uint64_t(d.cap_words)) return;
-  __shared__ uint32_t sh[33];
   uint32_t carry = d.fed_nmod[fs];
   uint32_t* ms = d.module_start + size_t(e) * (kMaxNumModules + 1);
-  for (uint32_t b = 0; b < nw; b += blockDim.x) {
-    uint32_t k = b + threadIdx.x;
-    bool fl = k < nw && module_start_flag(d, ebase, wo + k);
-    uint32_t tot;
-    uint32_t ex = block_excl_scan(fl ? 1u : 0u, sh, &tot);
+  for (uint32_t k0 = 0; k0 < nw; k0 += 32) {
+    const uint32_t k = k0 + lane;
+    const bool fl = k < nw && module_start_flag(d, ebase, wo + k);
+    const uint32_t bal = __ballot_sync(0xffffffffu, fl);
     if (fl) {
-      uint32_t r = carry + ex;
-      uint32_t i1 = wo + k + 1;  // 1-based digi index
+      const uint32_t r = carry + __popc(bal & lt);
+      const uint32_t i1 = wo + k + 1;  // 1-based digi index
       // a module id starting a second run: the event's charge cut runs in serial order
       const uint16_t id = uint16_t(d.mid[ebase + wo + k]);
       if (id < 2048u) {
@@ -397,7 +406,7 @@ __global__ void k_modstart_fill(Dev d) {
       if (r < uint32_t(kMaxNumModules - 1)) ms[r + 1] = i1;
       else atomicMax(&ms[kMaxNumModules], i1);
     }
-    carry += tot;
+    carry += __popc(bal);
   }
 }
 
@@ -413,17 +422,18 @@ void launch_raw(const Dev& d, const Launch& L, const int16_t* fed_slot_of) {
   dim3 g(NF, d.E);
   k_unpack<<<g, 256, 0, L.s>>>(d);
   L.mark("unpack_calib");
-  k_modstart_count<<<g, 256, 0, L.s>>>(d);
+  const dim3 gm(div_up(NF, kModWarps), d.E);
+  k_modstart_count<<<gm, 32 * kModWarps, 0, L.s>>>(d);
   k_modstart_scan<<<d.E, 256, 0, L.s>>>(d);
-  k_modstart_fill<<<g, 256, 0, L.s>>>(d);
+  k_modstart_fill<<<gm, 32 * kModWarps, 0, L.s>>>(d);
   L.mark("module_starts");
 }
 
 void launch_modstart(const Dev& d, const Launch& L) {
-  dim3 g(d.n_fed_slots, d.E);
-  k_modstart_count<<<g, 256, 0, L.s>>>(d);
+  const dim3 gm(div_up(d.n_fed_slots, kModWarps), d.E);
+  k_modstart_count<<<gm, 32 * kModWarps, 0, L.s>>>(d);
   k_modstart_scan<<<d.E, 256, 0, L.s>>>(d);
-  k_modstart_fill<<<g, 256, 0, L.s>>>(d);
+  k_modstart_fill<<<gm, 32 * kModWarps, 0, L.s>>>(d);
 }
 
 void launch_ev_scan(const Dev& d, cudaStream_t s, int count_off, int base_off) {

@@ -28,7 +28,7 @@ constexpr int kNPairs = 19;
 constexpr int kTupleStride = 32 * 1024;
 constexpr int kMaxCellsPerHit = 128;
 constexpr int kCellRows = 64;
-constexpr int kTpParts = 1024;  // parts of the tuple record pool
+constexpr int kTpParts = 4096;  // parts of the tuple record pool
 constexpr int kTpStride = 32;   // words between the parts' counters
 constexpr int kMaxActiveColumns = 512 * 1024 / 8;  // MAX_NUM_OF_ACTIVE_DOUBLETS, the default column cap
 constexpr uint32_t kHitIdBits = 21;                // event-local hit ids are below 2^21

@@ -99,7 +99,7 @@ def test_batch_ca_matches_oracle(conditions, orc, events_pu50):
 
 
 def test_batch_ca_with_overflowing_tuple_pool(conditions, orc, events_pu50, monkeypatch):
-    """The count pass keeps each tuple's record in a pool of 1024 parts, from which the fill
+    """The count pass keeps each tuple's record in a pool of 4096 parts, from which the fill
     moves the tuples into place. With one record per part (PXL_TUPLE_POOL_PART, read when the
     context is created) a PU50 batch overflows the pool, and the fill walks the tuples again:
     the products must be the same."""
