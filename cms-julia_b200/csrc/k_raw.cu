@@ -252,14 +252,19 @@ __device__ __forceinline__ void unpack_word(const Dev& d, int e, uint32_t local,
   d.xx[g] = xx; d.yy[g] = yy; d.adc[g] = adc; d.mid[g] = mid; d.pdigi[g] = pdigi; d.rawid[g] = rawid;
 }
 
-// raw_to_digi_kernal + calib_digis for the words of one FED (blockIdx.x = FED slot). The payload
+// raw_to_digi_kernal + calib_digis for the words of one FED slot per warp (kUnpackWarps slots
+// per block: a FED holds a few hundred words, which one warp decodes in a few steps). The payload
 // is read with 128-bit loads where it sits on 4-byte boundaries (always, for FED sizes in whole
 // 64-bit words): the words before the first 16-byte boundary and after the last one are read
-// singly, the rest four per thread.
-__global__ void __launch_bounds__(256) k_unpack(Dev d) {
-  __shared__ __align__(16) uint32_t s_words[8][128];
-  const int f = blockIdx.x, e = blockIdx.y;
+// singly, the rest as 16-byte vectors.
+constexpr int kUnpackWarps = 8;
+
+__global__ void __launch_bounds__(32 * kUnpackWarps) k_unpack(Dev d) {
+  __shared__ __align__(16) uint32_t s_words[kUnpackWarps][128];
+  const unsigned lane = threadIdx.x & 31u, wq = threadIdx.x >> 5;
+  const int f = blockIdx.x * kUnpackWarps + int(wq), e = blockIdx.y;
   const int NF = d.n_fed_slots;
+  if (f >= NF) return;
   const size_t fs = size_t(e) * NF + f;
   const uint32_t nw = d.fed_nw[fs];
   if (nw == 0) return;
@@ -267,7 +272,7 @@ __global__ void __launch_bounds__(256) k_unpack(Dev d) {
   const uint32_t wo = d.fed_wo[fs];
   const uint64_t gbase = uint64_t(E.word_base) + wo;
   if (gbase + nw > uint64_t(d.cap_words)) {
-    if (threadIdx.x == 0) { atomic_or_warn(&d.ev[e], kWarnBuffer); atomicOr(d.status, kWarnBuffer); }
+    if (lane == 0) { atomic_or_warn(&d.ev[e], kWarnBuffer); atomicOr(d.status, kWarnBuffer); }
     return;
   }
   const uint8_t* src = d.raw + d.fed_src[fs];
@@ -289,15 +294,14 @@ __global__ void __launch_bounds__(256) k_unpack(Dev d) {
     const uint32_t* src32 = reinterpret_cast<const uint32_t*>(src);
     uint32_t head = uint32_t((16u - (reinterpret_cast<uintptr_t>(src) & 15u)) & 15u) >> 2;
     head = head < nw ? head : nw;
-    if (threadIdx.x < head) word(threadIdx.x, __ldg(src32 + threadIdx.x));
+    if (lane < head) word(lane, __ldg(src32 + lane));
     const uint32_t nvec = (nw - head) >> 2;
     const uint4* v = reinterpret_cast<const uint4*>(src32 + head);
-    // a warp loads 32 aligned 16-byte vectors (128 words) and decodes them word by word through
+    // the warp loads 32 aligned 16-byte vectors (128 words) and decodes them word by word through
     // shared memory, lane l taking words l, l + 32, l + 64, l + 96, so that the per-digi stores
     // of consecutive lanes stay consecutive
-    const unsigned lane = threadIdx.x & 31u, wq = threadIdx.x >> 5;
     uint32_t* sw = s_words[wq];
-    for (uint32_t j0 = 32u * wq; j0 < nvec; j0 += blockDim.x) {
+    for (uint32_t j0 = 0; j0 < nvec; j0 += 32) {
       if (j0 + lane < nvec) reinterpret_cast<uint4*>(sw)[lane] = __ldg(v + j0 + lane);
       __syncwarp();
       const uint32_t nwords = 4u * min(32u, nvec - j0);
@@ -308,9 +312,9 @@ __global__ void __launch_bounds__(256) k_unpack(Dev d) {
       }
       __syncwarp();
     }
-    for (uint32_t k = head + 4 * nvec + threadIdx.x; k < nw; k += blockDim.x) word(k, __ldg(src32 + k));
+    for (uint32_t k = head + 4 * nvec + lane; k < nw; k += 32) word(k, __ldg(src32 + k));
   } else {
-    for (uint32_t k = threadIdx.x; k < nw; k += blockDim.x) {
+    for (uint32_t k = lane; k < nw; k += 32) {
       uint32_t ww;
       memcpy(&ww, src + 4ull * k, 4);
       word(k, ww);
@@ -419,8 +423,7 @@ void launch_raw(const Dev& d, const Launch& L, const int16_t* fed_slot_of) {
   k_ev_scan<<<1, 1024, 0, L.s>>>(d.ev, d.E, int(offsetof(EvInfo, n_words)), int(offsetof(EvInfo, word_base)));
   launch_ev_clamp(d, L.s, int(offsetof(EvInfo, n_words)), int(offsetof(EvInfo, word_base)), d.cap_words);
   L.mark("fed_table");
-  dim3 g(NF, d.E);
-  k_unpack<<<g, 256, 0, L.s>>>(d);
+  k_unpack<<<dim3(div_up(NF, kUnpackWarps), d.E), 32 * kUnpackWarps, 0, L.s>>>(d);
   L.mark("unpack_calib");
   const dim3 gm(div_up(NF, kModWarps), d.E);
   k_modstart_count<<<gm, 32 * kModWarps, 0, L.s>>>(d);
