@@ -1343,7 +1343,9 @@ void launch_ca(const Dev& d, const Launch& L) {
     const WorkQueue q = plan(kTuneNtuplets, int(offsetof(EvInfo, n_cells)), 32 * kNtupWarps);
     k_ntuplets<true, true><<<ctas_nt, 32 * kNtupWarps, 0, L.s>>>(d, q);
   } else {
-    k_ntuplets<true, false><<<g(kTuneNtuplets), 32 * kNtupWarps, 0, L.s>>>(d, WorkQueue{});
+    // the walking fill returns at once unless the pool overflowed: a few blocks per event
+    k_ntuplets<true, false><<<dim3(std::min(L.bpe_of(kTuneNtuplets), 8), d.E), 32 * kNtupWarps, 0, L.s>>>(
+        d, WorkQueue{});
   }
   k_tuple_ends<<<div_up(d.E, 128), 128, 0, L.s>>>(d);
   L.mark("ntuplets_fill");
