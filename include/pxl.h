@@ -185,7 +185,10 @@ int32_t pxl_params_default(PxlParams* params);
 int32_t pxl_params_extended(PxlParams* params);
 
 /* Uploads the conditions and allocates every device buffer of a batch.
- * Replaces the ES producers' produce() and the producers' constructors. */
+ * Replaces the ES producers' produce() and the producers' constructors.
+ * Testing aid: the environment variable PXL_TUPLE_POOL_PART, when set at this call, sets the
+ * records per part of the tuple record pool (normally sized from max_tuples); a pool too small
+ * for a batch makes the tuple fill walk the trees again, with the same products. */
 int32_t pxl_ctx_create(const PxlConditions* conditions, const PxlParams* params, PxlCtx** ctx);
 int32_t pxl_ctx_destroy(PxlCtx* ctx);
 
