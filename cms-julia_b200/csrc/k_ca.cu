@@ -500,14 +500,24 @@ __global__ void k_cell_regions(Dev d) {
 
 // ---------------------------------------------------------------- outer-hit lists
 // cells ending on each hit: slots from the shifted scan of the counts the doublet fill took
+constexpr int kOhcUnroll = 4;  // cells (list entries) per thread and step, loads independent
+
 __global__ void k_ohc_fill(Dev d) {
   const int e = blockIdx.y;
   const EvInfo& E = d.ev[e];
   const uint64_t cb = E.cell_base;
   const uint32_t hb = E.hit_base;
-  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < E.n_cells; k += gridDim.x * blockDim.x) {
-    const uint64_t c = cb + k;
-    d.ohc_list[atomicAdd(&d.ohc_cnt[hb + d.cell_outer[c] + 1], 1u)] = uint32_t(c);
+  const uint32_t n = E.n_cells, stride = gridDim.x * blockDim.x;
+  for (uint32_t k0 = blockIdx.x * blockDim.x + threadIdx.x; k0 < n; k0 += kOhcUnroll * stride) {
+    uint32_t o[kOhcUnroll], slot[kOhcUnroll];
+#pragma unroll
+    for (int u = 0; u < kOhcUnroll; ++u) o[u] = k0 + u * stride < n ? d.cell_outer[cb + k0 + u * stride] : 0xffffffffu;
+#pragma unroll
+    for (int u = 0; u < kOhcUnroll; ++u)
+      if (o[u] != 0xffffffffu) slot[u] = atomicAdd(&d.ohc_cnt[hb + o[u] + 1], 1u);
+#pragma unroll
+    for (int u = 0; u < kOhcUnroll; ++u)
+      if (o[u] != 0xffffffffu) d.ohc_list[slot[u]] = uint32_t(cb + k0 + u * stride);
   }
 }
 
@@ -649,10 +659,25 @@ __global__ void __launch_bounds__(256) k_ohc_records(Dev d) {
   const EvInfo& E = d.ev[e];
   const uint32_t hb = E.hit_base;
   const uint32_t lo = d.ohc_cnt[hb], hi = d.ohc_cnt[uint64_t(hb) + E.n_hits];
-  for (uint32_t p = lo + blockIdx.x * blockDim.x + threadIdx.x; p < hi; p += gridDim.x * blockDim.x) {
-    const uint32_t oih = d.cell_inner[d.ohc_list[p]];
-    const float4 h = d.hit_xyzr[hb + oih];
-    d.ohc_rec[p] = make_float2(d.detind[hb + oih] < 96 ? -h.w : h.w, h.z);
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t p0 = lo + blockIdx.x * blockDim.x + threadIdx.x; p0 < hi; p0 += kOhcUnroll * stride) {
+    uint32_t ih[kOhcUnroll];
+#pragma unroll
+    for (int u = 0; u < kOhcUnroll; ++u) ih[u] = p0 + u * stride < hi ? d.ohc_list[p0 + u * stride] : 0xffffffffu;
+#pragma unroll
+    for (int u = 0; u < kOhcUnroll; ++u)
+      if (ih[u] != 0xffffffffu) ih[u] = d.cell_inner[ih[u]];
+    float4 h[kOhcUnroll];
+    int16_t det[kOhcUnroll];
+#pragma unroll
+    for (int u = 0; u < kOhcUnroll; ++u)
+      if (p0 + u * stride < hi) {
+        h[u] = d.hit_xyzr[hb + ih[u]];
+        det[u] = d.detind[hb + ih[u]];
+      }
+#pragma unroll
+    for (int u = 0; u < kOhcUnroll; ++u)
+      if (p0 + u * stride < hi) d.ohc_rec[p0 + u * stride] = make_float2(det[u] < 96 ? -h[u].w : h[u].w, h[u].z);
   }
 }
 
